@@ -1,0 +1,163 @@
+// capi_setup.cpp -- extern "C" entry points of the host setup API (include/fdtd_b200.h).
+#include "../../../include/fdtd_b200.h"
+#include "setup.hpp"
+
+#include <cstring>
+#include <exception>
+#include <string>
+#include <vector>
+
+struct fdtd_setup {
+    fdtd::SimSetup S;
+    // Storage backing the plain-data view.
+    std::vector<fdtd_dipole_v1> dipoles;
+    std::vector<fdtd_tls_region_v1> regions;
+    std::vector<fdtd_probe_v1> probes;
+    std::vector<double> uniform_kappa[3], unit_b[3], zero_c[3];
+};
+
+namespace {
+
+void write_err(char* err, std::size_t errlen, const std::string& msg) {
+    if (!err || errlen == 0) return;
+    std::size_t n = std::min(errlen - 1, msg.size());
+    std::memcpy(err, msg.data(), n);
+    err[n] = '\0';
+}
+
+// Returns a pointer to the named array and its length, or nullptr.
+const std::vector<double>* find_array(const fdtd_setup* s, const std::string& name, std::vector<double>& scratch) {
+    const fdtd::SimSetup& S = s->S;
+    static const char* axes = "xyz";
+    for (int a = 0; a < 3; ++a) {
+        const std::string ax(1, axes[a]);
+        if (name == ax + "_bounds") return &S.grid.bounds(a);
+        if (name == "d" + ax) return &S.grid.spacing(a);
+        if (name == "inv_d" + ax) return a == 0 ? &S.grid.inv_dx : a == 1 ? &S.grid.inv_dy : &S.grid.inv_dz;
+        if (name == "cpml_k" + ax) return &S.cpml.kappa[a];
+        if (name == "cpml_s" + ax) return &S.cpml.sigma[a];
+        if (name == "cpml_a" + ax) return &S.cpml.alpha[a];
+        if (name == "cpml_bE" + ax) return &S.cpml.bE[a];
+        if (name == "cpml_cE" + ax) return &S.cpml.cE[a];
+        if (name == "cpml_bH" + ax) return &S.cpml.bH[a];
+        if (name == "cpml_cH" + ax) return &S.cpml.cH[a];
+        if (name == "bE" + ax) return &S.mats.bE[a];
+        if (name == "aE" + ax) return &S.mats.aE[a];
+        if (name == "bH" + ax) return &S.mats.bH[a];
+        if (name == "aH" + ax) return &S.mats.aH[a];
+    }
+    if (name == "n_grid") {
+        if (S.scene.NxT == 0) return nullptr;
+        S.scene.n_grid(scratch);
+        return &scratch;
+    }
+    if (name == "tls_region_map") {
+        scratch.assign(S.tls.cell_region_map.begin(), S.tls.cell_region_map.end());
+        return &scratch;
+    }
+    if (name == "tls_Nu") return &S.tls.Nu;
+    if (name == "tls_Ng") return &S.tls.Ng;
+    if (name == "tls_Ndip") return &S.tls.Ndip;
+    if (name == "dft_freqs") return &S.dft_freqs;
+    if (name == "source_J") {  // J(n) for n < N_STEPS of the first dipole
+        scratch.clear();
+        if (!S.sources.empty())
+            for (std::size_t n = 0; n < S.n_steps; ++n) scratch.push_back(S.sources[0].current_density(n, S.dt));
+        return &scratch;
+    }
+    return nullptr;
+}
+
+}  // namespace
+
+extern "C" {
+
+int fdtd_setup_parse(const char* params_text, int mesh_only, fdtd_setup** out, char* err, size_t errlen) {
+    if (!params_text || !out) {
+        write_err(err, errlen, "null argument");
+        return FDTD_ERR_INVALID;
+    }
+    *out = nullptr;
+    try {
+        auto* s = new fdtd_setup();
+        s->S = fdtd::SimSetup::from_params(fdtd::ParamFile::parse(params_text), mesh_only == 0);
+        const fdtd::SimSetup& S = s->S;
+        for (const auto& d : S.sources)
+            s->dipoles.push_back({d.i, d.j, d.k, d.polarization, int32_t(d.waveform), d.cell_area, d.I0, d.f0,
+                                  d.tau, d.t0, d.t_shift});
+        for (const auto& r : S.tls.regions)
+            s->regions.push_back({r.params.kapa_coeff, r.params.pa2, r.params.pa3, r.params.inv_dt, r.params.tau,
+                                  r.params.hbar, r.params.omega_a, r.params.N0_total, r.params.pump_rate,
+                                  r.params.enable_population_clamp ? 1 : 0, 0});
+        for (const auto& p : S.probes)
+            for (int c : p.components) s->probes.push_back({p.i, p.j, p.k, c, 0});
+        *out = s;
+        return FDTD_OK;
+    } catch (const std::exception& e) {
+        write_err(err, errlen, e.what());
+        return FDTD_ERR_PARSE;
+    }
+}
+
+int fdtd_setup_view(const fdtd_setup* s, fdtd_setup_v1* v) {
+    if (!s || !v) return FDTD_ERR_INVALID;
+    const fdtd::SimSetup& S = s->S;
+    std::memset(v, 0, sizeof(*v));
+    v->struct_size = sizeof(fdtd_setup_v1);
+    v->precision = (S.precision == "fp64") ? FDTD_PREC_FP64 : FDTD_PREC_FP32;
+    v->NxT = S.NxT; v->NyT = S.NyT; v->NzT = S.NzT;
+    v->npml = uint32_t(S.npml);
+    v->save_every = uint32_t(S.save_every);
+    v->dt = S.dt;
+    v->dx = S.grid.dx.data(); v->dy = S.grid.dy.data(); v->dz = S.grid.dz.data();
+    v->inv_dx = S.grid.inv_dx.data(); v->inv_dy = S.grid.inv_dy.data(); v->inv_dz = S.grid.inv_dz.data();
+    for (int a = 0; a < 3; ++a) {
+        v->cpml_kappa[a] = S.cpml.kappa[a].data();
+        v->cpml_bE[a] = S.cpml.bE[a].data(); v->cpml_cE[a] = S.cpml.cE[a].data();
+        v->cpml_bH[a] = S.cpml.bH[a].data(); v->cpml_cH[a] = S.cpml.cH[a].data();
+        v->bE[a] = S.mats.bE[a].empty() ? nullptr : S.mats.bE[a].data();
+        v->aE[a] = S.mats.aE[a].empty() ? nullptr : S.mats.aE[a].data();
+        v->aH[a] = S.mats.aH[a].empty() ? nullptr : S.mats.aH[a].data();
+        v->bH[a] = S.mats.bH[a].empty() ? nullptr : S.mats.bH[a].data();
+    }
+    v->bH_uniform = S.dt / fdtd::phys::MU0;
+    v->n_dipoles = uint32_t(s->dipoles.size());
+    v->dipoles = s->dipoles.data();
+    v->n_tls_regions = uint32_t(s->regions.size());
+    v->tls_regions = s->regions.data();
+    v->tls_region_map = S.tls.cell_region_map.empty() ? nullptr : S.tls.cell_region_map.data();
+    v->tls_Nu = S.tls.Nu.empty() ? nullptr : S.tls.Nu.data();
+    v->tls_Ng = S.tls.Ng.empty() ? nullptr : S.tls.Ng.data();
+    v->n_probes = uint32_t(s->probes.size());
+    v->probes = s->probes.data();
+    v->n_dft_freqs = uint32_t(S.dft_freqs.size());
+    v->dft_freqs = S.dft_freqs.data();
+    v->monitor_interval = uint32_t(S.stability_interval);
+    v->max_E = S.stability_max_E;
+    v->max_P = S.stability_max_P;
+    v->conservation_err = S.stability_conservation;
+    v->growth_rate = S.stability_growth;
+    return FDTD_OK;
+}
+
+int fdtd_setup_array_len(const fdtd_setup* s, const char* name, uint64_t* len) {
+    if (!s || !name || !len) return FDTD_ERR_INVALID;
+    std::vector<double> scratch;
+    const std::vector<double>* a = find_array(s, name, scratch);
+    if (!a) return FDTD_ERR_INVALID;
+    *len = a->size();
+    return FDTD_OK;
+}
+
+int fdtd_setup_array(const fdtd_setup* s, const char* name, double* out, uint64_t len) {
+    if (!s || !name || !out) return FDTD_ERR_INVALID;
+    std::vector<double> scratch;
+    const std::vector<double>* a = find_array(s, name, scratch);
+    if (!a || a->size() != len) return FDTD_ERR_INVALID;
+    std::memcpy(out, a->data(), len * sizeof(double));
+    return FDTD_OK;
+}
+
+void fdtd_setup_destroy(fdtd_setup* s) { delete s; }
+
+}  // extern "C"

@@ -1,0 +1,397 @@
+// kernels.cuh -- sm_100a stepping kernels of the Yee FDTD loop.
+//
+// Device layout: every 3-D array is stored x-fastest, (k, j, i) -> (k*NyT + j)*NxP + i,
+// rows padded to NxP (a multiple of 128 bytes).  A thread owns W = 16/sizeof(T)
+// consecutive x cells (one 128-bit load per array), a warp owns one 32*W-cell row
+// segment, and each thread marches in +z through a chunk of planes carrying the
+// z-neighbour plane in registers (2.5D blocking).  x-neighbours come from the adjacent
+// lane by warp shuffle (one scalar load at the warp edge), y-neighbours from the
+// adjacent row through L1.
+//
+// Physics per step n (reference order, src/3D_FDTD_version008.cpp:269-328):
+//   k_update_H : H -= bH * curl E with the CPML psi_H recursion fused in
+//                (fdtd_update_H src/fdtd_stepper.hpp:8-47 + apply_after_H src/boundary.hpp:150-225)
+//   k_update_E : polarization P^{n+1} (src/two_level_system.hpp:574-609), E += bE*(curl H - J - dP/dt)
+//                with psi_E fused (src/fdtd_stepper.hpp:49-89, src/two_level_system.hpp:299-342,
+//                src/boundary.hpp:227-300), then the population update with E^{n+1}
+//                (src/two_level_system.hpp:612-666), all in one pass over the cell.
+// CPML psi lives only in the PML slabs: x-slab [k][j][2np], y-slab [k][2np][NxP],
+// z-slab [2np][j][NxP], index 0 for the low side, np.. for the high side.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstdint>
+
+namespace fdtdk {
+
+constexpr unsigned kFull = 0xffffffffu;
+constexpr int kBlockY = 8;    // rows (warps) per block
+constexpr int kMaxSources = 8;
+
+template <typename T> struct Vec;
+template <> struct Vec<float> {
+    static constexpr int W = 4;
+    __device__ __forceinline__ static void ld(const float* p, float (&a)[4]) {
+        float4 t = *reinterpret_cast<const float4*>(p);
+        a[0] = t.x; a[1] = t.y; a[2] = t.z; a[3] = t.w;
+    }
+    __device__ __forceinline__ static void ldg(const float* p, float (&a)[4]) {
+        float4 t = __ldg(reinterpret_cast<const float4*>(p));
+        a[0] = t.x; a[1] = t.y; a[2] = t.z; a[3] = t.w;
+    }
+    __device__ __forceinline__ static void st(float* p, const float (&a)[4]) {
+        *reinterpret_cast<float4*>(p) = make_float4(a[0], a[1], a[2], a[3]);
+    }
+};
+template <> struct Vec<double> {
+    static constexpr int W = 2;
+    __device__ __forceinline__ static void ld(const double* p, double (&a)[2]) {
+        double2 t = *reinterpret_cast<const double2*>(p);
+        a[0] = t.x; a[1] = t.y;
+    }
+    __device__ __forceinline__ static void ldg(const double* p, double (&a)[2]) {
+        double2 t = __ldg(reinterpret_cast<const double2*>(p));
+        a[0] = t.x; a[1] = t.y;
+    }
+    __device__ __forceinline__ static void st(double* p, const double (&a)[2]) {
+        *reinterpret_cast<double2*>(p) = make_double2(a[0], a[1]);
+    }
+};
+
+// Per gain region constants (TwoLevelParams after finalize_with_dt), in compute type T.
+template <typename T>
+struct GainCoef {
+    T kapaN0;          // kapa_coeff * Ndip
+    T pa2, pa3, inv_dt;
+    T inv_N0;          // 1 / Ng0
+    T N0;
+    T dt, inv_tau, inv_hbar_omega, pump;
+    int clamp;         // TLS_ENABLE_CLAMP renormalisation
+    int active;        // Ndip > 0
+};
+
+template <typename T>
+struct StepArgs {
+    int NxT, NyT, NzT, NxP, np;
+    long long plane;  // NxP * NyT
+    T *Ex, *Ey, *Ez, *Hx, *Hy, *Hz;
+    const T *bEx, *bEy, *bEz;
+    T bH;
+    const T *idx, *idy, *idz;         // 1/dx (padded to NxP), 1/dy, 1/dz
+    const T *ik[3];                   // 1/kappa per axis
+    const T *pbE[3], *pcE[3], *pbH[3], *pcH[3];
+    // psi_H: 0 Hx_y, 1 Hx_z, 2 Hy_z, 3 Hy_x, 4 Hz_x, 5 Hz_y ; psi_E likewise for E
+    T *psiH[6], *psiE[6];
+    // gain block: bounding box of the gain cells, x-fastest with row length gX
+    int gain, gi0, gj0, gk0, gX, gY, gZ;
+    const int8_t* greg;               // region id per bbox cell, -1 = none
+    T *P0, *P1;                       // polarization ping-pong: P^n lives in slot (n & 1)
+    T *Nu, *Ng;
+    const GainCoef<T>* gcoef;
+    const unsigned* status;           // nonzero: a monitor step failed, skip all work
+};
+
+// Per-step arguments of the E kernel.
+struct ESrc {
+    int n;                 // number of point sources
+    int parity;            // step & 1
+    int si[kMaxSources], sj[kMaxSources], sk[kMaxSources], sc[kMaxSources];
+    double J[kMaxSources]; // I((n+1/2)dt)/cell_area
+};
+
+__device__ __forceinline__ bool in_pml(int n, int N, int np) { return n < np || n >= N - np; }
+__device__ __forceinline__ int slab_index(int n, int N, int np) { return n < np ? n : n - (N - 2 * np); }
+
+// ---------------------------------------------------------------------------------
+template <typename T>
+__global__ void __launch_bounds__(32 * kBlockY)
+k_update_H(const StepArgs<T> a, const int kchunk) {
+    constexpr int W = Vec<T>::W;
+    if (*a.status) return;
+    const int lane = threadIdx.x;
+    const int j = blockIdx.y * kBlockY + threadIdx.y;
+    if (j >= a.NyT - 1) return;  // whole warp: a warp is one row
+    const int kb = blockIdx.z * kchunk;
+    const int ke = min(kb + kchunk, a.NzT - 1);
+    if (kb >= ke) return;
+    const int i0 = (blockIdx.x * 32 + lane) * W;
+    const bool act = i0 < a.NxT;
+    const int np = a.np, np2 = 2 * np;
+    const T bH = a.bH;
+
+    T idx[W];
+#pragma unroll
+    for (int e = 0; e < W; ++e) idx[e] = act ? __ldg(a.idx + i0 + e) : T(0);
+    const T idy = __ldg(a.idy + j);
+    const bool ypml = in_pml(j, a.NyT, np);
+    const int jy = ypml ? slab_index(j, a.NyT, np) : 0;
+    T yb = 1, yc = 0, yik = 1;
+    if (ypml) { yb = __ldg(a.pbH[1] + j); yc = __ldg(a.pcH[1] + j); yik = __ldg(a.ik[1] + j); }
+    const bool xpml = act && (i0 < np || i0 + W > a.NxT - np);
+
+    const size_t row = size_t(j) * a.NxP + i0;
+    T ex0[W], ey0[W];
+    if (act) {
+        Vec<T>::ldg(a.Ex + size_t(kb) * a.plane + row, ex0);
+        Vec<T>::ldg(a.Ey + size_t(kb) * a.plane + row, ey0);
+    } else {
+#pragma unroll
+        for (int e = 0; e < W; ++e) ex0[e] = ey0[e] = T(0);
+    }
+
+    for (int k = kb; k < ke; ++k) {
+        const size_t c = size_t(k) * a.plane + row;
+        T ex1[W], ey1[W], ez[W], exj[W], ezj[W], hx[W], hy[W], hz[W];
+        if (act) {
+            Vec<T>::ldg(a.Ex + c + a.plane, ex1);
+            Vec<T>::ldg(a.Ey + c + a.plane, ey1);
+            Vec<T>::ldg(a.Ez + c, ez);
+            Vec<T>::ldg(a.Ex + c + a.NxP, exj);
+            Vec<T>::ldg(a.Ez + c + a.NxP, ezj);
+            Vec<T>::ld(a.Hx + c, hx);
+            Vec<T>::ld(a.Hy + c, hy);
+            Vec<T>::ld(a.Hz + c, hz);
+        } else {
+#pragma unroll
+            for (int e = 0; e < W; ++e) ex1[e] = ey1[e] = ez[e] = exj[e] = ezj[e] = hx[e] = hy[e] = hz[e] = T(0);
+        }
+        T eyn = __shfl_down_sync(kFull, ey0[0], 1);
+        T ezn = __shfl_down_sync(kFull, ez[0], 1);
+        if (lane == 31) {
+            const bool nxt = act && (i0 + W < a.NxT);
+            eyn = nxt ? __ldg(a.Ey + c + W) : T(0);
+            ezn = nxt ? __ldg(a.Ez + c + W) : T(0);
+        }
+        const T idz = __ldg(a.idz + k);
+        const bool zpml = in_pml(k, a.NzT, np);
+        T zb = 1, zc = 0, zik = 1;
+        size_t zs = 0, ys = 0;
+        T pxy[W], pzy[W], pxz[W], pyz[W];  // psi Hx_y, Hz_y, Hx_z, Hy_z
+        if (zpml) {
+            zb = __ldg(a.pbH[2] + k); zc = __ldg(a.pcH[2] + k); zik = __ldg(a.ik[2] + k);
+            zs = (size_t(slab_index(k, a.NzT, np)) * a.NyT + j) * a.NxP + i0;
+            if (act) { Vec<T>::ld(a.psiH[1] + zs, pxz); Vec<T>::ld(a.psiH[2] + zs, pyz); }
+        }
+        if (ypml) {
+            ys = (size_t(k) * np2 + jy) * a.NxP + i0;
+            if (act) { Vec<T>::ld(a.psiH[0] + ys, pxy); Vec<T>::ld(a.psiH[5] + ys, pzy); }
+        }
+#pragma unroll
+        for (int e = 0; e < W; ++e) {
+            const int i = i0 + e;
+            if (i >= a.NxT - 1) continue;  // last x plane (and padding) never updated
+            const T eyx = (e < W - 1) ? ey0[e + 1] : eyn;
+            const T ezx = (e < W - 1) ? ez[e + 1] : ezn;
+            T dEz_dy = (ezj[e] - ez[e]) * idy;
+            T dEy_dz = (ey1[e] - ey0[e]) * idz;
+            T dEx_dz = (ex1[e] - ex0[e]) * idz;
+            T dEz_dx = (ezx - ez[e]) * idx[e];
+            T dEy_dx = (eyx - ey0[e]) * idx[e];
+            T dEx_dy = (exj[e] - ex0[e]) * idy;
+            if (ypml) {
+                pxy[e] = yb * pxy[e] + yc * dEz_dy; dEz_dy = dEz_dy * yik + pxy[e];
+                pzy[e] = yb * pzy[e] + yc * dEx_dy; dEx_dy = dEx_dy * yik + pzy[e];
+            }
+            if (zpml) {
+                pxz[e] = zb * pxz[e] + zc * dEy_dz; dEy_dz = dEy_dz * zik + pxz[e];
+                pyz[e] = zb * pyz[e] + zc * dEx_dz; dEx_dz = dEx_dz * zik + pyz[e];
+            }
+            if (xpml && in_pml(i, a.NxT, np)) {
+                const size_t xs = (size_t(k) * a.NyT + j) * np2 + slab_index(i, a.NxT, np);
+                const T b = __ldg(a.pbH[0] + i), cc = __ldg(a.pcH[0] + i), ik = __ldg(a.ik[0] + i);
+                T ps = b * a.psiH[3][xs] + cc * dEz_dx;
+                a.psiH[3][xs] = ps;
+                dEz_dx = dEz_dx * ik + ps;
+                ps = b * a.psiH[4][xs] + cc * dEy_dx;
+                a.psiH[4][xs] = ps;
+                dEy_dx = dEy_dx * ik + ps;
+            }
+            hx[e] = hx[e] - bH * (dEz_dy - dEy_dz);
+            hy[e] = hy[e] - bH * (dEx_dz - dEz_dx);
+            hz[e] = hz[e] - bH * (dEy_dx - dEx_dy);
+        }
+        if (act) {
+            Vec<T>::st(a.Hx + c, hx);
+            Vec<T>::st(a.Hy + c, hy);
+            Vec<T>::st(a.Hz + c, hz);
+            if (zpml) { Vec<T>::st(a.psiH[1] + zs, pxz); Vec<T>::st(a.psiH[2] + zs, pyz); }
+            if (ypml) { Vec<T>::st(a.psiH[0] + ys, pxy); Vec<T>::st(a.psiH[5] + ys, pzy); }
+        }
+#pragma unroll
+        for (int e = 0; e < W; ++e) { ex0[e] = ex1[e]; ey0[e] = ey1[e]; }
+    }
+}
+
+// ---------------------------------------------------------------------------------
+template <typename T>
+__global__ void __launch_bounds__(32 * kBlockY)
+k_update_E(const StepArgs<T> a, const int kchunk, const ESrc src) {
+    constexpr int W = Vec<T>::W;
+    if (*a.status) return;
+    const int lane = threadIdx.x;
+    const int j = blockIdx.y * kBlockY + threadIdx.y;
+    if (j < 1 || j >= a.NyT) return;  // E is updated for j >= 1 only
+    const int kb = max(int(blockIdx.z) * kchunk, 1);
+    const int ke = min(int(blockIdx.z) * kchunk + kchunk, a.NzT);
+    if (kb >= ke) return;
+    const int i0 = (blockIdx.x * 32 + lane) * W;
+    const bool act = i0 < a.NxT;
+    const int np = a.np, np2 = 2 * np;
+
+    T idx[W];
+#pragma unroll
+    for (int e = 0; e < W; ++e) idx[e] = act ? __ldg(a.idx + i0 + e) : T(0);
+    const T idy = __ldg(a.idy + j);
+    const bool ypml = in_pml(j, a.NyT, np);
+    const int jy = ypml ? slab_index(j, a.NyT, np) : 0;
+    T yb = 1, yc = 0, yik = 1;
+    if (ypml) { yb = __ldg(a.pbE[1] + j); yc = __ldg(a.pcE[1] + j); yik = __ldg(a.ik[1] + j); }
+    const bool xpml = act && (i0 < np || i0 + W > a.NxT - np);
+    const bool grow = a.gain && j >= a.gj0 && j < a.gj0 + a.gY && i0 + W > a.gi0 && i0 < a.gi0 + a.gX;
+    T* const Pcur = src.parity ? a.P1 : a.P0;
+    T* const Pold = src.parity ? a.P0 : a.P1;  // holds P^{n-1}, receives P^{n+1}
+
+    const size_t row = size_t(j) * a.NxP + i0;
+    T hxm[W], hym[W];  // Hx, Hy at k-1
+    if (act) {
+        Vec<T>::ldg(a.Hx + size_t(kb - 1) * a.plane + row, hxm);
+        Vec<T>::ldg(a.Hy + size_t(kb - 1) * a.plane + row, hym);
+    } else {
+#pragma unroll
+        for (int e = 0; e < W; ++e) hxm[e] = hym[e] = T(0);
+    }
+
+    for (int k = kb; k < ke; ++k) {
+        const size_t c = size_t(k) * a.plane + row;
+        T ex[W], ey[W], ez[W], bx[W], by[W], bz[W], hx[W], hy[W], hz[W], hzj[W], hxj[W];
+        if (act) {
+            Vec<T>::ld(a.Ex + c, ex);
+            Vec<T>::ld(a.Ey + c, ey);
+            Vec<T>::ld(a.Ez + c, ez);
+            Vec<T>::ldg(a.bEx + c, bx);
+            Vec<T>::ldg(a.bEy + c, by);
+            Vec<T>::ldg(a.bEz + c, bz);
+            Vec<T>::ldg(a.Hx + c, hx);
+            Vec<T>::ldg(a.Hy + c, hy);
+            Vec<T>::ldg(a.Hz + c, hz);
+            Vec<T>::ldg(a.Hz + c - a.NxP, hzj);
+            Vec<T>::ldg(a.Hx + c - a.NxP, hxj);
+        } else {
+#pragma unroll
+            for (int e = 0; e < W; ++e)
+                ex[e] = ey[e] = ez[e] = bx[e] = by[e] = bz[e] = hx[e] = hy[e] = hz[e] = hzj[e] = hxj[e] = T(0);
+        }
+        T hzp = __shfl_up_sync(kFull, hz[W - 1], 1);
+        T hyp = __shfl_up_sync(kFull, hy[W - 1], 1);
+        if (lane == 0) {
+            const bool prv = act && i0 > 0;
+            hzp = prv ? __ldg(a.Hz + c - 1) : T(0);
+            hyp = prv ? __ldg(a.Hy + c - 1) : T(0);
+        }
+        const T idz = __ldg(a.idz + k);
+        const bool zpml = in_pml(k, a.NzT, np);
+        T zb = 1, zc = 0, zik = 1;
+        size_t zs = 0, ys = 0;
+        T pxy[W], pzy[W], pxz[W], pyz[W];  // psi Ex_y, Ez_y, Ex_z, Ey_z
+        if (zpml) {
+            zb = __ldg(a.pbE[2] + k); zc = __ldg(a.pcE[2] + k); zik = __ldg(a.ik[2] + k);
+            zs = (size_t(slab_index(k, a.NzT, np)) * a.NyT + j) * a.NxP + i0;
+            if (act) { Vec<T>::ld(a.psiE[1] + zs, pxz); Vec<T>::ld(a.psiE[2] + zs, pyz); }
+        }
+        if (ypml) {
+            ys = (size_t(k) * np2 + jy) * a.NxP + i0;
+            if (act) { Vec<T>::ld(a.psiE[0] + ys, pxy); Vec<T>::ld(a.psiE[5] + ys, pzy); }
+        }
+        const bool gplane = grow && k >= a.gk0 && k < a.gk0 + a.gZ;
+#pragma unroll
+        for (int e = 0; e < W; ++e) {
+            const int i = i0 + e;
+            if (i < 1 || i >= a.NxT) continue;  // x = 0 plane and padding never updated
+            const T hzx = (e > 0) ? hz[e - 1] : hzp;
+            const T hyx = (e > 0) ? hy[e - 1] : hyp;
+            T dHz_dy = (hz[e] - hzj[e]) * idy;
+            T dHy_dz = (hy[e] - hym[e]) * idz;
+            T dHx_dz = (hx[e] - hxm[e]) * idz;
+            T dHz_dx = (hz[e] - hzx) * idx[e];
+            T dHy_dx = (hy[e] - hyx) * idx[e];
+            T dHx_dy = (hx[e] - hxj[e]) * idy;
+            if (ypml) {
+                pxy[e] = yb * pxy[e] + yc * dHz_dy; dHz_dy = dHz_dy * yik + pxy[e];
+                pzy[e] = yb * pzy[e] + yc * dHx_dy; dHx_dy = dHx_dy * yik + pzy[e];
+            }
+            if (zpml) {
+                pxz[e] = zb * pxz[e] + zc * dHy_dz; dHy_dz = dHy_dz * zik + pxz[e];
+                pyz[e] = zb * pyz[e] + zc * dHx_dz; dHx_dz = dHx_dz * zik + pyz[e];
+            }
+            if (xpml && in_pml(i, a.NxT, np)) {
+                const size_t xs = (size_t(k) * a.NyT + j) * np2 + slab_index(i, a.NxT, np);
+                const T b = __ldg(a.pbE[0] + i), cc = __ldg(a.pcE[0] + i), ik = __ldg(a.ik[0] + i);
+                T ps = b * a.psiE[3][xs] + cc * dHz_dx;
+                a.psiE[3][xs] = ps;
+                dHz_dx = dHz_dx * ik + ps;
+                ps = b * a.psiE[4][xs] + cc * dHy_dx;
+                a.psiE[4][xs] = ps;
+                dHy_dx = dHy_dx * ik + ps;
+            }
+            T Jx = 0, Jy = 0, Jz = 0;
+            for (int s = 0; s < src.n; ++s) {
+                if (src.si[s] == i && src.sj[s] == j && src.sk[s] == k) {
+                    const T v = T(src.J[s]);
+                    if (src.sc[s] == 0) Jx += v;
+                    else if (src.sc[s] == 1) Jy += v;
+                    else Jz += v;
+                }
+            }
+            ex[e] = ex[e] + bx[e] * ((dHz_dy - dHy_dz) - Jx);
+            ey[e] = ey[e] + by[e] * ((dHx_dz - dHz_dx) - Jy);
+            // Two-level gain: polarization with E^n, E update with -dP/dt, populations with E^{n+1}.
+            int r = -1;
+            size_t gidx = 0;
+            if (gplane && i >= a.gi0 && i < a.gi0 + a.gX) {
+                gidx = (size_t(k - a.gk0) * a.gY + (j - a.gj0)) * a.gX + (i - a.gi0);
+                r = a.greg[gidx];
+            }
+            if (r >= 0 && a.gcoef[r].active) {
+                const GainCoef<T> g = a.gcoef[r];
+                const T ez_old = ez[e];
+                const T P = Pcur[gidx], Pp = Pold[gidx];
+                T Nu = a.Nu[gidx], Ng = a.Ng[gidx];
+                const T ng_frac = (Ng - Nu) * g.inv_N0;
+                const T Pn = g.kapaN0 * (ng_frac * ez_old) + g.pa2 * P + g.pa3 * Pp;
+                const T dP = (Pn - P) * g.inv_dt;
+                ez[e] = ez[e] + bz[e] * (((dHy_dx - dHx_dy) - Jz) - dP);
+                const T e_avg = T(0.5) * (ez[e] + ez_old);
+                const T stim = e_avg * (Pn - P) * g.inv_dt * g.inv_hbar_omega;
+                T dNu = -g.inv_tau * Nu + stim;
+                T dNg = g.inv_tau * Nu - stim;
+                if (g.pump != T(0)) { dNu += g.pump * Ng; dNg -= g.pump * Ng; }
+                Nu = Nu + g.dt * dNu;
+                Ng = Ng + g.dt * dNg;
+                Nu = fmax(T(0), Nu);
+                Ng = fmax(T(0), Ng);
+                if (g.clamp) {
+                    const T tot = Nu + Ng;
+                    if (tot > T(1e-30)) { const T sc = g.N0 / tot; Nu *= sc; Ng *= sc; }
+                    Nu = fmin(Nu, g.N0);
+                    Ng = g.N0 - Nu;
+                }
+                Pold[gidx] = Pn;
+                a.Nu[gidx] = Nu;
+                a.Ng[gidx] = Ng;
+            } else {
+                ez[e] = ez[e] + bz[e] * ((dHy_dx - dHx_dy) - Jz);
+            }
+        }
+        if (act) {
+            Vec<T>::st(a.Ex + c, ex);
+            Vec<T>::st(a.Ey + c, ey);
+            Vec<T>::st(a.Ez + c, ez);
+            if (zpml) { Vec<T>::st(a.psiE[1] + zs, pxz); Vec<T>::st(a.psiE[2] + zs, pyz); }
+            if (ypml) { Vec<T>::st(a.psiE[0] + ys, pxy); Vec<T>::st(a.psiE[5] + ys, pzy); }
+        }
+#pragma unroll
+        for (int e = 0; e < W; ++e) { hxm[e] = hx[e]; hym[e] = hy[e]; }
+    }
+}
+
+}  // namespace fdtdk

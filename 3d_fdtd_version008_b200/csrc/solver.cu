@@ -1,0 +1,861 @@
+// solver.cu -- resident device state of one FDTD solve and the stepper C ABI.
+//
+// One fdtd_handle owns, on one GPU: the six field arrays (x-fastest, padded rows), the
+// three bE coefficient arrays, the 1-D spacing/CPML profiles, psi only inside the PML
+// slabs, the gain block (bounding box of the gain cells: region id, P ping-pong, Nu,
+// Ng), probe series / DFT accumulators and the stability-monitor state.  fdtd_run()
+// issues, per step, k_update_H, k_update_E, the probe/DFT kernel and on monitor steps
+// the FP64 diagnostic reduction, on the handle's stream.  All device memory comes from
+// cudaMalloc at create time (staging for layout transposes on first use).
+#include "../../include/fdtd_b200.h"
+#include "host/waveform.hpp"
+#include "kernels.cuh"
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <numbers>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+namespace fdtdk {
+
+// ================================================================ small kernels
+// idx3 (z fastest, FP64) <-> device layout (x fastest, padded), 32x32 tiles over (k, i)
+// for each j.
+template <typename T>
+__global__ void k_from_idx3(const double* __restrict__ src, T* __restrict__ dst, int NxT, int NyT, int NzT,
+                            int NxP) {
+    __shared__ double tile[32][33];
+    const int j = blockIdx.z;
+    const int k0 = blockIdx.x * 32, i0 = blockIdx.y * 32;
+    for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+        const int i = i0 + r, k = k0 + threadIdx.x;
+        tile[r][threadIdx.x] = (i < NxT && k < NzT) ? src[(size_t(i) * NyT + j) * NzT + k] : 0.0;
+    }
+    __syncthreads();
+    for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+        const int k = k0 + r, i = i0 + threadIdx.x;
+        if (i < NxT && k < NzT) dst[(size_t(k) * NyT + j) * NxP + i] = T(tile[threadIdx.x][r]);
+    }
+}
+
+template <typename T>
+__global__ void k_to_idx3(const T* __restrict__ src, double* __restrict__ dst, int NxT, int NyT, int NzT, int NxP) {
+    __shared__ double tile[32][33];
+    const int j = blockIdx.z;
+    const int k0 = blockIdx.x * 32, i0 = blockIdx.y * 32;
+    for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+        const int k = k0 + r, i = i0 + threadIdx.x;
+        tile[threadIdx.x][r] = (i < NxT && k < NzT) ? double(src[(size_t(k) * NyT + j) * NxP + i]) : 0.0;
+    }
+    __syncthreads();
+    for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+        const int i = i0 + r, k = k0 + threadIdx.x;
+        if (i < NxT && k < NzT) dst[(size_t(i) * NyT + j) * NzT + k] = tile[r][threadIdx.x];
+    }
+}
+
+// Gather (to_dev = 0) or scatter (to_dev = 1) the gain block from / to an idx3 array.
+template <typename T>
+__global__ void k_gain_block(double* __restrict__ full, T* __restrict__ blk, const int8_t* __restrict__ reg, int gi0,
+                             int gj0, int gk0, int gX, int gY, int gZ, int NyT, int NzT, int to_dev) {
+    const size_t n = size_t(gX) * gY * gZ;
+    for (size_t t = blockIdx.x * size_t(blockDim.x) + threadIdx.x; t < n; t += size_t(gridDim.x) * blockDim.x) {
+        const int i = int(t % gX) + gi0;
+        const int j = int((t / gX) % gY) + gj0;
+        const int k = int(t / (size_t(gX) * gY)) + gk0;
+        const size_t id = (size_t(i) * NyT + j) * NzT + k;
+        if (to_dev) blk[t] = reg[t] >= 0 ? T(full[id]) : T(0);
+        else if (reg[t] >= 0) full[id] = double(blk[t]);
+    }
+}
+
+struct ProbeDev {
+    long long off;  // device-layout offset of the probe cell
+    int comp;
+};
+
+template <typename T>
+__device__ double probe_value(const StepArgs<T>& a, const ProbeDev& p) {
+    const size_t o = size_t(p.off);
+    auto v = [&](const T* f) { return double(f[o]); };
+    switch (p.comp) {
+        case 0: return v(a.Ex);
+        case 1: return v(a.Ey);
+        case 2: return v(a.Ez);
+        case 3: return v(a.Hx);
+        case 4: return v(a.Hy);
+        case 5: return v(a.Hz);
+        case 6: return sqrt(v(a.Ex) * v(a.Ex) + v(a.Ey) * v(a.Ey) + v(a.Ez) * v(a.Ez));
+        case 7: return sqrt(v(a.Hx) * v(a.Hx) + v(a.Hy) * v(a.Hy) + v(a.Hz) * v(a.Hz));
+        case 8: return v(a.Ey) * v(a.Hz) - v(a.Ez) * v(a.Hy);
+        case 9: return v(a.Ez) * v(a.Hx) - v(a.Ex) * v(a.Hz);
+        case 10: return v(a.Ex) * v(a.Hy) - v(a.Ey) * v(a.Hx);
+        case 11: {
+            double sx = v(a.Ey) * v(a.Hz) - v(a.Ez) * v(a.Hy);
+            double sy = v(a.Ez) * v(a.Hx) - v(a.Ex) * v(a.Hz);
+            double sz = v(a.Ex) * v(a.Hy) - v(a.Ey) * v(a.Hx);
+            return sqrt(sx * sx + sy * sy + sz * sz);
+        }
+    }
+    return 0.0;
+}
+
+// Point probes after the E update of step n: sample (every save_every steps) and the
+// FP64 DFT accumulation X_m += v * exp(-i 2 pi f_m t) * dt at t = (n+1) dt.
+// One thread per (probe, frequency).
+template <typename T>
+__global__ void k_probe_dft(const StepArgs<T> a, const ProbeDev* __restrict__ probes, int nprobes,
+                            const double* __restrict__ freqs, int nf, double* __restrict__ dft,
+                            double* __restrict__ series, long long sample, double t, double dt) {
+    if (*a.status) return;
+    const int per = nf > 0 ? nf : 1;
+    const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+    if (tid >= nprobes * per) return;
+    const int p = tid / per, m = tid % per;
+    const double v = probe_value(a, probes[p]);
+    if (m == 0 && sample >= 0) series[size_t(sample) * nprobes + p] = v;
+    if (nf > 0) {
+        double s, c;
+        sincospi(2.0 * freqs[m] * t, &s, &c);
+        double* acc = dft + 2 * (size_t(p) * nf + m);
+        acc[0] += v * c * dt;
+        acc[1] -= v * s * dt;
+    }
+}
+
+struct DiagAccum {
+    unsigned long long maxE, maxP;  // bit patterns of non-negative doubles
+    unsigned flags;                 // bit0 E, bit1 H, bit2 P, bit3 populations non-finite
+    unsigned pad;
+    double sum_pop, sum_N0, int_Nu, int_Ng, p_energy;
+};
+
+struct MonitorState {
+    double prev_max_E;
+    unsigned instability_count;
+    int stable;
+    // last evaluation
+    unsigned long long step;
+    double max_E, max_P, cons, int_Nu, int_Ng, p_energy;
+    unsigned flags;
+    int has_gain;
+    // thresholds
+    double thr_E, thr_P, thr_cons, thr_growth;
+};
+
+__device__ __forceinline__ double warp_sum(double v) {
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
+    return v;
+}
+__device__ __forceinline__ double warp_max(double v) {
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(kFull, v, o));
+    return v;
+}
+
+// Block-wide reduction of 7 quantities into the accumulator (one atomic each per block).
+__device__ void block_commit(DiagAccum* acc, double mE, double mP, unsigned fl, double s0, double s1, double s2,
+                             double s3, double s4) {
+    __shared__ double sh[8][32];
+    __shared__ unsigned shf;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    if (threadIdx.x == 0) shf = 0;
+    __syncthreads();
+    mE = warp_max(mE); mP = warp_max(mP);
+    s0 = warp_sum(s0); s1 = warp_sum(s1); s2 = warp_sum(s2); s3 = warp_sum(s3); s4 = warp_sum(s4);
+    if (fl) atomicOr(&shf, fl);
+    if (lane == 0) {
+        sh[0][wid] = mE; sh[1][wid] = mP; sh[2][wid] = s0; sh[3][wid] = s1;
+        sh[4][wid] = s2; sh[5][wid] = s3; sh[6][wid] = s4;
+    }
+    __syncthreads();
+    if (wid == 0) {
+        double v[7];
+        for (int q = 0; q < 7; ++q) v[q] = lane < nw ? sh[q][lane] : 0.0;
+        v[0] = warp_max(v[0]); v[1] = warp_max(v[1]);
+        for (int q = 2; q < 7; ++q) v[q] = warp_sum(v[q]);
+        if (lane == 0) {
+            atomicMax(&acc->maxE, (unsigned long long)__double_as_longlong(v[0]));
+            atomicMax(&acc->maxP, (unsigned long long)__double_as_longlong(v[1]));
+            if (shf) atomicOr(&acc->flags, shf);
+            if (v[2] != 0.0) atomicAdd(&acc->sum_pop, v[2]);
+            if (v[3] != 0.0) atomicAdd(&acc->sum_N0, v[3]);
+            if (v[4] != 0.0) atomicAdd(&acc->int_Nu, v[4]);
+            if (v[5] != 0.0) atomicAdd(&acc->int_Ng, v[5]);
+            if (v[6] != 0.0) atomicAdd(&acc->p_energy, v[6]);
+        }
+    }
+}
+
+// FP64 scans of StabilityMonitor::check_stability (src/stability_monitor.hpp:42-135),
+// calculate_conservation_error (:155-170), compute_integrated_Nu/Ng and
+// compute_polarization_energy (src/two_level_system.hpp:344-418) over the fields after
+// the step.  Field arrays are scanned as flat padded arrays (padding holds zeros).
+template <typename T>
+__global__ void k_monitor_reduce(const StepArgs<T> a, size_t nflat, const double* __restrict__ dxs,
+                                 const double* __restrict__ dys, const double* __restrict__ dzs, int parity_next,
+                                 DiagAccum* acc) {
+    if (*a.status) return;
+    double mE = 0.0, mP = 0.0, s0 = 0, s1 = 0, s2 = 0, s3 = 0, s4 = 0;
+    unsigned fl = 0;
+    const size_t stride = size_t(gridDim.x) * blockDim.x;
+    for (size_t t = blockIdx.x * size_t(blockDim.x) + threadIdx.x; t < nflat; t += stride) {
+        const double ex = double(a.Ex[t]), ey = double(a.Ey[t]), ez = double(a.Ez[t]);
+        if (!isfinite(ex) || !isfinite(ey) || !isfinite(ez)) fl |= 1u;
+        else mE = fmax(mE, fmax(fabs(ex), fmax(fabs(ey), fabs(ez))));
+        if (!isfinite(double(a.Hx[t])) || !isfinite(double(a.Hy[t])) || !isfinite(double(a.Hz[t]))) fl |= 2u;
+    }
+    if (a.gain) {
+        const T* Pn = parity_next ? a.P1 : a.P0;
+        const T* Po = parity_next ? a.P0 : a.P1;
+        const size_t ng = size_t(a.gX) * a.gY * a.gZ;
+        for (size_t t = blockIdx.x * size_t(blockDim.x) + threadIdx.x; t < ng; t += stride) {
+            const int r = a.greg[t];
+            if (r < 0 || !a.gcoef[r].active) continue;
+            const int i = int(t % a.gX) + a.gi0;
+            const int j = int((t / a.gX) % a.gY) + a.gj0;
+            const int k = int(t / (size_t(a.gX) * a.gY)) + a.gk0;
+            const double P = double(Pn[t]), Pp = double(Po[t]);
+            const double Nu = double(a.Nu[t]), Ng = double(a.Ng[t]);
+            if (!isfinite(P) || !isfinite(Pp)) fl |= 4u;
+            else mP = fmax(mP, fabs(P));
+            if (!isfinite(Nu) || !isfinite(Ng)) fl |= 8u;
+            const double N0 = double(a.gcoef[r].N0);
+            if (N0 > 1e10) { s0 += Nu + Ng; s1 += N0; }
+            const double dV = dxs[i] * dys[j] * dzs[k];
+            s2 += Nu * dV;
+            s3 += Ng * dV;
+            const double ez = double(a.Ez[(size_t(k) * a.NyT + j) * a.NxP + i]);
+            s4 += -0.5 * P * ez * dV;
+        }
+    }
+    block_commit(acc, mE, mP, fl, s0, s1, s2, s3, s4);
+}
+
+// One thread: the StabilityMonitor decision for monitor step `step`; sets the abort
+// word when the reference would terminate (NaN/Inf anywhere, or > 10 threshold warnings).
+__global__ void k_monitor_eval(DiagAccum* acc, MonitorState* ms, unsigned* status, unsigned long long step) {
+    if (*status) return;
+    const double max_E = __longlong_as_double((long long)acc->maxE);
+    const double max_P = __longlong_as_double((long long)acc->maxP);
+    const unsigned fl = acc->flags;
+    double cons = 0.0;
+    if (ms->has_gain && acc->sum_N0 >= 1e-30) cons = fabs(acc->sum_pop - acc->sum_N0) / acc->sum_N0;
+    ms->step = step;
+    ms->max_E = max_E;
+    ms->max_P = ms->has_gain ? max_P : 0.0;
+    ms->cons = cons;
+    ms->int_Nu = acc->int_Nu;
+    ms->int_Ng = acc->int_Ng;
+    ms->p_energy = acc->p_energy;
+    ms->flags = fl;
+    bool fatal = (fl & 3u) != 0 || (ms->has_gain && (fl & 12u) != 0);
+    if (!fatal) {
+        if (max_E > ms->thr_E) ms->instability_count++;
+        if (ms->has_gain && max_P > ms->thr_P) ms->instability_count++;
+        if (step > 0 && step % 100 == 0 && ms->prev_max_E > 1e-20) ms->prev_max_E = max_E;
+        else if (step == 0 || ms->prev_max_E < 1e-20) ms->prev_max_E = fmax(max_E, 1e-20);
+        if (ms->instability_count > 10) fatal = true;
+    }
+    if (fatal) {
+        ms->stable = 0;
+        *status = 1u;
+    }
+    acc->maxE = 0; acc->maxP = 0; acc->flags = 0;
+    acc->sum_pop = acc->sum_N0 = acc->int_Nu = acc->int_Ng = acc->p_energy = 0.0;
+}
+
+}  // namespace fdtdk
+
+// ==================================================================== host side
+namespace {
+
+using namespace fdtdk;
+
+struct Failure : std::runtime_error {
+    int code;
+    Failure(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+void ck(cudaError_t e, const char* what) {
+    if (e == cudaSuccess) return;
+    const int code = (e == cudaErrorMemoryAllocation) ? FDTD_ERR_OOM : FDTD_ERR_CUDA;
+    throw Failure(code, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+size_t round_up(size_t v, size_t m) { return (v + m - 1) / m * m; }
+
+class SolverBase {
+public:
+    virtual ~SolverBase() = default;
+    virtual void run(uint64_t n) = 0;
+    virtual void set_field(int comp, const double* h) = 0;
+    virtual void get_field(int comp, double* h) = 0;
+    virtual void set_tls(int which, const double* h) = 0;
+    virtual void get_tls(int which, double* h) = 0;
+    virtual void probe_series(double* out, uint64_t max, uint64_t* n) = 0;
+    virtual void dft(uint32_t p, double* re, double* im) = 0;
+    virtual void diagnostics(fdtd_diagnostics_v1* d) = 0;
+    virtual void sync() = 0;
+    virtual void set_timing(int mode) = 0;
+    virtual void timing(fdtd_timing_v1* t) = 0;
+    uint64_t steps = 0, launches = 0, dev_bytes = 0;
+    int device = 0;
+};
+
+template <typename T>
+class Solver final : public SolverBase {
+public:
+    explicit Solver(const fdtd_setup_v1& s, int dev);
+    ~Solver() override;
+    void run(uint64_t n) override;
+    void set_field(int comp, const double* h) override;
+    void get_field(int comp, double* h) override;
+    void set_tls(int which, const double* h) override;
+    void get_tls(int which, double* h) override;
+    void probe_series(double* out, uint64_t max, uint64_t* n) override;
+    void dft(uint32_t p, double* re, double* im) override;
+    void diagnostics(fdtd_diagnostics_v1* d) override;
+    void sync() override { ck(cudaStreamSynchronize(st_), "cudaStreamSynchronize"); }
+    void set_timing(int mode) override;
+    void timing(fdtd_timing_v1* t) override { *t = tm_; }
+
+private:
+    template <typename U> U* alloc(size_t n, bool zero = true) {
+        void* p = nullptr;
+        ck(cudaMalloc(&p, std::max<size_t>(n, 1) * sizeof(U)), "cudaMalloc");
+        ptrs_.push_back(p);
+        dev_bytes += std::max<size_t>(n, 1) * sizeof(U);
+        if (zero) ck(cudaMemsetAsync(p, 0, std::max<size_t>(n, 1) * sizeof(U), st_), "cudaMemsetAsync");
+        return static_cast<U*>(p);
+    }
+    template <typename U> U* upload(const std::vector<U>& v) {
+        U* d = alloc<U>(v.size(), false);
+        ck(cudaMemcpyAsync(d, v.data(), v.size() * sizeof(U), cudaMemcpyHostToDevice, st_), "cudaMemcpyAsync");
+        return d;
+    }
+    double* staging();
+    void to_device(const double* host_idx3, T* dst);
+    void from_device(const T* src, double* host_idx3);
+    void ensure_series(uint64_t samples);
+
+    cudaStream_t st_ = nullptr;
+    std::vector<void*> ptrs_;
+    StepArgs<T> a_{};
+    int NxT_, NyT_, NzT_, NxP_, np_;
+    size_t plane_, nflat_;
+    int kchunkH_ = 1, kchunkE_ = 1;
+    dim3 gridH_, gridE_;
+    double dt_;
+    // sources
+    std::vector<fdtd_dipole_v1> dip_;
+    // detectors
+    uint32_t save_every_ = 1, nprobes_ = 0, nf_ = 0;
+    ProbeDev* d_probes_ = nullptr;
+    double *d_freqs_ = nullptr, *d_dft_ = nullptr, *d_series_ = nullptr;
+    uint64_t series_cap_ = 0, series_count_ = 0;
+    // monitor
+    uint32_t interval_ = 0;
+    double *d_dx_ = nullptr, *d_dy_ = nullptr, *d_dz_ = nullptr;
+    DiagAccum* d_acc_ = nullptr;
+    MonitorState* d_ms_ = nullptr;
+    unsigned* d_status_ = nullptr;
+    double* d_stage_ = nullptr;
+    bool has_gain_ = false;
+    // event timing: ev_[0..3] bracket H, E and the auxiliary kernels of one step
+    int timing_ = FDTD_TIMING_OFF;
+    cudaEvent_t ev_[4] = {nullptr, nullptr, nullptr, nullptr};
+    fdtd_timing_v1 tm_{};
+};
+
+template <typename T>
+Solver<T>::Solver(const fdtd_setup_v1& s, int dev) {
+    device = dev;
+    ck(cudaSetDevice(dev), "cudaSetDevice");
+    ck(cudaStreamCreateWithFlags(&st_, cudaStreamNonBlocking), "cudaStreamCreate");
+    constexpr int W = Vec<T>::W;
+    NxT_ = int(s.NxT); NyT_ = int(s.NyT); NzT_ = int(s.NzT);
+    np_ = int(s.npml);
+    NxP_ = int(round_up(size_t(NxT_), 128 / sizeof(T)));
+    plane_ = size_t(NxP_) * NyT_;
+    nflat_ = plane_ * NzT_;
+    dt_ = s.dt;
+    const size_t N = size_t(NxT_) * NyT_ * NzT_;
+
+    StepArgs<T>& a = a_;
+    a.NxT = NxT_; a.NyT = NyT_; a.NzT = NzT_; a.NxP = NxP_; a.np = np_;
+    a.plane = (long long)plane_;
+    T* f[6];
+    for (int c = 0; c < 6; ++c) f[c] = alloc<T>(nflat_);
+    a.Ex = f[0]; a.Ey = f[1]; a.Ez = f[2]; a.Hx = f[3]; a.Hy = f[4]; a.Hz = f[5];
+
+    // bH must be uniform and aE = aH = 1 (sigma = 0, mu_r = 1).
+    double bH = s.bH_uniform;
+    for (int c = 0; c < 3; ++c) {
+        if (s.aE[c]) for (size_t q = 0; q < N; ++q) if (s.aE[c][q] != 1.0) throw Failure(FDTD_ERR_UNSUPPORTED, "aE != 1 (lossy material) is not supported");
+        if (s.aH[c]) for (size_t q = 0; q < N; ++q) if (s.aH[c][q] != 1.0) throw Failure(FDTD_ERR_UNSUPPORTED, "aH != 1 (magnetic loss) is not supported");
+        if (s.bH[c]) {
+            if (c == 0) bH = s.bH[0][0];
+            for (size_t q = 0; q < N; ++q) if (s.bH[c][q] != bH) throw Failure(FDTD_ERR_UNSUPPORTED, "non-uniform bH (mu_r != 1) is not supported");
+        }
+    }
+    a.bH = T(bH);
+    T* be[3];
+    for (int c = 0; c < 3; ++c) {
+        be[c] = alloc<T>(nflat_);
+        to_device(s.bE[c], be[c]);
+    }
+    a.bEx = be[0]; a.bEy = be[1]; a.bEz = be[2];
+
+    // 1-D arrays
+    std::vector<T> idx(NxP_, T(0)), idy(NyT_), idz(NzT_);
+    for (int i = 0; i < NxT_; ++i) idx[i] = T(s.inv_dx[i]);
+    for (int j = 0; j < NyT_; ++j) idy[j] = T(s.inv_dy[j]);
+    for (int k = 0; k < NzT_; ++k) idz[k] = T(s.inv_dz[k]);
+    a.idx = upload(idx); a.idy = upload(idy); a.idz = upload(idz);
+    const int Ns[3] = {NxT_, NyT_, NzT_};
+    for (int ax = 0; ax < 3; ++ax) {
+        const int n = Ns[ax];
+        const int len = ax == 0 ? NxP_ : n;
+        std::vector<T> ik(len, T(1)), bE(len, T(1)), cE(len, T(0)), bHp(len, T(1)), cH(len, T(0));
+        for (int q = 0; q < n; ++q) {
+            ik[q] = T(1.0 / s.cpml_kappa[ax][q]);
+            bE[q] = T(s.cpml_bE[ax][q]); cE[q] = T(s.cpml_cE[ax][q]);
+            bHp[q] = T(s.cpml_bH[ax][q]); cH[q] = T(s.cpml_cH[ax][q]);
+        }
+        a.ik[ax] = upload(ik);
+        a.pbE[ax] = upload(bE); a.pcE[ax] = upload(cE);
+        a.pbH[ax] = upload(bHp); a.pcH[ax] = upload(cH);
+    }
+    // psi slabs
+    const size_t np2 = size_t(2 * np_);
+    for (int q = 0; q < 6; ++q) { a.psiH[q] = nullptr; a.psiE[q] = nullptr; }
+    if (np_ > 0) {
+        const size_t xs = size_t(NzT_) * NyT_ * np2, ys = size_t(NzT_) * np2 * NxP_, zs = np2 * NyT_ * NxP_;
+        // 0 *_y, 1 *_z, 2 *_z, 3 *_x, 4 *_x, 5 *_y
+        const size_t sz[6] = {ys, zs, zs, xs, xs, ys};
+        for (int q = 0; q < 6; ++q) { a.psiH[q] = alloc<T>(sz[q]); a.psiE[q] = alloc<T>(sz[q]); }
+    }
+
+    // gain block
+    a.gain = 0;
+    a.greg = nullptr; a.P0 = a.P1 = a.Nu = a.Ng = nullptr; a.gcoef = nullptr;
+    a.gi0 = a.gj0 = a.gk0 = 0; a.gX = a.gY = a.gZ = 0;
+    if (s.n_tls_regions > 0) {
+        if (!s.tls_region_map || !s.tls_regions) throw Failure(FDTD_ERR_INVALID, "gain regions without region map");
+        if (s.n_tls_regions > 127) throw Failure(FDTD_ERR_UNSUPPORTED, "more than 127 gain regions");
+        int lo[3] = {NxT_, NyT_, NzT_}, hi[3] = {-1, -1, -1};
+        for (int i = 0; i < NxT_; ++i)
+            for (int j = 0; j < NyT_; ++j)
+                for (int k = 0; k < NzT_; ++k) {
+                    const int32_t r = s.tls_region_map[(size_t(i) * NyT_ + j) * NzT_ + k];
+                    if (r < 0) continue;
+                    if (r >= int32_t(s.n_tls_regions)) throw Failure(FDTD_ERR_INVALID, "region map entry out of range");
+                    if (i == 0 || j == 0 || k == 0)
+                        throw Failure(FDTD_ERR_UNSUPPORTED, "gain cells on the i=0/j=0/k=0 boundary planes");
+                    lo[0] = std::min(lo[0], i); hi[0] = std::max(hi[0], i);
+                    lo[1] = std::min(lo[1], j); hi[1] = std::max(hi[1], j);
+                    lo[2] = std::min(lo[2], k); hi[2] = std::max(hi[2], k);
+                }
+        if (hi[0] >= 0) {
+            has_gain_ = true;
+            a.gain = 1;
+            a.gi0 = lo[0]; a.gj0 = lo[1]; a.gk0 = lo[2];
+            a.gX = hi[0] - lo[0] + 1; a.gY = hi[1] - lo[1] + 1; a.gZ = hi[2] - lo[2] + 1;
+            const size_t ng = size_t(a.gX) * a.gY * a.gZ;
+            std::vector<int8_t> reg(ng);
+            for (int k = 0; k < a.gZ; ++k)
+                for (int j = 0; j < a.gY; ++j)
+                    for (int i = 0; i < a.gX; ++i)
+                        reg[(size_t(k) * a.gY + j) * a.gX + i] = int8_t(
+                            s.tls_region_map[(size_t(i + a.gi0) * NyT_ + (j + a.gj0)) * NzT_ + (k + a.gk0)]);
+            a.greg = upload(reg);
+            a.P0 = alloc<T>(ng); a.P1 = alloc<T>(ng); a.Nu = alloc<T>(ng); a.Ng = alloc<T>(ng);
+            std::vector<GainCoef<T>> gc(s.n_tls_regions);
+            for (uint32_t r = 0; r < s.n_tls_regions; ++r) {
+                const fdtd_tls_region_v1& R = s.tls_regions[r];
+                GainCoef<T>& g = gc[r];
+                g.kapaN0 = T(R.kapa_coeff * R.N0);
+                g.pa2 = T(R.pa2); g.pa3 = T(R.pa3); g.inv_dt = T(R.inv_dt);
+                g.inv_N0 = T(R.N0 > 0 ? 1.0 / R.N0 : 0.0);
+                g.N0 = T(R.N0);
+                g.dt = T(s.dt);
+                g.inv_tau = T(1.0 / R.tau);
+                g.inv_hbar_omega = T(1.0 / (R.hbar * R.omega_a));
+                g.pump = T(R.pump_rate);
+                g.clamp = R.enable_population_clamp;
+                g.active = R.N0 > 0 ? 1 : 0;
+            }
+            a.gcoef = upload(gc);
+            if (s.tls_Nu) set_tls(FDTD_TLS_NU, s.tls_Nu);
+            if (s.tls_Ng) set_tls(FDTD_TLS_NG, s.tls_Ng);
+        }
+    }
+
+    // sources
+    if (s.n_dipoles > uint32_t(kMaxSources)) throw Failure(FDTD_ERR_UNSUPPORTED, "more than 8 point sources");
+    for (uint32_t q = 0; q < s.n_dipoles; ++q) {
+        const fdtd_dipole_v1& d = s.dipoles[q];
+        if (d.i >= s.NxT || d.j >= s.NyT || d.k >= s.NzT) throw Failure(FDTD_ERR_INVALID, "source cell outside the grid");
+        if (d.polarization < 0 || d.polarization > 5) throw Failure(FDTD_ERR_INVALID, "source polarization must be 0..5");
+        dip_.push_back(d);
+    }
+
+    // probes / DFT
+    save_every_ = std::max<uint32_t>(1, s.save_every);
+    nprobes_ = s.n_probes;
+    nf_ = s.n_dft_freqs;
+    if (nprobes_) {
+        std::vector<ProbeDev> pd(nprobes_);
+        for (uint32_t q = 0; q < nprobes_; ++q) {
+            const fdtd_probe_v1& p = s.probes[q];
+            if (p.i >= s.NxT || p.j >= s.NyT || p.k >= s.NzT || p.component < 0 || p.component > 11)
+                throw Failure(FDTD_ERR_INVALID, "probe outside the grid or bad component");
+            pd[q].off = (long long)((size_t(p.k) * NyT_ + p.j) * NxP_ + p.i);
+            pd[q].comp = p.component;
+        }
+        d_probes_ = upload(pd);
+        if (nf_) {
+            d_freqs_ = upload(std::vector<double>(s.dft_freqs, s.dft_freqs + nf_));
+            d_dft_ = alloc<double>(size_t(2) * nprobes_ * nf_);
+        }
+    }
+
+    // monitor
+    interval_ = s.monitor_interval;
+    d_dx_ = upload(std::vector<double>(s.dx, s.dx + NxT_));
+    d_dy_ = upload(std::vector<double>(s.dy, s.dy + NyT_));
+    d_dz_ = upload(std::vector<double>(s.dz, s.dz + NzT_));
+    d_acc_ = alloc<DiagAccum>(1);
+    MonitorState ms{};
+    ms.stable = 1;
+    ms.has_gain = has_gain_ ? 1 : 0;
+    ms.thr_E = s.max_E; ms.thr_P = s.max_P; ms.thr_cons = s.conservation_err; ms.thr_growth = s.growth_rate;
+    d_ms_ = upload(std::vector<MonitorState>{ms});
+    d_status_ = alloc<unsigned>(1);
+    a.status = d_status_;
+
+    // launch shapes: z-chunks so that the grid holds several waves of blocks
+    const int gx = int((NxT_ + 32 * W - 1) / (32 * W));
+    auto chunk = [&](int rows, int planes) {
+        const int bxy = std::max(1, gx * ((rows + kBlockY - 1) / kBlockY));
+        const int want = std::max(1, (148 * 16 + bxy - 1) / bxy);
+        const int zc = std::max(1, std::min(want, std::max(1, planes / 8)));
+        return std::max(1, (planes + zc - 1) / zc);
+    };
+    kchunkH_ = chunk(NyT_ - 1, NzT_ - 1);
+    kchunkE_ = chunk(NyT_, NzT_);
+    gridH_ = dim3(gx, (NyT_ - 1 + kBlockY - 1) / kBlockY, (NzT_ - 1 + kchunkH_ - 1) / kchunkH_);
+    gridE_ = dim3(gx, (NyT_ + kBlockY - 1) / kBlockY, (NzT_ + kchunkE_ - 1) / kchunkE_);
+    ck(cudaStreamSynchronize(st_), "setup upload");
+}
+
+template <typename T>
+void Solver<T>::set_timing(int mode) {
+    if (mode < FDTD_TIMING_OFF || mode > FDTD_TIMING_KERNELS) throw Failure(FDTD_ERR_INVALID, "bad timing mode");
+    ck(cudaSetDevice(device), "cudaSetDevice");
+    if (mode != FDTD_TIMING_OFF && !ev_[0])
+        for (auto& e : ev_) ck(cudaEventCreate(&e), "cudaEventCreate");
+    timing_ = mode;
+    tm_ = fdtd_timing_v1{};
+}
+
+template <typename T>
+Solver<T>::~Solver() {
+    cudaSetDevice(device);
+    if (st_) cudaStreamSynchronize(st_);
+    for (auto& e : ev_) if (e) cudaEventDestroy(e);
+    for (void* p : ptrs_) cudaFree(p);
+    if (d_stage_) cudaFree(d_stage_);
+    if (st_) cudaStreamDestroy(st_);
+}
+
+template <typename T>
+double* Solver<T>::staging() {
+    if (!d_stage_) {
+        ck(cudaMalloc(&d_stage_, size_t(NxT_) * NyT_ * NzT_ * sizeof(double)), "cudaMalloc staging");
+        dev_bytes += size_t(NxT_) * NyT_ * NzT_ * sizeof(double);
+    }
+    return d_stage_;
+}
+
+template <typename T>
+void Solver<T>::to_device(const double* h, T* dst) {
+    if (!h) throw Failure(FDTD_ERR_INVALID, "null host array");
+    double* sbuf = staging();
+    ck(cudaMemcpyAsync(sbuf, h, size_t(NxT_) * NyT_ * NzT_ * sizeof(double), cudaMemcpyHostToDevice, st_), "H2D");
+    dim3 g((NzT_ + 31) / 32, (NxT_ + 31) / 32, NyT_), b(32, 8);
+    k_from_idx3<T><<<g, b, 0, st_>>>(sbuf, dst, NxT_, NyT_, NzT_, NxP_);
+    ++launches;
+    ck(cudaGetLastError(), "k_from_idx3");
+    ck(cudaStreamSynchronize(st_), "to_device");
+}
+
+template <typename T>
+void Solver<T>::from_device(const T* src, double* h) {
+    if (!h) throw Failure(FDTD_ERR_INVALID, "null host array");
+    double* sbuf = staging();
+    dim3 g((NzT_ + 31) / 32, (NxT_ + 31) / 32, NyT_), b(32, 8);
+    k_to_idx3<T><<<g, b, 0, st_>>>(src, sbuf, NxT_, NyT_, NzT_, NxP_);
+    ++launches;
+    ck(cudaGetLastError(), "k_to_idx3");
+    ck(cudaMemcpyAsync(h, sbuf, size_t(NxT_) * NyT_ * NzT_ * sizeof(double), cudaMemcpyDeviceToHost, st_), "D2H");
+    ck(cudaStreamSynchronize(st_), "from_device");
+}
+
+template <typename T>
+void Solver<T>::set_field(int comp, const double* h) {
+    if (comp < 0 || comp > 5) throw Failure(FDTD_ERR_INVALID, "component must be 0..5");
+    T* f[6] = {a_.Ex, a_.Ey, a_.Ez, a_.Hx, a_.Hy, a_.Hz};
+    to_device(h, f[comp]);
+}
+
+template <typename T>
+void Solver<T>::get_field(int comp, double* h) {
+    if (comp < 0 || comp > 5) throw Failure(FDTD_ERR_INVALID, "component must be 0..5");
+    const T* f[6] = {a_.Ex, a_.Ey, a_.Ez, a_.Hx, a_.Hy, a_.Hz};
+    from_device(f[comp], h);
+}
+
+template <typename T>
+void Solver<T>::set_tls(int which, const double* h) {
+    if (which < 0 || which > 3) throw Failure(FDTD_ERR_INVALID, "which must be FDTD_TLS_*");
+    if (!has_gain_) throw Failure(FDTD_ERR_INVALID, "solve has no gain region");
+    T* dst = which == FDTD_TLS_PZ ? ((steps & 1) ? a_.P1 : a_.P0)
+           : which == FDTD_TLS_PZ_PREV ? ((steps & 1) ? a_.P0 : a_.P1)
+           : which == FDTD_TLS_NU ? a_.Nu : a_.Ng;
+    double* sbuf = staging();
+    ck(cudaMemcpyAsync(sbuf, h, size_t(NxT_) * NyT_ * NzT_ * sizeof(double), cudaMemcpyHostToDevice, st_), "H2D");
+    k_gain_block<T><<<592, 256, 0, st_>>>(sbuf, dst, a_.greg, a_.gi0, a_.gj0, a_.gk0, a_.gX, a_.gY, a_.gZ, NyT_, NzT_, 1);
+    ++launches;
+    ck(cudaGetLastError(), "k_gain_block");
+    ck(cudaStreamSynchronize(st_), "set_tls");
+}
+
+template <typename T>
+void Solver<T>::get_tls(int which, double* h) {
+    if (which < 0 || which > 3) throw Failure(FDTD_ERR_INVALID, "which must be FDTD_TLS_*");
+    const size_t N = size_t(NxT_) * NyT_ * NzT_;
+    std::memset(h, 0, N * sizeof(double));
+    if (!has_gain_) return;
+    T* src = which == FDTD_TLS_PZ ? ((steps & 1) ? a_.P1 : a_.P0)
+           : which == FDTD_TLS_PZ_PREV ? ((steps & 1) ? a_.P0 : a_.P1)
+           : which == FDTD_TLS_NU ? a_.Nu : a_.Ng;
+    double* sbuf = staging();
+    ck(cudaMemsetAsync(sbuf, 0, N * sizeof(double), st_), "memset");
+    k_gain_block<T><<<592, 256, 0, st_>>>(sbuf, src, a_.greg, a_.gi0, a_.gj0, a_.gk0, a_.gX, a_.gY, a_.gZ, NyT_, NzT_, 0);
+    ++launches;
+    ck(cudaGetLastError(), "k_gain_block");
+    ck(cudaMemcpyAsync(h, sbuf, N * sizeof(double), cudaMemcpyDeviceToHost, st_), "D2H");
+    ck(cudaStreamSynchronize(st_), "get_tls");
+}
+
+template <typename T>
+void Solver<T>::ensure_series(uint64_t samples) {
+    if (nprobes_ == 0 || samples <= series_cap_) return;
+    uint64_t cap = std::max<uint64_t>(samples, series_cap_ * 2);
+    double* d = nullptr;
+    ck(cudaMalloc(&d, cap * nprobes_ * sizeof(double)), "cudaMalloc series");
+    if (d_series_) {
+        ck(cudaMemcpyAsync(d, d_series_, series_count_ * nprobes_ * sizeof(double), cudaMemcpyDeviceToDevice, st_), "series copy");
+        ck(cudaStreamSynchronize(st_), "series copy");
+        cudaFree(d_series_);
+        dev_bytes -= series_cap_ * nprobes_ * sizeof(double);
+    }
+    d_series_ = d;
+    dev_bytes += cap * nprobes_ * sizeof(double);
+    series_cap_ = cap;
+}
+
+template <typename T>
+void Solver<T>::run(uint64_t n) {
+    ck(cudaSetDevice(device), "cudaSetDevice");
+    const uint64_t n0 = steps;
+    const uint64_t last = n0 + n;  // exclusive
+    ensure_series((last + save_every_ - 1) / save_every_);
+    const dim3 blk(32, kBlockY);
+    ESrc src{};
+    src.n = int(dip_.size());
+    for (int q = 0; q < src.n; ++q) {
+        src.si[q] = int(dip_[q].i); src.sj[q] = int(dip_[q].j); src.sk[q] = int(dip_[q].k);
+        src.sc[q] = dip_[q].polarization % 3;
+    }
+    const int pthreads = int(nprobes_ * std::max<uint32_t>(nf_, 1));
+    const bool per_kernel = timing_ == FDTD_TIMING_KERNELS;
+    if (timing_ == FDTD_TIMING_RUN) ck(cudaEventRecord(ev_[0], st_), "cudaEventRecord");
+    for (uint64_t s = n0; s < last; ++s) {
+        if (per_kernel) ck(cudaEventRecord(ev_[0], st_), "cudaEventRecord");
+        k_update_H<T><<<gridH_, blk, 0, st_>>>(a_, kchunkH_);
+        if (per_kernel) ck(cudaEventRecord(ev_[1], st_), "cudaEventRecord");
+        src.parity = int(s & 1);
+        for (int q = 0; q < src.n; ++q) {
+            const fdtd_dipole_v1& d = dip_[q];
+            src.J[q] = fdtd::current_density(d.waveform, s, dt_, d.I0, d.f0, d.tau, d.t0, d.t_shift, d.cell_area);
+        }
+        k_update_E<T><<<gridE_, blk, 0, st_>>>(a_, kchunkE_, src);
+        if (per_kernel) ck(cudaEventRecord(ev_[2], st_), "cudaEventRecord");
+        launches += 2;
+        if (nprobes_) {
+            const long long sample = (s % save_every_ == 0) ? (long long)(s / save_every_) : -1;
+            k_probe_dft<T><<<(pthreads + 127) / 128, 128, 0, st_>>>(a_, d_probes_, int(nprobes_), d_freqs_, int(nf_),
+                                                                      d_dft_, d_series_, sample, double(s + 1) * dt_, dt_);
+            ++launches;
+            if (sample >= 0) series_count_ = uint64_t(sample) + 1;
+        }
+        if (interval_ && s % interval_ == 0) {
+            k_monitor_reduce<T><<<4 * 148, 256, 0, st_>>>(a_, nflat_, d_dx_, d_dy_, d_dz_, int((s + 1) & 1), d_acc_);
+            k_monitor_eval<<<1, 1, 0, st_>>>(d_acc_, d_ms_, d_status_, s);
+            launches += 2;
+        }
+        if (per_kernel) {
+            ck(cudaEventRecord(ev_[3], st_), "cudaEventRecord");
+            ck(cudaEventSynchronize(ev_[3]), "cudaEventSynchronize");
+            float a = 0, b = 0, c = 0;
+            ck(cudaEventElapsedTime(&a, ev_[0], ev_[1]), "cudaEventElapsedTime");
+            ck(cudaEventElapsedTime(&b, ev_[1], ev_[2]), "cudaEventElapsedTime");
+            ck(cudaEventElapsedTime(&c, ev_[2], ev_[3]), "cudaEventElapsedTime");
+            tm_.h_ms += a; tm_.e_ms += b; tm_.aux_ms += c;
+            tm_.steps += 1;
+        }
+    }
+    if (timing_ == FDTD_TIMING_RUN) ck(cudaEventRecord(ev_[3], st_), "cudaEventRecord");
+    ck(cudaGetLastError(), "step kernels");
+    unsigned status = 0;
+    ck(cudaMemcpyAsync(&status, d_status_, sizeof(unsigned), cudaMemcpyDeviceToHost, st_), "status");
+    ck(cudaStreamSynchronize(st_), "run");
+    if (timing_ == FDTD_TIMING_RUN) {
+        float ms = 0;
+        ck(cudaEventElapsedTime(&ms, ev_[0], ev_[3]), "cudaEventElapsedTime");
+        tm_.run_ms += ms;
+        tm_.steps += n;
+    }
+    if (status) {
+        MonitorState ms{};
+        ck(cudaMemcpy(&ms, d_ms_, sizeof(ms), cudaMemcpyDeviceToHost), "monitor state");
+        steps = ms.step + 1;
+        series_count_ = std::min<uint64_t>(series_count_, (steps + save_every_ - 1) / save_every_);
+        throw Failure(FDTD_ERR_UNSTABLE, "stability monitor stopped the solve at step " + std::to_string(ms.step));
+    }
+    steps = last;
+}
+
+template <typename T>
+void Solver<T>::probe_series(double* out, uint64_t max, uint64_t* n) {
+    const uint64_t cnt = std::min<uint64_t>(series_count_, max);
+    if (n) *n = series_count_;
+    if (cnt && nprobes_ && out)
+        ck(cudaMemcpy(out, d_series_, cnt * nprobes_ * sizeof(double), cudaMemcpyDeviceToHost), "series D2H");
+}
+
+template <typename T>
+void Solver<T>::dft(uint32_t p, double* re, double* im) {
+    if (p >= nprobes_ || nf_ == 0) throw Failure(FDTD_ERR_INVALID, "no DFT for this probe");
+    std::vector<double> buf(2 * size_t(nf_));
+    ck(cudaMemcpy(buf.data(), d_dft_ + 2 * size_t(p) * nf_, buf.size() * sizeof(double), cudaMemcpyDeviceToHost), "dft D2H");
+    for (uint32_t m = 0; m < nf_; ++m) { re[m] = buf[2 * m]; im[m] = buf[2 * m + 1]; }
+}
+
+template <typename T>
+void Solver<T>::diagnostics(fdtd_diagnostics_v1* d) {
+    MonitorState ms{};
+    ck(cudaMemcpy(&ms, d_ms_, sizeof(ms), cudaMemcpyDeviceToHost), "monitor state");
+    std::memset(d, 0, sizeof(*d));
+    d->step = ms.step;
+    d->steps_done = steps;
+    d->max_E = ms.max_E;
+    d->max_P = ms.max_P;
+    d->conservation_err = ms.cons;
+    d->integrated_Nu = ms.int_Nu;
+    d->integrated_Ng = ms.int_Ng;
+    d->polarization_energy = ms.p_energy;
+    d->nan_flags = ms.flags;
+    d->instability_count = ms.instability_count;
+    d->stable = ms.stable;
+}
+
+}  // namespace
+
+// ==================================================================== C ABI
+struct fdtd_handle {
+    std::unique_ptr<SolverBase> s;
+    std::string err;
+};
+
+namespace {
+thread_local std::string g_err;
+
+template <typename F>
+int guarded(fdtd_handle* h, F&& f) {
+    try {
+        f();
+        return FDTD_OK;
+    } catch (const Failure& e) {
+        (h ? h->err : g_err) = e.what();
+        return e.code;
+    } catch (const std::exception& e) {
+        (h ? h->err : g_err) = e.what();
+        return FDTD_ERR_INVALID;
+    }
+}
+}  // namespace
+
+extern "C" {
+
+int fdtd_create(const fdtd_setup_v1* s, int device, fdtd_handle** out) {
+    if (!s || !out) { g_err = "null argument"; return FDTD_ERR_INVALID; }
+    *out = nullptr;
+    if (s->struct_size != sizeof(fdtd_setup_v1)) { g_err = "fdtd_setup_v1.struct_size mismatch"; return FDTD_ERR_INVALID; }
+    if (s->NxT < 3 || s->NyT < 3 || s->NzT < 3 || s->NxT > (1u << 30) || s->NyT > (1u << 30) || s->NzT > (1u << 30)) {
+        g_err = "grid dimensions out of range"; return FDTD_ERR_INVALID;
+    }
+    if (2 * uint64_t(s->npml) >= s->NxT || 2 * uint64_t(s->npml) >= s->NyT || 2 * uint64_t(s->npml) >= s->NzT) {
+        g_err = "npml too large for the grid"; return FDTD_ERR_INVALID;
+    }
+    if (!s->bE[0] || !s->bE[1] || !s->bE[2] || !s->inv_dx || !s->inv_dy || !s->inv_dz || !s->dx || !s->dy || !s->dz) {
+        g_err = "missing required setup arrays"; return FDTD_ERR_INVALID;
+    }
+    for (int a = 0; a < 3; ++a)
+        if (!s->cpml_kappa[a] || !s->cpml_bE[a] || !s->cpml_cE[a] || !s->cpml_bH[a] || !s->cpml_cH[a]) {
+            g_err = "missing CPML profile arrays"; return FDTD_ERR_INVALID;
+        }
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        g_err = "no CUDA device available";
+        return FDTD_ERR_NO_DEVICE;
+    }
+    if (device < 0 || device >= ndev) { g_err = "device index out of range"; return FDTD_ERR_INVALID; }
+    auto* h = new fdtd_handle();
+    const int rc = guarded(nullptr, [&] {
+        if (s->precision == FDTD_PREC_FP64) h->s = std::make_unique<Solver<double>>(*s, device);
+        else if (s->precision == FDTD_PREC_FP32) h->s = std::make_unique<Solver<float>>(*s, device);
+        else throw Failure(FDTD_ERR_UNSUPPORTED, "precision must be FDTD_PREC_FP32 or FDTD_PREC_FP64");
+    });
+    if (rc != FDTD_OK) { delete h; return rc; }
+    *out = h;
+    return FDTD_OK;
+}
+
+int fdtd_set_field(fdtd_handle* h, int c, const double* a) { if (!h) return FDTD_ERR_INVALID; return guarded(h, [&] { h->s->set_field(c, a); }); }
+int fdtd_get_field(fdtd_handle* h, int c, double* a) { if (!h) return FDTD_ERR_INVALID; return guarded(h, [&] { h->s->get_field(c, a); }); }
+int fdtd_set_tls_state(fdtd_handle* h, int w, const double* a) { if (!h) return FDTD_ERR_INVALID; return guarded(h, [&] { h->s->set_tls(w, a); }); }
+int fdtd_get_tls_state(fdtd_handle* h, int w, double* a) { if (!h) return FDTD_ERR_INVALID; return guarded(h, [&] { h->s->get_tls(w, a); }); }
+int fdtd_run(fdtd_handle* h, uint64_t n) { if (!h) return FDTD_ERR_INVALID; return guarded(h, [&] { h->s->run(n); }); }
+int fdtd_steps_done(const fdtd_handle* h, uint64_t* n) { if (!h || !n) return FDTD_ERR_INVALID; *n = h->s->steps; return FDTD_OK; }
+int fdtd_get_probe_series(fdtd_handle* h, double* out, uint64_t max, uint64_t* n) { if (!h) return FDTD_ERR_INVALID; return guarded(h, [&] { h->s->probe_series(out, max, n); }); }
+int fdtd_get_dft(fdtd_handle* h, uint32_t p, double* re, double* im) { if (!h || !re || !im) return FDTD_ERR_INVALID; return guarded(h, [&] { h->s->dft(p, re, im); }); }
+int fdtd_get_diagnostics(fdtd_handle* h, fdtd_diagnostics_v1* d) { if (!h || !d) return FDTD_ERR_INVALID; return guarded(h, [&] { h->s->diagnostics(d); }); }
+int fdtd_device_bytes(const fdtd_handle* h, uint64_t* b) { if (!h || !b) return FDTD_ERR_INVALID; *b = h->s->dev_bytes; return FDTD_OK; }
+int fdtd_kernel_launches(const fdtd_handle* h, uint64_t* n) { if (!h || !n) return FDTD_ERR_INVALID; *n = h->s->launches; return FDTD_OK; }
+int fdtd_set_timing(fdtd_handle* h, int mode) { if (!h) return FDTD_ERR_INVALID; return guarded(h, [&] { h->s->set_timing(mode); }); }
+int fdtd_get_timing(fdtd_handle* h, fdtd_timing_v1* t) { if (!h || !t) return FDTD_ERR_INVALID; return guarded(h, [&] { h->s->timing(t); }); }
+int fdtd_synchronize(fdtd_handle* h) { if (!h) return FDTD_ERR_INVALID; return guarded(h, [&] { h->s->sync(); }); }
+const char* fdtd_last_error(const fdtd_handle* h) { return h ? h->err.c_str() : g_err.c_str(); }
+void fdtd_destroy(fdtd_handle* h) { delete h; }
+
+}  // extern "C"

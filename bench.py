@@ -1,0 +1,339 @@
+"""Benchmark of the B200 FDTD stepper (one JSON line on rank 0).
+
+Workload (default): the 512^3 single solve with CPML and gain -- 512^3 core cells at
+20 nm + 12-cell CPML (536^3 = 154 M total cells), an n = 3.4 slab with a two-level gain
+layer, dipole source, Ez probe with a 21-frequency DFT, FP32 storage
+(3d_fdtd_version008_b200/configs/b512_gain_slab.params).
+
+A bench "step" is one fdtd_run() call that advances the solve by S = --fdtd-steps time
+steps (default 10).  `value` = total cell-updates / device time of K bench steps, in
+Mcell-updates/s, measured with CUDA events on the library's stream (the library records
+them; fdtd_get_timing) bracketed by barriers and synchronisation, max over ranks.  The
+field state (~7 GB) is far larger than L2 (126 MB), so no L2 flush is needed.
+
+Multi-GPU (--gpus N under torchrun): replicas -- every rank runs an independent solve of
+the same workload (the reference has no distributed path; a single solve does not shard
+here), value = all ranks' cell-updates / max over ranks of the device time.
+
+e2e: the same metric through the public C ABI from host buffers: fdtd_create from the host
+setup (H2D of the bE arrays and 1-D profiles, layout transpose on the device), K runs of S
+steps each followed by a D2H read of that run's probe samples, a D2H read of the final Ez
+field, fdtd_destroy -- all inside the timed region (wall clock, synchronised).
+
+--impl reference: times the reference's own CPU loop (oracle/_ref/ref_harness_native, the
+reference headers compiled with its CMake flags and OpenMP on all host cores) on the bounded
+CPU sample of the workload (216^3 total cells, same per-cell physics); falls back to the
+oracle's C restatement when the reference binary is absent.
+"""
+from __future__ import annotations
+
+import argparse
+import importlib
+import json
+import os
+import pathlib
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = pathlib.Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+PKG = importlib.import_module("3d_fdtd_version008_b200")
+
+WORKLOADS = {
+    "b512": ("b512_gain_slab.params", "b512_gain_slab_cpu_sample.params",
+             "512^3 core (536^3 total) uniform 20 nm, 12-cell CPML, n=3.4 slab with 200 nm two-level gain layer "
+             "(pump 1e9/s), z dipole, Ez probe + 21-freq DFT"),
+    "c1": ("c1_gain_slab.params", "c1_gain_slab.params",
+           "C1 non-uniform mesh + gain slab (201x201x69 total)"),
+    "c0": ("c0_dipole_sphere.params", "c0_dipole_sphere.params",
+           "C0 64^3 + 8-cell CPML (80^3 total), dielectric sphere, dipole"),
+}
+
+
+def peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.QUERY}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except FileNotFoundError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+            except ValueError:
+                continue
+            for name, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def algorithmic_bytes(setup, word: int):
+    """Compulsory bytes per step of the two-sweep algorithm (storage word `word` bytes).
+
+    H sweep: read E(3) H(3), write H(3) = 9 words/cell; E sweep: read H(3) E(3) bE(3), write
+    E(3) = 12 words/cell; + 2 words per active CPML psi (4 per axis, 2 per sweep) in that
+    axis' slab; + gain cells: read P^n, P^{n-1}, Nu, Ng and write P^{n+1}, Nu, Ng = 7 words."""
+    NxT, NyT, NzT = setup.shape
+    npml = int(setup.view.npml)
+    cells = NxT * NyT * NzT
+    slab = sum(2 * npml * (cells // n) for n in (NxT, NyT, NzT))  # cells inside each axis' slab, summed
+    gain = int((setup.array("tls_region_map") >= 0).sum()) if setup.view.n_tls_regions else 0
+    h = 9 * word * cells + 2 * 2 * word * slab
+    e = 12 * word * cells + 2 * 2 * word * slab + 7 * word * gain
+    return {"cells": cells, "h_bytes": h, "e_bytes": e, "step_bytes": h + e,
+            "per_cell": (h + e) / cells, "slab_cells": slab, "gain_cells": gain}
+
+
+def dist_setup(n_gpus: int):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        from datetime import timedelta
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600))
+        return rank, local, world, dist
+    return rank, local, 1, None
+
+
+def reduce_max(dist, value: float) -> float:
+    if dist is None:
+        return value
+    import torch
+    t = torch.tensor([value], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(dist):
+    if dist is not None:
+        dist.barrier()
+
+
+def cpu_reference(sample_cfg: str, steps: int, warmup: int, fdtd_steps: int):
+    """Times the reference CPU loop on the bounded sample; returns (Mcell/s, info)."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle
+    cores = os.cpu_count() or 1
+    n = warmup + steps
+    path = PKG.config_path(sample_cfg)
+    if oracle.REF_HARNESS_NATIVE.exists():
+        t_setup = time.time()
+        r = oracle.run_harness(path, 0, "--no-fields", native=True, env={"OMP_NUM_THREADS": str(cores)})
+        shape = [r["meta"][k] for k in ("NxT", "NyT", "NzT")]
+        r = oracle.run_harness(path, n * fdtd_steps, "--no-fields", native=True, env={"OMP_NUM_THREADS": str(cores)})
+        loop_s = float(r["meta"]["loop_seconds"])
+        cells = shape[0] * shape[1] * shape[2]
+        del t_setup
+        kind, exe = "reference", "oracle/_ref/ref_harness_native (reference headers, -O3 -march=native -fopenmp)"
+    else:
+        s = PKG.Setup.from_file(path)
+        o = oracle.OracleSolve(s, 0)
+        t0 = time.time()
+        o.run(n * fdtd_steps, threads=cores)
+        loop_s = time.time() - t0
+        shape = list(s.shape)
+        cells = s.shape[0] * s.shape[1] * s.shape[2]
+        kind, exe = "port", "oracle/lib/libfdtd_oracle.so (C restatement, OpenMP)"
+    value = cells * n * fdtd_steps / loop_s / 1e6
+    sample = (f"{sample_cfg}: {shape[0]}x{shape[1]}x{shape[2]} total cells, {n * fdtd_steps} steps of the "
+              f"reference loop (H, CPML-H, E with gain, CPML-E, probe, populations), {exe}, "
+              f"{cores} threads, loop wall time {loop_s:.2f} s")
+    return value, {"value": round(value, 3), "unit": "Mcell-updates/s", "cores": cores, "kind": kind,
+                   "sample": sample}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--workload", default="b512", choices=sorted(WORKLOADS))
+    ap.add_argument("--fdtd-steps", type=int, default=10, help="time steps per bench step")
+    ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        ap.error("--warmup must be >= 3")
+    cfg, sample_cfg, desc = WORKLOADS[args.workload]
+    rank, local, world, dist = dist_setup(args.gpus)
+    S, K, W = args.fdtd_steps, args.steps, args.warmup
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        value, info = cpu_reference(sample_cfg, K, W, S)
+        line = {"metric": "Mcell-updates/s", "value": round(value, 3), "unit": "Mcell-updates/s", "n_gpus": args.gpus,
+                "steps": K, "warmup": W, "higher_is_better": True, "impl": "reference", "scaling": "weak",
+                "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "config": {"workload": desc + " -- bounded CPU sample", "sample_config": sample_cfg,
+                           "fdtd_steps_per_step": S},
+                "cpu_baseline": info,
+                "e2e": {"value": round(value, 3), "unit": "Mcell-updates/s", "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 0}}
+        print(json.dumps(line))
+        return
+
+    prec = PKG.PREC_FP64 if args.precision == "fp64" else PKG.PREC_FP32
+    word = 8 if prec == PKG.PREC_FP64 else 4
+    setup = PKG.Setup.from_file(PKG.config_path(cfg))
+    cells = setup.shape[0] * setup.shape[1] * setup.shape[2]
+    alg = algorithmic_bytes(setup, word)
+
+    # ---------------------------------------------------------------- device-resident value
+    sol = PKG.Solver(setup, device=local, precision=prec)
+    for _ in range(W):
+        sol.run(S)
+    sol.synchronize()
+    sol.set_timing(PKG.TIMING_RUN)  # one event pair per run() call on the library's stream
+    barrier(dist)
+    clocks = ClockSampler(local)
+    clocks.start()
+    t_wall = time.perf_counter()
+    launches_a = sol.kernel_launches
+    for _ in range(K):
+        sol.run(S)
+    sol.synchronize()
+    t_wall = time.perf_counter() - t_wall
+    launches_b = sol.kernel_launches
+    clk = clocks.stop()
+    barrier(dist)
+    dev_ms = sol.timing()["run_ms"]
+    dev_ms_max = reduce_max(dist, dev_ms)
+    # roofline pass: per-kernel events (one sync per step), a few bench steps after the timed region
+    sol.set_timing(PKG.TIMING_KERNELS)
+    for _ in range(min(K, 5)):
+        sol.run(S)
+    tm = sol.timing()
+    steps_total = K * S
+    value = cells * steps_total * world / (dev_ms_max * 1e-3) / 1e6
+    peak, peak_src = peaks()
+    e_avg_ms = tm["e_ms"] / tm["steps"]
+    h_avg_ms = tm["h_ms"] / tm["steps"]
+    achieved_e = alg["e_bytes"] / (e_avg_ms * 1e-3) / 1e9
+    achieved_step = alg["step_bytes"] / ((e_avg_ms + h_avg_ms) * 1e-3) / 1e9
+    traffic = None
+    prof = ROOT / "profiles" / f"k_update_E_{args.workload}_{args.precision}_traffic.json"
+    if prof.exists():
+        traffic = json.loads(prof.read_text()).get("dram_bytes_per_launch")
+    sol.close()
+    del sol
+
+    # ---------------------------------------------------------------- e2e through the C ABI
+    e2e = None
+    if not args.no_e2e:
+        import numpy as np
+        barrier(dist)
+        t0 = time.perf_counter()
+        s2 = PKG.Solver(setup, device=local, precision=prec)
+        h2d = 3 * cells * 8 + sum(8 * n for n in setup.shape) * 16
+        if setup.view.n_tls_regions:
+            h2d += 2 * cells * 8 + cells * 4
+        d2h = 0
+        for _ in range(K):
+            s2.run(S)
+            series = s2.probe_series()
+            d2h += series[-S:].nbytes
+        ez = s2.field("Ez")
+        d2h += ez.nbytes
+        s2.close()
+        t_e2e = time.perf_counter() - t0
+        t_e2e = reduce_max(dist, t_e2e)
+        e2e = {"value": round(cells * steps_total * world / t_e2e / 1e6, 3), "unit": "Mcell-updates/s",
+               "h2d_bytes_per_step": int(h2d / K), "d2h_bytes_per_step": int(d2h / K),
+               "seconds": round(t_e2e, 4)}
+        del ez, series, np
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        _, cpu = cpu_reference(sample_cfg, 3, 3, 10 if args.workload == "b512" else S)
+
+    if rank != 0:
+        return
+    line = {
+        "metric": "Mcell-updates/s",
+        "value": round(value, 3),
+        "unit": "Mcell-updates/s",
+        "n_gpus": world,
+        "steps": K,
+        "warmup": W,
+        "ms_per_step": round(dev_ms_max / K, 4),
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32" if word == 4 else "f64",
+        "data": "synthetic",
+        "config": {"workload": desc, "config_file": cfg, "total_cells": cells, "grid": list(setup.shape),
+                   "fdtd_steps_per_step": S, "parallelism": "replicas" if world > 1 else "single GPU",
+                   "l2": "state (~%.1f GB) larger than L2, no flush" % (alg["cells"] * word * 9 / 1e9),
+                   "hbm_gbs_step": round(achieved_step, 1),
+                   "algorithmic_bytes_per_cell_step": round(alg["per_cell"], 2),
+                   "wall_ms_per_step": round(t_wall * 1e3 / K, 4)},
+        "roofline": {"bound": "hbm", "kernel": "k_update_E", "achieved": round(achieved_e, 1), "peak": peak,
+                     "unit": "GB/s", "frac": round(achieved_e / peak, 4), "peak_source": peak_src,
+                     "traffic": traffic, "algorithmic_bytes_per_launch": alg["e_bytes"],
+                     "avg_launch_ms": round(e_avg_ms, 5),
+                     "h_kernel": {"achieved": round(alg["h_bytes"] / (h_avg_ms * 1e-3) / 1e9, 1),
+                                  "avg_launch_ms": round(h_avg_ms, 5)}},
+        "e2e": e2e,
+        "cpu_baseline": cpu,
+        "gpu_launches": int(launches_b - launches_a),
+        "clocks": clk,
+    }
+    print(json.dumps(line))
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

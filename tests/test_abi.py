@@ -1,0 +1,65 @@
+"""The C-ABI library loads without a GPU, exports every symbol of include/fdtd_b200.h,
+reports setup errors the way the header documents, and refuses to step without a device
+(no CPU fallback)."""
+import ctypes
+import re
+
+import pytest
+
+from conftest import ROOT
+
+
+def header_symbols():
+    text = (ROOT / "include" / "fdtd_b200.h").read_text()
+    return sorted(set(re.findall(r"\b(fdtd_[a-z_0-9]+)\s*\(", text)))
+
+
+def test_library_exports_every_header_symbol(pkg):
+    lib = ctypes.CDLL(str(pkg.library_path()))
+    syms = header_symbols()
+    assert len(syms) >= 20
+    missing = [s for s in syms if not hasattr(lib, s)]
+    assert not missing, missing
+    assert sorted(pkg.EXPORTED_SYMBOLS) == syms
+
+
+def test_parse_error_reports_message(pkg):
+    with pytest.raises(pkg.FdtdError) as e:
+        pkg.Setup.from_text("MESH_MODE = 0\nNX = abc\n")
+    assert e.value.code == 6 and "NX" in str(e.value)
+    with pytest.raises(pkg.FdtdError) as e:
+        pkg.Setup.from_text("this line has no equals sign\n")
+    assert e.value.code == 6
+    with pytest.raises(pkg.FdtdError):
+        pkg.Setup.from_text("MESH_MODE = 0\nSTRUCTURES += prism, 2.0, 0, 1, 0, 1, 0, 1\n")
+    with pytest.raises(pkg.FdtdError):
+        pkg.Setup.from_text("MESH_MODE = 0\nBOUNDARY_TYPE = 0\n")  # PEC: not handled by the stepper
+
+
+def test_unknown_setup_array_is_an_error(pkg):
+    s = pkg.Setup.from_file(pkg.config_path("c0_dipole_sphere.params"), mesh_only=True)
+    with pytest.raises(pkg.FdtdError):
+        s.array("no_such_array")
+
+
+def test_create_without_device_fails_loudly(pkg):
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    s = pkg.Setup.from_file(pkg.config_path("c0_dipole_sphere.params"))
+    with pytest.raises(pkg.FdtdError) as e:
+        pkg.Solver(s)
+    assert e.value.code == pkg.FDTD_ERR_NO_DEVICE
+
+
+def test_create_validates_view(pkg):
+    s = pkg.Setup.from_file(pkg.config_path("c0_dipole_sphere.params"), mesh_only=True)
+    v = pkg.SetupV1.from_buffer_copy(s.view)
+    v.struct_size = 4
+    with pytest.raises(pkg.FdtdError) as e:
+        pkg.Solver(s, view=v)
+    assert e.value.code == 1
+    v = pkg.SetupV1.from_buffer_copy(s.view)  # mesh-only setup has no bE arrays
+    with pytest.raises(pkg.FdtdError) as e:
+        pkg.Solver(s, view=v)
+    assert e.value.code == 1

@@ -1,0 +1,233 @@
+"""GPU parity: the CUDA stepper (called through the C ABI) against the reference's golden
+state and against the oracle on the shipped configs.
+
+Tolerances: FP64 mode <= 1e-12 relative L2 (the accuracy judge).  FP32 mode <= 1e-5
+relative L2 while the field is active; where the pulse has left the domain the bound is
+3x the drift of the oracle's FP32 twin (same formulas, FP32 storage), the floor any FP32
+storage reaches (precision)."""
+import sys
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN, field_rel_l2, golden
+
+pytestmark = pytest.mark.gpu
+FIELDS = ("Ex", "Ey", "Ez", "Hx", "Hy", "Hz")
+
+
+def fields(obj):
+    return {c: obj.field(c) for c in FIELDS}
+
+
+def ref_fields(g, shape):
+    return {c: g[c].reshape(shape) for c in FIELDS}
+
+
+def rel(a, b):
+    d = float(np.linalg.norm(np.ravel(b)))
+    return float(np.linalg.norm(np.ravel(a) - np.ravel(b))) / (d if d else 1.0)
+
+
+def golden_solver(pkg, case, precision):
+    g = golden(case)
+    s = pkg.Setup.from_file(GOLDEN / "cases" / (case + ".params"))
+    sol = pkg.Solver(s, precision=precision)
+    seed = g["meta"].get("noise_seed")
+    if seed is not None:
+        sys.path.insert(0, str(GOLDEN))
+        from make_golden import initial_noise
+        for c, v in initial_noise(case, int(np.prod(sol.shape))).items():
+            sol.set_field(c, v.reshape(sol.shape))
+    return g, s, sol
+
+
+@pytest.mark.parametrize("precision,tol", [(1, 1e-12), (0, 1e-5)])
+def test_sphere_case_matches_reference(pkg, precision, tol):
+    g, s, sol = golden_solver(pkg, "step_g0_sphere", precision)
+    sol.run(g["meta"]["steps"])
+    ref = ref_fields(g, sol.shape)
+    mine = fields(sol)
+    assert field_rel_l2(mine, ref, "E") <= tol
+    assert field_rel_l2(mine, ref, "H") <= tol
+    series = sol.probe_series()
+    assert series.shape == (g["meta"]["steps"], 4)
+    assert rel(series, g["probe_series"].reshape(series.shape)) <= tol
+
+
+@pytest.mark.parametrize("precision,tol", [(1, 1e-12), (0, 1e-5)])
+def test_gain_case_matches_reference(pkg, precision, tol):
+    g, s, sol = golden_solver(pkg, "step_g1_gain", precision)
+    sol.run(g["meta"]["steps"])
+    ref = ref_fields(g, sol.shape)
+    mine = fields(sol)
+    assert field_rel_l2(mine, ref, "E") <= tol
+    assert field_rel_l2(mine, ref, "H") <= tol
+    gain = g["tls_region_map"].reshape(sol.shape) >= 0
+    for c in ("Pz", "Pz_prev"):
+        assert rel(sol.tls_state(c)[gain], g[c].reshape(sol.shape)[gain]) <= max(tol, 1e-5 if precision == 0 else tol), c
+    for c in ("Nu", "Ng"):
+        assert rel(sol.tls_state(c)[gain], g[c].reshape(sol.shape)[gain]) <= (1e-12 if precision == 1 else 1e-6), c
+    series = sol.probe_series()
+    assert rel(series, g["probe_series"].reshape(series.shape)) <= tol
+
+
+def test_c0_fp32_active_field_within_1e5(pkg, oracle):
+    s = pkg.Setup.from_file(pkg.config_path("c0_dipole_sphere.params"))
+    o = oracle.OracleSolve(s, 0)
+    o.run(600)
+    sol = pkg.Solver(s, precision=0)
+    sol.run(600)
+    ref = {c: o.field(c) for c in FIELDS}
+    mine = fields(sol)
+    assert field_rel_l2(mine, ref, "E") <= 1e-5
+    assert field_rel_l2(mine, ref, "H") <= 1e-5
+
+
+def test_c0_full_run_probe_dft_and_fp32_floor(pkg, oracle):
+    s = pkg.Setup.from_file(pkg.config_path("c0_dipole_sphere.params"))
+    steps = 2000
+    o64 = oracle.OracleSolve(s, 0)
+    p64 = o64.run(steps)[:, 0]
+    o32 = oracle.OracleSolve(s, 1)
+    p32 = o32.run(steps)[:, 0]
+    sol = pkg.Solver(s, precision=0)
+    sol.run(steps)
+    pg = sol.probe_series()[:, 0]
+    ref = {c: o64.field(c) for c in FIELDS}
+    twin = {c: o32.field(c) for c in FIELDS}
+    mine = fields(sol)
+    for kind in "EH":
+        floor = field_rel_l2(twin, ref, kind)
+        assert field_rel_l2(mine, ref, kind) <= max(1e-5, 3.0 * floor), kind
+    assert rel(pg, p64) <= max(1e-5, 3.0 * rel(p32, p64))
+    freqs = s.array("dft_freqs")
+    d_ref = oracle.dft(p64, s.dt, freqs)
+    d_gpu = sol.dft(0)
+    assert rel(d_gpu, d_ref) <= 1e-5
+
+
+def test_c0_fp64_matches_oracle(pkg, oracle):
+    s = pkg.Setup.from_file(pkg.config_path("c0_dipole_sphere.params"))
+    o = oracle.OracleSolve(s, 0)
+    p = o.run(400)[:, 0]
+    sol = pkg.Solver(s, precision=1)
+    sol.run(400)
+    ref = {c: o.field(c) for c in FIELDS}
+    mine = fields(sol)
+    assert field_rel_l2(mine, ref, "E") <= 1e-12
+    assert field_rel_l2(mine, ref, "H") <= 1e-12
+    assert rel(sol.probe_series()[:, 0], p) <= 1e-12
+    assert rel(sol.dft(0), oracle.dft(p, s.dt, s.array("dft_freqs"))) <= 1e-12
+
+
+@pytest.mark.parametrize("pump", ["0", "1e9"])
+def test_c1_gain_slab_vs_oracle(pkg, oracle, pump):
+    s = pkg.Setup.from_file(pkg.config_path("c1_gain_slab.params"), overrides={"PUMP_RATE": pump})
+    rng = np.random.default_rng(1)
+    o = oracle.OracleSolve(s, 0)
+    init = {c: rng.normal(0.0, 1e-6, o.E[0].size) for c in ("Ex", "Ey", "Ez")}
+    for c, v in init.items():
+        o.E["xyz".index(c[1])][:] = v
+    steps = 120
+    o.run(steps)
+    for precision, tol in ((1, 1e-12), (0, 1e-5)):
+        sol = pkg.Solver(s, precision=precision)
+        for c, v in init.items():
+            sol.set_field(c, v.reshape(sol.shape))
+        sol.run(steps)
+        ref = {c: o.field(c) for c in FIELDS}
+        mine = fields(sol)
+        assert field_rel_l2(mine, ref, "E") <= tol, precision
+        assert field_rel_l2(mine, ref, "H") <= tol, precision
+        gain = s.array("tls_region_map").reshape(sol.shape) >= 0
+        assert rel(sol.tls_state("Pz")[gain], o.Pz.reshape(sol.shape)[gain]) <= max(tol, 1e-5)
+        assert rel(sol.tls_state("Nu")[gain], o.Nu.reshape(sol.shape)[gain]) <= (1e-12 if precision else 1e-5)
+        sol.close()
+
+
+def test_split_runs_equal_one_run(pkg):
+    s = pkg.Setup.from_file(GOLDEN / "cases" / "step_g1_gain.params")
+    a = pkg.Solver(s, precision=0)
+    a.run(37)
+    b = pkg.Solver(s, precision=0)
+    b.run(17)
+    b.run(20)
+    assert a.steps_done == b.steps_done == 37
+    for c in FIELDS:
+        assert np.array_equal(a.field(c), b.field(c)), c
+    for c in ("Pz", "Pz_prev", "Nu", "Ng"):
+        assert np.array_equal(a.tls_state(c), b.tls_state(c)), c
+    assert np.array_equal(a.probe_series(), b.probe_series())
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_field_and_state_round_trip(pkg, precision):
+    s = pkg.Setup.from_file(GOLDEN / "cases" / "step_g1_gain.params")
+    sol = pkg.Solver(s, precision=precision)
+    rng = np.random.default_rng(5)
+    for c in FIELDS:
+        v = rng.normal(size=sol.shape)
+        sol.set_field(c, v)
+        got = sol.field(c)
+        want = v if precision == 1 else v.astype(np.float32).astype(np.float64)
+        assert np.array_equal(got, want), c
+    gain = s.array("tls_region_map").reshape(sol.shape) >= 0
+    v = rng.normal(size=sol.shape)
+    sol.set_tls_state("Nu", v)
+    got = sol.tls_state("Nu")
+    want = v if precision == 1 else v.astype(np.float32).astype(np.float64)
+    assert np.array_equal(got[gain], want[gain]) and np.all(got[~gain] == 0)
+
+
+def test_monitor_stops_on_nan(pkg):
+    s = pkg.Setup.from_file(pkg.config_path("c0_dipole_sphere.params"))
+    sol = pkg.Solver(s, precision=0)
+    ez = np.zeros(sol.shape)
+    ez[40, 40, 40] = np.nan
+    sol.set_field("Ez", ez)
+    with pytest.raises(pkg.FdtdError) as e:
+        sol.run(50)
+    assert e.value.code == pkg.FDTD_ERR_UNSTABLE
+    d = sol.diagnostics()
+    assert d["stable"] == 0 and d["step"] == 0 and (d["nan_flags"] & 1)
+    assert sol.steps_done == 1
+    with pytest.raises(pkg.FdtdError):
+        sol.run(5)  # the handle stays stopped, like the reference's early return
+
+
+def test_monitor_counts_threshold_warnings(pkg):
+    s = pkg.Setup.from_file(pkg.config_path("c0_dipole_sphere.params"),
+                            overrides={"STABILITY_MAX_E": "1e-300", "STABILITY_MONITOR_INTERVAL": "10"})
+    sol = pkg.Solver(s, precision=0)
+    with pytest.raises(pkg.FdtdError) as e:
+        sol.run(300)
+    assert e.value.code == pkg.FDTD_ERR_UNSTABLE
+    d = sol.diagnostics()
+    # > 10 warnings: the 11th monitor step (n = 100) is fatal in StabilityMonitor::check_stability
+    assert d["instability_count"] == 11 and d["step"] == 100 and sol.steps_done == 101
+
+
+def test_diagnostics_match_oracle_integrals(pkg, oracle):
+    s = pkg.Setup.from_file(GOLDEN / "cases" / "step_g1_gain.params",
+                            overrides={"STABILITY_MONITOR_INTERVAL": "10"})
+    o = oracle.OracleSolve(s, 0)
+    o.run(31)  # last monitor step of a 40-step run is n = 30
+    sol = pkg.Solver(s, precision=1)
+    sol.run(40)
+    d = sol.diagnostics()
+    assert d["step"] == 30 and d["stable"] == 1
+    shape = sol.shape
+    dV = (s.array("dx")[:, None, None] * s.array("dy")[None, :, None] * s.array("dz")[None, None, :]).ravel()
+    gain = s.array("tls_region_map") >= 0
+    assert abs(d["integrated_Nu"] - np.sum(o.Nu[gain] * dV[gain])) <= 1e-10 * abs(np.sum(o.Nu[gain] * dV[gain]))
+    assert abs(d["integrated_Ng"] - np.sum(o.Ng[gain] * dV[gain])) <= 1e-10 * abs(np.sum(o.Ng[gain] * dV[gain]))
+    pe = np.sum(-0.5 * o.Pz[gain] * o.E[2][gain] * dV[gain])
+    assert abs(d["polarization_energy"] - pe) <= 1e-9 * abs(pe)
+    maxE = max(np.abs(o.E[q]).max() for q in range(3))
+    assert abs(d["max_E"] - maxE) <= 1e-12 * maxE
+    N0 = np.where(gain, 1e24, 0.0)
+    cons = abs(np.sum((o.Nu + o.Ng)[gain]) - np.sum(N0[gain])) / np.sum(N0[gain])
+    assert abs(d["conservation_err"] - cons) <= 1e-9 + 1e-6 * cons
+    assert sol.kernel_launches > 0 and sol.device_bytes > 0
+    del shape
