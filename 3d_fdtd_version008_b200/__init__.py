@@ -45,7 +45,7 @@ EXPORTED_SYMBOLS = (
     "fdtd_setup_destroy", "fdtd_create", "fdtd_set_field", "fdtd_get_field",
     "fdtd_set_tls_state", "fdtd_get_tls_state", "fdtd_run", "fdtd_steps_done",
     "fdtd_get_probe_series", "fdtd_get_dft", "fdtd_get_diagnostics", "fdtd_device_bytes",
-    "fdtd_kernel_launches", "fdtd_set_timing", "fdtd_get_timing", "fdtd_synchronize", "fdtd_last_error",
+    "fdtd_kernel_launches", "fdtd_set_timing", "fdtd_get_timing", "fdtd_set_kernel_path", "fdtd_synchronize", "fdtd_last_error",
     "fdtd_destroy",
 )
 
@@ -146,6 +146,7 @@ def load_library() -> C.CDLL:
         "fdtd_kernel_launches": (C.c_int, [vp, C.POINTER(C.c_uint64)]),
         "fdtd_set_timing": (C.c_int, [vp, C.c_int]),
         "fdtd_get_timing": (C.c_int, [vp, C.POINTER(TimingV1)]),
+        "fdtd_set_kernel_path": (C.c_int, [vp, C.c_int]),
         "fdtd_synchronize": (C.c_int, [vp]),
         "fdtd_last_error": (C.c_char_p, [vp]),
         "fdtd_destroy": (None, [vp]),
@@ -224,7 +225,7 @@ class Solver:
     """One resident solve on one GPU (fdtd_create ... fdtd_destroy)."""
 
     def __init__(self, setup: Setup, device: int = 0, precision: Optional[int] = None,
-                 view: Optional[SetupV1] = None):
+                 view: Optional[SetupV1] = None, kernel_path: Optional[int] = None):
         lib = load_library()
         v = view if view is not None else setup.view
         if precision is not None:
@@ -238,6 +239,8 @@ class Solver:
             raise FdtdError(rc, lib.fdtd_last_error(None).decode())
         self._h = h
         self.shape = (int(v.NxT), int(v.NyT), int(v.NzT))
+        if kernel_path is not None:
+            self.set_kernel_path(kernel_path)
         self.n_probes = int(v.n_probes)
         self.n_freqs = int(v.n_dft_freqs)
 
@@ -315,6 +318,10 @@ class Solver:
         t = TimingV1()
         self._check(load_library().fdtd_get_timing(self._h, C.byref(t)), "fdtd_get_timing")
         return {"steps": t.steps, "run_ms": t.run_ms, "h_ms": t.h_ms, "e_ms": t.e_ms, "aux_ms": t.aux_ms}
+
+    def set_kernel_path(self, path: int) -> None:
+        """0 = fused H+E step, 1 = separate H and E sweeps (default); before the first step."""
+        self._check(load_library().fdtd_set_kernel_path(self._h, int(path)), "fdtd_set_kernel_path")
 
     def synchronize(self) -> None:
         self._check(load_library().fdtd_synchronize(self._h), "fdtd_synchronize")

@@ -10,11 +10,15 @@
 #include "../../include/fdtd_b200.h"
 #include "host/waveform.hpp"
 #include "kernels.cuh"
+#include "fused.cuh"
 
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
 #include <numbers>
@@ -303,6 +307,7 @@ public:
     virtual void diagnostics(fdtd_diagnostics_v1* d) = 0;
     virtual void sync() = 0;
     virtual void set_timing(int mode) = 0;
+    virtual void set_path(int path) = 0;
     virtual void timing(fdtd_timing_v1* t) = 0;
     uint64_t steps = 0, launches = 0, dev_bytes = 0;
     int device = 0;
@@ -323,6 +328,11 @@ public:
     void diagnostics(fdtd_diagnostics_v1* d) override;
     void sync() override { ck(cudaStreamSynchronize(st_), "cudaStreamSynchronize"); }
     void set_timing(int mode) override;
+    void set_path(int path) override {
+        if (path != 0 && path != 1) throw Failure(FDTD_ERR_INVALID, "kernel path must be 0 (fused) or 1 (two-sweep)");
+        if (steps != 0) throw Failure(FDTD_ERR_INVALID, "the kernel path can only change before the first step");
+        path_ = path;
+    }
     void timing(fdtd_timing_v1* t) override { *t = tm_; }
 
 private:
@@ -368,6 +378,21 @@ private:
     double* d_stage_ = nullptr;
     bool has_gain_ = false;
     // event timing: ev_[0..3] bracket H, E and the auxiliary kernels of one step
+    // kernel path 0: k_step_fused (fields and psi_H double-buffered, cur_ = buffer holding
+    // the latest state); path 1 (default, measured faster on B200): k_update_H +
+    // k_update_E in place on buffer 0.
+    int path_ = 1, cur_ = 0;
+    T* fld_[2][6] = {};
+    T* psiH_[2][6] = {};
+    FusedMaps maps_[2];
+    int kchunkF_ = 1;
+    dim3 gridF_;
+    size_t smemF_ = 0;
+    int threadsF_ = 0, shapeF_ = 0;
+    void (*launchF_)(dim3, int, size_t, cudaStream_t, const FusedMaps&, const FusedArgs<T>&, int, const ESrc&) = nullptr;
+    void point_args_at(int buf);
+    void build_fused();
+    template <typename Shape> void setup_fused();
     int timing_ = FDTD_TIMING_OFF;
     cudaEvent_t ev_[4] = {nullptr, nullptr, nullptr, nullptr};
     fdtd_timing_v1 tm_{};
@@ -390,9 +415,9 @@ Solver<T>::Solver(const fdtd_setup_v1& s, int dev) {
     StepArgs<T>& a = a_;
     a.NxT = NxT_; a.NyT = NyT_; a.NzT = NzT_; a.NxP = NxP_; a.np = np_;
     a.plane = (long long)plane_;
-    T* f[6];
-    for (int c = 0; c < 6; ++c) f[c] = alloc<T>(nflat_);
-    a.Ex = f[0]; a.Ey = f[1]; a.Ez = f[2]; a.Hx = f[3]; a.Hy = f[4]; a.Hz = f[5];
+    for (int b = 0; b < 2; ++b)
+        for (int c = 0; c < 6; ++c) fld_[b][c] = alloc<T>(nflat_);
+    point_args_at(0);
 
     // bH must be uniform and aE = aH = 1 (sigma = 0, mu_r = 1).
     double bH = s.bH_uniform;
@@ -439,7 +464,12 @@ Solver<T>::Solver(const fdtd_setup_v1& s, int dev) {
         const size_t xs = size_t(NzT_) * NyT_ * np2, ys = size_t(NzT_) * np2 * NxP_, zs = np2 * NyT_ * NxP_;
         // 0 *_y, 1 *_z, 2 *_z, 3 *_x, 4 *_x, 5 *_y
         const size_t sz[6] = {ys, zs, zs, xs, xs, ys};
-        for (int q = 0; q < 6; ++q) { a.psiH[q] = alloc<T>(sz[q]); a.psiE[q] = alloc<T>(sz[q]); }
+        for (int q = 0; q < 6; ++q) {
+            psiH_[0][q] = alloc<T>(sz[q]);
+            psiH_[1][q] = alloc<T>(sz[q]);
+            a.psiE[q] = alloc<T>(sz[q]);
+            a.psiH[q] = psiH_[0][q];
+        }
     }
 
     // gain block
@@ -552,7 +582,84 @@ Solver<T>::Solver(const fdtd_setup_v1& s, int dev) {
     kchunkE_ = chunk(NyT_, NzT_);
     gridH_ = dim3(gx, (NyT_ - 1 + kBlockY - 1) / kBlockY, (NzT_ - 1 + kchunkH_ - 1) / kchunkH_);
     gridE_ = dim3(gx, (NyT_ + kBlockY - 1) / kBlockY, (NzT_ + kchunkE_ - 1) / kchunkE_);
+    build_fused();
+    if (const char* p = std::getenv("FDTD_B200_KERNEL_PATH")) set_path(std::atoi(p));
     ck(cudaStreamSynchronize(st_), "setup upload");
+}
+
+template <typename T>
+void Solver<T>::point_args_at(int buf) {
+    a_.Ex = fld_[buf][0]; a_.Ey = fld_[buf][1]; a_.Ez = fld_[buf][2];
+    a_.Hx = fld_[buf][3]; a_.Hy = fld_[buf][4]; a_.Hz = fld_[buf][5];
+}
+
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    if (!fn) {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        ck(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q), "cudaGetDriverEntryPoint");
+        if (q != cudaDriverEntryPointSuccess || !p) throw Failure(FDTD_ERR_CUDA, "cuTensorMapEncodeTiled unavailable");
+        fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    }
+    return fn;
+}
+
+// Tensor maps over the padded device layout (x fastest): E/H boxes of the fused tile plus
+// its halo, bE boxes of the tile.  Base addresses come from cudaMalloc (256-byte aligned);
+// row and plane strides are multiples of 128 bytes.
+template <typename T>
+void Solver<T>::build_fused() {
+    const char* env = std::getenv("FDTD_B200_FUSED_SHAPE");
+    shapeF_ = env ? std::atoi(env) : 0;
+    if (shapeF_ == 1) setup_fused<typename ShapeSet<T>::S1>();
+    else if (shapeF_ == 2) setup_fused<typename ShapeSet<T>::S2>();
+    else { shapeF_ = 0; setup_fused<typename ShapeSet<T>::S0>(); }
+}
+
+template <typename T>
+template <typename Shape>
+void Solver<T>::setup_fused() {
+    using S = FusedSmem<T, Shape>;
+    auto enc = tensor_map_encoder();
+    auto make = [&](const T* base, int bx, int by) {
+        CUtensorMap m;
+        cuuint64_t dims[3] = {cuuint64_t(NxP_), cuuint64_t(NyT_), cuuint64_t(NzT_)};
+        cuuint64_t strides[2] = {cuuint64_t(NxP_) * sizeof(T), cuuint64_t(plane_) * sizeof(T)};
+        cuuint32_t box[3] = {cuuint32_t(bx), cuuint32_t(by), 1u};
+        cuuint32_t es[3] = {1u, 1u, 1u};
+        CUresult r = enc(&m, sizeof(T) == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3,
+                         const_cast<T*>(base), dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                         CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                         CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+        if (r != CUDA_SUCCESS) throw Failure(FDTD_ERR_CUDA, "cuTensorMapEncodeTiled failed (" + std::to_string(int(r)) + ")");
+        return m;
+    };
+    const T* bE[3] = {a_.bEx, a_.bEy, a_.bEz};
+    for (int b = 0; b < 2; ++b) {
+        for (int c = 0; c < 3; ++c) {
+            maps_[b].E[c] = make(fld_[b][c], S::PX, S::PY);
+            maps_[b].H[c] = make(fld_[b][3 + c], S::PX, S::PY);
+            maps_[b].B[c] = make(bE[c], S::TX, S::TY);
+        }
+    }
+    smemF_ = sizeof(S);
+    threadsF_ = Shape::THREADS;
+    launchF_ = &launch_fused<T, Shape>;
+    ck(cudaFuncSetAttribute(k_step_fused<T, Shape>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smemF_)),
+       "cudaFuncSetAttribute");
+    int per_sm = 1, sms = 148;
+    ck(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_step_fused<T, Shape>, threadsF_, smemF_),
+       "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
+    ck(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device), "cudaDeviceGetAttribute");
+    if (per_sm < 1) throw Failure(FDTD_ERR_CUDA, "fused step kernel does not fit on an SM");
+    const int gx = (NxT_ + S::TX - 1) / S::TX, gy = (NyT_ + S::TY - 1) / S::TY;
+    // z-chunks: about 8 waves of resident blocks, chunks of at least 32 planes
+    const int resident = sms * per_sm;
+    const int want = std::max(1, (resident * 8 + gx * gy - 1) / (gx * gy));
+    const int zc = std::max(1, std::min(want, NzT_ / 32));
+    kchunkF_ = (NzT_ + zc - 1) / zc;
+    gridF_ = dim3(gx, gy, (NzT_ + kchunkF_ - 1) / kchunkF_);
 }
 
 template <typename T>
@@ -611,15 +718,17 @@ void Solver<T>::from_device(const T* src, double* h) {
 template <typename T>
 void Solver<T>::set_field(int comp, const double* h) {
     if (comp < 0 || comp > 5) throw Failure(FDTD_ERR_INVALID, "component must be 0..5");
-    T* f[6] = {a_.Ex, a_.Ey, a_.Ez, a_.Hx, a_.Hy, a_.Hz};
-    to_device(h, f[comp]);
+    // Both buffers: cells the reference never updates must hold the same value in each.
+    to_device(h, fld_[cur_][comp]);
+    ck(cudaMemcpyAsync(fld_[1 - cur_][comp], fld_[cur_][comp], nflat_ * sizeof(T), cudaMemcpyDeviceToDevice, st_),
+       "field copy");
+    ck(cudaStreamSynchronize(st_), "set_field");
 }
 
 template <typename T>
 void Solver<T>::get_field(int comp, double* h) {
     if (comp < 0 || comp > 5) throw Failure(FDTD_ERR_INVALID, "component must be 0..5");
-    const T* f[6] = {a_.Ex, a_.Ey, a_.Ez, a_.Hx, a_.Hy, a_.Hz};
-    from_device(f[comp], h);
+    from_device(fld_[cur_][comp], h);
 }
 
 template <typename T>
@@ -689,17 +798,33 @@ void Solver<T>::run(uint64_t n) {
     const bool per_kernel = timing_ == FDTD_TIMING_KERNELS;
     if (timing_ == FDTD_TIMING_RUN) ck(cudaEventRecord(ev_[0], st_), "cudaEventRecord");
     for (uint64_t s = n0; s < last; ++s) {
-        if (per_kernel) ck(cudaEventRecord(ev_[0], st_), "cudaEventRecord");
-        k_update_H<T><<<gridH_, blk, 0, st_>>>(a_, kchunkH_);
-        if (per_kernel) ck(cudaEventRecord(ev_[1], st_), "cudaEventRecord");
         src.parity = int(s & 1);
         for (int q = 0; q < src.n; ++q) {
             const fdtd_dipole_v1& d = dip_[q];
             src.J[q] = fdtd::current_density(d.waveform, s, dt_, d.I0, d.f0, d.tau, d.t0, d.t_shift, d.cell_area);
         }
-        k_update_E<T><<<gridE_, blk, 0, st_>>>(a_, kchunkE_, src);
+        if (per_kernel) ck(cudaEventRecord(ev_[0], st_), "cudaEventRecord");
+        if (path_ == 0) {
+            FusedArgs<T> fa;
+            fa.a = a_;
+            for (int q = 0; q < 6; ++q) {
+                fa.psiHs[q] = psiH_[cur_][q];
+                fa.psiHd[q] = psiH_[1 - cur_][q];
+            }
+            for (int c = 0; c < 3; ++c) { fa.dE[c] = fld_[1 - cur_][c]; fa.dH[c] = fld_[1 - cur_][3 + c]; }
+            fa.status_w = d_status_;
+            if (per_kernel) ck(cudaEventRecord(ev_[1], st_), "cudaEventRecord");
+            launchF_(gridF_, threadsF_, smemF_, st_, maps_[cur_], fa, kchunkF_, src);
+            cur_ = 1 - cur_;
+            point_args_at(cur_);
+            launches += 1;
+        } else {
+            k_update_H<T><<<gridH_, blk, 0, st_>>>(a_, kchunkH_);
+            if (per_kernel) ck(cudaEventRecord(ev_[1], st_), "cudaEventRecord");
+            k_update_E<T><<<gridE_, blk, 0, st_>>>(a_, kchunkE_, src);
+            launches += 2;
+        }
         if (per_kernel) ck(cudaEventRecord(ev_[2], st_), "cudaEventRecord");
-        launches += 2;
         if (nprobes_) {
             const long long sample = (s % save_every_ == 0) ? (long long)(s / save_every_) : -1;
             k_probe_dft<T><<<(pthreads + 127) / 128, 128, 0, st_>>>(a_, d_probes_, int(nprobes_), d_freqs_, int(nf_),
@@ -734,6 +859,8 @@ void Solver<T>::run(uint64_t n) {
         tm_.run_ms += ms;
         tm_.steps += n;
     }
+    if (status & kStatusTimeout)
+        throw Failure(FDTD_ERR_TIMEOUT, "a bounded device wait expired (TMA copy did not arrive); state is invalid");
     if (status) {
         MonitorState ms{};
         ck(cudaMemcpy(&ms, d_ms_, sizeof(ms), cudaMemcpyDeviceToHost), "monitor state");
@@ -810,7 +937,8 @@ int fdtd_create(const fdtd_setup_v1* s, int device, fdtd_handle** out) {
     if (!s || !out) { g_err = "null argument"; return FDTD_ERR_INVALID; }
     *out = nullptr;
     if (s->struct_size != sizeof(fdtd_setup_v1)) { g_err = "fdtd_setup_v1.struct_size mismatch"; return FDTD_ERR_INVALID; }
-    if (s->NxT < 3 || s->NyT < 3 || s->NzT < 3 || s->NxT > (1u << 30) || s->NyT > (1u << 30) || s->NzT > (1u << 30)) {
+    // NyT is a grid dimension (z) of the layout-transpose kernels: at most 65535.
+    if (s->NxT < 3 || s->NyT < 3 || s->NzT < 3 || s->NxT > (1u << 30) || s->NyT > 65535 || s->NzT > (1u << 30)) {
         g_err = "grid dimensions out of range"; return FDTD_ERR_INVALID;
     }
     if (2 * uint64_t(s->npml) >= s->NxT || 2 * uint64_t(s->npml) >= s->NyT || 2 * uint64_t(s->npml) >= s->NzT) {
@@ -854,6 +982,7 @@ int fdtd_device_bytes(const fdtd_handle* h, uint64_t* b) { if (!h || !b) return 
 int fdtd_kernel_launches(const fdtd_handle* h, uint64_t* n) { if (!h || !n) return FDTD_ERR_INVALID; *n = h->s->launches; return FDTD_OK; }
 int fdtd_set_timing(fdtd_handle* h, int mode) { if (!h) return FDTD_ERR_INVALID; return guarded(h, [&] { h->s->set_timing(mode); }); }
 int fdtd_get_timing(fdtd_handle* h, fdtd_timing_v1* t) { if (!h || !t) return FDTD_ERR_INVALID; return guarded(h, [&] { h->s->timing(t); }); }
+int fdtd_set_kernel_path(fdtd_handle* h, int path) { if (!h) return FDTD_ERR_INVALID; return guarded(h, [&] { h->s->set_path(path); }); }
 int fdtd_synchronize(fdtd_handle* h) { if (!h) return FDTD_ERR_INVALID; return guarded(h, [&] { h->s->sync(); }); }
 const char* fdtd_last_error(const fdtd_handle* h) { return h ? h->err.c_str() : g_err.c_str(); }
 void fdtd_destroy(fdtd_handle* h) { delete h; }

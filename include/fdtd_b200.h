@@ -212,6 +212,9 @@ int fdtd_kernel_launches(const fdtd_handle *h, uint64_t *n);
 /* Select FDTD_TIMING_OFF / _RUN / _KERNELS; any call resets the totals. */
 int fdtd_set_timing(fdtd_handle *h, int mode);
 int fdtd_get_timing(fdtd_handle *h, fdtd_timing_v1 *out);
+/* Kernel path, before the first step only: 0 = one fused H+E launch per step with
+ * TMA-staged planes, 1 = separate H and E sweeps (default).  Results agree to rounding. */
+int fdtd_set_kernel_path(fdtd_handle *h, int path);
 /* Block until all device work of the handle is complete. */
 int fdtd_synchronize(fdtd_handle *h);
 /* Message of the last failing call on h (or of the last global failure when h is NULL). */

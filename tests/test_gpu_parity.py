@@ -231,3 +231,76 @@ def test_diagnostics_match_oracle_integrals(pkg, oracle):
     assert abs(d["conservation_err"] - cons) <= 1e-9 + 1e-6 * cons
     assert sol.kernel_launches > 0 and sol.device_bytes > 0
     del shape
+
+
+@pytest.mark.parametrize("precision,tol", [(1, 1e-13), (0, 2e-6)])
+def test_fused_and_two_sweep_paths_agree(pkg, precision, tol):
+    """The fused H+E launch and the separate sweeps compute the same update (rounding aside)."""
+    s = pkg.Setup.from_file(GOLDEN / "cases" / "step_g1_gain.params", overrides={"PUMP_RATE": "1e11"})
+    out = []
+    for path in (0, 1):
+        sol = pkg.Solver(s, precision=precision, kernel_path=path)
+        rng = np.random.default_rng(11)
+        for c in ("Ex", "Ey", "Ez"):
+            sol.set_field(c, rng.normal(0, 1e-3, sol.shape))
+        sol.run(33)
+        out.append((fields(sol), {c: sol.tls_state(c) for c in ("Pz", "Nu")}, sol.probe_series()))
+        sol.close()
+    (f0, g0, p0), (f1, g1, p1) = out
+    assert field_rel_l2(f0, f1, "E") <= tol and field_rel_l2(f0, f1, "H") <= tol
+    assert rel(g0["Pz"], g1["Pz"]) <= max(tol, 1e-5) and rel(g0["Nu"], g1["Nu"]) <= max(tol, 1e-6)
+    assert rel(p0, p1) <= tol
+
+
+@pytest.mark.parametrize("precision,tol", [(1, 1e-12), (0, 1e-5)])
+def test_two_sweep_path_matches_reference(pkg, precision, tol):
+    g, s, _ = golden_solver(pkg, "step_g0_sphere", precision)
+    sol = pkg.Solver(s, precision=precision, kernel_path=1)
+    sol.run(g["meta"]["steps"])
+    ref = ref_fields(g, sol.shape)
+    mine = fields(sol)
+    assert field_rel_l2(mine, ref, "E") <= tol and field_rel_l2(mine, ref, "H") <= tol
+
+
+@pytest.mark.parametrize("precision,tol", [(1, 1e-12), (0, 1e-5)])
+def test_fused_path_matches_reference(pkg, precision, tol):
+    for case in ("step_g0_sphere", "step_g1_gain"):
+        g = golden(case)
+        s = pkg.Setup.from_file(GOLDEN / "cases" / (case + ".params"))
+        sol = pkg.Solver(s, precision=precision, kernel_path=0)
+        if g["meta"].get("noise_seed") is not None:
+            sys.path.insert(0, str(GOLDEN))
+            from make_golden import initial_noise
+            for c, v in initial_noise(case, int(np.prod(sol.shape))).items():
+                sol.set_field(c, v.reshape(sol.shape))
+        sol.run(g["meta"]["steps"])
+        ref = ref_fields(g, sol.shape)
+        mine = fields(sol)
+        assert field_rel_l2(mine, ref, "E") <= tol, case
+        assert field_rel_l2(mine, ref, "H") <= tol, case
+
+
+def test_kernel_path_fixed_after_first_step(pkg):
+    s = pkg.Setup.from_file(GOLDEN / "cases" / "step_g0_sphere.params")
+    sol = pkg.Solver(s)
+    sol.run(1)
+    with pytest.raises(pkg.FdtdError):
+        sol.set_kernel_path(1)
+
+
+def test_fused_path_tile_edges_on_odd_grid(pkg, oracle):
+    """Fused path on a grid that is not a multiple of its tile in any axis, CPML on every face."""
+    text = (GOLDEN / "cases" / "step_g0_sphere.params").read_text()
+    text = text.replace("NX = 10", "NX = 71").replace("NY = 9", "NY = 37").replace("NZ = 8", "NZ = 45")
+    text = text.replace("DOMAIN_X_MAX = 250e-9", "DOMAIN_X_MAX = 1775e-9").replace("DOMAIN_Y_MAX = 225e-9", "DOMAIN_Y_MAX = 925e-9")
+    text = text.replace("DOMAIN_Z_MAX = 200e-9", "DOMAIN_Z_MAX = 1125e-9")
+    s = pkg.Setup.from_text(text)
+    o = oracle.OracleSolve(s, 0)
+    o.run(80)
+    for precision, tol in ((1, 1e-12), (0, 1e-5)):
+        sol = pkg.Solver(s, precision=precision, kernel_path=0)
+        sol.run(80)
+        ref = {c: o.field(c) for c in FIELDS}
+        mine = fields(sol)
+        assert field_rel_l2(mine, ref, "E") <= tol, precision
+        assert field_rel_l2(mine, ref, "H") <= tol, precision
