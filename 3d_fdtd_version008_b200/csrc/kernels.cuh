@@ -102,7 +102,111 @@ struct ESrc {
 __device__ __forceinline__ bool in_pml(int n, int N, int np) { return n < np || n >= N - np; }
 __device__ __forceinline__ int slab_index(int n, int N, int np) { return n < np ? n : n - (N - 2 * np); }
 
+// x-slab psi ([k][j][2 np]) of one W-cell vector.  Both arrays are read before any psi
+// store is issued: the compiler may not move a load of one psi array above a store to the
+// other, and a read-after-store chain per cell would cost one memory round trip each.
+template <typename T>
+__device__ __forceinline__ void xpsi_load(const T* p3, const T* p4, const StepArgs<T>& a, int k, int j, int i0,
+                                          T (&x3)[Vec<T>::W], T (&x4)[Vec<T>::W]) {
+    const size_t row = (size_t(k) * a.NyT + j) * (2 * a.np);
+#pragma unroll
+    for (int e = 0; e < Vec<T>::W; ++e) {
+        const int i = i0 + e;
+        const bool in = i < a.NxT && in_pml(i, a.NxT, a.np);
+        const size_t q = row + (in ? slab_index(i, a.NxT, a.np) : 0);
+        x3[e] = in ? p3[q] : T(0);
+        x4[e] = in ? p4[q] : T(0);
+    }
+}
+
+// Writes back the x-slab psi of the cells ilo <= i < ihi of the vector.
+template <typename T>
+__device__ __forceinline__ void xpsi_store(T* p3, T* p4, const StepArgs<T>& a, int k, int j, int i0, int ilo, int ihi,
+                                           const T (&x3)[Vec<T>::W], const T (&x4)[Vec<T>::W]) {
+    const size_t row = (size_t(k) * a.NyT + j) * (2 * a.np);
+#pragma unroll
+    for (int e = 0; e < Vec<T>::W; ++e) {
+        const int i = i0 + e;
+        if (i >= ilo && i < ihi && in_pml(i, a.NxT, a.np)) {
+            const size_t q = row + slab_index(i, a.NxT, a.np);
+            p3[q] = x3[e];
+            p4[q] = x4[e];
+        }
+    }
+}
+
+// True when a point source sits on one of the W cells (i0.., j, k).
+__device__ __forceinline__ bool src_in_vector(const ESrc& src, int i0, int j, int k, int W) {
+    bool hit = false;
+    for (int s = 0; s < src.n; ++s)
+        hit |= src.sj[s] == j && src.sk[s] == k && src.si[s] >= i0 && src.si[s] < i0 + W;
+    return hit;
+}
+
+// Plain-vector updates: no CPML slab, gain cell or source in the W cells, every cell
+// updated.  Same operations in the same order as the general update with psi, J and dP/dt
+// absent; the general path carries per-cell tests that cost more issue slots than the
+// arithmetic itself, and about 85 % of the cells of a CPML-bounded grid are plain.
+template <typename T>
+__device__ __forceinline__ void h_plain(const StepArgs<T>& a, const size_t c, const T (&ex0)[Vec<T>::W],
+                                        const T (&ex1)[Vec<T>::W], const T (&ey0)[Vec<T>::W],
+                                        const T (&ey1)[Vec<T>::W], const T (&ez)[Vec<T>::W],
+                                        const T (&exj)[Vec<T>::W], const T (&ezj)[Vec<T>::W], const T eyn,
+                                        const T ezn, T (&hx)[Vec<T>::W], T (&hy)[Vec<T>::W], T (&hz)[Vec<T>::W],
+                                        const T (&idx)[Vec<T>::W], const T idy, const T idz) {
+    constexpr int W = Vec<T>::W;
+    const T bH = a.bH;
+#pragma unroll
+    for (int e = 0; e < W; ++e) {
+        const T eyx = (e < W - 1) ? ey0[e + 1] : eyn;
+        const T ezx = (e < W - 1) ? ez[e + 1] : ezn;
+        const T dEz_dy = (ezj[e] - ez[e]) * idy;
+        const T dEy_dz = (ey1[e] - ey0[e]) * idz;
+        const T dEx_dz = (ex1[e] - ex0[e]) * idz;
+        const T dEz_dx = (ezx - ez[e]) * idx[e];
+        const T dEy_dx = (eyx - ey0[e]) * idx[e];
+        const T dEx_dy = (exj[e] - ex0[e]) * idy;
+        hx[e] = hx[e] - bH * (dEz_dy - dEy_dz);
+        hy[e] = hy[e] - bH * (dEx_dz - dEz_dx);
+        hz[e] = hz[e] - bH * (dEy_dx - dEx_dy);
+    }
+    Vec<T>::st(a.Hx + c, hx);
+    Vec<T>::st(a.Hy + c, hy);
+    Vec<T>::st(a.Hz + c, hz);
+}
+
+template <typename T>
+__device__ __forceinline__ void e_plain(const StepArgs<T>& a, const size_t c, T (&ex)[Vec<T>::W], T (&ey)[Vec<T>::W],
+                                        T (&ez)[Vec<T>::W], const T (&bx)[Vec<T>::W], const T (&by)[Vec<T>::W],
+                                        const T (&bz)[Vec<T>::W], const T (&hx)[Vec<T>::W],
+                                        const T (&hy)[Vec<T>::W], const T (&hz)[Vec<T>::W],
+                                        const T (&hzj)[Vec<T>::W], const T (&hxj)[Vec<T>::W],
+                                        const T (&hxm)[Vec<T>::W], const T (&hym)[Vec<T>::W], const T hzp,
+                                        const T hyp, const T (&idx)[Vec<T>::W], const T idy, const T idz) {
+    constexpr int W = Vec<T>::W;
+#pragma unroll
+    for (int e = 0; e < W; ++e) {
+        const T hzx = (e > 0) ? hz[e - 1] : hzp;
+        const T hyx = (e > 0) ? hy[e - 1] : hyp;
+        const T dHz_dy = (hz[e] - hzj[e]) * idy;
+        const T dHy_dz = (hy[e] - hym[e]) * idz;
+        const T dHx_dz = (hx[e] - hxm[e]) * idz;
+        const T dHz_dx = (hz[e] - hzx) * idx[e];
+        const T dHy_dx = (hy[e] - hyx) * idx[e];
+        const T dHx_dy = (hx[e] - hxj[e]) * idy;
+        ex[e] = ex[e] + bx[e] * (dHz_dy - dHy_dz);
+        ey[e] = ey[e] + by[e] * (dHx_dz - dHz_dx);
+        ez[e] = ez[e] + bz[e] * (dHy_dx - dHx_dy);
+    }
+    Vec<T>::st(a.Ex + c, ex);
+    Vec<T>::st(a.Ey + c, ey);
+    Vec<T>::st(a.Ez + c, ez);
+}
+
 // ---------------------------------------------------------------------------------
+// Every load of an iteration (the vectors, the x-neighbour across the warp edge, 1/dz,
+// the CPML psi of the vector) is issued before the first use of any of them, so a vector
+// costs one memory round trip per plane whatever slab it lies in.
 template <typename T>
 __global__ void __launch_bounds__(32 * kBlockY)
 k_update_H(const StepArgs<T> a, const int kchunk) {
@@ -128,6 +232,7 @@ k_update_H(const StepArgs<T> a, const int kchunk) {
     T yb = 1, yc = 0, yik = 1;
     if (ypml) { yb = __ldg(a.pbH[1] + j); yc = __ldg(a.pcH[1] + j); yik = __ldg(a.ik[1] + j); }
     const bool xpml = act && (i0 < np || i0 + W > a.NxT - np);
+    const bool plain_row = act && !ypml && !xpml && i0 + W <= a.NxT - 1;
 
     const size_t row = size_t(j) * a.NxP + i0;
     T ex0[W], ey0[W];
@@ -155,13 +260,8 @@ k_update_H(const StepArgs<T> a, const int kchunk) {
 #pragma unroll
             for (int e = 0; e < W; ++e) ex1[e] = ey1[e] = ez[e] = exj[e] = ezj[e] = hx[e] = hy[e] = hz[e] = T(0);
         }
-        T eyn = __shfl_down_sync(kFull, ey0[0], 1);
-        T ezn = __shfl_down_sync(kFull, ez[0], 1);
-        if (lane == 31) {
-            const bool nxt = act && (i0 + W < a.NxT);
-            eyn = nxt ? __ldg(a.Ey + c + W) : T(0);
-            ezn = nxt ? __ldg(a.Ez + c + W) : T(0);
-        }
+        T eye = T(0), eze = T(0);
+        if (lane == 31 && act && i0 + W < a.NxT) { eye = __ldg(a.Ey + c + W); eze = __ldg(a.Ez + c + W); }
         const T idz = __ldg(a.idz + k);
         const bool zpml = in_pml(k, a.NzT, np);
         T zb = 1, zc = 0, zik = 1;
@@ -175,6 +275,18 @@ k_update_H(const StepArgs<T> a, const int kchunk) {
         if (ypml) {
             ys = (size_t(k) * np2 + jy) * a.NxP + i0;
             if (act) { Vec<T>::ld(a.psiH[0] + ys, pxy); Vec<T>::ld(a.psiH[5] + ys, pzy); }
+        }
+        T x3[W], x4[W];  // psi Hy_x, Hz_x
+        if (xpml) xpsi_load(a.psiH[3], a.psiH[4], a, k, j, i0, x3, x4);
+        // x-neighbour at i0+W: the next lane's first cell, the loaded one for lane 31
+        T eyn = __shfl_down_sync(kFull, ey0[0], 1);
+        T ezn = __shfl_down_sync(kFull, ez[0], 1);
+        if (lane == 31) { eyn = eye; ezn = eze; }
+        if (plain_row && !zpml) {
+            h_plain(a, c, ex0, ex1, ey0, ey1, ez, exj, ezj, eyn, ezn, hx, hy, hz, idx, idy, idz);
+#pragma unroll
+            for (int e = 0; e < W; ++e) { ex0[e] = ex1[e]; ey0[e] = ey1[e]; }
+            continue;
         }
 #pragma unroll
         for (int e = 0; e < W; ++e) {
@@ -197,14 +309,11 @@ k_update_H(const StepArgs<T> a, const int kchunk) {
                 pyz[e] = zb * pyz[e] + zc * dEx_dz; dEx_dz = dEx_dz * zik + pyz[e];
             }
             if (xpml && in_pml(i, a.NxT, np)) {
-                const size_t xs = (size_t(k) * a.NyT + j) * np2 + slab_index(i, a.NxT, np);
                 const T b = __ldg(a.pbH[0] + i), cc = __ldg(a.pcH[0] + i), ik = __ldg(a.ik[0] + i);
-                T ps = b * a.psiH[3][xs] + cc * dEz_dx;
-                a.psiH[3][xs] = ps;
-                dEz_dx = dEz_dx * ik + ps;
-                ps = b * a.psiH[4][xs] + cc * dEy_dx;
-                a.psiH[4][xs] = ps;
-                dEy_dx = dEy_dx * ik + ps;
+                x3[e] = b * x3[e] + cc * dEz_dx;
+                dEz_dx = dEz_dx * ik + x3[e];
+                x4[e] = b * x4[e] + cc * dEy_dx;
+                dEy_dx = dEy_dx * ik + x4[e];
             }
             hx[e] = hx[e] - bH * (dEz_dy - dEy_dz);
             hy[e] = hy[e] - bH * (dEx_dz - dEz_dx);
@@ -216,6 +325,7 @@ k_update_H(const StepArgs<T> a, const int kchunk) {
             Vec<T>::st(a.Hz + c, hz);
             if (zpml) { Vec<T>::st(a.psiH[1] + zs, pxz); Vec<T>::st(a.psiH[2] + zs, pyz); }
             if (ypml) { Vec<T>::st(a.psiH[0] + ys, pxy); Vec<T>::st(a.psiH[5] + ys, pzy); }
+            if (xpml) xpsi_store(a.psiH[3], a.psiH[4], a, k, j, i0, 0, a.NxT - 1, x3, x4);
         }
 #pragma unroll
         for (int e = 0; e < W; ++e) { ex0[e] = ex1[e]; ey0[e] = ey1[e]; }
@@ -248,6 +358,7 @@ k_update_E(const StepArgs<T> a, const int kchunk, const ESrc src) {
     if (ypml) { yb = __ldg(a.pbE[1] + j); yc = __ldg(a.pcE[1] + j); yik = __ldg(a.ik[1] + j); }
     const bool xpml = act && (i0 < np || i0 + W > a.NxT - np);
     const bool grow = a.gain && j >= a.gj0 && j < a.gj0 + a.gY && i0 + W > a.gi0 && i0 < a.gi0 + a.gX;
+    const bool plain_row = act && !ypml && !xpml && i0 >= 1 && i0 + W <= a.NxT;
     T* const Pcur = src.parity ? a.P1 : a.P0;
     T* const Pold = src.parity ? a.P0 : a.P1;  // holds P^{n-1}, receives P^{n+1}
 
@@ -281,13 +392,8 @@ k_update_E(const StepArgs<T> a, const int kchunk, const ESrc src) {
             for (int e = 0; e < W; ++e)
                 ex[e] = ey[e] = ez[e] = bx[e] = by[e] = bz[e] = hx[e] = hy[e] = hz[e] = hzj[e] = hxj[e] = T(0);
         }
-        T hzp = __shfl_up_sync(kFull, hz[W - 1], 1);
-        T hyp = __shfl_up_sync(kFull, hy[W - 1], 1);
-        if (lane == 0) {
-            const bool prv = act && i0 > 0;
-            hzp = prv ? __ldg(a.Hz + c - 1) : T(0);
-            hyp = prv ? __ldg(a.Hy + c - 1) : T(0);
-        }
+        T hze = T(0), hye = T(0);
+        if (lane == 0 && act && i0 > 0) { hze = __ldg(a.Hz + c - 1); hye = __ldg(a.Hy + c - 1); }
         const T idz = __ldg(a.idz + k);
         const bool zpml = in_pml(k, a.NzT, np);
         T zb = 1, zc = 0, zik = 1;
@@ -302,7 +408,19 @@ k_update_E(const StepArgs<T> a, const int kchunk, const ESrc src) {
             ys = (size_t(k) * np2 + jy) * a.NxP + i0;
             if (act) { Vec<T>::ld(a.psiE[0] + ys, pxy); Vec<T>::ld(a.psiE[5] + ys, pzy); }
         }
+        T x3[W], x4[W];  // psi Ey_x, Ez_x
+        if (xpml) xpsi_load(a.psiE[3], a.psiE[4], a, k, j, i0, x3, x4);
+        // x-neighbour at i0-1: the previous lane's last cell, the loaded one for lane 0
+        T hzp = __shfl_up_sync(kFull, hz[W - 1], 1);
+        T hyp = __shfl_up_sync(kFull, hy[W - 1], 1);
+        if (lane == 0) { hzp = hze; hyp = hye; }
         const bool gplane = grow && k >= a.gk0 && k < a.gk0 + a.gZ;
+        if (plain_row && !zpml && !gplane && !src_in_vector(src, i0, j, k, W)) {
+            e_plain(a, c, ex, ey, ez, bx, by, bz, hx, hy, hz, hzj, hxj, hxm, hym, hzp, hyp, idx, idy, idz);
+#pragma unroll
+            for (int e = 0; e < W; ++e) { hxm[e] = hx[e]; hym[e] = hy[e]; }
+            continue;
+        }
 #pragma unroll
         for (int e = 0; e < W; ++e) {
             const int i = i0 + e;
@@ -324,14 +442,11 @@ k_update_E(const StepArgs<T> a, const int kchunk, const ESrc src) {
                 pyz[e] = zb * pyz[e] + zc * dHx_dz; dHx_dz = dHx_dz * zik + pyz[e];
             }
             if (xpml && in_pml(i, a.NxT, np)) {
-                const size_t xs = (size_t(k) * a.NyT + j) * np2 + slab_index(i, a.NxT, np);
                 const T b = __ldg(a.pbE[0] + i), cc = __ldg(a.pcE[0] + i), ik = __ldg(a.ik[0] + i);
-                T ps = b * a.psiE[3][xs] + cc * dHz_dx;
-                a.psiE[3][xs] = ps;
-                dHz_dx = dHz_dx * ik + ps;
-                ps = b * a.psiE[4][xs] + cc * dHy_dx;
-                a.psiE[4][xs] = ps;
-                dHy_dx = dHy_dx * ik + ps;
+                x3[e] = b * x3[e] + cc * dHz_dx;
+                dHz_dx = dHz_dx * ik + x3[e];
+                x4[e] = b * x4[e] + cc * dHy_dx;
+                dHy_dx = dHy_dx * ik + x4[e];
             }
             T Jx = 0, Jy = 0, Jz = 0;
             for (int s = 0; s < src.n; ++s) {
@@ -388,6 +503,7 @@ k_update_E(const StepArgs<T> a, const int kchunk, const ESrc src) {
             Vec<T>::st(a.Ez + c, ez);
             if (zpml) { Vec<T>::st(a.psiE[1] + zs, pxz); Vec<T>::st(a.psiE[2] + zs, pyz); }
             if (ypml) { Vec<T>::st(a.psiE[0] + ys, pxy); Vec<T>::st(a.psiE[5] + ys, pzy); }
+            if (xpml) xpsi_store(a.psiE[3], a.psiE[4], a, k, j, i0, 1, a.NxT, x3, x4);
         }
 #pragma unroll
         for (int e = 0; e < W; ++e) { hxm[e] = hx[e]; hym[e] = hy[e]; }
