@@ -31,6 +31,7 @@ STATUS_NAMES = {
     4: "FDTD_ERR_UNSTABLE", 5: "FDTD_ERR_TIMEOUT", 6: "FDTD_ERR_PARSE",
     7: "FDTD_ERR_UNSUPPORTED", 8: "FDTD_ERR_NO_DEVICE",
 }
+FDTD_ERR_INVALID = 1
 FDTD_ERR_UNSTABLE = 4
 FDTD_ERR_NO_DEVICE = 8
 PREC_FP32, PREC_FP64 = 0, 1
@@ -46,7 +47,7 @@ EXPORTED_SYMBOLS = (
     "fdtd_set_tls_state", "fdtd_get_tls_state", "fdtd_run", "fdtd_steps_done",
     "fdtd_get_probe_series", "fdtd_get_dft", "fdtd_get_diagnostics", "fdtd_device_bytes",
     "fdtd_kernel_launches", "fdtd_set_timing", "fdtd_get_timing", "fdtd_set_kernel_path", "fdtd_synchronize", "fdtd_last_error",
-    "fdtd_destroy",
+    "fdtd_destroy", "fdtd_field_scan_noalloc",
 )
 
 
@@ -104,6 +105,10 @@ class DiagnosticsV1(C.Structure):
                 ("stable", C.c_int32), ("reserved", C.c_int32)]
 
 
+class FieldScanV1(C.Structure):
+    _fields_ = [("max_E", C.c_double), ("nan_flags", C.c_uint32), ("reserved", C.c_uint32)]
+
+
 class TimingV1(C.Structure):
     _fields_ = [("steps", C.c_uint64), ("run_ms", C.c_double), ("h_ms", C.c_double), ("e_ms", C.c_double),
                 ("aux_ms", C.c_double)]
@@ -150,6 +155,7 @@ def load_library() -> C.CDLL:
         "fdtd_synchronize": (C.c_int, [vp]),
         "fdtd_last_error": (C.c_char_p, [vp]),
         "fdtd_destroy": (None, [vp]),
+        "fdtd_field_scan_noalloc": (C.c_int, [C.c_int, vp, vp, vp, vp, vp, vp, C.c_uint64, vp, vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -336,6 +342,18 @@ class Solver:
             self.close()
         except Exception:
             pass
+
+
+def field_scan_noalloc(precision: int, fields, n: int, out_ptr: int, stream: int = 0) -> None:
+    """fdtd_field_scan_noalloc: the monitor's field scan (max |E|, non-finite flags) over n
+    cells of six caller-owned device arrays `fields` = (Ex, Ey, Ez, Hx, Hy, Hz) given as
+    device addresses, into the 16-byte device record at out_ptr, on `stream`; allocates no
+    device memory (for callers that cannot allocate).  Overlapping calls race."""
+    ptrs = [C.c_void_p(int(p)) for p in fields]
+    rc = load_library().fdtd_field_scan_noalloc(int(precision), *ptrs, C.c_uint64(int(n)), C.c_void_p(int(out_ptr)),
+                                                C.c_void_p(int(stream)))
+    if rc != 0:
+        raise FdtdError(rc, (load_library().fdtd_last_error(None) or b"").decode())
 
 
 def config_path(name: str) -> pathlib.Path:

@@ -988,3 +988,8 @@ const char* fdtd_last_error(const fdtd_handle* h) { return h ? h->err.c_str() : 
 void fdtd_destroy(fdtd_handle* h) { delete h; }
 
 }  // extern "C"
+
+// Lets other translation units of the library report through fdtd_last_error(NULL).
+namespace fdtd_internal {
+__attribute__((visibility("hidden"))) void set_global_error(const std::string& msg) { g_err = msg; }
+}

@@ -221,6 +221,31 @@ int fdtd_synchronize(fdtd_handle *h);
 const char *fdtd_last_error(const fdtd_handle *h);
 void fdtd_destroy(fdtd_handle *h);
 
+/* ---- Field scan without device allocation.  No counterpart in the reference: it exists
+ * for callers that cannot call cudaMalloc when they need the scan -- an application that
+ * runs the stepper inside its own device memory pool or arena (which owns all device
+ * memory and forbids side allocations), a callback running under its allocator's lock, or
+ * code whose watchdog treats any device allocation as a fault.  It computes what the
+ * stepper's stability monitor computes over the fields (max |E| over cells whose three E
+ * values are finite; bit0 = some E value non-finite, bit1 = some H value non-finite) over n
+ * cells of six caller-owned device arrays (any common layout), and writes the result into
+ * a caller-owned device record, on `stream` (a cudaStream_t; NULL = the default stream).
+ * Nothing is allocated: the scratch is a fixed 256 KiB device array inside the library,
+ * held on every GPU that loads the library until the process exits, which bounds n by
+ * FDTD_FIELD_SCAN_MAX_CELLS (larger n: FDTD_ERR_INVALID with a message; scan in pieces).
+ * The first call on each device (with that device current) looks up the array's device
+ * address; make that first call before any stream capture.  All calls share the one
+ * scratch array: calls that overlap on the GPU race and give wrong results -- serialise
+ * them (one stream per device, or events).  Errors: fdtd_last_error(NULL). */
+#define FDTD_FIELD_SCAN_MAX_CELLS (16384ull * 16384ull)
+typedef struct fdtd_field_scan_v1 {
+    double max_E;       /* max |Ex|,|Ey|,|Ez| over cells whose three E values are finite */
+    uint32_t nan_flags; /* bit0 E, bit1 H */
+    uint32_t reserved;
+} fdtd_field_scan_v1;
+int fdtd_field_scan_noalloc(int precision, const void *ex, const void *ey, const void *ez, const void *hx,
+                            const void *hy, const void *hz, uint64_t n, fdtd_field_scan_v1 *out, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
