@@ -204,11 +204,12 @@ __device__ __forceinline__ void e_plain(const StepArgs<T>& a, const size_t c, T 
 }
 
 // ---------------------------------------------------------------------------------
+// Two resident blocks per SM (at most 128 registers; a third block would spill).
 // Every load of an iteration (the vectors, the x-neighbour across the warp edge, 1/dz,
 // the CPML psi of the vector) is issued before the first use of any of them, so a vector
 // costs one memory round trip per plane whatever slab it lies in.
 template <typename T>
-__global__ void __launch_bounds__(32 * kBlockY)
+__global__ void __launch_bounds__(32 * kBlockY, 2)
 k_update_H(const StepArgs<T> a, const int kchunk) {
     constexpr int W = Vec<T>::W;
     if (*a.status) return;
@@ -334,7 +335,7 @@ k_update_H(const StepArgs<T> a, const int kchunk) {
 
 // ---------------------------------------------------------------------------------
 template <typename T>
-__global__ void __launch_bounds__(32 * kBlockY)
+__global__ void __launch_bounds__(32 * kBlockY, 2)
 k_update_E(const StepArgs<T> a, const int kchunk, const ESrc src) {
     constexpr int W = Vec<T>::W;
     if (*a.status) return;

@@ -208,11 +208,20 @@ __global__ void k_monitor_reduce(const StepArgs<T> a, size_t nflat, const double
     double mE = 0.0, mP = 0.0, s0 = 0, s1 = 0, s2 = 0, s3 = 0, s4 = 0;
     unsigned fl = 0;
     const size_t stride = size_t(gridDim.x) * blockDim.x;
-    for (size_t t = blockIdx.x * size_t(blockDim.x) + threadIdx.x; t < nflat; t += stride) {
-        const double ex = double(a.Ex[t]), ey = double(a.Ey[t]), ez = double(a.Ez[t]);
-        if (!isfinite(ex) || !isfinite(ey) || !isfinite(ez)) fl |= 1u;
-        else mE = fmax(mE, fmax(fabs(ex), fmax(fabs(ey), fabs(ez))));
-        if (!isfinite(double(a.Hx[t])) || !isfinite(double(a.Hy[t])) || !isfinite(double(a.Hz[t]))) fl |= 2u;
+    // 16-byte vectors: nflat is a multiple of the padded row, itself a multiple of W
+    constexpr int W = Vec<T>::W;
+    for (size_t v = blockIdx.x * size_t(blockDim.x) + threadIdx.x; v < nflat / W; v += stride) {
+        const size_t t = v * W;
+        T ex[W], ey[W], ez[W], hx[W], hy[W], hz[W];
+        Vec<T>::ldg(a.Ex + t, ex); Vec<T>::ldg(a.Ey + t, ey); Vec<T>::ldg(a.Ez + t, ez);
+        Vec<T>::ldg(a.Hx + t, hx); Vec<T>::ldg(a.Hy + t, hy); Vec<T>::ldg(a.Hz + t, hz);
+#pragma unroll
+        for (int e = 0; e < W; ++e) {
+            const double x = double(ex[e]), y = double(ey[e]), z = double(ez[e]);
+            if (!isfinite(x) || !isfinite(y) || !isfinite(z)) fl |= 1u;
+            else mE = fmax(mE, fmax(fabs(x), fmax(fabs(y), fabs(z))));
+            if (!isfinite(double(hx[e])) || !isfinite(double(hy[e])) || !isfinite(double(hz[e]))) fl |= 2u;
+        }
     }
     if (a.gain) {
         const T* Pn = parity_next ? a.P1 : a.P0;
@@ -390,6 +399,9 @@ private:
     size_t smemF_ = 0;
     int threadsF_ = 0, shapeF_ = 0;
     void (*launchF_)(dim3, int, size_t, cudaStream_t, const FusedMaps&, const FusedArgs<T>&, int, const ESrc&) = nullptr;
+    bool fused_ready_ = false;
+    size_t psi_sz_[6] = {};
+    void ensure_fused();
     void point_args_at(int buf);
     void build_fused();
     template <typename Shape> void setup_fused();
@@ -415,8 +427,8 @@ Solver<T>::Solver(const fdtd_setup_v1& s, int dev) {
     StepArgs<T>& a = a_;
     a.NxT = NxT_; a.NyT = NyT_; a.NzT = NzT_; a.NxP = NxP_; a.np = np_;
     a.plane = (long long)plane_;
-    for (int b = 0; b < 2; ++b)
-        for (int c = 0; c < 6; ++c) fld_[b][c] = alloc<T>(nflat_);
+    // buffer 1 (fields and psi_H) exists only for the fused path, made at its first step
+    for (int c = 0; c < 6; ++c) fld_[0][c] = alloc<T>(nflat_);
     point_args_at(0);
 
     // bH must be uniform and aE = aH = 1 (sigma = 0, mu_r = 1).
@@ -465,8 +477,8 @@ Solver<T>::Solver(const fdtd_setup_v1& s, int dev) {
         // 0 *_y, 1 *_z, 2 *_z, 3 *_x, 4 *_x, 5 *_y
         const size_t sz[6] = {ys, zs, zs, xs, xs, ys};
         for (int q = 0; q < 6; ++q) {
+            psi_sz_[q] = sz[q];
             psiH_[0][q] = alloc<T>(sz[q]);
-            psiH_[1][q] = alloc<T>(sz[q]);
             a.psiE[q] = alloc<T>(sz[q]);
             a.psiH[q] = psiH_[0][q];
         }
@@ -582,7 +594,6 @@ Solver<T>::Solver(const fdtd_setup_v1& s, int dev) {
     kchunkE_ = chunk(NyT_, NzT_);
     gridH_ = dim3(gx, (NyT_ - 1 + kBlockY - 1) / kBlockY, (NzT_ - 1 + kchunkH_ - 1) / kchunkH_);
     gridE_ = dim3(gx, (NyT_ + kBlockY - 1) / kBlockY, (NzT_ + kchunkE_ - 1) / kchunkE_);
-    build_fused();
     if (const char* p = std::getenv("FDTD_B200_KERNEL_PATH")) set_path(std::atoi(p));
     ck(cudaStreamSynchronize(st_), "setup upload");
 }
@@ -608,6 +619,24 @@ PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
 // Tensor maps over the padded device layout (x fastest): E/H boxes of the fused tile plus
 // its halo, bE boxes of the tile.  Base addresses come from cudaMalloc (256-byte aligned);
 // row and plane strides are multiples of 128 bytes.
+// First step of the fused path: the second field / psi_H buffer starts as a copy of the
+// first, then the tensor maps over both are encoded.
+template <typename T>
+void Solver<T>::ensure_fused() {
+    if (fused_ready_) return;
+    for (int c = 0; c < 6; ++c) {
+        fld_[1][c] = alloc<T>(nflat_, false);
+        ck(cudaMemcpyAsync(fld_[1][c], fld_[0][c], nflat_ * sizeof(T), cudaMemcpyDeviceToDevice, st_), "field copy");
+    }
+    for (int q = 0; q < 6; ++q) {
+        if (!psiH_[0][q]) continue;
+        psiH_[1][q] = alloc<T>(psi_sz_[q], false);
+        ck(cudaMemcpyAsync(psiH_[1][q], psiH_[0][q], psi_sz_[q] * sizeof(T), cudaMemcpyDeviceToDevice, st_), "psi copy");
+    }
+    build_fused();
+    fused_ready_ = true;
+}
+
 template <typename T>
 void Solver<T>::build_fused() {
     const char* env = std::getenv("FDTD_B200_FUSED_SHAPE");
@@ -718,10 +747,12 @@ void Solver<T>::from_device(const T* src, double* h) {
 template <typename T>
 void Solver<T>::set_field(int comp, const double* h) {
     if (comp < 0 || comp > 5) throw Failure(FDTD_ERR_INVALID, "component must be 0..5");
-    // Both buffers: cells the reference never updates must hold the same value in each.
+    // Both buffers of the fused path: cells the reference never updates must hold the same
+    // value in each.
     to_device(h, fld_[cur_][comp]);
-    ck(cudaMemcpyAsync(fld_[1 - cur_][comp], fld_[cur_][comp], nflat_ * sizeof(T), cudaMemcpyDeviceToDevice, st_),
-       "field copy");
+    if (fused_ready_)
+        ck(cudaMemcpyAsync(fld_[1 - cur_][comp], fld_[cur_][comp], nflat_ * sizeof(T), cudaMemcpyDeviceToDevice, st_),
+           "field copy");
     ck(cudaStreamSynchronize(st_), "set_field");
 }
 
@@ -784,6 +815,7 @@ void Solver<T>::ensure_series(uint64_t samples) {
 template <typename T>
 void Solver<T>::run(uint64_t n) {
     ck(cudaSetDevice(device), "cudaSetDevice");
+    if (path_ == 0) ensure_fused();
     const uint64_t n0 = steps;
     const uint64_t last = n0 + n;  // exclusive
     ensure_series((last + save_every_ - 1) / save_every_);
@@ -833,7 +865,7 @@ void Solver<T>::run(uint64_t n) {
             if (sample >= 0) series_count_ = uint64_t(sample) + 1;
         }
         if (interval_ && s % interval_ == 0) {
-            k_monitor_reduce<T><<<4 * 148, 256, 0, st_>>>(a_, nflat_, d_dx_, d_dy_, d_dz_, int((s + 1) & 1), d_acc_);
+            k_monitor_reduce<T><<<8 * 148, 256, 0, st_>>>(a_, nflat_, d_dx_, d_dy_, d_dz_, int((s + 1) & 1), d_acc_);
             k_monitor_eval<<<1, 1, 0, st_>>>(d_acc_, d_ms_, d_status_, s);
             launches += 2;
         }
