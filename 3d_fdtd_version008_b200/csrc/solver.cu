@@ -359,6 +359,15 @@ private:
         return d;
     }
     double* staging();
+    // Host <-> device copies of FP64 arrays through two pinned chunks: the host-side copy of
+    // one chunk (OpenMP) overlaps the DMA of the other.
+    static constexpr size_t kPinBytes = size_t(32) << 20;
+    void* pin_[2] = {nullptr, nullptr};
+    cudaEvent_t pin_ev_[2] = {nullptr, nullptr};
+    void ensure_pinned();
+    void h2d(const double* h, double* d, size_t n);
+    void d2h(const double* d, double* h, size_t n);
+    void upload_gain_box(const double* idx3, const std::vector<int8_t>& reg, T* dst);
     void to_device(const double* host_idx3, T* dst);
     void from_device(const T* src, double* host_idx3);
     void ensure_series(uint64_t samples);
@@ -433,13 +442,17 @@ Solver<T>::Solver(const fdtd_setup_v1& s, int dev) {
 
     // bH must be uniform and aE = aH = 1 (sigma = 0, mu_r = 1).
     double bH = s.bH_uniform;
+    if (s.bH[0]) bH = s.bH[0][0];
+    auto all_equal = [N](const double* v, double x) {  // OpenMP scan of a full-grid array
+        long long bad = 0;
+#pragma omp parallel for reduction(+ : bad) schedule(static)
+        for (long long q = 0; q < (long long)N; ++q) bad += v[q] != x;
+        return bad == 0;
+    };
     for (int c = 0; c < 3; ++c) {
-        if (s.aE[c]) for (size_t q = 0; q < N; ++q) if (s.aE[c][q] != 1.0) throw Failure(FDTD_ERR_UNSUPPORTED, "aE != 1 (lossy material) is not supported");
-        if (s.aH[c]) for (size_t q = 0; q < N; ++q) if (s.aH[c][q] != 1.0) throw Failure(FDTD_ERR_UNSUPPORTED, "aH != 1 (magnetic loss) is not supported");
-        if (s.bH[c]) {
-            if (c == 0) bH = s.bH[0][0];
-            for (size_t q = 0; q < N; ++q) if (s.bH[c][q] != bH) throw Failure(FDTD_ERR_UNSUPPORTED, "non-uniform bH (mu_r != 1) is not supported");
-        }
+        if (s.aE[c] && !all_equal(s.aE[c], 1.0)) throw Failure(FDTD_ERR_UNSUPPORTED, "aE != 1 (lossy material) is not supported");
+        if (s.aH[c] && !all_equal(s.aH[c], 1.0)) throw Failure(FDTD_ERR_UNSUPPORTED, "aH != 1 (magnetic loss) is not supported");
+        if (s.bH[c] && !all_equal(s.bH[c], bH)) throw Failure(FDTD_ERR_UNSUPPORTED, "non-uniform bH (mu_r != 1) is not supported");
     }
     a.bH = T(bH);
     T* be[3];
@@ -491,19 +504,25 @@ Solver<T>::Solver(const fdtd_setup_v1& s, int dev) {
     if (s.n_tls_regions > 0) {
         if (!s.tls_region_map || !s.tls_regions) throw Failure(FDTD_ERR_INVALID, "gain regions without region map");
         if (s.n_tls_regions > 127) throw Failure(FDTD_ERR_UNSUPPORTED, "more than 127 gain regions");
-        int lo[3] = {NxT_, NyT_, NzT_}, hi[3] = {-1, -1, -1};
+        int lo0 = NxT_, lo1 = NyT_, lo2 = NzT_, hi0 = -1, hi1 = -1, hi2 = -1;
+        long long out_of_range = 0, on_boundary = 0;
+        const int nreg = int(s.n_tls_regions);
+#pragma omp parallel for reduction(min : lo0, lo1, lo2) reduction(max : hi0, hi1, hi2) \
+    reduction(+ : out_of_range, on_boundary) schedule(static)
         for (int i = 0; i < NxT_; ++i)
             for (int j = 0; j < NyT_; ++j)
                 for (int k = 0; k < NzT_; ++k) {
                     const int32_t r = s.tls_region_map[(size_t(i) * NyT_ + j) * NzT_ + k];
                     if (r < 0) continue;
-                    if (r >= int32_t(s.n_tls_regions)) throw Failure(FDTD_ERR_INVALID, "region map entry out of range");
-                    if (i == 0 || j == 0 || k == 0)
-                        throw Failure(FDTD_ERR_UNSUPPORTED, "gain cells on the i=0/j=0/k=0 boundary planes");
-                    lo[0] = std::min(lo[0], i); hi[0] = std::max(hi[0], i);
-                    lo[1] = std::min(lo[1], j); hi[1] = std::max(hi[1], j);
-                    lo[2] = std::min(lo[2], k); hi[2] = std::max(hi[2], k);
+                    out_of_range += r >= nreg;
+                    on_boundary += (i == 0 || j == 0 || k == 0);
+                    lo0 = std::min(lo0, i); hi0 = std::max(hi0, i);
+                    lo1 = std::min(lo1, j); hi1 = std::max(hi1, j);
+                    lo2 = std::min(lo2, k); hi2 = std::max(hi2, k);
                 }
+        if (out_of_range) throw Failure(FDTD_ERR_INVALID, "region map entry out of range");
+        if (on_boundary) throw Failure(FDTD_ERR_UNSUPPORTED, "gain cells on the i=0/j=0/k=0 boundary planes");
+        const int lo[3] = {lo0, lo1, lo2}, hi[3] = {hi0, hi1, hi2};
         if (hi[0] >= 0) {
             has_gain_ = true;
             a.gain = 1;
@@ -534,8 +553,8 @@ Solver<T>::Solver(const fdtd_setup_v1& s, int dev) {
                 g.active = R.N0 > 0 ? 1 : 0;
             }
             a.gcoef = upload(gc);
-            if (s.tls_Nu) set_tls(FDTD_TLS_NU, s.tls_Nu);
-            if (s.tls_Ng) set_tls(FDTD_TLS_NG, s.tls_Ng);
+            if (s.tls_Nu) upload_gain_box(s.tls_Nu, reg, a.Nu);
+            if (s.tls_Ng) upload_gain_box(s.tls_Ng, reg, a.Ng);
         }
     }
 
@@ -708,6 +727,10 @@ Solver<T>::~Solver() {
     for (auto& e : ev_) if (e) cudaEventDestroy(e);
     for (void* p : ptrs_) cudaFree(p);
     if (d_stage_) cudaFree(d_stage_);
+    for (int b = 0; b < 2; ++b) {
+        if (pin_[b]) cudaFreeHost(pin_[b]);
+        if (pin_ev_[b]) cudaEventDestroy(pin_ev_[b]);
+    }
     if (st_) cudaStreamDestroy(st_);
 }
 
@@ -721,10 +744,80 @@ double* Solver<T>::staging() {
 }
 
 template <typename T>
+void Solver<T>::ensure_pinned() {
+    for (int b = 0; b < 2; ++b) {
+        if (!pin_[b]) ck(cudaHostAlloc(&pin_[b], kPinBytes, cudaHostAllocDefault), "cudaHostAlloc");
+        if (!pin_ev_[b]) ck(cudaEventCreateWithFlags(&pin_ev_[b], cudaEventDisableTiming), "cudaEventCreate");
+    }
+}
+
+// memcpy split over the host threads (the pageable side of a chunk copy)
+static void par_copy(void* dst, const void* src, size_t bytes) {
+    const size_t piece = size_t(1) << 20;
+    const long long n = (long long)((bytes + piece - 1) / piece);
+#pragma omp parallel for schedule(static)
+    for (long long q = 0; q < n; ++q) {
+        const size_t o = size_t(q) * piece;
+        std::memcpy(static_cast<char*>(dst) + o, static_cast<const char*>(src) + o, std::min(piece, bytes - o));
+    }
+}
+
+template <typename T>
+void Solver<T>::h2d(const double* h, double* d, size_t n) {
+    ensure_pinned();
+    const size_t chunk = kPinBytes / sizeof(double);
+    for (size_t off = 0, it = 0; off < n; off += chunk, ++it) {
+        const int b = int(it & 1);
+        const size_t m = std::min(chunk, n - off);
+        ck(cudaEventSynchronize(pin_ev_[b]), "pinned buffer");  // its previous DMA is done
+        par_copy(pin_[b], h + off, m * sizeof(double));
+        ck(cudaMemcpyAsync(d + off, pin_[b], m * sizeof(double), cudaMemcpyHostToDevice, st_), "H2D");
+        ck(cudaEventRecord(pin_ev_[b], st_), "cudaEventRecord");
+    }
+}
+
+template <typename T>
+void Solver<T>::d2h(const double* d, double* h, size_t n) {
+    ensure_pinned();
+    const size_t chunk = kPinBytes / sizeof(double);
+    const size_t nch = (n + chunk - 1) / chunk;
+    auto issue = [&](size_t it) {
+        const size_t off = it * chunk, m = std::min(chunk, n - off);
+        ck(cudaMemcpyAsync(pin_[it & 1], d + off, m * sizeof(double), cudaMemcpyDeviceToHost, st_), "D2H");
+        ck(cudaEventRecord(pin_ev_[it & 1], st_), "cudaEventRecord");
+    };
+    if (nch) issue(0);
+    for (size_t it = 0; it < nch; ++it) {
+        if (it + 1 < nch) issue(it + 1);  // the other buffer was drained in the previous iteration
+        const size_t off = it * chunk, m = std::min(chunk, n - off);
+        ck(cudaEventSynchronize(pin_ev_[it & 1]), "D2H chunk");
+        par_copy(h + off, pin_[it & 1], m * sizeof(double));
+    }
+}
+
+// Initial gain state: the bounding box is cut out of the idx3 array on the host (cells
+// outside the gain regions hold 0, as k_gain_block stores them) and only the box is copied.
+template <typename T>
+void Solver<T>::upload_gain_box(const double* h, const std::vector<int8_t>& reg, T* dst) {
+    const int gX = a_.gX, gY = a_.gY, gZ = a_.gZ;
+    std::vector<T> box(size_t(gX) * gY * gZ);
+#pragma omp parallel for schedule(static)
+    for (int k = 0; k < gZ; ++k)
+        for (int j = 0; j < gY; ++j)
+            for (int i = 0; i < gX; ++i) {
+                const size_t t = (size_t(k) * gY + j) * gX + i;
+                const size_t id = (size_t(i + a_.gi0) * NyT_ + (j + a_.gj0)) * NzT_ + (k + a_.gk0);
+                box[t] = reg[t] >= 0 ? T(h[id]) : T(0);
+            }
+    ck(cudaMemcpyAsync(dst, box.data(), box.size() * sizeof(T), cudaMemcpyHostToDevice, st_), "gain box");
+    ck(cudaStreamSynchronize(st_), "gain box");
+}
+
+template <typename T>
 void Solver<T>::to_device(const double* h, T* dst) {
     if (!h) throw Failure(FDTD_ERR_INVALID, "null host array");
     double* sbuf = staging();
-    ck(cudaMemcpyAsync(sbuf, h, size_t(NxT_) * NyT_ * NzT_ * sizeof(double), cudaMemcpyHostToDevice, st_), "H2D");
+    h2d(h, sbuf, size_t(NxT_) * NyT_ * NzT_);
     dim3 g((NzT_ + 31) / 32, (NxT_ + 31) / 32, NyT_), b(32, 8);
     k_from_idx3<T><<<g, b, 0, st_>>>(sbuf, dst, NxT_, NyT_, NzT_, NxP_);
     ++launches;
@@ -740,7 +833,7 @@ void Solver<T>::from_device(const T* src, double* h) {
     k_to_idx3<T><<<g, b, 0, st_>>>(src, sbuf, NxT_, NyT_, NzT_, NxP_);
     ++launches;
     ck(cudaGetLastError(), "k_to_idx3");
-    ck(cudaMemcpyAsync(h, sbuf, size_t(NxT_) * NyT_ * NzT_ * sizeof(double), cudaMemcpyDeviceToHost, st_), "D2H");
+    d2h(sbuf, h, size_t(NxT_) * NyT_ * NzT_);
     ck(cudaStreamSynchronize(st_), "from_device");
 }
 
@@ -770,7 +863,7 @@ void Solver<T>::set_tls(int which, const double* h) {
            : which == FDTD_TLS_PZ_PREV ? ((steps & 1) ? a_.P0 : a_.P1)
            : which == FDTD_TLS_NU ? a_.Nu : a_.Ng;
     double* sbuf = staging();
-    ck(cudaMemcpyAsync(sbuf, h, size_t(NxT_) * NyT_ * NzT_ * sizeof(double), cudaMemcpyHostToDevice, st_), "H2D");
+    h2d(h, sbuf, size_t(NxT_) * NyT_ * NzT_);
     k_gain_block<T><<<592, 256, 0, st_>>>(sbuf, dst, a_.greg, a_.gi0, a_.gj0, a_.gk0, a_.gX, a_.gY, a_.gZ, NyT_, NzT_, 1);
     ++launches;
     ck(cudaGetLastError(), "k_gain_block");
@@ -791,7 +884,7 @@ void Solver<T>::get_tls(int which, double* h) {
     k_gain_block<T><<<592, 256, 0, st_>>>(sbuf, src, a_.greg, a_.gi0, a_.gj0, a_.gk0, a_.gX, a_.gY, a_.gZ, NyT_, NzT_, 0);
     ++launches;
     ck(cudaGetLastError(), "k_gain_block");
-    ck(cudaMemcpyAsync(h, sbuf, N * sizeof(double), cudaMemcpyDeviceToHost, st_), "D2H");
+    d2h(sbuf, h, N);
     ck(cudaStreamSynchronize(st_), "get_tls");
 }
 
