@@ -204,23 +204,28 @@ __device__ __forceinline__ void e_plain(const StepArgs<T>& a, const size_t c, T 
 }
 
 // ---------------------------------------------------------------------------------
-// Two resident blocks per SM (at most 128 registers; a third block would spill).
-// Every load of an iteration (the vectors, the x-neighbour across the warp edge, 1/dz,
-// the CPML psi of the vector) is issued before the first use of any of them, so a vector
-// costs one memory round trip per plane whatever slab it lies in.
-template <typename T>
-__global__ void __launch_bounds__(32 * kBlockY, 2)
-k_update_H(const StepArgs<T> a, const int kchunk) {
+// Launch geometry of the sweeps.  The x range of a row is split into the interior
+// [xi0, xi1) -- W-aligned vectors with no x-slab cell -- covered by gxi block columns of
+// 32-vector warp segments, and the edge vectors outside it (nl on the left, ne in total),
+// which one extra block column packs er rows at a time, one thread per edge vector.
+// Interior warps therefore never diverge on the x slab, and edge threads all take the
+// general path together.
+struct SweepGeom {
+    int xi0, xi1;  // interior x range (cells)
+    int gxi;       // interior block columns
+    int nl, ne;    // edge vectors per row: on the left, in total
+    int er;        // rows per edge block
+};
+
+// One thread's column of W-cell vectors (i0.., j, kb..ke-1), marching in +z.
+// Every load of an iteration (the vectors, the x-neighbour at the warp or interior edge,
+// 1/dz, the CPML psi of the vector) is issued before the first use of any of them, so a
+// vector costs one memory round trip per plane whatever slab it lies in.  EDGE columns
+// read the x-neighbour from memory (lanes hold other rows); interior columns shuffle it.
+template <typename T, bool EDGE>
+__device__ __forceinline__ void h_column(const StepArgs<T>& a, const SweepGeom& g, const int j, const int i0,
+                                         const bool act, const int kb, const int ke, const int lane) {
     constexpr int W = Vec<T>::W;
-    if (*a.status) return;
-    const int lane = threadIdx.x;
-    const int j = blockIdx.y * kBlockY + threadIdx.y;
-    if (j >= a.NyT - 1) return;  // whole warp: a warp is one row
-    const int kb = blockIdx.z * kchunk;
-    const int ke = min(kb + kchunk, a.NzT - 1);
-    if (kb >= ke) return;
-    const int i0 = (blockIdx.x * 32 + lane) * W;
-    const bool act = i0 < a.NxT;
     const int np = a.np, np2 = 2 * np;
     const T bH = a.bH;
 
@@ -232,8 +237,11 @@ k_update_H(const StepArgs<T> a, const int kchunk) {
     const int jy = ypml ? slab_index(j, a.NyT, np) : 0;
     T yb = 1, yc = 0, yik = 1;
     if (ypml) { yb = __ldg(a.pbH[1] + j); yc = __ldg(a.pcH[1] + j); yik = __ldg(a.ik[1] + j); }
-    const bool xpml = act && (i0 < np || i0 + W > a.NxT - np);
+    const bool xpml = EDGE && act && (i0 < np || i0 + W > a.NxT - np);
     const bool plain_row = act && !ypml && !xpml && i0 + W <= a.NxT - 1;
+    // Ey, Ez at i0+W come from memory at the warp edge, at the end of the interior (the
+    // next lane then holds no interior vector) and for every edge column
+    const bool nload = EDGE || lane == 31 || i0 + W >= g.xi1;
 
     const size_t row = size_t(j) * a.NxP + i0;
     T ex0[W], ey0[W];
@@ -262,7 +270,7 @@ k_update_H(const StepArgs<T> a, const int kchunk) {
             for (int e = 0; e < W; ++e) ex1[e] = ey1[e] = ez[e] = exj[e] = ezj[e] = hx[e] = hy[e] = hz[e] = T(0);
         }
         T eye = T(0), eze = T(0);
-        if (lane == 31 && act && i0 + W < a.NxT) { eye = __ldg(a.Ey + c + W); eze = __ldg(a.Ez + c + W); }
+        if (nload && act && i0 + W < a.NxT) { eye = __ldg(a.Ey + c + W); eze = __ldg(a.Ez + c + W); }
         const T idz = __ldg(a.idz + k);
         const bool zpml = in_pml(k, a.NzT, np);
         T zb = 1, zc = 0, zik = 1;
@@ -279,10 +287,13 @@ k_update_H(const StepArgs<T> a, const int kchunk) {
         }
         T x3[W], x4[W];  // psi Hy_x, Hz_x
         if (xpml) xpsi_load(a.psiH[3], a.psiH[4], a, k, j, i0, x3, x4);
-        // x-neighbour at i0+W: the next lane's first cell, the loaded one for lane 31
-        T eyn = __shfl_down_sync(kFull, ey0[0], 1);
-        T ezn = __shfl_down_sync(kFull, ez[0], 1);
-        if (lane == 31) { eyn = eye; ezn = eze; }
+        // x-neighbour at i0+W: the next lane's first cell, or the loaded one
+        T eyn = eye, ezn = eze;
+        if (!EDGE) {
+            const T sy = __shfl_down_sync(kFull, ey0[0], 1);
+            const T sz = __shfl_down_sync(kFull, ez[0], 1);
+            if (!nload) { eyn = sy; ezn = sz; }
+        }
         if (plain_row && !zpml) {
             h_plain(a, c, ex0, ex1, ey0, ey1, ez, exj, ezj, eyn, ezn, hx, hy, hz, idx, idy, idz);
 #pragma unroll
@@ -333,20 +344,37 @@ k_update_H(const StepArgs<T> a, const int kchunk) {
     }
 }
 
-// ---------------------------------------------------------------------------------
+// Two resident blocks per SM (at most 128 registers; a third block would spill).
 template <typename T>
 __global__ void __launch_bounds__(32 * kBlockY, 2)
-k_update_E(const StepArgs<T> a, const int kchunk, const ESrc src) {
+k_update_H(const StepArgs<T> a, const int kchunk, const SweepGeom g) {
     constexpr int W = Vec<T>::W;
     if (*a.status) return;
     const int lane = threadIdx.x;
-    const int j = blockIdx.y * kBlockY + threadIdx.y;
-    if (j < 1 || j >= a.NyT) return;  // E is updated for j >= 1 only
-    const int kb = max(int(blockIdx.z) * kchunk, 1);
-    const int ke = min(int(blockIdx.z) * kchunk + kchunk, a.NzT);
+    const int kb = blockIdx.z * kchunk;
+    const int ke = min(kb + kchunk, a.NzT - 1);
     if (kb >= ke) return;
-    const int i0 = (blockIdx.x * 32 + lane) * W;
-    const bool act = i0 < a.NxT;
+    if (int(blockIdx.x) < g.gxi) {
+        const int j = blockIdx.y * kBlockY + threadIdx.y;
+        if (j >= a.NyT - 1) return;  // whole warp: a warp is one row
+        const int i0 = g.xi0 + (blockIdx.x * 32 + lane) * W;
+        h_column<T, false>(a, g, j, i0, i0 < g.xi1, kb, ke, lane);
+    } else {
+        const int t = threadIdx.y * 32 + lane;
+        const int rr = t / g.ne, v = t - rr * g.ne;
+        const int j = blockIdx.y * g.er + rr;
+        if (rr >= g.er || j >= a.NyT - 1) return;
+        const int i0 = v < g.nl ? v * W : g.xi1 + (v - g.nl) * W;
+        if (i0 >= a.NxT) return;
+        h_column<T, true>(a, g, j, i0, true, kb, ke, lane);
+    }
+}
+
+// ---------------------------------------------------------------------------------
+template <typename T, bool EDGE>
+__device__ __forceinline__ void e_column(const StepArgs<T>& a, const SweepGeom& g, const ESrc& src, const int j,
+                                         const int i0, const bool act, const int kb, const int ke, const int lane) {
+    constexpr int W = Vec<T>::W;
     const int np = a.np, np2 = 2 * np;
 
     T idx[W];
@@ -357,9 +385,12 @@ k_update_E(const StepArgs<T> a, const int kchunk, const ESrc src) {
     const int jy = ypml ? slab_index(j, a.NyT, np) : 0;
     T yb = 1, yc = 0, yik = 1;
     if (ypml) { yb = __ldg(a.pbE[1] + j); yc = __ldg(a.pcE[1] + j); yik = __ldg(a.ik[1] + j); }
-    const bool xpml = act && (i0 < np || i0 + W > a.NxT - np);
+    const bool xpml = EDGE && act && (i0 < np || i0 + W > a.NxT - np);
     const bool grow = a.gain && j >= a.gj0 && j < a.gj0 + a.gY && i0 + W > a.gi0 && i0 < a.gi0 + a.gX;
     const bool plain_row = act && !ypml && !xpml && i0 >= 1 && i0 + W <= a.NxT;
+    // Hz, Hy at i0-1 come from memory at the warp edge (lane 0, which also holds the first
+    // interior vector) and for every edge column
+    const bool pload = EDGE || lane == 0;
     T* const Pcur = src.parity ? a.P1 : a.P0;
     T* const Pold = src.parity ? a.P0 : a.P1;  // holds P^{n-1}, receives P^{n+1}
 
@@ -394,7 +425,7 @@ k_update_E(const StepArgs<T> a, const int kchunk, const ESrc src) {
                 ex[e] = ey[e] = ez[e] = bx[e] = by[e] = bz[e] = hx[e] = hy[e] = hz[e] = hzj[e] = hxj[e] = T(0);
         }
         T hze = T(0), hye = T(0);
-        if (lane == 0 && act && i0 > 0) { hze = __ldg(a.Hz + c - 1); hye = __ldg(a.Hy + c - 1); }
+        if (pload && act && i0 > 0) { hze = __ldg(a.Hz + c - 1); hye = __ldg(a.Hy + c - 1); }
         const T idz = __ldg(a.idz + k);
         const bool zpml = in_pml(k, a.NzT, np);
         T zb = 1, zc = 0, zik = 1;
@@ -411,10 +442,13 @@ k_update_E(const StepArgs<T> a, const int kchunk, const ESrc src) {
         }
         T x3[W], x4[W];  // psi Ey_x, Ez_x
         if (xpml) xpsi_load(a.psiE[3], a.psiE[4], a, k, j, i0, x3, x4);
-        // x-neighbour at i0-1: the previous lane's last cell, the loaded one for lane 0
-        T hzp = __shfl_up_sync(kFull, hz[W - 1], 1);
-        T hyp = __shfl_up_sync(kFull, hy[W - 1], 1);
-        if (lane == 0) { hzp = hze; hyp = hye; }
+        // x-neighbour at i0-1: the previous lane's last cell, or the loaded one
+        T hzp = hze, hyp = hye;
+        if (!EDGE) {
+            const T sz = __shfl_up_sync(kFull, hz[W - 1], 1);
+            const T sy = __shfl_up_sync(kFull, hy[W - 1], 1);
+            if (!pload) { hzp = sz; hyp = sy; }
+        }
         const bool gplane = grow && k >= a.gk0 && k < a.gk0 + a.gZ;
         if (plain_row && !zpml && !gplane && !src_in_vector(src, i0, j, k, W)) {
             e_plain(a, c, ex, ey, ez, bx, by, bz, hx, hy, hz, hzj, hxj, hxm, hym, hzp, hyp, idx, idy, idz);
@@ -508,6 +542,31 @@ k_update_E(const StepArgs<T> a, const int kchunk, const ESrc src) {
         }
 #pragma unroll
         for (int e = 0; e < W; ++e) { hxm[e] = hx[e]; hym[e] = hy[e]; }
+    }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(32 * kBlockY, 2)
+k_update_E(const StepArgs<T> a, const int kchunk, const ESrc src, const SweepGeom g) {
+    constexpr int W = Vec<T>::W;
+    if (*a.status) return;
+    const int lane = threadIdx.x;
+    const int kb = max(int(blockIdx.z) * kchunk, 1);
+    const int ke = min(int(blockIdx.z) * kchunk + kchunk, a.NzT);
+    if (kb >= ke) return;
+    if (int(blockIdx.x) < g.gxi) {
+        const int j = blockIdx.y * kBlockY + threadIdx.y;
+        if (j < 1 || j >= a.NyT) return;  // E is updated for j >= 1 only; whole warp
+        const int i0 = g.xi0 + (blockIdx.x * 32 + lane) * W;
+        e_column<T, false>(a, g, src, j, i0, i0 < g.xi1, kb, ke, lane);
+    } else {
+        const int t = threadIdx.y * 32 + lane;
+        const int rr = t / g.ne, v = t - rr * g.ne;
+        const int j = blockIdx.y * g.er + rr;
+        if (rr >= g.er || j < 1 || j >= a.NyT) return;
+        const int i0 = v < g.nl ? v * W : g.xi1 + (v - g.nl) * W;
+        if (i0 >= a.NxT) return;
+        e_column<T, true>(a, g, src, j, i0, true, kb, ke, lane);
     }
 }
 

@@ -378,6 +378,7 @@ private:
     int NxT_, NyT_, NzT_, NxP_, np_;
     size_t plane_, nflat_;
     int kchunkH_ = 1, kchunkE_ = 1;
+    SweepGeom geom_{};
     dim3 gridH_, gridE_;
     double dt_;
     // sources
@@ -601,8 +602,18 @@ Solver<T>::Solver(const fdtd_setup_v1& s, int dev) {
     d_status_ = alloc<unsigned>(1);
     a.status = d_status_;
 
+    // x split: W-aligned interior without x-slab cells, and the edge vectors around it
+    SweepGeom& g = geom_;
+    g.xi0 = int(round_up(size_t(np_), size_t(W)));
+    g.xi1 = std::max(g.xi0, ((NxT_ - np_) / W) * W);
+    g.gxi = (g.xi1 - g.xi0 + 32 * W - 1) / (32 * W);
+    g.nl = g.xi0 / W;
+    g.ne = g.nl + std::max(0, (NxT_ - g.xi1 + W - 1) / W);
+    if (g.ne > 32 * kBlockY) throw Failure(FDTD_ERR_UNSUPPORTED, "CPML too thick for the sweep launch shape");
+    g.er = g.ne ? (32 * kBlockY) / g.ne : 1;
+    const int gx = g.gxi + (g.ne ? 1 : 0);
+    const int gyE = std::max((NyT_ + kBlockY - 1) / kBlockY, g.ne ? (NyT_ + g.er - 1) / g.er : 0);
     // launch shapes: z-chunks so that the grid holds several waves of blocks
-    const int gx = int((NxT_ + 32 * W - 1) / (32 * W));
     auto chunk = [&](int rows, int planes) {
         const int bxy = std::max(1, gx * ((rows + kBlockY - 1) / kBlockY));
         const int want = std::max(1, (148 * 16 + bxy - 1) / bxy);
@@ -611,8 +622,9 @@ Solver<T>::Solver(const fdtd_setup_v1& s, int dev) {
     };
     kchunkH_ = chunk(NyT_ - 1, NzT_ - 1);
     kchunkE_ = chunk(NyT_, NzT_);
-    gridH_ = dim3(gx, (NyT_ - 1 + kBlockY - 1) / kBlockY, (NzT_ - 1 + kchunkH_ - 1) / kchunkH_);
-    gridE_ = dim3(gx, (NyT_ + kBlockY - 1) / kBlockY, (NzT_ + kchunkE_ - 1) / kchunkE_);
+    if (gyE > 65535) throw Failure(FDTD_ERR_INVALID, "grid too large for the sweep launch shape (NyT)");
+    gridH_ = dim3(gx, gyE, (NzT_ - 1 + kchunkH_ - 1) / kchunkH_);
+    gridE_ = dim3(gx, gyE, (NzT_ + kchunkE_ - 1) / kchunkE_);
     if (const char* p = std::getenv("FDTD_B200_KERNEL_PATH")) set_path(std::atoi(p));
     ck(cudaStreamSynchronize(st_), "setup upload");
 }
@@ -944,9 +956,9 @@ void Solver<T>::run(uint64_t n) {
             point_args_at(cur_);
             launches += 1;
         } else {
-            k_update_H<T><<<gridH_, blk, 0, st_>>>(a_, kchunkH_);
+            k_update_H<T><<<gridH_, blk, 0, st_>>>(a_, kchunkH_, geom_);
             if (per_kernel) ck(cudaEventRecord(ev_[1], st_), "cudaEventRecord");
-            k_update_E<T><<<gridE_, blk, 0, st_>>>(a_, kchunkE_, src);
+            k_update_E<T><<<gridE_, blk, 0, st_>>>(a_, kchunkE_, src, geom_);
             launches += 2;
         }
         if (per_kernel) ck(cudaEventRecord(ev_[2], st_), "cudaEventRecord");
