@@ -34,7 +34,7 @@ STATUS_NAMES = {
 FDTD_ERR_INVALID = 1
 FDTD_ERR_UNSTABLE = 4
 FDTD_ERR_NO_DEVICE = 8
-PREC_FP32, PREC_FP64 = 0, 1
+PREC_FP32, PREC_FP64, PREC_FP16, PREC_BF16 = 0, 1, 2, 3
 TIMING_OFF, TIMING_RUN, TIMING_KERNELS = 0, 1, 2
 COMPONENTS = {"Ex": 0, "Ey": 1, "Ez": 2, "Hx": 3, "Hy": 4, "Hz": 5,
               "E_mag": 6, "H_mag": 7, "Sx": 8, "Sy": 9, "Sz": 10, "S_mag": 11}
@@ -95,6 +95,7 @@ class SetupV1(C.Structure):
         ("n_dft_freqs", C.c_uint32), ("dft_freqs", _dptr),
         ("monitor_interval", C.c_uint32), ("max_E", C.c_double), ("max_P", C.c_double),
         ("conservation_err", C.c_double), ("growth_rate", C.c_double),
+        ("field_scale", C.c_double),
     ]
 
 

@@ -104,7 +104,10 @@ int fdtd_setup_view(const fdtd_setup* s, fdtd_setup_v1* v) {
     const fdtd::SimSetup& S = s->S;
     std::memset(v, 0, sizeof(*v));
     v->struct_size = sizeof(fdtd_setup_v1);
-    v->precision = (S.precision == "fp64") ? FDTD_PREC_FP64 : FDTD_PREC_FP32;
+    v->precision = S.precision == "fp64" ? FDTD_PREC_FP64
+                 : S.precision == "fp16" ? FDTD_PREC_FP16
+                 : S.precision == "bf16" ? FDTD_PREC_BF16 : FDTD_PREC_FP32;
+    v->field_scale = S.field_scale;
     v->NxT = S.NxT; v->NyT = S.NyT; v->NzT = S.NzT;
     v->npml = uint32_t(S.npml);
     v->save_every = uint32_t(S.save_every);

@@ -483,6 +483,9 @@ SimSetup SimSetup::from_params(const ParamFile& pf, bool bake) {
     S.stability_conservation = pf.num("STABILITY_CONSERVATION_ERR", 0.01);
     S.stability_growth = pf.num("STABILITY_GROWTH_RATE", 10.0);
     S.precision = pf.str("PRECISION", "fp32");
+    if (S.precision != "fp32" && S.precision != "fp64" && S.precision != "fp16" && S.precision != "bf16")
+        throw std::runtime_error("PRECISION must be fp32, fp64, fp16 or bf16");
+    S.field_scale = pf.num("FIELD_SCALE", 0.0);
     S.noise_amplitude = pf.num("NOISE_AMPLITUDE", 0.0);
     S.seed = uint64_t(pf.num("SEED", 1));
     const real pump = pf.num("PUMP_RATE", 0.0);

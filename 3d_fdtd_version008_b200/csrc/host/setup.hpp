@@ -244,7 +244,8 @@ struct SimSetup {
     std::vector<PointProbe> probes;
     // build-only keys
     std::vector<real> dft_freqs;
-    std::string precision = "fp32";
+    std::string precision = "fp32";  // fp32 | fp64 | fp16 | bf16
+    real field_scale = 0;            // FP16/BF16 storage scale sE (0 = automatic)
     real noise_amplitude = 0;
     uint64_t seed = 1;
     std::size_t stability_interval = 10;

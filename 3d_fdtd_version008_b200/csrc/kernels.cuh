@@ -19,6 +19,8 @@
 // z-slab [2np][j][NxP], index 0 for the low side, np.. for the high side.
 #pragma once
 
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 #include <cstdint>
 
@@ -58,7 +60,86 @@ template <> struct Vec<double> {
     }
 };
 
+// Field / psi storage.  S is the type held in memory, T the type the update computes in;
+// a thread moves W = Vec<T>::W consecutive cells per array (16 bytes of T, 8 bytes of a
+// 16-bit S).
+template <typename S, typename T> struct Fld;
+template <typename T> struct Fld<T, T> {
+    __device__ __forceinline__ static void ld(const T* p, T (&a)[Vec<T>::W]) { Vec<T>::ld(p, a); }
+    __device__ __forceinline__ static void ldg(const T* p, T (&a)[Vec<T>::W]) { Vec<T>::ldg(p, a); }
+    __device__ __forceinline__ static void st(T* p, const T (&a)[Vec<T>::W]) { Vec<T>::st(p, a); }
+};
+template <> struct Fld<__half, float> {
+    __device__ __forceinline__ static void ld(const __half* p, float (&a)[4]) {
+        const uint2 u = *reinterpret_cast<const uint2*>(p);
+        const float2 lo = __half22float2(*reinterpret_cast<const __half2*>(&u.x));
+        const float2 hi = __half22float2(*reinterpret_cast<const __half2*>(&u.y));
+        a[0] = lo.x; a[1] = lo.y; a[2] = hi.x; a[3] = hi.y;
+    }
+    __device__ __forceinline__ static void ldg(const __half* p, float (&a)[4]) {
+        const uint2 u = __ldg(reinterpret_cast<const uint2*>(p));
+        const float2 lo = __half22float2(*reinterpret_cast<const __half2*>(&u.x));
+        const float2 hi = __half22float2(*reinterpret_cast<const __half2*>(&u.y));
+        a[0] = lo.x; a[1] = lo.y; a[2] = hi.x; a[3] = hi.y;
+    }
+    __device__ __forceinline__ static void st(__half* p, const float (&a)[4]) {
+        const __half2 lo = __floats2half2_rn(a[0], a[1]), hi = __floats2half2_rn(a[2], a[3]);
+        uint2 u;
+        u.x = *reinterpret_cast<const unsigned*>(&lo);
+        u.y = *reinterpret_cast<const unsigned*>(&hi);
+        *reinterpret_cast<uint2*>(p) = u;
+    }
+};
+template <> struct Fld<__nv_bfloat16, float> {
+    __device__ __forceinline__ static void ld(const __nv_bfloat16* p, float (&a)[4]) {
+        const uint2 u = *reinterpret_cast<const uint2*>(p);
+        const float2 lo = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&u.x));
+        const float2 hi = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&u.y));
+        a[0] = lo.x; a[1] = lo.y; a[2] = hi.x; a[3] = hi.y;
+    }
+    __device__ __forceinline__ static void ldg(const __nv_bfloat16* p, float (&a)[4]) {
+        const uint2 u = __ldg(reinterpret_cast<const uint2*>(p));
+        const float2 lo = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&u.x));
+        const float2 hi = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&u.y));
+        a[0] = lo.x; a[1] = lo.y; a[2] = hi.x; a[3] = hi.y;
+    }
+    __device__ __forceinline__ static void st(__nv_bfloat16* p, const float (&a)[4]) {
+        const __nv_bfloat162 lo = __floats2bfloat162_rn(a[0], a[1]), hi = __floats2bfloat162_rn(a[2], a[3]);
+        uint2 u;
+        u.x = *reinterpret_cast<const unsigned*>(&lo);
+        u.y = *reinterpret_cast<const unsigned*>(&hi);
+        *reinterpret_cast<uint2*>(p) = u;
+    }
+};
+
+// Scalar conversions between the storage and compute types.
+__device__ __forceinline__ float to_c(float v) { return v; }
+__device__ __forceinline__ double to_c(double v) { return v; }
+__device__ __forceinline__ float to_c(__half v) { return __half2float(v); }
+__device__ __forceinline__ float to_c(__nv_bfloat16 v) { return __bfloat162float(v); }
+__device__ __forceinline__ void put(float& d, float v) { d = v; }
+__device__ __forceinline__ void put(double& d, double v) { d = v; }
+__device__ __forceinline__ void put(__half& d, float v) { d = __float2half_rn(v); }
+__device__ __forceinline__ void put(__nv_bfloat16& d, float v) { d = __float2bfloat16_rn(v); }
+// FP64 host value -> storage type (set-up and field writes)
+template <typename S> __device__ __forceinline__ S from_d(double v);
+template <> __device__ __forceinline__ float from_d<float>(double v) { return float(v); }
+template <> __device__ __forceinline__ double from_d<double>(double v) { return v; }
+template <> __device__ __forceinline__ __half from_d<__half>(double v) { return __double2half(v); }
+template <> __device__ __forceinline__ __nv_bfloat16 from_d<__nv_bfloat16>(double v) { return __double2bfloat16(v); }
+
+// CPML: d_eff = d / kappa + psi.  With 16-bit storage psi is kept as psi * dx_min (the host
+// folds dx_min into the recursion's c coefficient) so it stays in the storage's range, and
+// is scaled back here by psc = 1 / dx_min; with S = T psi is stored as is.
+template <typename S, typename T>
+__device__ __forceinline__ T psi_eff(T d, T ik, T psi, T psc) {
+    if constexpr (sizeof(S) == sizeof(T)) return d * ik + psi;
+    else return d * ik + psi * psc;
+}
+
 // Per gain region constants (TwoLevelParams after finalize_with_dt), in compute type T.
+// With scaled field storage (E = sE * E', H = sH * H') kapaN0 and inv_hbar_omega carry
+// the factor sE and dp_scale = 1 / sH; unscaled storage has sE = sH = 1.
 template <typename T>
 struct GainCoef {
     T kapaN0;          // kapa_coeff * Ndip
@@ -66,22 +147,24 @@ struct GainCoef {
     T inv_N0;          // 1 / Ng0
     T N0;
     T dt, inv_tau, inv_hbar_omega, pump;
+    T dp_scale;        // 1 / sH: dP/dt enters the scaled Ez update as dP * dp_scale
     int clamp;         // TLS_ENABLE_CLAMP renormalisation
     int active;        // Ndip > 0
 };
 
-template <typename T>
+// Fields and CPML psi are stored as S, everything else as T.
+template <typename S, typename T = S>
 struct StepArgs {
     int NxT, NyT, NzT, NxP, np;
     long long plane;  // NxP * NyT
-    T *Ex, *Ey, *Ez, *Hx, *Hy, *Hz;
+    S *Ex, *Ey, *Ez, *Hx, *Hy, *Hz;
     const T *bEx, *bEy, *bEz;
     T bH;
     const T *idx, *idy, *idz;         // 1/dx (padded to NxP), 1/dy, 1/dz
     const T *ik[3];                   // 1/kappa per axis
     const T *pbE[3], *pcE[3], *pbH[3], *pcH[3];
     // psi_H: 0 Hx_y, 1 Hx_z, 2 Hy_z, 3 Hy_x, 4 Hz_x, 5 Hz_y ; psi_E likewise for E
-    T *psiH[6], *psiE[6];
+    S *psiH[6], *psiE[6];
     // gain block: bounding box of the gain cells, x-fastest with row length gX
     int gain, gi0, gj0, gk0, gX, gY, gZ;
     const int8_t* greg;               // region id per bbox cell, -1 = none
@@ -89,6 +172,7 @@ struct StepArgs {
     T *Nu, *Ng;
     const GainCoef<T>* gcoef;
     const unsigned* status;           // nonzero: a monitor step failed, skip all work
+    T psc;                            // psi scale (16-bit storage: 1 / dx_min; else 1)
 };
 
 // Per-step arguments of the E kernel.
@@ -105,8 +189,8 @@ __device__ __forceinline__ int slab_index(int n, int N, int np) { return n < np 
 // x-slab psi ([k][j][2 np]) of one W-cell vector.  Both arrays are read before any psi
 // store is issued: the compiler may not move a load of one psi array above a store to the
 // other, and a read-after-store chain per cell would cost one memory round trip each.
-template <typename T>
-__device__ __forceinline__ void xpsi_load(const T* p3, const T* p4, const StepArgs<T>& a, int k, int j, int i0,
+template <typename S, typename T>
+__device__ __forceinline__ void xpsi_load(const S* p3, const S* p4, const StepArgs<S, T>& a, int k, int j, int i0,
                                           T (&x3)[Vec<T>::W], T (&x4)[Vec<T>::W]) {
     const size_t row = (size_t(k) * a.NyT + j) * (2 * a.np);
 #pragma unroll
@@ -114,14 +198,14 @@ __device__ __forceinline__ void xpsi_load(const T* p3, const T* p4, const StepAr
         const int i = i0 + e;
         const bool in = i < a.NxT && in_pml(i, a.NxT, a.np);
         const size_t q = row + (in ? slab_index(i, a.NxT, a.np) : 0);
-        x3[e] = in ? p3[q] : T(0);
-        x4[e] = in ? p4[q] : T(0);
+        x3[e] = in ? T(to_c(p3[q])) : T(0);
+        x4[e] = in ? T(to_c(p4[q])) : T(0);
     }
 }
 
 // Writes back the x-slab psi of the cells ilo <= i < ihi of the vector.
-template <typename T>
-__device__ __forceinline__ void xpsi_store(T* p3, T* p4, const StepArgs<T>& a, int k, int j, int i0, int ilo, int ihi,
+template <typename S, typename T>
+__device__ __forceinline__ void xpsi_store(S* p3, S* p4, const StepArgs<S, T>& a, int k, int j, int i0, int ilo, int ihi,
                                            const T (&x3)[Vec<T>::W], const T (&x4)[Vec<T>::W]) {
     const size_t row = (size_t(k) * a.NyT + j) * (2 * a.np);
 #pragma unroll
@@ -129,8 +213,8 @@ __device__ __forceinline__ void xpsi_store(T* p3, T* p4, const StepArgs<T>& a, i
         const int i = i0 + e;
         if (i >= ilo && i < ihi && in_pml(i, a.NxT, a.np)) {
             const size_t q = row + slab_index(i, a.NxT, a.np);
-            p3[q] = x3[e];
-            p4[q] = x4[e];
+            put(p3[q], x3[e]);
+            put(p4[q], x4[e]);
         }
     }
 }
@@ -147,8 +231,8 @@ __device__ __forceinline__ bool src_in_vector(const ESrc& src, int i0, int j, in
 // updated.  Same operations in the same order as the general update with psi, J and dP/dt
 // absent; the general path carries per-cell tests that cost more issue slots than the
 // arithmetic itself, and about 85 % of the cells of a CPML-bounded grid are plain.
-template <typename T>
-__device__ __forceinline__ void h_plain(const StepArgs<T>& a, const size_t c, const T (&ex0)[Vec<T>::W],
+template <typename S, typename T>
+__device__ __forceinline__ void h_plain(const StepArgs<S, T>& a, const size_t c, const T (&ex0)[Vec<T>::W],
                                         const T (&ex1)[Vec<T>::W], const T (&ey0)[Vec<T>::W],
                                         const T (&ey1)[Vec<T>::W], const T (&ez)[Vec<T>::W],
                                         const T (&exj)[Vec<T>::W], const T (&ezj)[Vec<T>::W], const T eyn,
@@ -170,13 +254,13 @@ __device__ __forceinline__ void h_plain(const StepArgs<T>& a, const size_t c, co
         hy[e] = hy[e] - bH * (dEx_dz - dEz_dx);
         hz[e] = hz[e] - bH * (dEy_dx - dEx_dy);
     }
-    Vec<T>::st(a.Hx + c, hx);
-    Vec<T>::st(a.Hy + c, hy);
-    Vec<T>::st(a.Hz + c, hz);
+    Fld<S, T>::st(a.Hx + c, hx);
+    Fld<S, T>::st(a.Hy + c, hy);
+    Fld<S, T>::st(a.Hz + c, hz);
 }
 
-template <typename T>
-__device__ __forceinline__ void e_plain(const StepArgs<T>& a, const size_t c, T (&ex)[Vec<T>::W], T (&ey)[Vec<T>::W],
+template <typename S, typename T>
+__device__ __forceinline__ void e_plain(const StepArgs<S, T>& a, const size_t c, T (&ex)[Vec<T>::W], T (&ey)[Vec<T>::W],
                                         T (&ez)[Vec<T>::W], const T (&bx)[Vec<T>::W], const T (&by)[Vec<T>::W],
                                         const T (&bz)[Vec<T>::W], const T (&hx)[Vec<T>::W],
                                         const T (&hy)[Vec<T>::W], const T (&hz)[Vec<T>::W],
@@ -198,9 +282,9 @@ __device__ __forceinline__ void e_plain(const StepArgs<T>& a, const size_t c, T 
         ey[e] = ey[e] + by[e] * (dHx_dz - dHz_dx);
         ez[e] = ez[e] + bz[e] * (dHy_dx - dHx_dy);
     }
-    Vec<T>::st(a.Ex + c, ex);
-    Vec<T>::st(a.Ey + c, ey);
-    Vec<T>::st(a.Ez + c, ez);
+    Fld<S, T>::st(a.Ex + c, ex);
+    Fld<S, T>::st(a.Ey + c, ey);
+    Fld<S, T>::st(a.Ez + c, ez);
 }
 
 // ---------------------------------------------------------------------------------
@@ -222,8 +306,8 @@ struct SweepGeom {
 // 1/dz, the CPML psi of the vector) is issued before the first use of any of them, so a
 // vector costs one memory round trip per plane whatever slab it lies in.  EDGE columns
 // read the x-neighbour from memory (lanes hold other rows); interior columns shuffle it.
-template <typename T, bool EDGE>
-__device__ __forceinline__ void h_column(const StepArgs<T>& a, const SweepGeom& g, const int j, const int i0,
+template <typename S, typename T, bool EDGE>
+__device__ __forceinline__ void h_column(const StepArgs<S, T>& a, const SweepGeom& g, const int j, const int i0,
                                          const bool act, const int kb, const int ke, const int lane) {
     constexpr int W = Vec<T>::W;
     const int np = a.np, np2 = 2 * np;
@@ -246,8 +330,8 @@ __device__ __forceinline__ void h_column(const StepArgs<T>& a, const SweepGeom& 
     const size_t row = size_t(j) * a.NxP + i0;
     T ex0[W], ey0[W];
     if (act) {
-        Vec<T>::ldg(a.Ex + size_t(kb) * a.plane + row, ex0);
-        Vec<T>::ldg(a.Ey + size_t(kb) * a.plane + row, ey0);
+        Fld<S, T>::ldg(a.Ex + size_t(kb) * a.plane + row, ex0);
+        Fld<S, T>::ldg(a.Ey + size_t(kb) * a.plane + row, ey0);
     } else {
 #pragma unroll
         for (int e = 0; e < W; ++e) ex0[e] = ey0[e] = T(0);
@@ -257,20 +341,20 @@ __device__ __forceinline__ void h_column(const StepArgs<T>& a, const SweepGeom& 
         const size_t c = size_t(k) * a.plane + row;
         T ex1[W], ey1[W], ez[W], exj[W], ezj[W], hx[W], hy[W], hz[W];
         if (act) {
-            Vec<T>::ldg(a.Ex + c + a.plane, ex1);
-            Vec<T>::ldg(a.Ey + c + a.plane, ey1);
-            Vec<T>::ldg(a.Ez + c, ez);
-            Vec<T>::ldg(a.Ex + c + a.NxP, exj);
-            Vec<T>::ldg(a.Ez + c + a.NxP, ezj);
-            Vec<T>::ld(a.Hx + c, hx);
-            Vec<T>::ld(a.Hy + c, hy);
-            Vec<T>::ld(a.Hz + c, hz);
+            Fld<S, T>::ldg(a.Ex + c + a.plane, ex1);
+            Fld<S, T>::ldg(a.Ey + c + a.plane, ey1);
+            Fld<S, T>::ldg(a.Ez + c, ez);
+            Fld<S, T>::ldg(a.Ex + c + a.NxP, exj);
+            Fld<S, T>::ldg(a.Ez + c + a.NxP, ezj);
+            Fld<S, T>::ld(a.Hx + c, hx);
+            Fld<S, T>::ld(a.Hy + c, hy);
+            Fld<S, T>::ld(a.Hz + c, hz);
         } else {
 #pragma unroll
             for (int e = 0; e < W; ++e) ex1[e] = ey1[e] = ez[e] = exj[e] = ezj[e] = hx[e] = hy[e] = hz[e] = T(0);
         }
         T eye = T(0), eze = T(0);
-        if (nload && act && i0 + W < a.NxT) { eye = __ldg(a.Ey + c + W); eze = __ldg(a.Ez + c + W); }
+        if (nload && act && i0 + W < a.NxT) { eye = to_c(a.Ey[c + W]); eze = to_c(a.Ez[c + W]); }
         const T idz = __ldg(a.idz + k);
         const bool zpml = in_pml(k, a.NzT, np);
         T zb = 1, zc = 0, zik = 1;
@@ -279,14 +363,14 @@ __device__ __forceinline__ void h_column(const StepArgs<T>& a, const SweepGeom& 
         if (zpml) {
             zb = __ldg(a.pbH[2] + k); zc = __ldg(a.pcH[2] + k); zik = __ldg(a.ik[2] + k);
             zs = (size_t(slab_index(k, a.NzT, np)) * a.NyT + j) * a.NxP + i0;
-            if (act) { Vec<T>::ld(a.psiH[1] + zs, pxz); Vec<T>::ld(a.psiH[2] + zs, pyz); }
+            if (act) { Fld<S, T>::ld(a.psiH[1] + zs, pxz); Fld<S, T>::ld(a.psiH[2] + zs, pyz); }
         }
         if (ypml) {
             ys = (size_t(k) * np2 + jy) * a.NxP + i0;
-            if (act) { Vec<T>::ld(a.psiH[0] + ys, pxy); Vec<T>::ld(a.psiH[5] + ys, pzy); }
+            if (act) { Fld<S, T>::ld(a.psiH[0] + ys, pxy); Fld<S, T>::ld(a.psiH[5] + ys, pzy); }
         }
         T x3[W], x4[W];  // psi Hy_x, Hz_x
-        if (xpml) xpsi_load(a.psiH[3], a.psiH[4], a, k, j, i0, x3, x4);
+        if (xpml) xpsi_load<S, T>(a.psiH[3], a.psiH[4], a, k, j, i0, x3, x4);
         // x-neighbour at i0+W: the next lane's first cell, or the loaded one
         T eyn = eye, ezn = eze;
         if (!EDGE) {
@@ -295,7 +379,7 @@ __device__ __forceinline__ void h_column(const StepArgs<T>& a, const SweepGeom& 
             if (!nload) { eyn = sy; ezn = sz; }
         }
         if (plain_row && !zpml) {
-            h_plain(a, c, ex0, ex1, ey0, ey1, ez, exj, ezj, eyn, ezn, hx, hy, hz, idx, idy, idz);
+            h_plain<S, T>(a, c, ex0, ex1, ey0, ey1, ez, exj, ezj, eyn, ezn, hx, hy, hz, idx, idy, idz);
 #pragma unroll
             for (int e = 0; e < W; ++e) { ex0[e] = ex1[e]; ey0[e] = ey1[e]; }
             continue;
@@ -313,31 +397,31 @@ __device__ __forceinline__ void h_column(const StepArgs<T>& a, const SweepGeom& 
             T dEy_dx = (eyx - ey0[e]) * idx[e];
             T dEx_dy = (exj[e] - ex0[e]) * idy;
             if (ypml) {
-                pxy[e] = yb * pxy[e] + yc * dEz_dy; dEz_dy = dEz_dy * yik + pxy[e];
-                pzy[e] = yb * pzy[e] + yc * dEx_dy; dEx_dy = dEx_dy * yik + pzy[e];
+                pxy[e] = yb * pxy[e] + yc * dEz_dy; dEz_dy = psi_eff<S, T>(dEz_dy, yik, pxy[e], a.psc);
+                pzy[e] = yb * pzy[e] + yc * dEx_dy; dEx_dy = psi_eff<S, T>(dEx_dy, yik, pzy[e], a.psc);
             }
             if (zpml) {
-                pxz[e] = zb * pxz[e] + zc * dEy_dz; dEy_dz = dEy_dz * zik + pxz[e];
-                pyz[e] = zb * pyz[e] + zc * dEx_dz; dEx_dz = dEx_dz * zik + pyz[e];
+                pxz[e] = zb * pxz[e] + zc * dEy_dz; dEy_dz = psi_eff<S, T>(dEy_dz, zik, pxz[e], a.psc);
+                pyz[e] = zb * pyz[e] + zc * dEx_dz; dEx_dz = psi_eff<S, T>(dEx_dz, zik, pyz[e], a.psc);
             }
             if (xpml && in_pml(i, a.NxT, np)) {
                 const T b = __ldg(a.pbH[0] + i), cc = __ldg(a.pcH[0] + i), ik = __ldg(a.ik[0] + i);
                 x3[e] = b * x3[e] + cc * dEz_dx;
-                dEz_dx = dEz_dx * ik + x3[e];
+                dEz_dx = psi_eff<S, T>(dEz_dx, ik, x3[e], a.psc);
                 x4[e] = b * x4[e] + cc * dEy_dx;
-                dEy_dx = dEy_dx * ik + x4[e];
+                dEy_dx = psi_eff<S, T>(dEy_dx, ik, x4[e], a.psc);
             }
             hx[e] = hx[e] - bH * (dEz_dy - dEy_dz);
             hy[e] = hy[e] - bH * (dEx_dz - dEz_dx);
             hz[e] = hz[e] - bH * (dEy_dx - dEx_dy);
         }
         if (act) {
-            Vec<T>::st(a.Hx + c, hx);
-            Vec<T>::st(a.Hy + c, hy);
-            Vec<T>::st(a.Hz + c, hz);
-            if (zpml) { Vec<T>::st(a.psiH[1] + zs, pxz); Vec<T>::st(a.psiH[2] + zs, pyz); }
-            if (ypml) { Vec<T>::st(a.psiH[0] + ys, pxy); Vec<T>::st(a.psiH[5] + ys, pzy); }
-            if (xpml) xpsi_store(a.psiH[3], a.psiH[4], a, k, j, i0, 0, a.NxT - 1, x3, x4);
+            Fld<S, T>::st(a.Hx + c, hx);
+            Fld<S, T>::st(a.Hy + c, hy);
+            Fld<S, T>::st(a.Hz + c, hz);
+            if (zpml) { Fld<S, T>::st(a.psiH[1] + zs, pxz); Fld<S, T>::st(a.psiH[2] + zs, pyz); }
+            if (ypml) { Fld<S, T>::st(a.psiH[0] + ys, pxy); Fld<S, T>::st(a.psiH[5] + ys, pzy); }
+            if (xpml) xpsi_store<S, T>(a.psiH[3], a.psiH[4], a, k, j, i0, 0, a.NxT - 1, x3, x4);
         }
 #pragma unroll
         for (int e = 0; e < W; ++e) { ex0[e] = ex1[e]; ey0[e] = ey1[e]; }
@@ -345,9 +429,9 @@ __device__ __forceinline__ void h_column(const StepArgs<T>& a, const SweepGeom& 
 }
 
 // Two resident blocks per SM (at most 128 registers; a third block would spill).
-template <typename T>
+template <typename S, typename T>
 __global__ void __launch_bounds__(32 * kBlockY, 2)
-k_update_H(const StepArgs<T> a, const int kchunk, const SweepGeom g) {
+k_update_H(const StepArgs<S, T> a, const int kchunk, const SweepGeom g) {
     constexpr int W = Vec<T>::W;
     if (*a.status) return;
     const int lane = threadIdx.x;
@@ -358,7 +442,7 @@ k_update_H(const StepArgs<T> a, const int kchunk, const SweepGeom g) {
         const int j = blockIdx.y * kBlockY + threadIdx.y;
         if (j >= a.NyT - 1) return;  // whole warp: a warp is one row
         const int i0 = g.xi0 + (blockIdx.x * 32 + lane) * W;
-        h_column<T, false>(a, g, j, i0, i0 < g.xi1, kb, ke, lane);
+        h_column<S, T, false>(a, g, j, i0, i0 < g.xi1, kb, ke, lane);
     } else {
         const int t = threadIdx.y * 32 + lane;
         const int rr = t / g.ne, v = t - rr * g.ne;
@@ -366,13 +450,13 @@ k_update_H(const StepArgs<T> a, const int kchunk, const SweepGeom g) {
         if (rr >= g.er || j >= a.NyT - 1) return;
         const int i0 = v < g.nl ? v * W : g.xi1 + (v - g.nl) * W;
         if (i0 >= a.NxT) return;
-        h_column<T, true>(a, g, j, i0, true, kb, ke, lane);
+        h_column<S, T, true>(a, g, j, i0, true, kb, ke, lane);
     }
 }
 
 // ---------------------------------------------------------------------------------
-template <typename T, bool EDGE>
-__device__ __forceinline__ void e_column(const StepArgs<T>& a, const SweepGeom& g, const ESrc& src, const int j,
+template <typename S, typename T, bool EDGE>
+__device__ __forceinline__ void e_column(const StepArgs<S, T>& a, const SweepGeom& g, const ESrc& src, const int j,
                                          const int i0, const bool act, const int kb, const int ke, const int lane) {
     constexpr int W = Vec<T>::W;
     const int np = a.np, np2 = 2 * np;
@@ -397,8 +481,8 @@ __device__ __forceinline__ void e_column(const StepArgs<T>& a, const SweepGeom& 
     const size_t row = size_t(j) * a.NxP + i0;
     T hxm[W], hym[W];  // Hx, Hy at k-1
     if (act) {
-        Vec<T>::ldg(a.Hx + size_t(kb - 1) * a.plane + row, hxm);
-        Vec<T>::ldg(a.Hy + size_t(kb - 1) * a.plane + row, hym);
+        Fld<S, T>::ldg(a.Hx + size_t(kb - 1) * a.plane + row, hxm);
+        Fld<S, T>::ldg(a.Hy + size_t(kb - 1) * a.plane + row, hym);
     } else {
 #pragma unroll
         for (int e = 0; e < W; ++e) hxm[e] = hym[e] = T(0);
@@ -408,24 +492,24 @@ __device__ __forceinline__ void e_column(const StepArgs<T>& a, const SweepGeom& 
         const size_t c = size_t(k) * a.plane + row;
         T ex[W], ey[W], ez[W], bx[W], by[W], bz[W], hx[W], hy[W], hz[W], hzj[W], hxj[W];
         if (act) {
-            Vec<T>::ld(a.Ex + c, ex);
-            Vec<T>::ld(a.Ey + c, ey);
-            Vec<T>::ld(a.Ez + c, ez);
+            Fld<S, T>::ld(a.Ex + c, ex);
+            Fld<S, T>::ld(a.Ey + c, ey);
+            Fld<S, T>::ld(a.Ez + c, ez);
             Vec<T>::ldg(a.bEx + c, bx);
             Vec<T>::ldg(a.bEy + c, by);
             Vec<T>::ldg(a.bEz + c, bz);
-            Vec<T>::ldg(a.Hx + c, hx);
-            Vec<T>::ldg(a.Hy + c, hy);
-            Vec<T>::ldg(a.Hz + c, hz);
-            Vec<T>::ldg(a.Hz + c - a.NxP, hzj);
-            Vec<T>::ldg(a.Hx + c - a.NxP, hxj);
+            Fld<S, T>::ldg(a.Hx + c, hx);
+            Fld<S, T>::ldg(a.Hy + c, hy);
+            Fld<S, T>::ldg(a.Hz + c, hz);
+            Fld<S, T>::ldg(a.Hz + c - a.NxP, hzj);
+            Fld<S, T>::ldg(a.Hx + c - a.NxP, hxj);
         } else {
 #pragma unroll
             for (int e = 0; e < W; ++e)
                 ex[e] = ey[e] = ez[e] = bx[e] = by[e] = bz[e] = hx[e] = hy[e] = hz[e] = hzj[e] = hxj[e] = T(0);
         }
         T hze = T(0), hye = T(0);
-        if (pload && act && i0 > 0) { hze = __ldg(a.Hz + c - 1); hye = __ldg(a.Hy + c - 1); }
+        if (pload && act && i0 > 0) { hze = to_c(a.Hz[c - 1]); hye = to_c(a.Hy[c - 1]); }
         const T idz = __ldg(a.idz + k);
         const bool zpml = in_pml(k, a.NzT, np);
         T zb = 1, zc = 0, zik = 1;
@@ -434,14 +518,14 @@ __device__ __forceinline__ void e_column(const StepArgs<T>& a, const SweepGeom& 
         if (zpml) {
             zb = __ldg(a.pbE[2] + k); zc = __ldg(a.pcE[2] + k); zik = __ldg(a.ik[2] + k);
             zs = (size_t(slab_index(k, a.NzT, np)) * a.NyT + j) * a.NxP + i0;
-            if (act) { Vec<T>::ld(a.psiE[1] + zs, pxz); Vec<T>::ld(a.psiE[2] + zs, pyz); }
+            if (act) { Fld<S, T>::ld(a.psiE[1] + zs, pxz); Fld<S, T>::ld(a.psiE[2] + zs, pyz); }
         }
         if (ypml) {
             ys = (size_t(k) * np2 + jy) * a.NxP + i0;
-            if (act) { Vec<T>::ld(a.psiE[0] + ys, pxy); Vec<T>::ld(a.psiE[5] + ys, pzy); }
+            if (act) { Fld<S, T>::ld(a.psiE[0] + ys, pxy); Fld<S, T>::ld(a.psiE[5] + ys, pzy); }
         }
         T x3[W], x4[W];  // psi Ey_x, Ez_x
-        if (xpml) xpsi_load(a.psiE[3], a.psiE[4], a, k, j, i0, x3, x4);
+        if (xpml) xpsi_load<S, T>(a.psiE[3], a.psiE[4], a, k, j, i0, x3, x4);
         // x-neighbour at i0-1: the previous lane's last cell, or the loaded one
         T hzp = hze, hyp = hye;
         if (!EDGE) {
@@ -451,7 +535,7 @@ __device__ __forceinline__ void e_column(const StepArgs<T>& a, const SweepGeom& 
         }
         const bool gplane = grow && k >= a.gk0 && k < a.gk0 + a.gZ;
         if (plain_row && !zpml && !gplane && !src_in_vector(src, i0, j, k, W)) {
-            e_plain(a, c, ex, ey, ez, bx, by, bz, hx, hy, hz, hzj, hxj, hxm, hym, hzp, hyp, idx, idy, idz);
+            e_plain<S, T>(a, c, ex, ey, ez, bx, by, bz, hx, hy, hz, hzj, hxj, hxm, hym, hzp, hyp, idx, idy, idz);
 #pragma unroll
             for (int e = 0; e < W; ++e) { hxm[e] = hx[e]; hym[e] = hy[e]; }
             continue;
@@ -469,19 +553,19 @@ __device__ __forceinline__ void e_column(const StepArgs<T>& a, const SweepGeom& 
             T dHy_dx = (hy[e] - hyx) * idx[e];
             T dHx_dy = (hx[e] - hxj[e]) * idy;
             if (ypml) {
-                pxy[e] = yb * pxy[e] + yc * dHz_dy; dHz_dy = dHz_dy * yik + pxy[e];
-                pzy[e] = yb * pzy[e] + yc * dHx_dy; dHx_dy = dHx_dy * yik + pzy[e];
+                pxy[e] = yb * pxy[e] + yc * dHz_dy; dHz_dy = psi_eff<S, T>(dHz_dy, yik, pxy[e], a.psc);
+                pzy[e] = yb * pzy[e] + yc * dHx_dy; dHx_dy = psi_eff<S, T>(dHx_dy, yik, pzy[e], a.psc);
             }
             if (zpml) {
-                pxz[e] = zb * pxz[e] + zc * dHy_dz; dHy_dz = dHy_dz * zik + pxz[e];
-                pyz[e] = zb * pyz[e] + zc * dHx_dz; dHx_dz = dHx_dz * zik + pyz[e];
+                pxz[e] = zb * pxz[e] + zc * dHy_dz; dHy_dz = psi_eff<S, T>(dHy_dz, zik, pxz[e], a.psc);
+                pyz[e] = zb * pyz[e] + zc * dHx_dz; dHx_dz = psi_eff<S, T>(dHx_dz, zik, pyz[e], a.psc);
             }
             if (xpml && in_pml(i, a.NxT, np)) {
                 const T b = __ldg(a.pbE[0] + i), cc = __ldg(a.pcE[0] + i), ik = __ldg(a.ik[0] + i);
                 x3[e] = b * x3[e] + cc * dHz_dx;
-                dHz_dx = dHz_dx * ik + x3[e];
+                dHz_dx = psi_eff<S, T>(dHz_dx, ik, x3[e], a.psc);
                 x4[e] = b * x4[e] + cc * dHy_dx;
-                dHy_dx = dHy_dx * ik + x4[e];
+                dHy_dx = psi_eff<S, T>(dHy_dx, ik, x4[e], a.psc);
             }
             T Jx = 0, Jy = 0, Jz = 0;
             for (int s = 0; s < src.n; ++s) {
@@ -509,7 +593,7 @@ __device__ __forceinline__ void e_column(const StepArgs<T>& a, const SweepGeom& 
                 const T ng_frac = (Ng - Nu) * g.inv_N0;
                 const T Pn = g.kapaN0 * (ng_frac * ez_old) + g.pa2 * P + g.pa3 * Pp;
                 const T dP = (Pn - P) * g.inv_dt;
-                ez[e] = ez[e] + bz[e] * (((dHy_dx - dHx_dy) - Jz) - dP);
+                ez[e] = ez[e] + bz[e] * (((dHy_dx - dHx_dy) - Jz) - dP * g.dp_scale);
                 const T e_avg = T(0.5) * (ez[e] + ez_old);
                 const T stim = e_avg * (Pn - P) * g.inv_dt * g.inv_hbar_omega;
                 T dNu = -g.inv_tau * Nu + stim;
@@ -533,21 +617,21 @@ __device__ __forceinline__ void e_column(const StepArgs<T>& a, const SweepGeom& 
             }
         }
         if (act) {
-            Vec<T>::st(a.Ex + c, ex);
-            Vec<T>::st(a.Ey + c, ey);
-            Vec<T>::st(a.Ez + c, ez);
-            if (zpml) { Vec<T>::st(a.psiE[1] + zs, pxz); Vec<T>::st(a.psiE[2] + zs, pyz); }
-            if (ypml) { Vec<T>::st(a.psiE[0] + ys, pxy); Vec<T>::st(a.psiE[5] + ys, pzy); }
-            if (xpml) xpsi_store(a.psiE[3], a.psiE[4], a, k, j, i0, 1, a.NxT, x3, x4);
+            Fld<S, T>::st(a.Ex + c, ex);
+            Fld<S, T>::st(a.Ey + c, ey);
+            Fld<S, T>::st(a.Ez + c, ez);
+            if (zpml) { Fld<S, T>::st(a.psiE[1] + zs, pxz); Fld<S, T>::st(a.psiE[2] + zs, pyz); }
+            if (ypml) { Fld<S, T>::st(a.psiE[0] + ys, pxy); Fld<S, T>::st(a.psiE[5] + ys, pzy); }
+            if (xpml) xpsi_store<S, T>(a.psiE[3], a.psiE[4], a, k, j, i0, 1, a.NxT, x3, x4);
         }
 #pragma unroll
         for (int e = 0; e < W; ++e) { hxm[e] = hx[e]; hym[e] = hy[e]; }
     }
 }
 
-template <typename T>
+template <typename S, typename T>
 __global__ void __launch_bounds__(32 * kBlockY, 2)
-k_update_E(const StepArgs<T> a, const int kchunk, const ESrc src, const SweepGeom g) {
+k_update_E(const StepArgs<S, T> a, const int kchunk, const ESrc src, const SweepGeom g) {
     constexpr int W = Vec<T>::W;
     if (*a.status) return;
     const int lane = threadIdx.x;
@@ -558,7 +642,7 @@ k_update_E(const StepArgs<T> a, const int kchunk, const ESrc src, const SweepGeo
         const int j = blockIdx.y * kBlockY + threadIdx.y;
         if (j < 1 || j >= a.NyT) return;  // E is updated for j >= 1 only; whole warp
         const int i0 = g.xi0 + (blockIdx.x * 32 + lane) * W;
-        e_column<T, false>(a, g, src, j, i0, i0 < g.xi1, kb, ke, lane);
+        e_column<S, T, false>(a, g, src, j, i0, i0 < g.xi1, kb, ke, lane);
     } else {
         const int t = threadIdx.y * 32 + lane;
         const int rr = t / g.ne, v = t - rr * g.ne;
@@ -566,7 +650,7 @@ k_update_E(const StepArgs<T> a, const int kchunk, const ESrc src, const SweepGeo
         if (rr >= g.er || j < 1 || j >= a.NyT) return;
         const int i0 = v < g.nl ? v * W : g.xi1 + (v - g.nl) * W;
         if (i0 >= a.NxT) return;
-        e_column<T, true>(a, g, src, j, i0, true, kb, ke, lane);
+        e_column<S, T, true>(a, g, src, j, i0, true, kb, ke, lane);
     }
 }
 

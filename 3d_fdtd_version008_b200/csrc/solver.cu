@@ -17,6 +17,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <type_traits>
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
@@ -31,9 +32,10 @@ namespace fdtdk {
 // ================================================================ small kernels
 // idx3 (z fastest, FP64) <-> device layout (x fastest, padded), 32x32 tiles over (k, i)
 // for each j.
-template <typename T>
-__global__ void k_from_idx3(const double* __restrict__ src, T* __restrict__ dst, int NxT, int NyT, int NzT,
-                            int NxP) {
+// dst = scale * src (the storage's field scale), converted to the storage type D.
+template <typename D>
+__global__ void k_from_idx3(const double* __restrict__ src, D* __restrict__ dst, int NxT, int NyT, int NzT,
+                            int NxP, double scale) {
     __shared__ double tile[32][33];
     const int j = blockIdx.z;
     const int k0 = blockIdx.x * 32, i0 = blockIdx.y * 32;
@@ -44,18 +46,19 @@ __global__ void k_from_idx3(const double* __restrict__ src, T* __restrict__ dst,
     __syncthreads();
     for (int r = threadIdx.y; r < 32; r += blockDim.y) {
         const int k = k0 + r, i = i0 + threadIdx.x;
-        if (i < NxT && k < NzT) dst[(size_t(k) * NyT + j) * NxP + i] = T(tile[threadIdx.x][r]);
+        if (i < NxT && k < NzT) dst[(size_t(k) * NyT + j) * NxP + i] = from_d<D>(tile[threadIdx.x][r] * scale);
     }
 }
 
-template <typename T>
-__global__ void k_to_idx3(const T* __restrict__ src, double* __restrict__ dst, int NxT, int NyT, int NzT, int NxP) {
+template <typename D>
+__global__ void k_to_idx3(const D* __restrict__ src, double* __restrict__ dst, int NxT, int NyT, int NzT, int NxP,
+                          double scale) {
     __shared__ double tile[32][33];
     const int j = blockIdx.z;
     const int k0 = blockIdx.x * 32, i0 = blockIdx.y * 32;
     for (int r = threadIdx.y; r < 32; r += blockDim.y) {
         const int k = k0 + r, i = i0 + threadIdx.x;
-        tile[threadIdx.x][r] = (i < NxT && k < NzT) ? double(src[(size_t(k) * NyT + j) * NxP + i]) : 0.0;
+        tile[threadIdx.x][r] = (i < NxT && k < NzT) ? double(to_c(src[(size_t(k) * NyT + j) * NxP + i])) * scale : 0.0;
     }
     __syncthreads();
     for (int r = threadIdx.y; r < 32; r += blockDim.y) {
@@ -84,10 +87,11 @@ struct ProbeDev {
     int comp;
 };
 
-template <typename T>
-__device__ double probe_value(const StepArgs<T>& a, const ProbeDev& p) {
+// Probe value in physical units: stored E and H times their field scales es, hs.
+template <typename S, typename T>
+__device__ double probe_value(const StepArgs<S, T>& a, const ProbeDev& p, double es, double hs) {
     const size_t o = size_t(p.off);
-    auto v = [&](const T* f) { return double(f[o]); };
+    auto v = [&](const S* f) { return double(to_c(f[o])) * ((f == a.Ex || f == a.Ey || f == a.Ez) ? es : hs); };
     switch (p.comp) {
         case 0: return v(a.Ex);
         case 1: return v(a.Ey);
@@ -113,16 +117,16 @@ __device__ double probe_value(const StepArgs<T>& a, const ProbeDev& p) {
 // Point probes after the E update of step n: sample (every save_every steps) and the
 // FP64 DFT accumulation X_m += v * exp(-i 2 pi f_m t) * dt at t = (n+1) dt.
 // One thread per (probe, frequency).
-template <typename T>
-__global__ void k_probe_dft(const StepArgs<T> a, const ProbeDev* __restrict__ probes, int nprobes,
+template <typename S, typename T>
+__global__ void k_probe_dft(const StepArgs<S, T> a, const ProbeDev* __restrict__ probes, int nprobes,
                             const double* __restrict__ freqs, int nf, double* __restrict__ dft,
-                            double* __restrict__ series, long long sample, double t, double dt) {
+                            double* __restrict__ series, long long sample, double t, double dt, double es, double hs) {
     if (*a.status) return;
     const int per = nf > 0 ? nf : 1;
     const int tid = blockIdx.x * blockDim.x + threadIdx.x;
     if (tid >= nprobes * per) return;
     const int p = tid / per, m = tid % per;
-    const double v = probe_value(a, probes[p]);
+    const double v = probe_value(a, probes[p], es, hs);
     if (m == 0 && sample >= 0) series[size_t(sample) * nprobes + p] = v;
     if (nf > 0) {
         double s, c;
@@ -200,10 +204,10 @@ __device__ void block_commit(DiagAccum* acc, double mE, double mP, unsigned fl, 
 // calculate_conservation_error (:155-170), compute_integrated_Nu/Ng and
 // compute_polarization_energy (src/two_level_system.hpp:344-418) over the fields after
 // the step.  Field arrays are scanned as flat padded arrays (padding holds zeros).
-template <typename T>
-__global__ void k_monitor_reduce(const StepArgs<T> a, size_t nflat, const double* __restrict__ dxs,
+template <typename S, typename T>
+__global__ void k_monitor_reduce(const StepArgs<S, T> a, size_t nflat, const double* __restrict__ dxs,
                                  const double* __restrict__ dys, const double* __restrict__ dzs, int parity_next,
-                                 DiagAccum* acc) {
+                                 DiagAccum* acc, double es) {
     if (*a.status) return;
     double mE = 0.0, mP = 0.0, s0 = 0, s1 = 0, s2 = 0, s3 = 0, s4 = 0;
     unsigned fl = 0;
@@ -213,11 +217,11 @@ __global__ void k_monitor_reduce(const StepArgs<T> a, size_t nflat, const double
     for (size_t v = blockIdx.x * size_t(blockDim.x) + threadIdx.x; v < nflat / W; v += stride) {
         const size_t t = v * W;
         T ex[W], ey[W], ez[W], hx[W], hy[W], hz[W];
-        Vec<T>::ldg(a.Ex + t, ex); Vec<T>::ldg(a.Ey + t, ey); Vec<T>::ldg(a.Ez + t, ez);
-        Vec<T>::ldg(a.Hx + t, hx); Vec<T>::ldg(a.Hy + t, hy); Vec<T>::ldg(a.Hz + t, hz);
+        Fld<S, T>::ldg(a.Ex + t, ex); Fld<S, T>::ldg(a.Ey + t, ey); Fld<S, T>::ldg(a.Ez + t, ez);
+        Fld<S, T>::ldg(a.Hx + t, hx); Fld<S, T>::ldg(a.Hy + t, hy); Fld<S, T>::ldg(a.Hz + t, hz);
 #pragma unroll
         for (int e = 0; e < W; ++e) {
-            const double x = double(ex[e]), y = double(ey[e]), z = double(ez[e]);
+            const double x = double(ex[e]) * es, y = double(ey[e]) * es, z = double(ez[e]) * es;
             if (!isfinite(x) || !isfinite(y) || !isfinite(z)) fl |= 1u;
             else mE = fmax(mE, fmax(fabs(x), fmax(fabs(y), fabs(z))));
             if (!isfinite(double(hx[e])) || !isfinite(double(hy[e])) || !isfinite(double(hz[e]))) fl |= 2u;
@@ -243,7 +247,7 @@ __global__ void k_monitor_reduce(const StepArgs<T> a, size_t nflat, const double
             const double dV = dxs[i] * dys[j] * dzs[k];
             s2 += Nu * dV;
             s3 += Ng * dV;
-            const double ez = double(a.Ez[(size_t(k) * a.NyT + j) * a.NxP + i]);
+            const double ez = double(to_c(a.Ez[(size_t(k) * a.NyT + j) * a.NxP + i])) * es;
             s4 += -0.5 * P * ez * dV;
         }
     }
@@ -322,7 +326,10 @@ public:
     int device = 0;
 };
 
-template <typename T>
+// Fields and CPML psi stored as S, arithmetic in T (S = T for FP32 / FP64; S = __half or
+// __nv_bfloat16 with T = float for the 16-bit storage forms, whose stored values are
+// E' = E / sE and H' = H / sH).
+template <typename S, typename T>
 class Solver final : public SolverBase {
 public:
     explicit Solver(const fdtd_setup_v1& s, int dev);
@@ -339,6 +346,7 @@ public:
     void set_timing(int mode) override;
     void set_path(int path) override {
         if (path != 0 && path != 1) throw Failure(FDTD_ERR_INVALID, "kernel path must be 0 (fused) or 1 (two-sweep)");
+        if (path == 0 && !std::is_same_v<S, T>) throw Failure(FDTD_ERR_UNSUPPORTED, "the fused path needs FP32 or FP64 storage");
         if (steps != 0) throw Failure(FDTD_ERR_INVALID, "the kernel path can only change before the first step");
         path_ = path;
     }
@@ -368,13 +376,14 @@ private:
     void h2d(const double* h, double* d, size_t n);
     void d2h(const double* d, double* h, size_t n);
     void upload_gain_box(const double* idx3, const std::vector<int8_t>& reg, T* dst);
-    void to_device(const double* host_idx3, T* dst);
-    void from_device(const T* src, double* host_idx3);
+    template <typename D> void to_device(const double* host_idx3, D* dst, double scale = 1.0);
+    template <typename D> void from_device(const D* src, double* host_idx3, double scale = 1.0);
     void ensure_series(uint64_t samples);
 
     cudaStream_t st_ = nullptr;
     std::vector<void*> ptrs_;
-    StepArgs<T> a_{};
+    StepArgs<S, T> a_{};
+    double sE_ = 1.0, sH_ = 1.0;  // stored fields are E / sE_ and H / sH_
     int NxT_, NyT_, NzT_, NxP_, np_;
     size_t plane_, nflat_;
     int kchunkH_ = 1, kchunkE_ = 1;
@@ -401,8 +410,8 @@ private:
     // the latest state); path 1 (default, measured faster on B200): k_update_H +
     // k_update_E in place on buffer 0.
     int path_ = 1, cur_ = 0;
-    T* fld_[2][6] = {};
-    T* psiH_[2][6] = {};
+    S* fld_[2][6] = {};
+    S* psiH_[2][6] = {};
     FusedMaps maps_[2];
     int kchunkF_ = 1;
     dim3 gridF_;
@@ -420,25 +429,47 @@ private:
     fdtd_timing_v1 tm_{};
 };
 
-template <typename T>
-Solver<T>::Solver(const fdtd_setup_v1& s, int dev) {
+template <typename S, typename T>
+Solver<S, T>::Solver(const fdtd_setup_v1& s, int dev) {
     device = dev;
     ck(cudaSetDevice(dev), "cudaSetDevice");
     ck(cudaStreamCreateWithFlags(&st_, cudaStreamNonBlocking), "cudaStreamCreate");
     constexpr int W = Vec<T>::W;
     NxT_ = int(s.NxT); NyT_ = int(s.NyT); NzT_ = int(s.NzT);
     np_ = int(s.npml);
-    NxP_ = int(round_up(size_t(NxT_), 128 / sizeof(T)));
+    NxP_ = int(round_up(size_t(NxT_), 128 / sizeof(S)));
+    if constexpr (!std::is_same_v<S, T>) {
+        // 16-bit storage: E' = E / sE, H' = H / sH with sH = sE / eta0 so that E' and H' have
+        // the same magnitude.  FP16 needs sE near the field peak (its range ends at 65504 and
+        // its normal numbers at 6e-5): the estimate tau |I0| / (eps0 cell_area) -- the field a
+        // dipole's current would build in its cell over one pulse width without radiating --
+        // overshoots the peak by one to two decades, so sE is that over 64, as a power of two.
+        // BF16 has FP32's range: sE = 1.
+        double sE = s.field_scale;
+        if (!(sE > 0.0)) {
+            sE = 1.0;
+            if (std::is_same_v<S, __half>) {
+                double est = 0.0;
+                for (uint32_t q = 0; q < s.n_dipoles; ++q) {
+                    const fdtd_dipole_v1& d = s.dipoles[q];
+                    if (d.cell_area > 0) est = std::max(est, d.tau * std::fabs(d.I0) / (8.8541878128e-12 * d.cell_area));
+                }
+                if (est > 0) sE = std::exp2(std::round(std::log2(est / 64.0)));
+            }
+        }
+        sE_ = sE;
+        sH_ = sE / 376.730313668;
+    }
     plane_ = size_t(NxP_) * NyT_;
     nflat_ = plane_ * NzT_;
     dt_ = s.dt;
     const size_t N = size_t(NxT_) * NyT_ * NzT_;
 
-    StepArgs<T>& a = a_;
+    StepArgs<S, T>& a = a_;
     a.NxT = NxT_; a.NyT = NyT_; a.NzT = NzT_; a.NxP = NxP_; a.np = np_;
     a.plane = (long long)plane_;
     // buffer 1 (fields and psi_H) exists only for the fused path, made at its first step
-    for (int c = 0; c < 6; ++c) fld_[0][c] = alloc<T>(nflat_);
+    for (int c = 0; c < 6; ++c) fld_[0][c] = alloc<S>(nflat_);
     point_args_at(0);
 
     // bH must be uniform and aE = aH = 1 (sigma = 0, mu_r = 1).
@@ -455,11 +486,11 @@ Solver<T>::Solver(const fdtd_setup_v1& s, int dev) {
         if (s.aH[c] && !all_equal(s.aH[c], 1.0)) throw Failure(FDTD_ERR_UNSUPPORTED, "aH != 1 (magnetic loss) is not supported");
         if (s.bH[c] && !all_equal(s.bH[c], bH)) throw Failure(FDTD_ERR_UNSUPPORTED, "non-uniform bH (mu_r != 1) is not supported");
     }
-    a.bH = T(bH);
+    a.bH = T(bH * (sE_ / sH_));
     T* be[3];
     for (int c = 0; c < 3; ++c) {
         be[c] = alloc<T>(nflat_);
-        to_device(s.bE[c], be[c]);
+        to_device(s.bE[c], be[c], sH_ / sE_);
     }
     a.bEx = be[0]; a.bEy = be[1]; a.bEz = be[2];
 
@@ -469,6 +500,14 @@ Solver<T>::Solver(const fdtd_setup_v1& s, int dev) {
     for (int j = 0; j < NyT_; ++j) idy[j] = T(s.inv_dy[j]);
     for (int k = 0; k < NzT_; ++k) idz[k] = T(s.inv_dz[k]);
     a.idx = upload(idx); a.idy = upload(idy); a.idz = upload(idz);
+    // 16-bit storage keeps psi * dx_min (psi is a field derivative); full precision keeps psi
+    double psi_dx = 1.0;
+    if constexpr (!std::is_same_v<S, T>) {
+        psi_dx = *std::min_element(s.dx, s.dx + NxT_);
+        psi_dx = std::min(psi_dx, *std::min_element(s.dy, s.dy + NyT_));
+        psi_dx = std::min(psi_dx, *std::min_element(s.dz, s.dz + NzT_));
+    }
+    a.psc = T(1.0 / psi_dx);
     const int Ns[3] = {NxT_, NyT_, NzT_};
     for (int ax = 0; ax < 3; ++ax) {
         const int n = Ns[ax];
@@ -476,8 +515,8 @@ Solver<T>::Solver(const fdtd_setup_v1& s, int dev) {
         std::vector<T> ik(len, T(1)), bE(len, T(1)), cE(len, T(0)), bHp(len, T(1)), cH(len, T(0));
         for (int q = 0; q < n; ++q) {
             ik[q] = T(1.0 / s.cpml_kappa[ax][q]);
-            bE[q] = T(s.cpml_bE[ax][q]); cE[q] = T(s.cpml_cE[ax][q]);
-            bHp[q] = T(s.cpml_bH[ax][q]); cH[q] = T(s.cpml_cH[ax][q]);
+            bE[q] = T(s.cpml_bE[ax][q]); cE[q] = T(s.cpml_cE[ax][q] * psi_dx);
+            bHp[q] = T(s.cpml_bH[ax][q]); cH[q] = T(s.cpml_cH[ax][q] * psi_dx);
         }
         a.ik[ax] = upload(ik);
         a.pbE[ax] = upload(bE); a.pcE[ax] = upload(cE);
@@ -492,8 +531,8 @@ Solver<T>::Solver(const fdtd_setup_v1& s, int dev) {
         const size_t sz[6] = {ys, zs, zs, xs, xs, ys};
         for (int q = 0; q < 6; ++q) {
             psi_sz_[q] = sz[q];
-            psiH_[0][q] = alloc<T>(sz[q]);
-            a.psiE[q] = alloc<T>(sz[q]);
+            psiH_[0][q] = alloc<S>(sz[q]);
+            a.psiE[q] = alloc<S>(sz[q]);
             a.psiH[q] = psiH_[0][q];
         }
     }
@@ -542,13 +581,14 @@ Solver<T>::Solver(const fdtd_setup_v1& s, int dev) {
             for (uint32_t r = 0; r < s.n_tls_regions; ++r) {
                 const fdtd_tls_region_v1& R = s.tls_regions[r];
                 GainCoef<T>& g = gc[r];
-                g.kapaN0 = T(R.kapa_coeff * R.N0);
+                g.kapaN0 = T(R.kapa_coeff * R.N0 * sE_);
                 g.pa2 = T(R.pa2); g.pa3 = T(R.pa3); g.inv_dt = T(R.inv_dt);
                 g.inv_N0 = T(R.N0 > 0 ? 1.0 / R.N0 : 0.0);
                 g.N0 = T(R.N0);
                 g.dt = T(s.dt);
                 g.inv_tau = T(1.0 / R.tau);
-                g.inv_hbar_omega = T(1.0 / (R.hbar * R.omega_a));
+                g.inv_hbar_omega = T(sE_ / (R.hbar * R.omega_a));
+                g.dp_scale = T(1.0 / sH_);
                 g.pump = T(R.pump_rate);
                 g.clamp = R.enable_population_clamp;
                 g.active = R.N0 > 0 ? 1 : 0;
@@ -567,6 +607,7 @@ Solver<T>::Solver(const fdtd_setup_v1& s, int dev) {
         if (d.polarization < 0 || d.polarization > 5) throw Failure(FDTD_ERR_INVALID, "source polarization must be 0..5");
         dip_.push_back(d);
     }
+
 
     // probes / DFT
     save_every_ = std::max<uint32_t>(1, s.save_every);
@@ -629,8 +670,8 @@ Solver<T>::Solver(const fdtd_setup_v1& s, int dev) {
     ck(cudaStreamSynchronize(st_), "setup upload");
 }
 
-template <typename T>
-void Solver<T>::point_args_at(int buf) {
+template <typename S, typename T>
+void Solver<S, T>::point_args_at(int buf) {
     a_.Ex = fld_[buf][0]; a_.Ey = fld_[buf][1]; a_.Ez = fld_[buf][2];
     a_.Hx = fld_[buf][3]; a_.Hy = fld_[buf][4]; a_.Hz = fld_[buf][5];
 }
@@ -652,24 +693,24 @@ PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
 // row and plane strides are multiples of 128 bytes.
 // First step of the fused path: the second field / psi_H buffer starts as a copy of the
 // first, then the tensor maps over both are encoded.
-template <typename T>
-void Solver<T>::ensure_fused() {
+template <typename S, typename T>
+void Solver<S, T>::ensure_fused() {
     if (fused_ready_) return;
     for (int c = 0; c < 6; ++c) {
-        fld_[1][c] = alloc<T>(nflat_, false);
-        ck(cudaMemcpyAsync(fld_[1][c], fld_[0][c], nflat_ * sizeof(T), cudaMemcpyDeviceToDevice, st_), "field copy");
+        fld_[1][c] = alloc<S>(nflat_, false);
+        ck(cudaMemcpyAsync(fld_[1][c], fld_[0][c], nflat_ * sizeof(S), cudaMemcpyDeviceToDevice, st_), "field copy");
     }
     for (int q = 0; q < 6; ++q) {
         if (!psiH_[0][q]) continue;
-        psiH_[1][q] = alloc<T>(psi_sz_[q], false);
-        ck(cudaMemcpyAsync(psiH_[1][q], psiH_[0][q], psi_sz_[q] * sizeof(T), cudaMemcpyDeviceToDevice, st_), "psi copy");
+        psiH_[1][q] = alloc<S>(psi_sz_[q], false);
+        ck(cudaMemcpyAsync(psiH_[1][q], psiH_[0][q], psi_sz_[q] * sizeof(S), cudaMemcpyDeviceToDevice, st_), "psi copy");
     }
     build_fused();
     fused_ready_ = true;
 }
 
-template <typename T>
-void Solver<T>::build_fused() {
+template <typename S, typename T>
+void Solver<S, T>::build_fused() {
     const char* env = std::getenv("FDTD_B200_FUSED_SHAPE");
     shapeF_ = env ? std::atoi(env) : 0;
     if (shapeF_ == 1) setup_fused<typename ShapeSet<T>::S1>();
@@ -677,10 +718,10 @@ void Solver<T>::build_fused() {
     else { shapeF_ = 0; setup_fused<typename ShapeSet<T>::S0>(); }
 }
 
-template <typename T>
+template <typename S, typename T>
 template <typename Shape>
-void Solver<T>::setup_fused() {
-    using S = FusedSmem<T, Shape>;
+void Solver<S, T>::setup_fused() {
+    using SM = FusedSmem<T, Shape>;
     auto enc = tensor_map_encoder();
     auto make = [&](const T* base, int bx, int by) {
         CUtensorMap m;
@@ -698,12 +739,12 @@ void Solver<T>::setup_fused() {
     const T* bE[3] = {a_.bEx, a_.bEy, a_.bEz};
     for (int b = 0; b < 2; ++b) {
         for (int c = 0; c < 3; ++c) {
-            maps_[b].E[c] = make(fld_[b][c], S::PX, S::PY);
-            maps_[b].H[c] = make(fld_[b][3 + c], S::PX, S::PY);
-            maps_[b].B[c] = make(bE[c], S::TX, S::TY);
+            maps_[b].E[c] = make(fld_[b][c], SM::PX, SM::PY);
+            maps_[b].H[c] = make(fld_[b][3 + c], SM::PX, SM::PY);
+            maps_[b].B[c] = make(bE[c], SM::TX, SM::TY);
         }
     }
-    smemF_ = sizeof(S);
+    smemF_ = sizeof(SM);
     threadsF_ = Shape::THREADS;
     launchF_ = &launch_fused<T, Shape>;
     ck(cudaFuncSetAttribute(k_step_fused<T, Shape>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smemF_)),
@@ -713,7 +754,7 @@ void Solver<T>::setup_fused() {
        "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
     ck(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device), "cudaDeviceGetAttribute");
     if (per_sm < 1) throw Failure(FDTD_ERR_CUDA, "fused step kernel does not fit on an SM");
-    const int gx = (NxT_ + S::TX - 1) / S::TX, gy = (NyT_ + S::TY - 1) / S::TY;
+    const int gx = (NxT_ + SM::TX - 1) / SM::TX, gy = (NyT_ + SM::TY - 1) / SM::TY;
     // z-chunks: about 8 waves of resident blocks, chunks of at least 32 planes
     const int resident = sms * per_sm;
     const int want = std::max(1, (resident * 8 + gx * gy - 1) / (gx * gy));
@@ -722,8 +763,8 @@ void Solver<T>::setup_fused() {
     gridF_ = dim3(gx, gy, (NzT_ + kchunkF_ - 1) / kchunkF_);
 }
 
-template <typename T>
-void Solver<T>::set_timing(int mode) {
+template <typename S, typename T>
+void Solver<S, T>::set_timing(int mode) {
     if (mode < FDTD_TIMING_OFF || mode > FDTD_TIMING_KERNELS) throw Failure(FDTD_ERR_INVALID, "bad timing mode");
     ck(cudaSetDevice(device), "cudaSetDevice");
     if (mode != FDTD_TIMING_OFF && !ev_[0])
@@ -732,8 +773,8 @@ void Solver<T>::set_timing(int mode) {
     tm_ = fdtd_timing_v1{};
 }
 
-template <typename T>
-Solver<T>::~Solver() {
+template <typename S, typename T>
+Solver<S, T>::~Solver() {
     cudaSetDevice(device);
     if (st_) cudaStreamSynchronize(st_);
     for (auto& e : ev_) if (e) cudaEventDestroy(e);
@@ -746,8 +787,8 @@ Solver<T>::~Solver() {
     if (st_) cudaStreamDestroy(st_);
 }
 
-template <typename T>
-double* Solver<T>::staging() {
+template <typename S, typename T>
+double* Solver<S, T>::staging() {
     if (!d_stage_) {
         ck(cudaMalloc(&d_stage_, size_t(NxT_) * NyT_ * NzT_ * sizeof(double)), "cudaMalloc staging");
         dev_bytes += size_t(NxT_) * NyT_ * NzT_ * sizeof(double);
@@ -755,8 +796,8 @@ double* Solver<T>::staging() {
     return d_stage_;
 }
 
-template <typename T>
-void Solver<T>::ensure_pinned() {
+template <typename S, typename T>
+void Solver<S, T>::ensure_pinned() {
     for (int b = 0; b < 2; ++b) {
         if (!pin_[b]) ck(cudaHostAlloc(&pin_[b], kPinBytes, cudaHostAllocDefault), "cudaHostAlloc");
         if (!pin_ev_[b]) ck(cudaEventCreateWithFlags(&pin_ev_[b], cudaEventDisableTiming), "cudaEventCreate");
@@ -774,8 +815,8 @@ static void par_copy(void* dst, const void* src, size_t bytes) {
     }
 }
 
-template <typename T>
-void Solver<T>::h2d(const double* h, double* d, size_t n) {
+template <typename S, typename T>
+void Solver<S, T>::h2d(const double* h, double* d, size_t n) {
     ensure_pinned();
     const size_t chunk = kPinBytes / sizeof(double);
     for (size_t off = 0, it = 0; off < n; off += chunk, ++it) {
@@ -788,8 +829,8 @@ void Solver<T>::h2d(const double* h, double* d, size_t n) {
     }
 }
 
-template <typename T>
-void Solver<T>::d2h(const double* d, double* h, size_t n) {
+template <typename S, typename T>
+void Solver<S, T>::d2h(const double* d, double* h, size_t n) {
     ensure_pinned();
     const size_t chunk = kPinBytes / sizeof(double);
     const size_t nch = (n + chunk - 1) / chunk;
@@ -809,8 +850,8 @@ void Solver<T>::d2h(const double* d, double* h, size_t n) {
 
 // Initial gain state: the bounding box is cut out of the idx3 array on the host (cells
 // outside the gain regions hold 0, as k_gain_block stores them) and only the box is copied.
-template <typename T>
-void Solver<T>::upload_gain_box(const double* h, const std::vector<int8_t>& reg, T* dst) {
+template <typename S, typename T>
+void Solver<S, T>::upload_gain_box(const double* h, const std::vector<int8_t>& reg, T* dst) {
     const int gX = a_.gX, gY = a_.gY, gZ = a_.gZ;
     std::vector<T> box(size_t(gX) * gY * gZ);
 #pragma omp parallel for schedule(static)
@@ -825,50 +866,52 @@ void Solver<T>::upload_gain_box(const double* h, const std::vector<int8_t>& reg,
     ck(cudaStreamSynchronize(st_), "gain box");
 }
 
-template <typename T>
-void Solver<T>::to_device(const double* h, T* dst) {
+template <typename S, typename T>
+template <typename D>
+void Solver<S, T>::to_device(const double* h, D* dst, double scale) {
     if (!h) throw Failure(FDTD_ERR_INVALID, "null host array");
     double* sbuf = staging();
     h2d(h, sbuf, size_t(NxT_) * NyT_ * NzT_);
     dim3 g((NzT_ + 31) / 32, (NxT_ + 31) / 32, NyT_), b(32, 8);
-    k_from_idx3<T><<<g, b, 0, st_>>>(sbuf, dst, NxT_, NyT_, NzT_, NxP_);
+    k_from_idx3<D><<<g, b, 0, st_>>>(sbuf, dst, NxT_, NyT_, NzT_, NxP_, scale);
     ++launches;
     ck(cudaGetLastError(), "k_from_idx3");
     ck(cudaStreamSynchronize(st_), "to_device");
 }
 
-template <typename T>
-void Solver<T>::from_device(const T* src, double* h) {
+template <typename S, typename T>
+template <typename D>
+void Solver<S, T>::from_device(const D* src, double* h, double scale) {
     if (!h) throw Failure(FDTD_ERR_INVALID, "null host array");
     double* sbuf = staging();
     dim3 g((NzT_ + 31) / 32, (NxT_ + 31) / 32, NyT_), b(32, 8);
-    k_to_idx3<T><<<g, b, 0, st_>>>(src, sbuf, NxT_, NyT_, NzT_, NxP_);
+    k_to_idx3<D><<<g, b, 0, st_>>>(src, sbuf, NxT_, NyT_, NzT_, NxP_, scale);
     ++launches;
     ck(cudaGetLastError(), "k_to_idx3");
     d2h(sbuf, h, size_t(NxT_) * NyT_ * NzT_);
     ck(cudaStreamSynchronize(st_), "from_device");
 }
 
-template <typename T>
-void Solver<T>::set_field(int comp, const double* h) {
+template <typename S, typename T>
+void Solver<S, T>::set_field(int comp, const double* h) {
     if (comp < 0 || comp > 5) throw Failure(FDTD_ERR_INVALID, "component must be 0..5");
     // Both buffers of the fused path: cells the reference never updates must hold the same
     // value in each.
-    to_device(h, fld_[cur_][comp]);
+    to_device(h, fld_[cur_][comp], 1.0 / (comp < 3 ? sE_ : sH_));
     if (fused_ready_)
-        ck(cudaMemcpyAsync(fld_[1 - cur_][comp], fld_[cur_][comp], nflat_ * sizeof(T), cudaMemcpyDeviceToDevice, st_),
+        ck(cudaMemcpyAsync(fld_[1 - cur_][comp], fld_[cur_][comp], nflat_ * sizeof(S), cudaMemcpyDeviceToDevice, st_),
            "field copy");
     ck(cudaStreamSynchronize(st_), "set_field");
 }
 
-template <typename T>
-void Solver<T>::get_field(int comp, double* h) {
+template <typename S, typename T>
+void Solver<S, T>::get_field(int comp, double* h) {
     if (comp < 0 || comp > 5) throw Failure(FDTD_ERR_INVALID, "component must be 0..5");
-    from_device(fld_[cur_][comp], h);
+    from_device(fld_[cur_][comp], h, comp < 3 ? sE_ : sH_);
 }
 
-template <typename T>
-void Solver<T>::set_tls(int which, const double* h) {
+template <typename S, typename T>
+void Solver<S, T>::set_tls(int which, const double* h) {
     if (which < 0 || which > 3) throw Failure(FDTD_ERR_INVALID, "which must be FDTD_TLS_*");
     if (!has_gain_) throw Failure(FDTD_ERR_INVALID, "solve has no gain region");
     T* dst = which == FDTD_TLS_PZ ? ((steps & 1) ? a_.P1 : a_.P0)
@@ -882,8 +925,8 @@ void Solver<T>::set_tls(int which, const double* h) {
     ck(cudaStreamSynchronize(st_), "set_tls");
 }
 
-template <typename T>
-void Solver<T>::get_tls(int which, double* h) {
+template <typename S, typename T>
+void Solver<S, T>::get_tls(int which, double* h) {
     if (which < 0 || which > 3) throw Failure(FDTD_ERR_INVALID, "which must be FDTD_TLS_*");
     const size_t N = size_t(NxT_) * NyT_ * NzT_;
     std::memset(h, 0, N * sizeof(double));
@@ -900,8 +943,8 @@ void Solver<T>::get_tls(int which, double* h) {
     ck(cudaStreamSynchronize(st_), "get_tls");
 }
 
-template <typename T>
-void Solver<T>::ensure_series(uint64_t samples) {
+template <typename S, typename T>
+void Solver<S, T>::ensure_series(uint64_t samples) {
     if (nprobes_ == 0 || samples <= series_cap_) return;
     uint64_t cap = std::max<uint64_t>(samples, series_cap_ * 2);
     double* d = nullptr;
@@ -917,10 +960,12 @@ void Solver<T>::ensure_series(uint64_t samples) {
     series_cap_ = cap;
 }
 
-template <typename T>
-void Solver<T>::run(uint64_t n) {
+template <typename S, typename T>
+void Solver<S, T>::run(uint64_t n) {
     ck(cudaSetDevice(device), "cudaSetDevice");
-    if (path_ == 0) ensure_fused();
+    if constexpr (std::is_same_v<S, T>) {
+        if (path_ == 0) ensure_fused();
+    }
     const uint64_t n0 = steps;
     const uint64_t last = n0 + n;  // exclusive
     ensure_series((last + save_every_ - 1) / save_every_);
@@ -938,10 +983,14 @@ void Solver<T>::run(uint64_t n) {
         src.parity = int(s & 1);
         for (int q = 0; q < src.n; ++q) {
             const fdtd_dipole_v1& d = dip_[q];
-            src.J[q] = fdtd::current_density(d.waveform, s, dt_, d.I0, d.f0, d.tau, d.t0, d.t_shift, d.cell_area);
+            src.J[q] = fdtd::current_density(d.waveform, s, dt_, d.I0, d.f0, d.tau, d.t0, d.t_shift, d.cell_area) *
+                       (1.0 / sH_);
         }
         if (per_kernel) ck(cudaEventRecord(ev_[0], st_), "cudaEventRecord");
-        if (path_ == 0) {
+        bool fused_step = false;
+        if constexpr (std::is_same_v<S, T>) fused_step = path_ == 0;
+        if (fused_step) {
+            if constexpr (std::is_same_v<S, T>) {
             FusedArgs<T> fa;
             fa.a = a_;
             for (int q = 0; q < 6; ++q) {
@@ -955,22 +1004,24 @@ void Solver<T>::run(uint64_t n) {
             cur_ = 1 - cur_;
             point_args_at(cur_);
             launches += 1;
+            }
         } else {
-            k_update_H<T><<<gridH_, blk, 0, st_>>>(a_, kchunkH_, geom_);
+            k_update_H<S, T><<<gridH_, blk, 0, st_>>>(a_, kchunkH_, geom_);
             if (per_kernel) ck(cudaEventRecord(ev_[1], st_), "cudaEventRecord");
-            k_update_E<T><<<gridE_, blk, 0, st_>>>(a_, kchunkE_, src, geom_);
+            k_update_E<S, T><<<gridE_, blk, 0, st_>>>(a_, kchunkE_, src, geom_);
             launches += 2;
         }
         if (per_kernel) ck(cudaEventRecord(ev_[2], st_), "cudaEventRecord");
         if (nprobes_) {
             const long long sample = (s % save_every_ == 0) ? (long long)(s / save_every_) : -1;
-            k_probe_dft<T><<<(pthreads + 127) / 128, 128, 0, st_>>>(a_, d_probes_, int(nprobes_), d_freqs_, int(nf_),
-                                                                      d_dft_, d_series_, sample, double(s + 1) * dt_, dt_);
+            k_probe_dft<S, T><<<(pthreads + 127) / 128, 128, 0, st_>>>(a_, d_probes_, int(nprobes_), d_freqs_, int(nf_),
+                                                                         d_dft_, d_series_, sample, double(s + 1) * dt_, dt_,
+                                                                         sE_, sH_);
             ++launches;
             if (sample >= 0) series_count_ = uint64_t(sample) + 1;
         }
         if (interval_ && s % interval_ == 0) {
-            k_monitor_reduce<T><<<8 * 148, 256, 0, st_>>>(a_, nflat_, d_dx_, d_dy_, d_dz_, int((s + 1) & 1), d_acc_);
+            k_monitor_reduce<S, T><<<8 * 148, 256, 0, st_>>>(a_, nflat_, d_dx_, d_dy_, d_dz_, int((s + 1) & 1), d_acc_, sE_);
             k_monitor_eval<<<1, 1, 0, st_>>>(d_acc_, d_ms_, d_status_, s);
             launches += 2;
         }
@@ -1008,24 +1059,24 @@ void Solver<T>::run(uint64_t n) {
     steps = last;
 }
 
-template <typename T>
-void Solver<T>::probe_series(double* out, uint64_t max, uint64_t* n) {
+template <typename S, typename T>
+void Solver<S, T>::probe_series(double* out, uint64_t max, uint64_t* n) {
     const uint64_t cnt = std::min<uint64_t>(series_count_, max);
     if (n) *n = series_count_;
     if (cnt && nprobes_ && out)
         ck(cudaMemcpy(out, d_series_, cnt * nprobes_ * sizeof(double), cudaMemcpyDeviceToHost), "series D2H");
 }
 
-template <typename T>
-void Solver<T>::dft(uint32_t p, double* re, double* im) {
+template <typename S, typename T>
+void Solver<S, T>::dft(uint32_t p, double* re, double* im) {
     if (p >= nprobes_ || nf_ == 0) throw Failure(FDTD_ERR_INVALID, "no DFT for this probe");
     std::vector<double> buf(2 * size_t(nf_));
     ck(cudaMemcpy(buf.data(), d_dft_ + 2 * size_t(p) * nf_, buf.size() * sizeof(double), cudaMemcpyDeviceToHost), "dft D2H");
     for (uint32_t m = 0; m < nf_; ++m) { re[m] = buf[2 * m]; im[m] = buf[2 * m + 1]; }
 }
 
-template <typename T>
-void Solver<T>::diagnostics(fdtd_diagnostics_v1* d) {
+template <typename S, typename T>
+void Solver<S, T>::diagnostics(fdtd_diagnostics_v1* d) {
     MonitorState ms{};
     ck(cudaMemcpy(&ms, d_ms_, sizeof(ms), cudaMemcpyDeviceToHost), "monitor state");
     std::memset(d, 0, sizeof(*d));
@@ -1097,9 +1148,11 @@ int fdtd_create(const fdtd_setup_v1* s, int device, fdtd_handle** out) {
     if (device < 0 || device >= ndev) { g_err = "device index out of range"; return FDTD_ERR_INVALID; }
     auto* h = new fdtd_handle();
     const int rc = guarded(nullptr, [&] {
-        if (s->precision == FDTD_PREC_FP64) h->s = std::make_unique<Solver<double>>(*s, device);
-        else if (s->precision == FDTD_PREC_FP32) h->s = std::make_unique<Solver<float>>(*s, device);
-        else throw Failure(FDTD_ERR_UNSUPPORTED, "precision must be FDTD_PREC_FP32 or FDTD_PREC_FP64");
+        if (s->precision == FDTD_PREC_FP64) h->s = std::make_unique<Solver<double, double>>(*s, device);
+        else if (s->precision == FDTD_PREC_FP32) h->s = std::make_unique<Solver<float, float>>(*s, device);
+        else if (s->precision == FDTD_PREC_FP16) h->s = std::make_unique<Solver<__half, float>>(*s, device);
+        else if (s->precision == FDTD_PREC_BF16) h->s = std::make_unique<Solver<__nv_bfloat16, float>>(*s, device);
+        else throw Failure(FDTD_ERR_UNSUPPORTED, "precision must be FDTD_PREC_FP32, _FP64, _FP16 or _BF16");
     });
     if (rc != FDTD_OK) { delete h; return rc; }
     *out = h;

@@ -116,19 +116,22 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def algorithmic_bytes(setup, word: int):
-    """Compulsory bytes per step of the two-sweep algorithm (storage word `word` bytes).
+def algorithmic_bytes(setup, word: int, coef_word: int = 0):
+    """Compulsory bytes per step of the two-sweep algorithm: fields and psi stored in `word`
+    bytes, bE and gain state in `coef_word` bytes (default: the same).
 
-    H sweep: read E(3) H(3), write H(3) = 9 words/cell; E sweep: read H(3) E(3) bE(3), write
-    E(3) = 12 words/cell; + 2 words per active CPML psi (4 per axis, 2 per sweep) in that
-    axis' slab; + gain cells: read P^n, P^{n-1}, Nu, Ng and write P^{n+1}, Nu, Ng = 7 words."""
+    H sweep: read E(3) H(3), write H(3) = 9 field words/cell; E sweep: read H(3) E(3), write
+    E(3) = 9 field words + bE(3) coefficient words; + 2 field words per active CPML psi (4 per
+    axis, 2 per sweep) in that axis' slab; + gain cells: read P^n, P^{n-1}, Nu, Ng and write
+    P^{n+1}, Nu, Ng = 7 coefficient words."""
+    cw = coef_word or word
     NxT, NyT, NzT = setup.shape
     npml = int(setup.view.npml)
     cells = NxT * NyT * NzT
     slab = sum(2 * npml * (cells // n) for n in (NxT, NyT, NzT))  # cells inside each axis' slab, summed
     gain = int((setup.array("tls_region_map") >= 0).sum()) if setup.view.n_tls_regions else 0
     h = 9 * word * cells + 2 * 2 * word * slab
-    e = 12 * word * cells + 2 * 2 * word * slab + 7 * word * gain
+    e = 9 * word * cells + 3 * cw * cells + 2 * 2 * word * slab + 7 * cw * gain
     return {"cells": cells, "h_bytes": h, "e_bytes": e, "step_bytes": h + e,
             "per_cell": (h + e) / cells, "slab_cells": slab, "gain_cells": gain}
 
@@ -211,7 +214,8 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--workload", default="b512", choices=sorted(WORKLOADS))
     ap.add_argument("--fdtd-steps", type=int, default=10, help="time steps per bench step")
-    ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
+    ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64", "fp16", "bf16"],
+                    help="field storage; fp16/bf16 store E, H, psi in 16 bits and compute in FP32")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     args = ap.parse_args()
@@ -236,11 +240,12 @@ def main():
         print(json.dumps(line))
         return
 
-    prec = PKG.PREC_FP64 if args.precision == "fp64" else PKG.PREC_FP32
-    word = 8 if prec == PKG.PREC_FP64 else 4
+    prec = {"fp32": PKG.PREC_FP32, "fp64": PKG.PREC_FP64, "fp16": PKG.PREC_FP16, "bf16": PKG.PREC_BF16}[args.precision]
+    word = {"fp32": 4, "fp64": 8, "fp16": 2, "bf16": 2}[args.precision]
+    coef_word = 8 if prec == PKG.PREC_FP64 else 4
     setup = PKG.Setup.from_file(PKG.config_path(cfg))
     cells = setup.shape[0] * setup.shape[1] * setup.shape[2]
-    alg = algorithmic_bytes(setup, word)
+    alg = algorithmic_bytes(setup, word, coef_word)
 
     # ---------------------------------------------------------------- device-resident value
     sol = PKG.Solver(setup, device=local, precision=prec)
@@ -297,7 +302,7 @@ def main():
             m = setup.array("tls_region_map").reshape(setup.shape) >= 0
             box = int(np.prod([np.ptp(np.nonzero(m.any(axis=tuple(x for x in range(3) if x != ax)))[0]) + 1
                                for ax in range(3)]))
-            h2d += box * (2 * word + 1)
+            h2d += box * (2 * coef_word + 1)
             del m
         barrier(dist)
         t0 = time.perf_counter()
@@ -334,7 +339,7 @@ def main():
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
-        "dtype": "f32" if word == 4 else "f64",
+        "dtype": {"fp32": "f32", "fp64": "f64", "fp16": "f32 (fp16 storage)", "bf16": "f32 (bf16 storage)"}[args.precision],
         "data": "synthetic",
         "config": {"workload": desc, "config_file": cfg, "total_cells": cells, "grid": list(setup.shape),
                    "fdtd_steps_per_step": S, "parallelism": "replicas" if world > 1 else "single GPU",

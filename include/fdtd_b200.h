@@ -49,7 +49,10 @@ enum {
 /* ------------------------------------------------------------ enums */
 typedef enum {
     FDTD_PREC_FP32 = 0, /* fields, CPML psi and gain state stored and updated in FP32 */
-    FDTD_PREC_FP64 = 1  /* everything in FP64: the accuracy judge */
+    FDTD_PREC_FP64 = 1, /* everything in FP64: the accuracy judge */
+    FDTD_PREC_FP16 = 2, /* E, H, CPML psi stored in FP16 as E / sE, H / sH (sH = sE / eta0),
+                           arithmetic, material, gain state in FP32 */
+    FDTD_PREC_BF16 = 3  /* the same with BF16 storage */
 } fdtd_precision;
 
 /* Field / detector components: Detectors::FieldComponent (src/detectors/idetector.hpp:19-29). */
@@ -135,6 +138,9 @@ typedef struct fdtd_setup_v1 {
     /* StabilityMonitor thresholds (src/user_config.hpp:156-160); interval 0 disables */
     uint32_t monitor_interval;
     double max_E, max_P, conservation_err, growth_rate;
+    /* FP16 / BF16 storage: the E field scale sE (stored E' = E / sE); 0 = automatic (FP16: the
+     * dipoles' tau |I0| / (eps0 cell_area) rounded up to a power of two; BF16: 1) */
+    double field_scale;
 } fdtd_setup_v1;
 
 /* Diagnostics of the most recent monitor step, FP64 device reductions
