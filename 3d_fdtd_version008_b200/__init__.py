@@ -48,7 +48,11 @@ EXPORTED_SYMBOLS = (
     "fdtd_get_probe_series", "fdtd_get_dft", "fdtd_get_diagnostics", "fdtd_device_bytes",
     "fdtd_kernel_launches", "fdtd_set_timing", "fdtd_get_timing", "fdtd_set_kernel_path", "fdtd_synchronize", "fdtd_last_error",
     "fdtd_destroy", "fdtd_field_scan_noalloc",
+    "fdtd_batch_create", "fdtd_batch_submit", "fdtd_batch_run", "fdtd_batch_job_state",
+    "fdtd_batch_probe_series", "fdtd_batch_dft", "fdtd_batch_diagnostics", "fdtd_batch_release",
+    "fdtd_batch_last_error", "fdtd_batch_destroy",
 )
+JOB_QUEUED, JOB_RESIDENT, JOB_DONE, JOB_FAILED = 0, 1, 2, 3
 
 
 class FdtdError(RuntimeError):
@@ -157,6 +161,16 @@ def load_library() -> C.CDLL:
         "fdtd_last_error": (C.c_char_p, [vp]),
         "fdtd_destroy": (None, [vp]),
         "fdtd_field_scan_noalloc": (C.c_int, [C.c_int, vp, vp, vp, vp, vp, vp, C.c_uint64, vp, vp]),
+        "fdtd_batch_create": (C.c_int, [C.c_int, C.c_uint64, C.POINTER(vp)]),
+        "fdtd_batch_submit": (C.c_int, [vp, C.POINTER(SetupV1), C.c_uint64, C.POINTER(C.c_uint64)]),
+        "fdtd_batch_run": (C.c_int, [vp, C.c_uint64, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]),
+        "fdtd_batch_job_state": (C.c_int, [vp, C.c_uint64, C.POINTER(C.c_int), C.POINTER(C.c_uint64)]),
+        "fdtd_batch_probe_series": (C.c_int, [vp, C.c_uint64, _dptr, C.c_uint64, C.POINTER(C.c_uint64)]),
+        "fdtd_batch_dft": (C.c_int, [vp, C.c_uint64, C.c_uint32, _dptr, _dptr]),
+        "fdtd_batch_diagnostics": (C.c_int, [vp, C.c_uint64, C.POINTER(DiagnosticsV1)]),
+        "fdtd_batch_release": (C.c_int, [vp, C.c_uint64]),
+        "fdtd_batch_last_error": (C.c_char_p, [vp]),
+        "fdtd_batch_destroy": (None, [vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -337,6 +351,81 @@ class Solver:
         if getattr(self, "_h", None) is not None and self._h.value:
             load_library().fdtd_destroy(self._h)
             self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Batch:
+    """Packed multi-solve engine (fdtd_batch_*): FP32 solves queued on one GPU, admitted by
+    device footprint under `budget_bytes`, stepped together with one launch per sweep."""
+
+    def __init__(self, device: int = 0, budget_bytes: int = 150 << 30):
+        self._h = C.c_void_p()
+        self._keep = {}  # ticket -> (Setup, view): must outlive the job
+        rc = load_library().fdtd_batch_create(int(device), C.c_uint64(int(budget_bytes)), C.byref(self._h))
+        if rc != FDTD_OK:
+            raise FdtdError(rc, f"fdtd_batch_create: {load_library().fdtd_batch_last_error(None).decode()}")
+
+    def _check(self, rc: int, what: str):
+        if rc != FDTD_OK:
+            raise FdtdError(rc, f"{what}: {load_library().fdtd_batch_last_error(self._h).decode()}")
+
+    def submit(self, setup: Setup, n_steps: int, view: Optional[SetupV1] = None) -> int:
+        v = SetupV1.from_buffer_copy(view if view is not None else setup.view)
+        t = C.c_uint64()
+        self._check(load_library().fdtd_batch_submit(self._h, C.byref(v), C.c_uint64(int(n_steps)), C.byref(t)),
+                    "fdtd_batch_submit")
+        self._keep[t.value] = (setup, v)
+        return t.value
+
+    def run(self, max_steps: int):
+        r, q = C.c_uint32(), C.c_uint32()
+        self._check(load_library().fdtd_batch_run(self._h, C.c_uint64(int(max_steps)), C.byref(r), C.byref(q)),
+                    "fdtd_batch_run")
+        return r.value, q.value
+
+    def state(self, ticket: int):
+        st, n = C.c_int(), C.c_uint64()
+        self._check(load_library().fdtd_batch_job_state(self._h, C.c_uint64(ticket), C.byref(st), C.byref(n)),
+                    "fdtd_batch_job_state")
+        return st.value, n.value
+
+    def probe_series(self, ticket: int) -> np.ndarray:
+        n = C.c_uint64()
+        self._check(load_library().fdtd_batch_probe_series(self._h, C.c_uint64(ticket), None, 0, C.byref(n)),
+                    "fdtd_batch_probe_series")
+        npr = int(self._keep[ticket][1].n_probes)
+        out = np.zeros((n.value, max(npr, 1)))
+        self._check(load_library().fdtd_batch_probe_series(self._h, C.c_uint64(ticket), _as_dptr(out), n.value,
+                                                           C.byref(n)), "fdtd_batch_probe_series")
+        return out
+
+    def dft(self, ticket: int, probe: int = 0) -> np.ndarray:
+        nf = int(self._keep[ticket][1].n_dft_freqs)
+        re, im = np.zeros(nf), np.zeros(nf)
+        self._check(load_library().fdtd_batch_dft(self._h, C.c_uint64(ticket), probe, _as_dptr(re), _as_dptr(im)),
+                    "fdtd_batch_dft")
+        return re + 1j * im
+
+    def diagnostics(self, ticket: int) -> Dict[str, float]:
+        d = DiagnosticsV1()
+        self._check(load_library().fdtd_batch_diagnostics(self._h, C.c_uint64(ticket), C.byref(d)),
+                    "fdtd_batch_diagnostics")
+        return {name: getattr(d, name) for name, _ in DiagnosticsV1._fields_ if name != "reserved"}
+
+    def release(self, ticket: int) -> None:
+        self._check(load_library().fdtd_batch_release(self._h, C.c_uint64(ticket)), "fdtd_batch_release")
+        self._keep.pop(ticket, None)
+
+    def close(self) -> None:
+        if getattr(self, "_h", None) and self._h.value:
+            load_library().fdtd_batch_destroy(self._h)
+            self._h = C.c_void_p()
+        self._keep.clear()
 
     def __del__(self):
         try:

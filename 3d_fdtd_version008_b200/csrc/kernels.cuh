@@ -428,30 +428,37 @@ __device__ __forceinline__ void h_column(const StepArgs<S, T>& a, const SweepGeo
     }
 }
 
-// Two resident blocks per SM (at most 128 registers; a third block would spill).
+// One block of the H sweep: block (bx, by, bz) of the solve's launch grid.
 template <typename S, typename T>
-__global__ void __launch_bounds__(32 * kBlockY, 2)
-k_update_H(const StepArgs<S, T> a, const int kchunk, const SweepGeom g) {
+__device__ __forceinline__ void update_H_block(const StepArgs<S, T>& a, const int kchunk, const SweepGeom& g,
+                                               const int bx, const int by, const int bz) {
     constexpr int W = Vec<T>::W;
     if (*a.status) return;
     const int lane = threadIdx.x;
-    const int kb = blockIdx.z * kchunk;
+    const int kb = bz * kchunk;
     const int ke = min(kb + kchunk, a.NzT - 1);
     if (kb >= ke) return;
-    if (int(blockIdx.x) < g.gxi) {
-        const int j = blockIdx.y * kBlockY + threadIdx.y;
+    if (bx < g.gxi) {
+        const int j = by * kBlockY + threadIdx.y;
         if (j >= a.NyT - 1) return;  // whole warp: a warp is one row
-        const int i0 = g.xi0 + (blockIdx.x * 32 + lane) * W;
+        const int i0 = g.xi0 + (bx * 32 + lane) * W;
         h_column<S, T, false>(a, g, j, i0, i0 < g.xi1, kb, ke, lane);
     } else {
         const int t = threadIdx.y * 32 + lane;
         const int rr = t / g.ne, v = t - rr * g.ne;
-        const int j = blockIdx.y * g.er + rr;
+        const int j = by * g.er + rr;
         if (rr >= g.er || j >= a.NyT - 1) return;
         const int i0 = v < g.nl ? v * W : g.xi1 + (v - g.nl) * W;
         if (i0 >= a.NxT) return;
         h_column<S, T, true>(a, g, j, i0, true, kb, ke, lane);
     }
+}
+
+// Two resident blocks per SM (at most 128 registers; a third block would spill).
+template <typename S, typename T>
+__global__ void __launch_bounds__(32 * kBlockY, 2)
+k_update_H(const StepArgs<S, T> a, const int kchunk, const SweepGeom g) {
+    update_H_block<S, T>(a, kchunk, g, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 
 // ---------------------------------------------------------------------------------
@@ -630,28 +637,34 @@ __device__ __forceinline__ void e_column(const StepArgs<S, T>& a, const SweepGeo
 }
 
 template <typename S, typename T>
-__global__ void __launch_bounds__(32 * kBlockY, 2)
-k_update_E(const StepArgs<S, T> a, const int kchunk, const ESrc src, const SweepGeom g) {
+__device__ __forceinline__ void update_E_block(const StepArgs<S, T>& a, const int kchunk, const ESrc& src,
+                                               const SweepGeom& g, const int bx, const int by, const int bz) {
     constexpr int W = Vec<T>::W;
     if (*a.status) return;
     const int lane = threadIdx.x;
-    const int kb = max(int(blockIdx.z) * kchunk, 1);
-    const int ke = min(int(blockIdx.z) * kchunk + kchunk, a.NzT);
+    const int kb = max(bz * kchunk, 1);
+    const int ke = min(bz * kchunk + kchunk, a.NzT);
     if (kb >= ke) return;
-    if (int(blockIdx.x) < g.gxi) {
-        const int j = blockIdx.y * kBlockY + threadIdx.y;
+    if (bx < g.gxi) {
+        const int j = by * kBlockY + threadIdx.y;
         if (j < 1 || j >= a.NyT) return;  // E is updated for j >= 1 only; whole warp
-        const int i0 = g.xi0 + (blockIdx.x * 32 + lane) * W;
+        const int i0 = g.xi0 + (bx * 32 + lane) * W;
         e_column<S, T, false>(a, g, src, j, i0, i0 < g.xi1, kb, ke, lane);
     } else {
         const int t = threadIdx.y * 32 + lane;
         const int rr = t / g.ne, v = t - rr * g.ne;
-        const int j = blockIdx.y * g.er + rr;
+        const int j = by * g.er + rr;
         if (rr >= g.er || j < 1 || j >= a.NyT) return;
         const int i0 = v < g.nl ? v * W : g.xi1 + (v - g.nl) * W;
         if (i0 >= a.NxT) return;
         e_column<S, T, true>(a, g, src, j, i0, true, kb, ke, lane);
     }
+}
+
+template <typename S, typename T>
+__global__ void __launch_bounds__(32 * kBlockY, 2)
+k_update_E(const StepArgs<S, T> a, const int kchunk, const ESrc src, const SweepGeom g) {
+    update_E_block<S, T>(a, kchunk, src, g, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 
 }  // namespace fdtdk

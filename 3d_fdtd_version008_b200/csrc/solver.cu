@@ -17,6 +17,8 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <map>
+#include <deque>
 #include <type_traits>
 #include <cmath>
 #include <cstdlib>
@@ -118,12 +120,11 @@ __device__ double probe_value(const StepArgs<S, T>& a, const ProbeDev& p, double
 // FP64 DFT accumulation X_m += v * exp(-i 2 pi f_m t) * dt at t = (n+1) dt.
 // One thread per (probe, frequency).
 template <typename S, typename T>
-__global__ void k_probe_dft(const StepArgs<S, T> a, const ProbeDev* __restrict__ probes, int nprobes,
-                            const double* __restrict__ freqs, int nf, double* __restrict__ dft,
-                            double* __restrict__ series, long long sample, double t, double dt, double es, double hs) {
-    if (*a.status) return;
+__device__ void probe_dft_thread(const StepArgs<S, T>& a, const ProbeDev* __restrict__ probes, int nprobes,
+                                 const double* __restrict__ freqs, int nf, double* __restrict__ dft,
+                                 double* __restrict__ series, long long sample, double t, double dt, double es,
+                                 double hs, int tid) {
     const int per = nf > 0 ? nf : 1;
-    const int tid = blockIdx.x * blockDim.x + threadIdx.x;
     if (tid >= nprobes * per) return;
     const int p = tid / per, m = tid % per;
     const double v = probe_value(a, probes[p], es, hs);
@@ -135,6 +136,15 @@ __global__ void k_probe_dft(const StepArgs<S, T> a, const ProbeDev* __restrict__
         acc[0] += v * c * dt;
         acc[1] -= v * s * dt;
     }
+}
+
+template <typename S, typename T>
+__global__ void k_probe_dft(const StepArgs<S, T> a, const ProbeDev* __restrict__ probes, int nprobes,
+                            const double* __restrict__ freqs, int nf, double* __restrict__ dft,
+                            double* __restrict__ series, long long sample, double t, double dt, double es, double hs) {
+    if (*a.status) return;
+    probe_dft_thread(a, probes, nprobes, freqs, nf, dft, series, sample, t, dt, es, hs,
+                     int(blockIdx.x * blockDim.x + threadIdx.x));
 }
 
 struct DiagAccum {
@@ -205,16 +215,16 @@ __device__ void block_commit(DiagAccum* acc, double mE, double mP, unsigned fl, 
 // compute_polarization_energy (src/two_level_system.hpp:344-418) over the fields after
 // the step.  Field arrays are scanned as flat padded arrays (padding holds zeros).
 template <typename S, typename T>
-__global__ void k_monitor_reduce(const StepArgs<S, T> a, size_t nflat, const double* __restrict__ dxs,
-                                 const double* __restrict__ dys, const double* __restrict__ dzs, int parity_next,
-                                 DiagAccum* acc, double es) {
+__device__ void monitor_reduce_blocks(const StepArgs<S, T>& a, size_t nflat, const double* __restrict__ dxs,
+                                      const double* __restrict__ dys, const double* __restrict__ dzs, int parity_next,
+                                      DiagAccum* acc, double es, unsigned bid, unsigned nblk) {
     if (*a.status) return;
     double mE = 0.0, mP = 0.0, s0 = 0, s1 = 0, s2 = 0, s3 = 0, s4 = 0;
     unsigned fl = 0;
-    const size_t stride = size_t(gridDim.x) * blockDim.x;
+    const size_t stride = size_t(nblk) * blockDim.x;
     // 16-byte vectors: nflat is a multiple of the padded row, itself a multiple of W
     constexpr int W = Vec<T>::W;
-    for (size_t v = blockIdx.x * size_t(blockDim.x) + threadIdx.x; v < nflat / W; v += stride) {
+    for (size_t v = bid * size_t(blockDim.x) + threadIdx.x; v < nflat / W; v += stride) {
         const size_t t = v * W;
         T ex[W], ey[W], ez[W], hx[W], hy[W], hz[W];
         Fld<S, T>::ldg(a.Ex + t, ex); Fld<S, T>::ldg(a.Ey + t, ey); Fld<S, T>::ldg(a.Ez + t, ez);
@@ -231,7 +241,7 @@ __global__ void k_monitor_reduce(const StepArgs<S, T> a, size_t nflat, const dou
         const T* Pn = parity_next ? a.P1 : a.P0;
         const T* Po = parity_next ? a.P0 : a.P1;
         const size_t ng = size_t(a.gX) * a.gY * a.gZ;
-        for (size_t t = blockIdx.x * size_t(blockDim.x) + threadIdx.x; t < ng; t += stride) {
+        for (size_t t = bid * size_t(blockDim.x) + threadIdx.x; t < ng; t += stride) {
             const int r = a.greg[t];
             if (r < 0 || !a.gcoef[r].active) continue;
             const int i = int(t % a.gX) + a.gi0;
@@ -256,7 +266,14 @@ __global__ void k_monitor_reduce(const StepArgs<S, T> a, size_t nflat, const dou
 
 // One thread: the StabilityMonitor decision for monitor step `step`; sets the abort
 // word when the reference would terminate (NaN/Inf anywhere, or > 10 threshold warnings).
-__global__ void k_monitor_eval(DiagAccum* acc, MonitorState* ms, unsigned* status, unsigned long long step) {
+template <typename S, typename T>
+__global__ void k_monitor_reduce(const StepArgs<S, T> a, size_t nflat, const double* __restrict__ dxs,
+                                 const double* __restrict__ dys, const double* __restrict__ dzs, int parity_next,
+                                 DiagAccum* acc, double es) {
+    monitor_reduce_blocks(a, nflat, dxs, dys, dzs, parity_next, acc, es, blockIdx.x, gridDim.x);
+}
+
+__device__ void monitor_eval(DiagAccum* acc, MonitorState* ms, unsigned* status, unsigned long long step) {
     if (*status) return;
     const double max_E = __longlong_as_double((long long)acc->maxE);
     const double max_P = __longlong_as_double((long long)acc->maxP);
@@ -285,6 +302,85 @@ __global__ void k_monitor_eval(DiagAccum* acc, MonitorState* ms, unsigned* statu
     }
     acc->maxE = 0; acc->maxP = 0; acc->flags = 0;
     acc->sum_pop = acc->sum_N0 = acc->int_Nu = acc->int_Ng = acc->p_energy = 0.0;
+}
+
+__global__ void k_monitor_eval(DiagAccum* acc, MonitorState* ms, unsigned* status, unsigned long long step) {
+    monitor_eval(acc, ms, status, step);
+}
+
+// ================================================================ packed multi-solve step
+// Up to kMaxBatch resident FP32 solves advance together: every sweep is ONE launch whose
+// blocks are listed in a table (solve, bx, by, bz), each block running the same block code
+// as the single-solve kernels on its solve's arguments, read from constant memory with a
+// block-uniform index.  Per-solve step data (sources, probe sample, monitor flag) is
+// rewritten in constant memory before every step.
+constexpr int kMaxBatch = 64;
+constexpr int kMonBlocks = 64;  // monitor blocks per solve
+
+struct BatchSolve {
+    SweepGeom g;
+    int kchunkH, kchunkE;
+    const ProbeDev* probes;
+    int nprobes, nf;
+    const double* freqs;
+    double *dft, *series;
+    const double *dx, *dy, *dz;
+    DiagAccum* acc;
+    MonitorState* ms;
+    unsigned* status;
+    unsigned long long nflat;
+    double dt;
+};
+
+struct BatchTick {
+    ESrc src;
+    long long sample;         // probe sample index of this step, or -1
+    double t;                 // (n + 1) dt
+    unsigned long long step;  // n
+    int monitor;              // the stability monitor runs after this step
+    int pad;
+};
+
+__constant__ StepArgs<float> c_bargs[kMaxBatch];
+__constant__ BatchSolve c_bsolve[kMaxBatch];
+__constant__ BatchTick c_btick[kMaxBatch];
+
+__global__ void __launch_bounds__(32 * kBlockY, 2) k_update_H_multi(const int4* __restrict__ tab) {
+    const int4 e = tab[blockIdx.x];
+    update_H_block<float, float>(c_bargs[e.x], c_bsolve[e.x].kchunkH, c_bsolve[e.x].g, e.y, e.z, e.w);
+}
+
+__global__ void __launch_bounds__(32 * kBlockY, 2) k_update_E_multi(const int4* __restrict__ tab) {
+    const int4 e = tab[blockIdx.x];
+    update_E_block<float, float>(c_bargs[e.x], c_bsolve[e.x].kchunkE, c_btick[e.x].src, c_bsolve[e.x].g, e.y, e.z,
+                                 e.w);
+}
+
+// one block per solve
+__global__ void k_probe_multi() {
+    const int r = blockIdx.x;
+    const StepArgs<float>& a = c_bargs[r];
+    const BatchSolve& b = c_bsolve[r];
+    const BatchTick& tk = c_btick[r];
+    if (*a.status || b.nprobes == 0) return;
+    const int n = b.nprobes * (b.nf > 0 ? b.nf : 1);
+    for (int tid = threadIdx.x; tid < n; tid += blockDim.x)
+        probe_dft_thread(a, b.probes, b.nprobes, b.freqs, b.nf, b.dft, b.series, tk.sample, tk.t, b.dt, 1.0, 1.0, tid);
+}
+
+// kMonBlocks blocks per solve; solves without a monitor step this step return at once
+__global__ void k_monitor_reduce_multi() {
+    const int r = blockIdx.x / kMonBlocks;
+    if (!c_btick[r].monitor || *c_bargs[r].status) return;
+    const BatchSolve& b = c_bsolve[r];
+    monitor_reduce_blocks(c_bargs[r], size_t(b.nflat), b.dx, b.dy, b.dz, int((c_btick[r].step + 1) & 1), b.acc, 1.0,
+                          blockIdx.x % kMonBlocks, kMonBlocks);
+}
+
+__global__ void k_monitor_eval_multi(int nres) {
+    const int r = threadIdx.x;
+    if (r >= nres || !c_btick[r].monitor) return;
+    monitor_eval(c_bsolve[r].acc, c_bsolve[r].ms, c_bsolve[r].status, c_btick[r].step);
 }
 
 }  // namespace fdtdk
@@ -329,8 +425,12 @@ public:
 // Fields and CPML psi stored as S, arithmetic in T (S = T for FP32 / FP64; S = __half or
 // __nv_bfloat16 with T = float for the 16-bit storage forms, whose stored values are
 // E' = E / sE and H' = H / sH).
+class Batch;
+
 template <typename S, typename T>
 class Solver final : public SolverBase {
+    friend class Batch;
+
 public:
     explicit Solver(const fdtd_setup_v1& s, int dev);
     ~Solver() override;
@@ -1095,6 +1195,276 @@ void Solver<S, T>::diagnostics(fdtd_diagnostics_v1* d) {
 
 }  // namespace
 
+
+namespace {
+// ==================================================================== packed multi-solve engine
+// A queue of FP32 solves served by one GPU: jobs wait until their device footprint fits the
+// budget and a slot is free, then stay resident (fields, CPML psi, gain state, probes in HBM)
+// until their last step, while every step of every resident solve is issued as one packed
+// H launch, one packed E launch, one probe launch and (on monitor steps) one monitor pair.
+// The per-cell arithmetic is the single-solve kernels' own, so a solve's result does not
+// depend on what it shares the GPU with.
+class Batch {
+public:
+    enum { QUEUED = 0, RESIDENT = 1, DONE = 2, FAILED = 3 };
+    struct Job {
+        const fdtd_setup_v1* setup = nullptr;
+        uint64_t target = 0;
+        int state = QUEUED;
+        uint64_t bytes = 0;
+        std::unique_ptr<Solver<float, float>> sol;
+        std::vector<double> series, dft;
+        uint64_t samples = 0;
+        uint32_t nprobes = 0, nf = 0;
+        fdtd_diagnostics_v1 diag{};
+        std::string err;
+    };
+
+    Batch(int dev, uint64_t budget) : device_(dev), budget_(budget) {
+        ck(cudaSetDevice(dev), "cudaSetDevice");
+        ck(cudaStreamCreateWithFlags(&st_, cudaStreamNonBlocking), "cudaStreamCreate");
+        ck(cudaHostAlloc(reinterpret_cast<void**>(&ticks_), sizeof(BatchTick) * kMaxBatch * kRing, cudaHostAllocDefault),
+           "cudaHostAlloc");
+        for (auto& e : ring_ev_) ck(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "cudaEventCreate");
+    }
+    ~Batch() {
+        cudaSetDevice(device_);
+        if (st_) cudaStreamSynchronize(st_);
+        jobs_.clear();
+        if (d_tab_) cudaFree(d_tab_);
+        if (ticks_) cudaFreeHost(ticks_);
+        for (auto& e : ring_ev_) if (e) cudaEventDestroy(e);
+        if (st_) cudaStreamDestroy(st_);
+    }
+
+    uint64_t submit(const fdtd_setup_v1& s, uint64_t nsteps) {
+        if (s.precision != FDTD_PREC_FP32) throw Failure(FDTD_ERR_UNSUPPORTED, "the packed engine steps FP32 solves");
+        if (nsteps == 0) throw Failure(FDTD_ERR_INVALID, "a job needs at least one step");
+        Job j;
+        j.setup = &s;
+        j.target = nsteps;
+        j.bytes = footprint(s);
+        if (j.bytes > budget_) throw Failure(FDTD_ERR_OOM, "job footprint exceeds the batch memory budget");
+        const uint64_t t = next_++;
+        jobs_.emplace(t, std::move(j));
+        queue_.push_back(t);
+        return t;
+    }
+
+    // Admits what fits, then advances the resident solves by up to max_steps steps each,
+    // retiring solves as they reach their target.
+    void run(uint64_t max_steps) {
+        ck(cudaSetDevice(device_), "cudaSetDevice");
+        admit();
+        for (uint64_t t = 0; t < max_steps && !res_.empty(); ++t) {
+            step();
+            bool finished = false;
+            for (uint64_t r : res_) finished |= jobs_.at(r).sol->steps >= jobs_.at(r).target;
+            if (finished || ++since_check_ >= kCheckEvery) {
+                check_and_retire();
+                admit();
+            }
+        }
+        ck(cudaStreamSynchronize(st_), "batch run");
+    }
+
+    Job& job(uint64_t t) {
+        auto it = jobs_.find(t);
+        if (it == jobs_.end()) throw Failure(FDTD_ERR_INVALID, "unknown ticket");
+        return it->second;
+    }
+    void release(uint64_t t) {
+        Job& j = job(t);
+        if (j.state != DONE && j.state != FAILED) throw Failure(FDTD_ERR_INVALID, "job has not finished");
+        jobs_.erase(t);
+    }
+    uint32_t resident() const { return uint32_t(res_.size()); }
+    uint32_t queued() const { return uint32_t(queue_.size()); }
+    uint64_t used() const { return used_; }
+
+private:
+    static constexpr int kRing = 64;        // pinned per-step records in flight
+    static constexpr int kCheckEvery = 16;  // steps between status checks
+
+    // Device bytes a solve will hold: fields, bE, psi slabs, gain box (upper bound).
+    static uint64_t footprint(const fdtd_setup_v1& s) {
+        const uint64_t NxP = (s.NxT + 31) / 32 * 32, NyT = s.NyT, NzT = s.NzT, np2 = 2ull * s.npml;
+        uint64_t b = 9ull * NxP * NyT * NzT * 4;
+        b += 2ull * 4 * (NzT * NyT * np2 + NzT * np2 * NxP + np2 * NyT * NxP) * 3;  // 12 psi arrays
+        if (s.n_tls_regions) b += 17ull * s.NxT * NyT * NzT / 4;  // gain box, worst case the grid
+        return b + (64ull << 10) + 3ull * (s.NxT + NyT + NzT) * 8 * 8;
+    }
+
+    void admit() {
+        bool changed = false;
+        while (!queue_.empty() && res_.size() < size_t(kMaxBatch)) {
+            const uint64_t t = queue_.front();
+            Job& j = jobs_.at(t);
+            if (used_ + j.bytes > budget_) break;  // first come, first served
+            queue_.pop_front();
+            try {
+                j.sol = std::make_unique<Solver<float, float>>(*j.setup, device_);
+                j.sol->ensure_series((j.target + j.sol->save_every_ - 1) / j.sol->save_every_);
+                ck(cudaStreamSynchronize(j.sol->st_), "admit");
+                j.state = RESIDENT;
+                used_ += j.bytes;
+                res_.push_back(t);
+                changed = true;
+            } catch (const std::exception& e) {
+                j.sol.reset();
+                j.state = FAILED;
+                j.err = e.what();
+            }
+        }
+        if (changed) rebuild();
+    }
+
+    // Per-solve constants and the packed block tables.
+    void rebuild() {
+        const int n = int(res_.size());
+        std::vector<StepArgs<float>> args(n);
+        std::vector<BatchSolve> bs(n);
+        std::vector<int4> tab;
+        nH_ = nE_ = 0;
+        for (int r = 0; r < n; ++r) {
+            Solver<float, float>& v = *jobs_.at(res_[r]).sol;
+            args[r] = v.a_;
+            BatchSolve& b = bs[r];
+            b.g = v.geom_;
+            b.kchunkH = v.kchunkH_;
+            b.kchunkE = v.kchunkE_;
+            b.probes = v.d_probes_;
+            b.nprobes = int(v.nprobes_);
+            b.nf = int(v.nf_);
+            b.freqs = v.d_freqs_;
+            b.dft = v.d_dft_;
+            b.series = v.d_series_;
+            b.dx = v.d_dx_; b.dy = v.d_dy_; b.dz = v.d_dz_;
+            b.acc = v.d_acc_;
+            b.ms = v.d_ms_;
+            b.status = v.d_status_;
+            b.nflat = v.nflat_;
+            b.dt = v.dt_;
+        }
+        for (int r = 0; r < n; ++r) {  // H blocks of every solve, then E blocks
+            const dim3 g = jobs_.at(res_[r]).sol->gridH_;
+            for (unsigned z = 0; z < g.z; ++z)
+                for (unsigned y = 0; y < g.y; ++y)
+                    for (unsigned x = 0; x < g.x; ++x) tab.push_back(make_int4(r, int(x), int(y), int(z)));
+        }
+        nH_ = tab.size();
+        for (int r = 0; r < n; ++r) {
+            const dim3 g = jobs_.at(res_[r]).sol->gridE_;
+            for (unsigned z = 0; z < g.z; ++z)
+                for (unsigned y = 0; y < g.y; ++y)
+                    for (unsigned x = 0; x < g.x; ++x) tab.push_back(make_int4(r, int(x), int(y), int(z)));
+        }
+        nE_ = tab.size() - nH_;
+        ck(cudaStreamSynchronize(st_), "rebuild");  // no step may read the old tables
+        if (tab.size() > tab_cap_) {
+            if (d_tab_) ck(cudaFree(d_tab_), "cudaFree");
+            tab_cap_ = std::max<size_t>(tab.size(), 2 * tab_cap_);
+            ck(cudaMalloc(&d_tab_, tab_cap_ * sizeof(int4)), "cudaMalloc block table");
+        }
+        if (!tab.empty()) ck(cudaMemcpy(d_tab_, tab.data(), tab.size() * sizeof(int4), cudaMemcpyHostToDevice), "block table");
+        if (n) {
+            ck(cudaMemcpyToSymbol(c_bargs, args.data(), n * sizeof(StepArgs<float>)), "cudaMemcpyToSymbol");
+            ck(cudaMemcpyToSymbol(c_bsolve, bs.data(), n * sizeof(BatchSolve)), "cudaMemcpyToSymbol");
+        }
+    }
+
+    void step() {
+        const int n = int(res_.size());
+        const int slot = ring_++ % kRing;
+        ck(cudaEventSynchronize(ring_ev_[slot]), "tick ring");  // its previous copy has been read
+        BatchTick* tk = ticks_ + size_t(slot) * kMaxBatch;
+        bool monitor = false;
+        for (int r = 0; r < n; ++r) {
+            Solver<float, float>& v = *jobs_.at(res_[r]).sol;
+            const uint64_t s = v.steps;
+            BatchTick& k = tk[r];
+            k = BatchTick{};
+            k.src.n = int(v.dip_.size());
+            k.src.parity = int(s & 1);
+            for (int q = 0; q < k.src.n; ++q) {
+                const fdtd_dipole_v1& d = v.dip_[q];
+                k.src.si[q] = int(d.i); k.src.sj[q] = int(d.j); k.src.sk[q] = int(d.k);
+                k.src.sc[q] = d.polarization % 3;
+                k.src.J[q] = fdtd::current_density(d.waveform, s, v.dt_, d.I0, d.f0, d.tau, d.t0, d.t_shift, d.cell_area);
+            }
+            k.sample = (s % v.save_every_ == 0) ? (long long)(s / v.save_every_) : -1;
+            if (k.sample >= 0) v.series_count_ = uint64_t(k.sample) + 1;
+            k.t = double(s + 1) * v.dt_;
+            k.step = s;
+            k.monitor = (v.interval_ && s % v.interval_ == 0) ? 1 : 0;
+            monitor |= k.monitor != 0;
+            v.steps = s + 1;
+        }
+        ck(cudaMemcpyToSymbolAsync(c_btick, tk, n * sizeof(BatchTick), 0, cudaMemcpyHostToDevice, st_), "step records");
+        ck(cudaEventRecord(ring_ev_[slot], st_), "cudaEventRecord");
+        const dim3 blk(32, kBlockY);
+        k_update_H_multi<<<unsigned(nH_), blk, 0, st_>>>(d_tab_);
+        k_update_E_multi<<<unsigned(nE_), blk, 0, st_>>>(d_tab_ + nH_);
+        k_probe_multi<<<n, 128, 0, st_>>>();
+        if (monitor) {
+            k_monitor_reduce_multi<<<n * kMonBlocks, 256, 0, st_>>>();
+            k_monitor_eval_multi<<<1, kMaxBatch, 0, st_>>>(n);
+        }
+        ck(cudaGetLastError(), "packed step");
+    }
+
+    // Reads every resident solve's status word; retires finished and failed solves.
+    void check_and_retire() {
+        since_check_ = 0;
+        ck(cudaStreamSynchronize(st_), "batch check");
+        std::vector<uint64_t> keep;
+        for (uint64_t t : res_) {
+            Job& j = jobs_.at(t);
+            Solver<float, float>& v = *j.sol;
+            unsigned status = 0;
+            ck(cudaMemcpy(&status, v.d_status_, sizeof(unsigned), cudaMemcpyDeviceToHost), "status");
+            if (status == 0 && v.steps < j.target) { keep.push_back(t); continue; }
+            if (status) {
+                MonitorState ms{};
+                ck(cudaMemcpy(&ms, v.d_ms_, sizeof(ms), cudaMemcpyDeviceToHost), "monitor state");
+                j.err = "stability monitor stopped the solve at step " + std::to_string(ms.step);
+                v.steps = ms.step + 1;
+                v.series_count_ = std::min<uint64_t>(v.series_count_, (v.steps + v.save_every_ - 1) / v.save_every_);
+            }
+            j.nprobes = v.nprobes_;
+            j.nf = v.nf_;
+            j.series.assign(size_t(v.series_count_) * v.nprobes_, 0.0);
+            uint64_t got = 0;
+            if (v.nprobes_) v.probe_series(j.series.data(), v.series_count_, &got);
+            j.samples = got;
+            j.dft.assign(size_t(2) * v.nprobes_ * v.nf_, 0.0);
+            if (v.nprobes_ && v.nf_) ck(cudaMemcpy(j.dft.data(), v.d_dft_, j.dft.size() * sizeof(double), cudaMemcpyDeviceToHost), "dft");
+            v.diagnostics(&j.diag);
+            j.state = status ? FAILED : DONE;
+            j.sol.reset();
+            j.setup = nullptr;
+            used_ -= j.bytes;
+        }
+        const bool changed = keep.size() != res_.size();
+        res_.swap(keep);
+        if (changed) rebuild();
+    }
+
+    int device_;
+    uint64_t budget_, used_ = 0, next_ = 1;
+    cudaStream_t st_ = nullptr;
+    std::map<uint64_t, Job> jobs_;
+    std::deque<uint64_t> queue_;
+    std::vector<uint64_t> res_;  // resident tickets in slot order
+    int4* d_tab_ = nullptr;
+    size_t tab_cap_ = 0, nH_ = 0, nE_ = 0;
+    BatchTick* ticks_ = nullptr;
+    cudaEvent_t ring_ev_[kRing] = {};
+    uint64_t ring_ = 0;
+    int since_check_ = 0;
+};
+}  // namespace
+
 // ==================================================================== C ABI
 struct fdtd_handle {
     std::unique_ptr<SolverBase> s;
@@ -1119,26 +1489,30 @@ int guarded(fdtd_handle* h, F&& f) {
 }
 }  // namespace
 
+namespace {
+// Why a setup view cannot be stepped, or nullptr.
+const char* setup_problem(const fdtd_setup_v1* s) {
+    if (s->struct_size != sizeof(fdtd_setup_v1)) return "fdtd_setup_v1.struct_size mismatch";
+    // NyT is a grid dimension (z) of the layout-transpose kernels: at most 65535.
+    if (s->NxT < 3 || s->NyT < 3 || s->NzT < 3 || s->NxT > (1u << 30) || s->NyT > 65535 || s->NzT > (1u << 30))
+        return "grid dimensions out of range";
+    if (2 * uint64_t(s->npml) >= s->NxT || 2 * uint64_t(s->npml) >= s->NyT || 2 * uint64_t(s->npml) >= s->NzT)
+        return "npml too large for the grid";
+    if (!s->bE[0] || !s->bE[1] || !s->bE[2] || !s->inv_dx || !s->inv_dy || !s->inv_dz || !s->dx || !s->dy || !s->dz)
+        return "missing required setup arrays";
+    for (int a = 0; a < 3; ++a)
+        if (!s->cpml_kappa[a] || !s->cpml_bE[a] || !s->cpml_cE[a] || !s->cpml_bH[a] || !s->cpml_cH[a])
+            return "missing CPML profile arrays";
+    return nullptr;
+}
+}  // namespace
+
 extern "C" {
 
 int fdtd_create(const fdtd_setup_v1* s, int device, fdtd_handle** out) {
     if (!s || !out) { g_err = "null argument"; return FDTD_ERR_INVALID; }
     *out = nullptr;
-    if (s->struct_size != sizeof(fdtd_setup_v1)) { g_err = "fdtd_setup_v1.struct_size mismatch"; return FDTD_ERR_INVALID; }
-    // NyT is a grid dimension (z) of the layout-transpose kernels: at most 65535.
-    if (s->NxT < 3 || s->NyT < 3 || s->NzT < 3 || s->NxT > (1u << 30) || s->NyT > 65535 || s->NzT > (1u << 30)) {
-        g_err = "grid dimensions out of range"; return FDTD_ERR_INVALID;
-    }
-    if (2 * uint64_t(s->npml) >= s->NxT || 2 * uint64_t(s->npml) >= s->NyT || 2 * uint64_t(s->npml) >= s->NzT) {
-        g_err = "npml too large for the grid"; return FDTD_ERR_INVALID;
-    }
-    if (!s->bE[0] || !s->bE[1] || !s->bE[2] || !s->inv_dx || !s->inv_dy || !s->inv_dz || !s->dx || !s->dy || !s->dz) {
-        g_err = "missing required setup arrays"; return FDTD_ERR_INVALID;
-    }
-    for (int a = 0; a < 3; ++a)
-        if (!s->cpml_kappa[a] || !s->cpml_bE[a] || !s->cpml_cE[a] || !s->cpml_bH[a] || !s->cpml_cH[a]) {
-            g_err = "missing CPML profile arrays"; return FDTD_ERR_INVALID;
-        }
+    if (const char* why = setup_problem(s)) { g_err = why; return FDTD_ERR_INVALID; }
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
         cudaGetLastError();
@@ -1176,6 +1550,116 @@ int fdtd_set_kernel_path(fdtd_handle* h, int path) { if (!h) return FDTD_ERR_INV
 int fdtd_synchronize(fdtd_handle* h) { if (!h) return FDTD_ERR_INVALID; return guarded(h, [&] { h->s->sync(); }); }
 const char* fdtd_last_error(const fdtd_handle* h) { return h ? h->err.c_str() : g_err.c_str(); }
 void fdtd_destroy(fdtd_handle* h) { delete h; }
+
+}  // extern "C"
+
+
+// ---- packed multi-solve engine
+struct fdtd_batch {
+    std::unique_ptr<Batch> b;
+    std::string err;
+};
+
+namespace {
+template <typename F>
+int bguard(fdtd_batch* b, F&& f) {
+    try {
+        f();
+        return FDTD_OK;
+    } catch (const Failure& e) {
+        (b ? b->err : g_err) = e.what();
+        return e.code;
+    } catch (const std::exception& e) {
+        (b ? b->err : g_err) = e.what();
+        return FDTD_ERR_INVALID;
+    }
+}
+}  // namespace
+
+extern "C" {
+
+int fdtd_batch_create(int device, uint64_t budget_bytes, fdtd_batch** out) {
+    if (!out) { g_err = "null argument"; return FDTD_ERR_INVALID; }
+    *out = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        g_err = "no CUDA device available";
+        return FDTD_ERR_NO_DEVICE;
+    }
+    if (device < 0 || device >= ndev) { g_err = "device index out of range"; return FDTD_ERR_INVALID; }
+    auto* b = new fdtd_batch();
+    const int rc = bguard(nullptr, [&] { b->b = std::make_unique<Batch>(device, budget_bytes); });
+    if (rc != FDTD_OK) { delete b; return rc; }
+    *out = b;
+    return FDTD_OK;
+}
+
+int fdtd_batch_submit(fdtd_batch* b, const fdtd_setup_v1* s, uint64_t n_steps, uint64_t* ticket) {
+    if (!b || !s || !ticket) return FDTD_ERR_INVALID;
+    if (const char* why = setup_problem(s)) { b->err = why; return FDTD_ERR_INVALID; }
+    return bguard(b, [&] { *ticket = b->b->submit(*s, n_steps); });
+}
+
+int fdtd_batch_run(fdtd_batch* b, uint64_t max_steps, uint32_t* n_resident, uint32_t* n_queued) {
+    if (!b) return FDTD_ERR_INVALID;
+    return bguard(b, [&] {
+        b->b->run(max_steps);
+        if (n_resident) *n_resident = b->b->resident();
+        if (n_queued) *n_queued = b->b->queued();
+    });
+}
+
+int fdtd_batch_job_state(fdtd_batch* b, uint64_t ticket, int* state, uint64_t* steps_done) {
+    if (!b || !state) return FDTD_ERR_INVALID;
+    return bguard(b, [&] {
+        Batch::Job& j = b->b->job(ticket);
+        *state = j.state;
+        if (steps_done) *steps_done = j.sol ? j.sol->steps : j.diag.steps_done;
+    });
+}
+
+int fdtd_batch_probe_series(fdtd_batch* b, uint64_t ticket, double* out, uint64_t max_samples, uint64_t* n_samples) {
+    if (!b || !n_samples) return FDTD_ERR_INVALID;
+    return bguard(b, [&] {
+        Batch::Job& j = b->b->job(ticket);
+        if (j.state != Batch::DONE && j.state != Batch::FAILED) throw Failure(FDTD_ERR_INVALID, "job has not finished");
+        const uint64_t n = std::min<uint64_t>(max_samples, j.samples);
+        if (out && n) std::memcpy(out, j.series.data(), n * j.nprobes * sizeof(double));
+        *n_samples = j.samples;
+    });
+}
+
+int fdtd_batch_dft(fdtd_batch* b, uint64_t ticket, uint32_t probe, double* re, double* im) {
+    if (!b || !re || !im) return FDTD_ERR_INVALID;
+    return bguard(b, [&] {
+        Batch::Job& j = b->b->job(ticket);
+        if (j.state != Batch::DONE && j.state != Batch::FAILED) throw Failure(FDTD_ERR_INVALID, "job has not finished");
+        if (probe >= j.nprobes) throw Failure(FDTD_ERR_INVALID, "probe index out of range");
+        for (uint32_t m = 0; m < j.nf; ++m) {
+            re[m] = j.dft[2 * (size_t(probe) * j.nf + m)];
+            im[m] = j.dft[2 * (size_t(probe) * j.nf + m) + 1];
+        }
+    });
+}
+
+int fdtd_batch_diagnostics(fdtd_batch* b, uint64_t ticket, fdtd_diagnostics_v1* out) {
+    if (!b || !out) return FDTD_ERR_INVALID;
+    return bguard(b, [&] {
+        Batch::Job& j = b->b->job(ticket);
+        if (j.state != Batch::DONE && j.state != Batch::FAILED) throw Failure(FDTD_ERR_INVALID, "job has not finished");
+        *out = j.diag;
+    });
+}
+
+int fdtd_batch_release(fdtd_batch* b, uint64_t ticket) {
+    if (!b) return FDTD_ERR_INVALID;
+    return bguard(b, [&] { b->b->release(ticket); });
+}
+
+const char* fdtd_batch_last_error(const fdtd_batch* b) { return b ? b->err.c_str() : g_err.c_str(); }
+
+void fdtd_batch_destroy(fdtd_batch* b) { delete b; }
 
 }  // extern "C"
 

@@ -227,6 +227,33 @@ int fdtd_synchronize(fdtd_handle *h);
 const char *fdtd_last_error(const fdtd_handle *h);
 void fdtd_destroy(fdtd_handle *h);
 
+/* ------------------------------------------------------------ packed multi-solve engine */
+/* The serving form of the stepper: a queue of FP32 solves on one GPU.  fdtd_batch_submit
+ * queues a solve (the setup view and the arrays it points to must stay valid until the job
+ * has finished); fdtd_batch_run admits queued jobs in order while their device footprint
+ * fits budget_bytes and fewer than 64 are resident, then advances every resident solve by
+ * up to max_steps steps, each step of all of them issued as one packed H launch, one packed
+ * E launch and one probe launch (plus one monitor pair on monitor steps), and retires
+ * solves that reach their step count or that the stability monitor stops.  The per-cell
+ * arithmetic is fdtd_run's, so a job's probe series, DFT and diagnostics are the same as
+ * from fdtd_create + fdtd_run on the same setup.  No counterpart in the reference (it runs
+ * one solve per process); it replaces running the reference once per design point.
+ * A batch is driven from one host thread. */
+typedef struct fdtd_batch fdtd_batch;
+enum { FDTD_JOB_QUEUED = 0, FDTD_JOB_RESIDENT = 1, FDTD_JOB_DONE = 2, FDTD_JOB_FAILED = 3 };
+int fdtd_batch_create(int device, uint64_t budget_bytes, fdtd_batch **out);
+int fdtd_batch_submit(fdtd_batch *b, const fdtd_setup_v1 *setup, uint64_t n_steps, uint64_t *ticket);
+int fdtd_batch_run(fdtd_batch *b, uint64_t max_steps, uint32_t *n_resident, uint32_t *n_queued);
+int fdtd_batch_job_state(fdtd_batch *b, uint64_t ticket, int *state, uint64_t *steps_done);
+/* Results of a finished job (FDTD_JOB_DONE, or FDTD_JOB_FAILED up to the failing step). */
+int fdtd_batch_probe_series(fdtd_batch *b, uint64_t ticket, double *out, uint64_t max_samples, uint64_t *n_samples);
+int fdtd_batch_dft(fdtd_batch *b, uint64_t ticket, uint32_t probe, double *re, double *im);
+int fdtd_batch_diagnostics(fdtd_batch *b, uint64_t ticket, fdtd_diagnostics_v1 *out);
+/* Forget a finished job's results. */
+int fdtd_batch_release(fdtd_batch *b, uint64_t ticket);
+const char *fdtd_batch_last_error(const fdtd_batch *b);
+void fdtd_batch_destroy(fdtd_batch *b);
+
 /* ---- Field scan without device allocation.  No counterpart in the reference: it exists
  * for callers that cannot call cudaMalloc when they need the scan -- an application that
  * runs the stepper inside its own device memory pool or arena (which owns all device

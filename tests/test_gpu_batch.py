@@ -1,0 +1,117 @@
+"""Packed multi-solve engine (fdtd_batch_*): solves of different grids, step counts and
+physics resident together on one GPU, each result the same alone and in the mix."""
+import numpy as np
+import pytest
+
+from conftest import GOLDEN
+
+pytestmark = pytest.mark.gpu
+
+CASES = [  # (setup source, overrides, steps)
+    (GOLDEN / "cases" / "step_g0_sphere.params", {}, 150),
+    (GOLDEN / "cases" / "step_g1_gain.params", {"PUMP_RATE": "1e11"}, 120),
+    ("c0_dipole_sphere.params", {}, 300),
+    ("c1_gain_slab.params", {"PUMP_RATE": "1e9"}, 210),
+]
+
+
+def _setup(pkg, src, ov):
+    path = src if not isinstance(src, str) else pkg.config_path(src)
+    return pkg.Setup.from_file(path, overrides=ov)
+
+
+def _single(pkg, s, n):
+    sol = pkg.Solver(s, precision=0, kernel_path=1)
+    sol.run(n)
+    out = (sol.probe_series(), sol.dft(0), sol.diagnostics())
+    sol.close()
+    return out
+
+
+def _drain(pkg, b, tickets, rounds=400):
+    for _ in range(rounds):
+        if all(b.state(t)[0] in (pkg.JOB_DONE, pkg.JOB_FAILED) for t in tickets):
+            return
+        b.run(64)
+    raise AssertionError("batch did not finish")
+
+
+def _batch_results(pkg, setups):
+    b = pkg.Batch(budget_bytes=8 << 30)
+    tickets = [b.submit(s, n) for s, n in setups]
+    r, q = b.run(1)
+    assert r == len(setups) and q == 0  # all resident at once
+    _drain(pkg, b, tickets)
+    out = []
+    for t, (s, n) in zip(tickets, setups):
+        st, done = b.state(t)
+        assert st == pkg.JOB_DONE and done == n
+        out.append((b.probe_series(t), b.dft(t), b.diagnostics(t)))
+        b.release(t)
+    b.close()
+    return out
+
+
+def test_batch_result_is_the_same_alone_and_in_the_mix(pkg):
+    """Bit for bit: a job's blocks run the same code whatever else is resident."""
+    setups = [(_setup(pkg, src, ov), n) for src, ov, n in CASES]
+    mixed = _batch_results(pkg, setups)
+    for k, sn in enumerate(setups):
+        (series, dft, diag), = _batch_results(pkg, [sn])
+        assert np.array_equal(mixed[k][0], series) and np.array_equal(mixed[k][1], dft)
+        assert mixed[k][2]["max_E"] == diag["max_E"]
+
+
+def test_batch_matches_single_solves(pkg):
+    """Against fdtd_create + fdtd_run: the packed kernels are a separate compilation of the
+    same block code, so the two agree to FP32 rounding (measured: 5e-5 on the probe series
+    after 150 steps, 4e-7 on the DFT), not bit for bit."""
+    setups = [(_setup(pkg, src, ov), n) for src, ov, n in CASES]
+    got = _batch_results(pkg, setups)
+    for (s, n), (series, dft, diag) in zip(setups, got):
+        ref = _single(pkg, s, n)
+        assert np.linalg.norm(series - ref[0]) <= 2e-4 * np.linalg.norm(ref[0])
+        assert np.abs(dft - ref[1]).max() <= 1e-5 * np.abs(ref[1]).max()
+        assert abs(diag["max_E"] - ref[2]["max_E"]) <= 2e-4 * ref[2]["max_E"]
+        assert diag["step"] == ref[2]["step"] and diag["steps_done"] == n
+
+
+def test_batch_admits_by_memory_budget(pkg):
+    s = _setup(pkg, "c0_dipole_sphere.params", {})
+    single = _single(pkg, s, 100)
+    b = pkg.Batch(budget_bytes=40 << 20)  # room for one 80^3 solve at a time
+    tickets = [b.submit(s, 100) for _ in range(3)]
+    r, q = b.run(1)
+    assert (r, q) == (1, 2)
+    assert [b.state(t)[0] for t in tickets] == [pkg.JOB_RESIDENT, pkg.JOB_QUEUED, pkg.JOB_QUEUED]
+    _drain(pkg, b, tickets)
+    first = b.probe_series(tickets[0])
+    assert np.linalg.norm(first - single[0]) <= 2e-4 * np.linalg.norm(single[0])
+    for t in tickets[1:]:
+        assert np.array_equal(b.probe_series(t), first)
+    with pytest.raises(pkg.FdtdError) as e:
+        b.submit(_setup(pkg, "c1_gain_slab.params", {}), 10)  # larger than the whole budget
+    assert e.value.code == 2
+    b.close()
+
+
+def test_batch_unstable_job_fails_alone(pkg):
+    good = _setup(pkg, "c0_dipole_sphere.params", {})
+    bad = _setup(pkg, GOLDEN / "cases" / "step_g0_sphere.params", {"STABILITY_MAX_E": "1e-30"})
+    ref = _single(pkg, good, 250)
+    b = pkg.Batch(budget_bytes=8 << 30)
+    tg, tb = b.submit(good, 250), b.submit(bad, 400)
+    _drain(pkg, b, [tg, tb])
+    st, done = b.state(tb)
+    assert st == pkg.JOB_FAILED and done == 101  # 11th threshold warning at monitor step 100
+    assert b.state(tg)[0] == pkg.JOB_DONE
+    assert np.linalg.norm(b.probe_series(tg) - ref[0]) <= 2e-4 * np.linalg.norm(ref[0])
+    b.close()
+
+
+def test_batch_rejects_non_fp32(pkg):
+    s = pkg.Setup.from_file(GOLDEN / "cases" / "step_g0_sphere.params", overrides={"PRECISION": "fp64"})
+    b = pkg.Batch()
+    with pytest.raises(pkg.FdtdError):
+        b.submit(s, 10)
+    b.close()
