@@ -455,7 +455,8 @@ public:
 private:
     template <typename U> U* alloc(size_t n, bool zero = true) {
         void* p = nullptr;
-        ck(cudaMalloc(&p, std::max<size_t>(n, 1) * sizeof(U)), "cudaMalloc");
+        // stream-ordered: freeing a retired solve does not stall the device for the others
+        ck(cudaMallocAsync(&p, std::max<size_t>(n, 1) * sizeof(U), st_), "cudaMallocAsync");
         ptrs_.push_back(p);
         dev_bytes += std::max<size_t>(n, 1) * sizeof(U);
         if (zero) ck(cudaMemsetAsync(p, 0, std::max<size_t>(n, 1) * sizeof(U), st_), "cudaMemsetAsync");
@@ -878,8 +879,8 @@ Solver<S, T>::~Solver() {
     cudaSetDevice(device);
     if (st_) cudaStreamSynchronize(st_);
     for (auto& e : ev_) if (e) cudaEventDestroy(e);
-    for (void* p : ptrs_) cudaFree(p);
-    if (d_stage_) cudaFree(d_stage_);
+    for (void* p : ptrs_) cudaFreeAsync(p, st_);
+    if (d_stage_) cudaFreeAsync(d_stage_, st_);
     for (int b = 0; b < 2; ++b) {
         if (pin_[b]) cudaFreeHost(pin_[b]);
         if (pin_ev_[b]) cudaEventDestroy(pin_ev_[b]);
@@ -890,7 +891,8 @@ Solver<S, T>::~Solver() {
 template <typename S, typename T>
 double* Solver<S, T>::staging() {
     if (!d_stage_) {
-        ck(cudaMalloc(&d_stage_, size_t(NxT_) * NyT_ * NzT_ * sizeof(double)), "cudaMalloc staging");
+        ck(cudaMallocAsync(reinterpret_cast<void**>(&d_stage_), size_t(NxT_) * NyT_ * NzT_ * sizeof(double), st_),
+           "cudaMallocAsync staging");
         dev_bytes += size_t(NxT_) * NyT_ * NzT_ * sizeof(double);
     }
     return d_stage_;
@@ -917,6 +919,11 @@ static void par_copy(void* dst, const void* src, size_t bytes) {
 
 template <typename S, typename T>
 void Solver<S, T>::h2d(const double* h, double* d, size_t n) {
+    if (n * sizeof(double) <= kPinBytes) {  // small grids: one copy, no pinned buffers to set up
+        ck(cudaMemcpyAsync(d, h, n * sizeof(double), cudaMemcpyHostToDevice, st_), "H2D");
+        ck(cudaStreamSynchronize(st_), "H2D");
+        return;
+    }
     ensure_pinned();
     const size_t chunk = kPinBytes / sizeof(double);
     for (size_t off = 0, it = 0; off < n; off += chunk, ++it) {
@@ -931,6 +938,11 @@ void Solver<S, T>::h2d(const double* h, double* d, size_t n) {
 
 template <typename S, typename T>
 void Solver<S, T>::d2h(const double* d, double* h, size_t n) {
+    if (n * sizeof(double) <= kPinBytes) {
+        ck(cudaMemcpyAsync(h, d, n * sizeof(double), cudaMemcpyDeviceToHost, st_), "D2H");
+        ck(cudaStreamSynchronize(st_), "D2H");
+        return;
+    }
     ensure_pinned();
     const size_t chunk = kPinBytes / sizeof(double);
     const size_t nch = (n + chunk - 1) / chunk;

@@ -206,6 +206,125 @@ def cpu_reference(sample_cfg: str, steps: int, warmup: int, fdtd_steps: int):
                    "sample": sample}
 
 
+# ------------------------------------------------------------------ serving (packed engine)
+def serving_job_text(core: tuple, steps_hint: int) -> str:
+    """A slab microcavity with a two-level gain layer (the 512^3 workload's recipe scaled to
+    a core of nx x ny x nz cells at 20 nm, 8-cell CPML), z dipole, Ez probe + DFT."""
+    nx, ny, nz = core
+    d = 20e-9
+    L = [n * d for n in core]
+    cx, cy, cz = (0.5 * l for l in L)
+    return "\n".join([
+        "MESH_MODE = 0", f"NX = {nx}", f"NY = {ny}", f"NZ = {nz}",
+        f"DX_UNIFORM = {d}", f"DY_UNIFORM = {d}", f"DZ_UNIFORM = {d}",
+        "DOMAIN_X_MIN = 0", f"DOMAIN_X_MAX = {L[0]}", "DOMAIN_Y_MIN = 0", f"DOMAIN_Y_MAX = {L[1]}",
+        "DOMAIN_Z_MIN = 0", f"DOMAIN_Z_MAX = {L[2]}",
+        "LAMBDA0 = 1550.1264633919338e-9", "CFL_FACTOR = 0.99", f"N_STEPS = {steps_hint}", "SAVE_EVERY = 1",
+        "CPML_NPML = 8", "CPML_M = 3.0", "CPML_RERR = 1e-6", "CPML_ALPHA0 = 0.05", "CPML_KAPPA_MAX = 5.0",
+        "CPML_ALPHA_LINEAR = true", "BACKGROUND_N = 1.0", "TLS_ENABLED = true", "MESH_OVERRIDE_ENABLED = false",
+        "TLS_MATERIALS += gain_1550, 1550.1264633919338e-9, 31415926535897.93, 1e-9, 5e23, 0.0",
+        f'STRUCTURES += box, 3.4, {0.1 * L[0]}, {0.9 * L[0]}, {0.1 * L[1]}, {0.9 * L[1]}, {cz - 110e-9}, {cz + 110e-9}, ""',
+        f"STRUCTURES += box, 3.4, {0.1 * L[0]}, {0.9 * L[0]}, {0.1 * L[1]}, {0.9 * L[1]}, {cz - 100e-9}, {cz + 100e-9}, gain_1550",
+        f"DIPOLE_SOURCES += true, {cx + 10e-9}, {cy + 10e-9}, {cz - 10e-9}, 1e-7, 193.4e12, 0, 0, 50e12, 3.0, 1, 2",
+        f"POINT_FIELD_DETECTORS += true, Ez_probe, {cx + 0.1 * L[0]}, {cy + 10e-9}, {cz - 10e-9}, 2",
+        "DFT_FREQS = 168e12, 218e12, 21", "PUMP_RATE = 1e9", "PRECISION = fp32", ""])
+
+
+def serving_bench(args):
+    """A stream of independent gain-slab solves (core edges log-uniform in 32..96 cells, aspect
+    1..2, steps uniform in 200..1000; FP32).  Throughput: all jobs queued at once, served by
+    the packed engine and one at a time by fdtd_create/fdtd_run.  Latency: the same jobs
+    arriving as a Poisson stream at 80 % of the packed engine's measured throughput; the
+    one-at-a-time server's latencies are its FIFO queue over its own measured service times."""
+    import numpy as np
+    rng = np.random.default_rng(3)
+    jobs = []
+    for _ in range(args.serving_jobs):
+        edge = float(np.exp(rng.uniform(np.log(32), np.log(96))))
+        asp = rng.uniform(1.0, 2.0, size=2)
+        core = (int(edge), int(max(16, edge / asp[0])), int(max(16, edge / asp[1])))
+        steps = int(rng.integers(200, 1001))
+        jobs.append((core, steps))
+    setups = [PKG.Setup.from_text(serving_job_text(c, n)) for c, n in jobs]
+    cells = [s.shape[0] * s.shape[1] * s.shape[2] for s in setups]
+    work = sum(c * n for c, (_, n) in zip(cells, jobs))
+    # warm-up outside the timed phases: CUDA context, module load, both code paths
+    w = PKG.Solver(setups[0], precision=PKG.PREC_FP32)
+    w.run(20)
+    w.close()
+    wb = PKG.Batch(budget_bytes=150 << 30)
+    wt = wb.submit(setups[0], 20)
+    while wb.state(wt)[0] < PKG.JOB_DONE:
+        wb.run(20)
+    wb.close()
+    # one at a time
+    service = []
+    for s, (_, n) in zip(setups, jobs):
+        t0 = time.perf_counter()
+        sol = PKG.Solver(s, precision=PKG.PREC_FP32)
+        sol.run(n)
+        sol.probe_series()
+        sol.close()
+        service.append(time.perf_counter() - t0)
+    plain_s = sum(service)
+    # packed, all queued at t = 0
+    b = PKG.Batch(budget_bytes=150 << 30)
+    t0 = time.perf_counter()
+    tickets = [b.submit(s, n) for s, (_, n) in zip(setups, jobs)]
+    pending = set(tickets)
+    while pending:
+        b.run(32)
+        for t in list(pending):
+            if b.state(t)[0] >= PKG.JOB_DONE:
+                b.probe_series(t)
+                b.release(t)
+                pending.discard(t)
+    packed_s = time.perf_counter() - t0
+    # Poisson arrivals at 80 % of the packed throughput
+    rate = 0.8 * len(jobs) / packed_s
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, size=len(jobs)))
+    lat_packed = [0.0] * len(jobs)
+    t0 = time.perf_counter()
+    submitted, pending, tick = 0, {}, {}
+    while submitted < len(jobs) or pending:
+        now = time.perf_counter() - t0
+        while submitted < len(jobs) and arrivals[submitted] <= now:
+            pending[b.submit(setups[submitted], jobs[submitted][1])] = submitted
+            submitted += 1
+        if pending:
+            b.run(16)
+        else:
+            time.sleep(max(0.0, min(arrivals[submitted] - now, 0.01)))
+        now = time.perf_counter() - t0
+        for t, k in list(pending.items()):
+            if b.state(t)[0] >= PKG.JOB_DONE:
+                b.release(t)
+                lat_packed[k] = now - arrivals[k]
+                del pending[t]
+    b.close()
+    lat_plain, free_at = [], 0.0
+    for k in range(len(jobs)):
+        start = max(arrivals[k], free_at)
+        free_at = start + service[k]
+        lat_plain.append(free_at - arrivals[k])
+    pct = lambda v, q: round(float(np.percentile(v, q)) * 1e3, 2)
+    line = {
+        "metric": "solves/s (packed multi-solve engine)", "value": round(len(jobs) / packed_s, 3), "unit": "solves/s",
+        "n_gpus": 1, "steps": len(jobs), "warmup": 0, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "serving: stream of gain-slab microcavities, core edge 32-96 cells (aspect 1-2), "
+                               "200-1000 steps, 8-cell CPML, FP32", "jobs": len(jobs),
+                   "cell_updates": int(work), "budget_GB": 150},
+        "packed": {"seconds": round(packed_s, 3), "Mcell_updates_per_s": round(work / packed_s / 1e6, 1),
+                   "p50_ms": pct(lat_packed, 50), "p95_ms": pct(lat_packed, 95), "p99_ms": pct(lat_packed, 99)},
+        "one_at_a_time": {"seconds": round(plain_s, 3), "Mcell_updates_per_s": round(work / plain_s / 1e6, 1),
+                          "p50_ms": pct(lat_plain, 50), "p95_ms": pct(lat_plain, 95), "p99_ms": pct(lat_plain, 99)},
+        "throughput_ratio": round(plain_s / packed_s, 2),
+        "arrival_rate_per_s": round(rate, 2),
+    }
+    print(json.dumps(line))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -216,6 +335,9 @@ def main():
     ap.add_argument("--fdtd-steps", type=int, default=10, help="time steps per bench step")
     ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64", "fp16", "bf16"],
                     help="field storage; fp16/bf16 store E, H, psi in 16 bits and compute in FP32")
+    ap.add_argument("--serving", action="store_true",
+                    help="serving form: a stream of small solves through the packed engine (own JSON line)")
+    ap.add_argument("--serving-jobs", type=int, default=48)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     args = ap.parse_args()
@@ -224,6 +346,11 @@ def main():
     cfg, sample_cfg, desc = WORKLOADS[args.workload]
     rank, local, world, dist = dist_setup(args.gpus)
     S, K, W = args.fdtd_steps, args.steps, args.warmup
+
+    if args.serving and args.impl != "reference":
+        if rank == 0:
+            serving_bench(args)
+        return
 
     if args.impl == "reference":
         if rank != 0:
