@@ -49,6 +49,9 @@ WORKLOADS = {
     "b256": ("b256_gain_slab.params", "b512_gain_slab_cpu_sample.params",
              "256^3 core (280^3 total) uniform 20 nm, 12-cell CPML, n=3.4 slab with 200 nm two-level gain layer "
              "(pump 1e9/s), z dipole, Ez probe + 21-freq DFT"),
+    "c2": ("c2_spheres_512.params", "b512_gain_slab_cpu_sample.params",
+           "512^3 core (536^3 total) uniform 20 nm, 12-cell CPML, 4000 seeded dielectric spheres (r 3-12 cells, "
+           "eps_r 2-12), z dipole, Ez probe + 21-freq DFT"),
     "c1": ("c1_gain_slab.params", "c1_gain_slab.params",
            "C1 non-uniform mesh + gain slab (201x201x69 total)"),
     "c0": ("c0_dipole_sphere.params", "c0_dipole_sphere.params",
@@ -325,6 +328,46 @@ def serving_bench(args):
     print(json.dumps(line))
 
 
+def precision_study(args):
+    """The 512^3 sphere solve (or --workload's) for --study-steps steps as FP64, FP32, FP16 and
+    BF16 storage: field L2 (E and H), probe series, DFT and DFT-peak errors against FP64."""
+    import numpy as np
+    cfg, _, desc = WORKLOADS[args.workload]
+    setup = PKG.Setup.from_file(PKG.config_path(cfg))
+    n = args.study_steps
+    comps = ("Ex", "Ey", "Ez", "Hx", "Hy", "Hz")
+    ref, res = {}, {}
+    for name, prec in (("fp64", PKG.PREC_FP64), ("fp32", PKG.PREC_FP32), ("fp16", PKG.PREC_FP16),
+                       ("bf16", PKG.PREC_BF16)):
+        sol = PKG.Solver(setup, precision=prec)
+        sol.set_timing(PKG.TIMING_RUN)
+        sol.run(n)
+        ms = sol.timing()["run_ms"]
+        series, dft = sol.probe_series()[:, 0], sol.dft(0)
+        if name == "fp64":
+            ref = {"f": {c: sol.field(c) for c in comps}, "series": series, "dft": dft}
+            res[name] = {"ms": round(ms, 1)}
+        else:
+            num = {"E": 0.0, "H": 0.0}
+            den = {"E": 0.0, "H": 0.0}
+            for c in comps:
+                f = sol.field(c)
+                num[c[0]] += float(np.sum((f - ref["f"][c]) ** 2))
+                den[c[0]] += float(np.sum(ref["f"][c] ** 2))
+                del f
+            res[name] = {"ms": round(ms, 1),
+                         "E_L2": float(np.sqrt(num["E"] / den["E"])), "H_L2": float(np.sqrt(num["H"] / den["H"])),
+                         "probe": float(np.linalg.norm(series - ref["series"]) / np.linalg.norm(ref["series"])),
+                         "dft": float(np.abs(dft - ref["dft"]).max() / np.abs(ref["dft"]).max()),
+                         "dft_peak_same": bool(np.argmax(np.abs(dft)) == np.argmax(np.abs(ref["dft"])))}
+        sol.close()
+    cells = setup.shape[0] * setup.shape[1] * setup.shape[2]
+    for v in res.values():
+        v["Gcell_per_s"] = round(cells * n / (v["ms"] * 1e-3) / 1e9, 2)
+    print(json.dumps({"metric": "precision study (errors against the FP64 solve)", "workload": desc,
+                      "config_file": cfg, "steps": n, "results": res}))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -338,6 +381,9 @@ def main():
     ap.add_argument("--serving", action="store_true",
                     help="serving form: a stream of small solves through the packed engine (own JSON line)")
     ap.add_argument("--serving-jobs", type=int, default=48)
+    ap.add_argument("--precision-study", action="store_true",
+                    help="FP64 / FP32 / FP16 / BF16 errors on --workload (own JSON line)")
+    ap.add_argument("--study-steps", type=int, default=5000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     args = ap.parse_args()
@@ -346,6 +392,11 @@ def main():
     cfg, sample_cfg, desc = WORKLOADS[args.workload]
     rank, local, world, dist = dist_setup(args.gpus)
     S, K, W = args.fdtd_steps, args.steps, args.warmup
+
+    if args.precision_study and args.impl != "reference":
+        if rank == 0:
+            precision_study(args)
+        return
 
     if args.serving and args.impl != "reference":
         if rank == 0:
