@@ -31,9 +31,6 @@
 
 namespace fdtdk {
 
-constexpr unsigned kStatusTimeout = 2u;
-constexpr unsigned long long kWaitNs = 2000000000ull;  // 2 s bound on any mbarrier wait
-
 // Tile / pipeline shape: TX x TY cells per block (TX a multiple of 16 / sizeof(T)),
 // THREADS threads, DEPTH stages in flight ahead of the one being consumed.
 template <typename T, int TX_, int TY_, int THREADS_, int DEPTH_, int MINB_>
@@ -84,11 +81,6 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, unsigned parity) {
     return ok != 0;
 }
 
-__device__ __forceinline__ unsigned long long global_ns() {
-    unsigned long long t;
-    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-    return t;
-}
 
 // Bounded wait: false once kWaitNs of wall time have passed without the phase completing.
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity) {

@@ -27,6 +27,14 @@
 namespace fdtdk {
 
 constexpr unsigned kFull = 0xffffffffu;
+constexpr unsigned kStatusTimeout = 2u;                // status bit: a bounded device wait expired
+constexpr unsigned long long kWaitNs = 2000000000ull;  // 2 s bound on any device-side wait
+
+__device__ __forceinline__ unsigned long long global_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
 constexpr int kBlockY = 8;    // rows (warps) per block
 constexpr int kMaxSources = 8;
 
@@ -44,6 +52,10 @@ template <> struct Vec<float> {
     __device__ __forceinline__ static void st(float* p, const float (&a)[4]) {
         *reinterpret_cast<float4*>(p) = make_float4(a[0], a[1], a[2], a[3]);
     }
+    __device__ __forceinline__ static void ldcg(const float* p, float (&a)[4]) {
+        float4 t = __ldcg(reinterpret_cast<const float4*>(p));
+        a[0] = t.x; a[1] = t.y; a[2] = t.z; a[3] = t.w;
+    }
 };
 template <> struct Vec<double> {
     static constexpr int W = 2;
@@ -58,6 +70,10 @@ template <> struct Vec<double> {
     __device__ __forceinline__ static void st(double* p, const double (&a)[2]) {
         *reinterpret_cast<double2*>(p) = make_double2(a[0], a[1]);
     }
+    __device__ __forceinline__ static void ldcg(const double* p, double (&a)[2]) {
+        double2 t = __ldcg(reinterpret_cast<const double2*>(p));
+        a[0] = t.x; a[1] = t.y;
+    }
 };
 
 // Field / psi storage.  S is the type held in memory, T the type the update computes in;
@@ -68,10 +84,17 @@ template <typename T> struct Fld<T, T> {
     __device__ __forceinline__ static void ld(const T* p, T (&a)[Vec<T>::W]) { Vec<T>::ld(p, a); }
     __device__ __forceinline__ static void ldg(const T* p, T (&a)[Vec<T>::W]) { Vec<T>::ldg(p, a); }
     __device__ __forceinline__ static void st(T* p, const T (&a)[Vec<T>::W]) { Vec<T>::st(p, a); }
+    __device__ __forceinline__ static void ldcg(const T* p, T (&a)[Vec<T>::W]) { Vec<T>::ldcg(p, a); }
 };
 template <> struct Fld<__half, float> {
     __device__ __forceinline__ static void ld(const __half* p, float (&a)[4]) {
         const uint2 u = *reinterpret_cast<const uint2*>(p);
+        const float2 lo = __half22float2(*reinterpret_cast<const __half2*>(&u.x));
+        const float2 hi = __half22float2(*reinterpret_cast<const __half2*>(&u.y));
+        a[0] = lo.x; a[1] = lo.y; a[2] = hi.x; a[3] = hi.y;
+    }
+    __device__ __forceinline__ static void ldcg(const __half* p, float (&a)[4]) {
+        const uint2 u = __ldcg(reinterpret_cast<const uint2*>(p));
         const float2 lo = __half22float2(*reinterpret_cast<const __half2*>(&u.x));
         const float2 hi = __half22float2(*reinterpret_cast<const __half2*>(&u.y));
         a[0] = lo.x; a[1] = lo.y; a[2] = hi.x; a[3] = hi.y;
@@ -97,6 +120,12 @@ template <> struct Fld<__nv_bfloat16, float> {
         const float2 hi = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&u.y));
         a[0] = lo.x; a[1] = lo.y; a[2] = hi.x; a[3] = hi.y;
     }
+    __device__ __forceinline__ static void ldcg(const __nv_bfloat16* p, float (&a)[4]) {
+        const uint2 u = __ldcg(reinterpret_cast<const uint2*>(p));
+        const float2 lo = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&u.x));
+        const float2 hi = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&u.y));
+        a[0] = lo.x; a[1] = lo.y; a[2] = hi.x; a[3] = hi.y;
+    }
     __device__ __forceinline__ static void ldg(const __nv_bfloat16* p, float (&a)[4]) {
         const uint2 u = __ldg(reinterpret_cast<const uint2*>(p));
         const float2 lo = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&u.x));
@@ -111,6 +140,18 @@ template <> struct Fld<__nv_bfloat16, float> {
         *reinterpret_cast<uint2*>(p) = u;
     }
 };
+
+// Scalar load through L2 only (no L1): values another SM wrote during this launch.
+__device__ __forceinline__ float ldcg1(const float* p) { return __ldcg(p); }
+__device__ __forceinline__ double ldcg1(const double* p) { return __ldcg(p); }
+__device__ __forceinline__ __half ldcg1(const __half* p) {
+    const unsigned short u = __ldcg(reinterpret_cast<const unsigned short*>(p));
+    return *reinterpret_cast<const __half*>(&u);
+}
+__device__ __forceinline__ __nv_bfloat16 ldcg1(const __nv_bfloat16* p) {
+    const unsigned short u = __ldcg(reinterpret_cast<const unsigned short*>(p));
+    return *reinterpret_cast<const __nv_bfloat16*>(&u);
+}
 
 // Scalar conversions between the storage and compute types.
 __device__ __forceinline__ float to_c(float v) { return v; }
@@ -462,9 +503,19 @@ k_update_H(const StepArgs<S, T> a, const int kchunk, const SweepGeom g) {
 }
 
 // ---------------------------------------------------------------------------------
-template <typename S, typename T, bool EDGE>
+// CG: H is read through L2 only -- the slab-ordered step (k_step_slabs) reads H that other
+// SMs wrote in the same launch, which a stale L1 line could hide.
+template <typename S, typename T, bool EDGE, bool CG = false>
 __device__ __forceinline__ void e_column(const StepArgs<S, T>& a, const SweepGeom& g, const ESrc& src, const int j,
                                          const int i0, const bool act, const int kb, const int ke, const int lane) {
+    auto ldH = [](const S* p, T (&v)[Vec<T>::W]) {
+        if constexpr (CG) Fld<S, T>::ldcg(p, v);
+        else Fld<S, T>::ldg(p, v);
+    };
+    auto ldH1 = [](const S* p) -> T {
+        if constexpr (CG) return T(to_c(ldcg1(p)));
+        else return T(to_c(*p));
+    };
     constexpr int W = Vec<T>::W;
     const int np = a.np, np2 = 2 * np;
 
@@ -488,8 +539,8 @@ __device__ __forceinline__ void e_column(const StepArgs<S, T>& a, const SweepGeo
     const size_t row = size_t(j) * a.NxP + i0;
     T hxm[W], hym[W];  // Hx, Hy at k-1
     if (act) {
-        Fld<S, T>::ldg(a.Hx + size_t(kb - 1) * a.plane + row, hxm);
-        Fld<S, T>::ldg(a.Hy + size_t(kb - 1) * a.plane + row, hym);
+        ldH(a.Hx + size_t(kb - 1) * a.plane + row, hxm);
+        ldH(a.Hy + size_t(kb - 1) * a.plane + row, hym);
     } else {
 #pragma unroll
         for (int e = 0; e < W; ++e) hxm[e] = hym[e] = T(0);
@@ -505,18 +556,18 @@ __device__ __forceinline__ void e_column(const StepArgs<S, T>& a, const SweepGeo
             Vec<T>::ldg(a.bEx + c, bx);
             Vec<T>::ldg(a.bEy + c, by);
             Vec<T>::ldg(a.bEz + c, bz);
-            Fld<S, T>::ldg(a.Hx + c, hx);
-            Fld<S, T>::ldg(a.Hy + c, hy);
-            Fld<S, T>::ldg(a.Hz + c, hz);
-            Fld<S, T>::ldg(a.Hz + c - a.NxP, hzj);
-            Fld<S, T>::ldg(a.Hx + c - a.NxP, hxj);
+            ldH(a.Hx + c, hx);
+            ldH(a.Hy + c, hy);
+            ldH(a.Hz + c, hz);
+            ldH(a.Hz + c - a.NxP, hzj);
+            ldH(a.Hx + c - a.NxP, hxj);
         } else {
 #pragma unroll
             for (int e = 0; e < W; ++e)
                 ex[e] = ey[e] = ez[e] = bx[e] = by[e] = bz[e] = hx[e] = hy[e] = hz[e] = hzj[e] = hxj[e] = T(0);
         }
         T hze = T(0), hye = T(0);
-        if (pload && act && i0 > 0) { hze = to_c(a.Hz[c - 1]); hye = to_c(a.Hy[c - 1]); }
+        if (pload && act && i0 > 0) { hze = ldH1(a.Hz + c - 1); hye = ldH1(a.Hy + c - 1); }
         const T idz = __ldg(a.idz + k);
         const bool zpml = in_pml(k, a.NzT, np);
         T zb = 1, zc = 0, zik = 1;
@@ -636,7 +687,7 @@ __device__ __forceinline__ void e_column(const StepArgs<S, T>& a, const SweepGeo
     }
 }
 
-template <typename S, typename T>
+template <typename S, typename T, bool CG = false>
 __device__ __forceinline__ void update_E_block(const StepArgs<S, T>& a, const int kchunk, const ESrc& src,
                                                const SweepGeom& g, const int bx, const int by, const int bz) {
     constexpr int W = Vec<T>::W;
@@ -649,7 +700,7 @@ __device__ __forceinline__ void update_E_block(const StepArgs<S, T>& a, const in
         const int j = by * kBlockY + threadIdx.y;
         if (j < 1 || j >= a.NyT) return;  // E is updated for j >= 1 only; whole warp
         const int i0 = g.xi0 + (bx * 32 + lane) * W;
-        e_column<S, T, false>(a, g, src, j, i0, i0 < g.xi1, kb, ke, lane);
+        e_column<S, T, false, CG>(a, g, src, j, i0, i0 < g.xi1, kb, ke, lane);
     } else {
         const int t = threadIdx.y * 32 + lane;
         const int rr = t / g.ne, v = t - rr * g.ne;
@@ -657,7 +708,7 @@ __device__ __forceinline__ void update_E_block(const StepArgs<S, T>& a, const in
         if (rr >= g.er || j < 1 || j >= a.NyT) return;
         const int i0 = v < g.nl ? v * W : g.xi1 + (v - g.nl) * W;
         if (i0 >= a.NxT) return;
-        e_column<S, T, true>(a, g, src, j, i0, true, kb, ke, lane);
+        e_column<S, T, true, CG>(a, g, src, j, i0, true, kb, ke, lane);
     }
 }
 
@@ -665,6 +716,76 @@ template <typename S, typename T>
 __global__ void __launch_bounds__(32 * kBlockY, 2)
 k_update_E(const StepArgs<S, T> a, const int kchunk, const ESrc src, const SweepGeom g) {
     update_E_block<S, T>(a, kchunk, src, g, blockIdx.x, blockIdx.y, blockIdx.z);
+}
+
+// ---------------------------------------------------------------------------------
+// Slab-ordered step: one persistent launch does the whole H + E step in slabs of P planes,
+// in the order H(0), H(1), E(0), H(2), E(1), ..., E(n-1), handed out through a global work
+// counter.  The schedule is a valid order for the Yee step: H(k) reads E(k), E(k+1) (not yet
+// updated: E of a slab is written only after H of that slab and of the slab below are done),
+// E(k) reads H(k), H(k-1) (done: E(s) waits for H(s) and H(s-1)).  E(s) runs about one slab
+// after H(s), while the E and H planes it reads are still in L2, so a cell costs DRAM bytes
+// for E, H and bE once each instead of E and H twice.  Blocks wait only on work handed out
+// before theirs (already running), so the waits always end; each is bounded by 2 s all the
+// same, after which the block flags the status word and leaves.
+struct SlabPlan {
+    int P;          // planes per slab
+    int nslab;
+    int gxH, nH;    // H tiles per slab: gxH columns x (nH / gxH) row groups
+    int gxE, nE;
+};
+
+__device__ __forceinline__ unsigned ld_acquire(const unsigned* p) {
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+template <typename S, typename T>
+__global__ void __launch_bounds__(32 * kBlockY, 2)
+k_step_slabs(const StepArgs<S, T> a, const ESrc src, const SweepGeom g, const SlabPlan p, unsigned* ctr,
+             unsigned* status_w) {
+    __shared__ int item_s;
+    const int tid = threadIdx.y * 32 + threadIdx.x;
+    const long long total = (long long)p.nslab * (p.nH + p.nE);
+    unsigned* const hdone = ctr + 1;
+    for (;;) {
+        if (tid == 0) item_s = int(atomicAdd(ctr, 1u));
+        __syncthreads();
+        const long long it = item_s;
+        __syncthreads();
+        if (it >= total) return;
+        // order: H(0) | H(1) E(0) | H(2) E(1) | ... | E(n-1)
+        int slab, r;
+        bool isH;
+        if (it < p.nH) { isH = true; slab = 0; r = int(it); }
+        else {
+            const long long q = it - p.nH;
+            const int pair = int(q / (p.nH + p.nE)), r2 = int(q % (p.nH + p.nE));
+            if (pair < p.nslab - 1 && r2 < p.nH) { isH = true; slab = pair + 1; r = r2; }
+            else { isH = false; slab = pair; r = pair < p.nslab - 1 ? r2 - p.nH : r2; }
+        }
+        if (isH) {
+            update_H_block<S, T>(a, p.P, g, r % p.gxH, r / p.gxH, slab);
+            __threadfence();  // this thread's H stores, before the block signals
+            __syncthreads();
+            if (tid == 0) atomicAdd(hdone + slab, 1u);
+        } else {
+            bool ok = true;
+            if (tid == 0) {
+                const unsigned long long t0 = global_ns();
+                while (ld_acquire(hdone + slab) < unsigned(p.nH) || (slab > 0 && ld_acquire(hdone + slab - 1) < unsigned(p.nH))) {
+                    if (global_ns() - t0 > kWaitNs) { ok = false; break; }
+                }
+            }
+            if (!__syncthreads_and(ok)) {
+                if (tid == 0) atomicOr(status_w, kStatusTimeout);
+                return;
+            }
+            update_E_block<S, T, true>(a, p.P, src, g, r % p.gxE, r / p.gxE, slab);
+            __syncthreads();
+        }
+    }
 }
 
 }  // namespace fdtdk

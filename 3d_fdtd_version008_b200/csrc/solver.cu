@@ -445,7 +445,8 @@ public:
     void sync() override { ck(cudaStreamSynchronize(st_), "cudaStreamSynchronize"); }
     void set_timing(int mode) override;
     void set_path(int path) override {
-        if (path != 0 && path != 1) throw Failure(FDTD_ERR_INVALID, "kernel path must be 0 (fused) or 1 (two-sweep)");
+        if (path < 0 || path > 2)
+            throw Failure(FDTD_ERR_INVALID, "kernel path must be 0 (fused), 1 (two sweeps) or 2 (slab-ordered step)");
         if (path == 0 && !std::is_same_v<S, T>) throw Failure(FDTD_ERR_UNSUPPORTED, "the fused path needs FP32 or FP64 storage");
         if (steps != 0) throw Failure(FDTD_ERR_INVALID, "the kernel path can only change before the first step");
         path_ = path;
@@ -489,6 +490,11 @@ private:
     size_t plane_, nflat_;
     int kchunkH_ = 1, kchunkE_ = 1;
     SweepGeom geom_{};
+    // path 2: k_step_slabs (persistent, slab-ordered H + E in one launch)
+    SlabPlan plan_{};
+    unsigned* d_ctr_ = nullptr;
+    dim3 gridS_;
+    void setup_slabs();
     dim3 gridH_, gridE_;
     double dt_;
     // sources
@@ -769,6 +775,26 @@ Solver<S, T>::Solver(const fdtd_setup_v1& s, int dev) {
     gridE_ = dim3(gx, gyE, (NzT_ + kchunkE_ - 1) / kchunkE_);
     if (const char* p = std::getenv("FDTD_B200_KERNEL_PATH")) set_path(std::atoi(p));
     ck(cudaStreamSynchronize(st_), "setup upload");
+}
+
+template <typename S, typename T>
+void Solver<S, T>::setup_slabs() {
+    int P = 4;
+    if (const char* e = std::getenv("FDTD_B200_SLAB_PLANES")) P = std::max(1, std::atoi(e));
+    plan_.P = P;
+    plan_.nslab = (NzT_ + P - 1) / P;
+    plan_.gxH = int(gridH_.x);
+    plan_.nH = int(gridH_.x * gridH_.y);
+    plan_.gxE = int(gridE_.x);
+    plan_.nE = int(gridE_.x * gridE_.y);
+    if ((long long)plan_.nslab * (plan_.nH + plan_.nE) > 0x7fffffffLL) throw Failure(FDTD_ERR_INVALID, "grid too large for the slab-ordered step");
+    d_ctr_ = alloc<unsigned>(size_t(plan_.nslab) + 1);
+    int sms = 148, per = 0;
+    ck(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device), "cudaDeviceGetAttribute");
+    ck(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_step_slabs<S, T>, 32 * kBlockY, 0),
+       "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
+    if (per < 1) throw Failure(FDTD_ERR_CUDA, "slab-ordered step kernel does not fit on an SM");
+    gridS_ = dim3(unsigned(sms * per));
 }
 
 template <typename S, typename T>
@@ -1078,6 +1104,7 @@ void Solver<S, T>::run(uint64_t n) {
     if constexpr (std::is_same_v<S, T>) {
         if (path_ == 0) ensure_fused();
     }
+    if (path_ == 2 && !d_ctr_) setup_slabs();
     const uint64_t n0 = steps;
     const uint64_t last = n0 + n;  // exclusive
     ensure_series((last + save_every_ - 1) / save_every_);
@@ -1117,6 +1144,12 @@ void Solver<S, T>::run(uint64_t n) {
             point_args_at(cur_);
             launches += 1;
             }
+        } else if (path_ == 2) {
+            ck(cudaMemsetAsync(d_ctr_, 0, (size_t(plan_.nslab) + 1) * sizeof(unsigned), st_), "cudaMemsetAsync");
+            if (per_kernel) ck(cudaEventRecord(ev_[0], st_), "cudaEventRecord");
+            k_step_slabs<S, T><<<gridS_, blk, 0, st_>>>(a_, src, geom_, plan_, d_ctr_, d_status_);
+            if (per_kernel) ck(cudaEventRecord(ev_[1], st_), "cudaEventRecord");
+            launches += 1;
         } else {
             k_update_H<S, T><<<gridH_, blk, 0, st_>>>(a_, kchunkH_, geom_);
             if (per_kernel) ck(cudaEventRecord(ev_[1], st_), "cudaEventRecord");

@@ -453,12 +453,13 @@ def main():
     steps_total = K * S
     value = replica_value(cells, steps_total, world, dev_ms_max)
     peak, peak_src = peaks()
-    fused = os.environ.get("FDTD_B200_KERNEL_PATH", "1") == "0"
+    path = int(os.environ.get("FDTD_B200_KERNEL_PATH", "1"))
+    fused = path in (0, 2)  # one launch per step carries the whole step's bytes
     e_avg_ms = tm["e_ms"] / tm["steps"]
     h_avg_ms = tm["h_ms"] / tm["steps"]
     achieved_step = alg["step_bytes"] / ((e_avg_ms + h_avg_ms) * 1e-3) / 1e9
     if fused:  # one launch per step: the dominant kernel carries the whole step's bytes
-        kern, kern_bytes, kern_ms = "k_step_fused", alg["step_bytes"], e_avg_ms + h_avg_ms
+        kern, kern_bytes, kern_ms = ("k_step_fused" if path == 0 else "k_step_slabs"), alg["step_bytes"], e_avg_ms + h_avg_ms
     else:
         kern, kern_bytes, kern_ms = "k_update_E", alg["e_bytes"], e_avg_ms
     achieved_e = kern_bytes / (kern_ms * 1e-3) / 1e9
@@ -521,7 +522,8 @@ def main():
         "data": "synthetic",
         "config": {"workload": desc, "config_file": cfg, "total_cells": cells, "grid": list(setup.shape),
                    "fdtd_steps_per_step": S, "parallelism": "replicas" if world > 1 else "single GPU",
-                   "kernel_path": "fused H+E (TMA)" if fused else "separate H and E sweeps",
+                   "kernel_path": {0: "fused H+E (TMA)", 1: "separate H and E sweeps",
+                                   2: "slab-ordered H+E step (one launch, L2-resident slabs)"}[path],
                    "fused_shape": os.environ.get("FDTD_B200_FUSED_SHAPE", "0"),
                    "l2": "state (~%.1f GB) larger than L2, no flush" % (alg["cells"] * word * 9 / 1e9),
                    "hbm_gbs_step": round(achieved_step, 1),

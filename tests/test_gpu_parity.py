@@ -234,11 +234,11 @@ def test_diagnostics_match_oracle_integrals(pkg, oracle):
 
 
 @pytest.mark.parametrize("precision,tol", [(1, 1e-13), (0, 2e-6)])
-def test_fused_and_two_sweep_paths_agree(pkg, precision, tol):
+def test_kernel_paths_agree(pkg, precision, tol):
     """The fused H+E launch and the separate sweeps compute the same update (rounding aside)."""
     s = pkg.Setup.from_file(GOLDEN / "cases" / "step_g1_gain.params", overrides={"PUMP_RATE": "1e11"})
     out = []
-    for path in (0, 1):
+    for path in (0, 1, 2):
         sol = pkg.Solver(s, precision=precision, kernel_path=path)
         rng = np.random.default_rng(11)
         for c in ("Ex", "Ey", "Ez"):
@@ -246,16 +246,18 @@ def test_fused_and_two_sweep_paths_agree(pkg, precision, tol):
         sol.run(33)
         out.append((fields(sol), {c: sol.tls_state(c) for c in ("Pz", "Nu")}, sol.probe_series()))
         sol.close()
-    (f0, g0, p0), (f1, g1, p1) = out
-    assert field_rel_l2(f0, f1, "E") <= tol and field_rel_l2(f0, f1, "H") <= tol
-    assert rel(g0["Pz"], g1["Pz"]) <= max(tol, 1e-5) and rel(g0["Nu"], g1["Nu"]) <= max(tol, 1e-6)
-    assert rel(p0, p1) <= tol
+    f1, g1, p1 = out[1]  # the two sweeps; the fused launch and the slab-ordered step against them
+    for f0, g0, p0 in (out[0], out[2]):
+        assert field_rel_l2(f0, f1, "E") <= tol and field_rel_l2(f0, f1, "H") <= tol
+        assert rel(g0["Pz"], g1["Pz"]) <= max(tol, 1e-5) and rel(g0["Nu"], g1["Nu"]) <= max(tol, 1e-6)
+        assert rel(p0, p1) <= tol
 
 
+@pytest.mark.parametrize("path", [1, 2])
 @pytest.mark.parametrize("precision,tol", [(1, 1e-12), (0, 1e-5)])
-def test_two_sweep_path_matches_reference(pkg, precision, tol):
+def test_sweep_paths_match_reference(pkg, precision, tol, path):
     g, s, _ = golden_solver(pkg, "step_g0_sphere", precision)
-    sol = pkg.Solver(s, precision=precision, kernel_path=1)
+    sol = pkg.Solver(s, precision=precision, kernel_path=path)
     sol.run(g["meta"]["steps"])
     ref = ref_fields(g, sol.shape)
     mine = fields(sol)
@@ -288,8 +290,12 @@ def test_kernel_path_fixed_after_first_step(pkg):
         sol.set_kernel_path(1)
 
 
-def test_fused_path_tile_edges_on_odd_grid(pkg, oracle):
-    """Fused path on a grid that is not a multiple of its tile in any axis, CPML on every face."""
+@pytest.mark.parametrize("path,planes", [(0, ""), (2, "1"), (2, "3"), (2, "4")])
+def test_tile_edges_on_odd_grid(pkg, oracle, path, planes, monkeypatch):
+    """A grid that is not a multiple of the fused tile or of the slab-ordered step's slab in any
+    axis, CPML on every face; the slab-ordered step with 1, 3 and 4 planes per slab."""
+    if planes:
+        monkeypatch.setenv("FDTD_B200_SLAB_PLANES", planes)
     text = (GOLDEN / "cases" / "step_g0_sphere.params").read_text()
     text = text.replace("NX = 10", "NX = 71").replace("NY = 9", "NY = 37").replace("NZ = 8", "NZ = 45")
     text = text.replace("DOMAIN_X_MAX = 250e-9", "DOMAIN_X_MAX = 1775e-9").replace("DOMAIN_Y_MAX = 225e-9", "DOMAIN_Y_MAX = 925e-9")
@@ -298,7 +304,7 @@ def test_fused_path_tile_edges_on_odd_grid(pkg, oracle):
     o = oracle.OracleSolve(s, 0)
     o.run(80)
     for precision, tol in ((1, 1e-12), (0, 1e-5)):
-        sol = pkg.Solver(s, precision=precision, kernel_path=0)
+        sol = pkg.Solver(s, precision=precision, kernel_path=path)
         sol.run(80)
         ref = {c: o.field(c) for c in FIELDS}
         mine = fields(sol)
