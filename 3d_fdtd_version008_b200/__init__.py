@@ -81,6 +81,13 @@ class ProbeV1(C.Structure):
                 ("reserved", C.c_int32)]
 
 
+class SheetV1(C.Structure):
+    _fields_ = [("axis", C.c_int32), ("comp", C.c_int32), ("plane", C.c_uint64), ("lo0", C.c_uint64),
+                ("hi0", C.c_uint64), ("lo1", C.c_uint64), ("hi1", C.c_uint64), ("d", C.c_double),
+                ("sign", C.c_double), ("waveform", C.c_int32), ("reserved", C.c_int32), ("E0", C.c_double),
+                ("f0", C.c_double), ("tau", C.c_double), ("t0", C.c_double), ("t_shift", C.c_double)]
+
+
 class SetupV1(C.Structure):
     _fields_ = [
         ("struct_size", C.c_uint32), ("precision", C.c_int32),
@@ -100,6 +107,7 @@ class SetupV1(C.Structure):
         ("monitor_interval", C.c_uint32), ("max_E", C.c_double), ("max_P", C.c_double),
         ("conservation_err", C.c_double), ("growth_rate", C.c_double),
         ("field_scale", C.c_double),
+        ("n_sheets", C.c_uint32), ("sheets", C.POINTER(SheetV1)),
     ]
 
 

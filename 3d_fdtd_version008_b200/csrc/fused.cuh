@@ -384,6 +384,7 @@ k_step_fused(const __grid_constant__ FusedMaps maps, const FusedArgs<T> f, const
                             }
                         }
                     }
+                    if (src.ns) sheet_J(src, i, ej, ke, Jx, Jy, Jz);
                     ex[e] = ex[e] + bx[e] * ((dHz_dy - dHy_dz) - Jx);
                     ey[e] = ey[e] + by[e] * ((dHx_dz - dHz_dx) - Jy);
                     int r = -1;

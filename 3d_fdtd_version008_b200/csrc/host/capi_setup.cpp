@@ -13,8 +13,21 @@ struct fdtd_setup {
     std::vector<fdtd_dipole_v1> dipoles;
     std::vector<fdtd_tls_region_v1> regions;
     std::vector<fdtd_probe_v1> probes;
+    std::vector<fdtd_sheet_v1> sheets;
     std::vector<double> uniform_kappa[3], unit_b[3], zero_c[3];
+    // aE = aH = 1 and bH uniform everywhere (lossless, mu_r = 1 -- what make_nk gives): the
+    // view then passes those arrays as NULL and the stepper skips scanning them
+    bool uniform_ah = false;
 };
+
+namespace {
+bool all_equal(const std::vector<double>& v, double x) {
+    long long bad = 0;
+#pragma omp parallel for reduction(+ : bad) schedule(static)
+    for (long long q = 0; q < (long long)v.size(); ++q) bad += v[q] != x;
+    return bad == 0;
+}
+}  // namespace
 
 namespace {
 
@@ -91,6 +104,14 @@ int fdtd_setup_parse(const char* params_text, int mesh_only, fdtd_setup** out, c
                                   r.params.enable_population_clamp ? 1 : 0, 0});
         for (const auto& p : S.probes)
             for (int c : p.components) s->probes.push_back({p.i, p.j, p.k, c, 0});
+        for (const auto& w : S.plane_waves)
+            s->sheets.push_back({w.axis, w.comp, w.plane, w.lo0, w.hi0, w.lo1, w.hi1, w.d, w.sign, int32_t(w.waveform), 0,
+                                 w.E0, w.f0, w.tau, w.t0, w.t_shift});
+        bool u = !S.mats.bH[0].empty();
+        for (int a = 0; a < 3 && u; ++a)
+            u = !S.mats.aE[a].empty() && !S.mats.aH[a].empty() && !S.mats.bH[a].empty() && all_equal(S.mats.aE[a], 1.0) &&
+                all_equal(S.mats.aH[a], 1.0) && all_equal(S.mats.bH[a], S.mats.bH[0][0]);
+        s->uniform_ah = u;
         *out = s;
         return FDTD_OK;
     } catch (const std::exception& e) {
@@ -119,11 +140,13 @@ int fdtd_setup_view(const fdtd_setup* s, fdtd_setup_v1* v) {
         v->cpml_bE[a] = S.cpml.bE[a].data(); v->cpml_cE[a] = S.cpml.cE[a].data();
         v->cpml_bH[a] = S.cpml.bH[a].data(); v->cpml_cH[a] = S.cpml.cH[a].data();
         v->bE[a] = S.mats.bE[a].empty() ? nullptr : S.mats.bE[a].data();
-        v->aE[a] = S.mats.aE[a].empty() ? nullptr : S.mats.aE[a].data();
-        v->aH[a] = S.mats.aH[a].empty() ? nullptr : S.mats.aH[a].data();
-        v->bH[a] = S.mats.bH[a].empty() ? nullptr : S.mats.bH[a].data();
+        v->aE[a] = (s->uniform_ah || S.mats.aE[a].empty()) ? nullptr : S.mats.aE[a].data();
+        v->aH[a] = (s->uniform_ah || S.mats.aH[a].empty()) ? nullptr : S.mats.aH[a].data();
+        v->bH[a] = (s->uniform_ah || S.mats.bH[a].empty()) ? nullptr : S.mats.bH[a].data();
     }
-    v->bH_uniform = S.dt / fdtd::phys::MU0;
+    v->bH_uniform = s->uniform_ah ? S.mats.bH[0][0] : S.dt / fdtd::phys::MU0;
+    v->n_sheets = uint32_t(s->sheets.size());
+    v->sheets = s->sheets.data();
     v->n_dipoles = uint32_t(s->dipoles.size());
     v->dipoles = s->dipoles.data();
     v->n_tls_regions = uint32_t(s->regions.size());

@@ -661,7 +661,48 @@ SimSetup SimSetup::from_params(const ParamFile& pf, bool bake) {
         }
         S.sources.push_back(src);
     }
-    require(pf.list("PLANE_WAVE_SOURCES").empty(), "PLANE_WAVE_SOURCES are not supported by the stepper yet");
+    // Plane-wave soft sources (make_plane_wave_source, src/sources/plane_wave_source.hpp:201-290,
+    // registered after the dipoles at src/params.hpp:643-679).
+    for (const auto& s : pf.list("PLANE_WAVE_SOURCES")) {
+        require(s.size() >= 17, "PLANE_WAVE_SOURCES entry needs 17 fields (PlaneWaveSourceDef order)");
+        if (!parse_bool(s[0])) continue;
+        const real pos = field(s, 1), amplitude = field(s, 2), frequency = field(s, 3), wavelength = field(s, 4);
+        const real tau = field(s, 5), df = field(s, 6), t0f = field(s, 7);
+        PlaneWave w;
+        w.waveform = to_waveform(int(field(s, 8)));
+        const int dir = int(field(s, 9));  // 0 +X, 1 -X, 2 +Y, 3 -Y, 4 +Z, 5 -Z, otherwise +Z
+        const int pol = to_polarization(int(field(s, 10)));
+        w.axis = (dir == 0 || dir == 1) ? 0 : (dir == 2 || dir == 3) ? 1 : 2;
+        w.sign = (dir == 1 || dir == 3 || dir == 5) ? -1.0 : 1.0;
+        const real c0 = 299792458.0;
+        w.f0 = frequency > 0.0 ? frequency : (wavelength > 0.0 ? c0 / wavelength : c0 / 500e-9);
+        w.tau = tau > 0.0 ? tau : (df > 0.0 ? 2.0 * std::sqrt(std::log(2.0)) / (std::numbers::pi * df) : 20.0 * S.dt);
+        w.t0 = t0f > 0.0 ? t0f * w.tau : 3.0 / w.f0;
+        w.t_shift = w.t0;
+        w.E0 = amplitude;
+        const std::size_t Nax[3] = {S.NxT, S.NyT, S.NzT}, np = S.npml;
+        std::size_t pi = S.grid.physical_to_index(w.axis, pos - S.domain_min[w.axis]);
+        pi = std::max(np + 1, std::min(pi, Nax[w.axis] - np - 2));
+        w.plane = pi;
+        const real mins[3] = {field(s, 11), field(s, 13), field(s, 15)}, maxs[3] = {field(s, 12), field(s, 14), field(s, 16)};
+        std::size_t lo[3], hi[3];
+        for (int a = 0; a < 3; ++a) {  // compute_bounds, on the domain-shifted coordinates
+            const real mn = mins[a] - S.domain_min[a], mx = maxs[a] - S.domain_min[a];
+            if (mn == 0.0 && mx == 0.0) { lo[a] = np; hi[a] = Nax[a] - np - 1; }
+            else {
+                lo[a] = std::max(np, S.grid.physical_to_index(a, mn));
+                hi[a] = std::min(Nax[a] - np - 1, S.grid.physical_to_index(a, mx));
+            }
+        }
+        const int u = w.axis == 0 ? 1 : 0, v = w.axis == 2 ? 1 : 2;  // in-plane axes
+        w.lo0 = lo[u]; w.hi0 = hi[u]; w.lo1 = lo[v]; w.hi1 = hi[v];
+        const std::vector<real>& dd = w.axis == 0 ? S.grid.dx : w.axis == 1 ? S.grid.dy : S.grid.dz;
+        w.d = dd[pi];
+        const int pc = pol % 3;  // Ex/Hx, Ey/Hy, Ez/Hz; only the two in-plane components are driven
+        w.comp = pc == w.axis ? -1 : pc;
+        if (w.comp >= 0) S.plane_waves.push_back(w);
+    }
+    require(S.plane_waves.size() <= 2, "at most 2 plane-wave sources");
 
     // Two-level gain regions (src/3D_FDTD_version008.cpp:100-164,
     // TLSRegionManager::add_region_from_structure / initialize, src/two_level_system.hpp:503-546).

@@ -188,6 +188,14 @@ struct DipoleSource {  // src/sources/dipole_source.hpp:11-85
     real current_density(std::size_t n, real dt) const;
 };
 
+struct PlaneWave {  // PlaneWaveSource (src/sources/plane_wave_source.hpp:19-72,201-290)
+    int axis = 2, comp = 0;     // propagation axis; J component driven (-1: none)
+    std::size_t plane = 0, lo0 = 0, hi0 = 0, lo1 = 0, hi1 = 0;
+    real d = 1, sign = 1;
+    Waveform waveform = Waveform::GaussianModulatedSine;
+    real E0 = 0, f0 = 0, tau = 0, t0 = 0, t_shift = 0;
+};
+
 // ---------------------------------------------------------------- two-level gain
 struct TlsParams {  // TwoLevelParams (src/two_level_system.hpp:17-110)
     real lambda0 = 1500e-9, omega_a = 0, gamma = 7e12, tau = 1e-12, mu_z = 0, N0_total = 1e25;
@@ -240,6 +248,7 @@ struct SimSetup {
     Scene scene;
     MaterialGrids mats;
     std::vector<DipoleSource> sources;
+    std::vector<PlaneWave> plane_waves;
     TlsSetup tls;
     std::vector<PointProbe> probes;
     // build-only keys

@@ -216,12 +216,20 @@ struct StepArgs {
     T psc;                            // psi scale (16-bit storage: 1 / dx_min; else 1)
 };
 
+constexpr int kMaxSheets = 2;
+
 // Per-step arguments of the E kernel.
 struct ESrc {
     int n;                 // number of point sources
     int parity;            // step & 1
     int si[kMaxSources], sj[kMaxSources], sk[kMaxSources], sc[kMaxSources];
     double J[kMaxSources]; // I((n+1/2)dt)/cell_area
+    // plane-wave sheets: J added on plane `pl` normal to `ax` over [lo0, hi0] x [lo1, hi1]
+    // (in-plane axes in x, y, z order), component `pc`
+    int ns;
+    int ax[kMaxSheets], pc[kMaxSheets], pl[kMaxSheets];
+    int lo0[kMaxSheets], hi0[kMaxSheets], lo1[kMaxSheets], hi1[kMaxSheets];
+    double sJ[kMaxSheets];
 };
 
 __device__ __forceinline__ bool in_pml(int n, int N, int np) { return n < np || n >= N - np; }
@@ -260,12 +268,40 @@ __device__ __forceinline__ void xpsi_store(S* p3, S* p4, const StepArgs<S, T>& a
     }
 }
 
-// True when a point source sits on one of the W cells (i0.., j, k).
+// True when a point source or (SH) a plane-wave sheet touches one of the W cells (i0.., j, k).
+template <bool SH>
 __device__ __forceinline__ bool src_in_vector(const ESrc& src, int i0, int j, int k, int W) {
     bool hit = false;
     for (int s = 0; s < src.n; ++s)
         hit |= src.sj[s] == j && src.sk[s] == k && src.si[s] >= i0 && src.si[s] < i0 + W;
+    if constexpr (SH) for (int s = 0; s < src.ns; ++s) {
+        if (src.ax[s] == 2)
+            hit |= k == src.pl[s] && j >= src.lo1[s] && j <= src.hi1[s] && i0 + W > src.lo0[s] && i0 <= src.hi0[s];
+        else if (src.ax[s] == 1)
+            hit |= j == src.pl[s] && k >= src.lo1[s] && k <= src.hi1[s] && i0 + W > src.lo0[s] && i0 <= src.hi0[s];
+        else
+            hit |= src.pl[s] >= i0 && src.pl[s] < i0 + W && j >= src.lo0[s] && j <= src.hi0[s] && k >= src.lo1[s] &&
+                   k <= src.hi1[s];
+    }
     return hit;
+}
+
+// J of the plane-wave sheets at cell (i, j, k), added after the point sources (the
+// reference's source registration order).
+template <typename T>
+__device__ __forceinline__ void sheet_J(const ESrc& src, int i, int j, int k, T& Jx, T& Jy, T& Jz) {
+    for (int s = 0; s < src.ns; ++s) {
+        bool in;
+        if (src.ax[s] == 2) in = k == src.pl[s] && i >= src.lo0[s] && i <= src.hi0[s] && j >= src.lo1[s] && j <= src.hi1[s];
+        else if (src.ax[s] == 1) in = j == src.pl[s] && i >= src.lo0[s] && i <= src.hi0[s] && k >= src.lo1[s] && k <= src.hi1[s];
+        else in = i == src.pl[s] && j >= src.lo0[s] && j <= src.hi0[s] && k >= src.lo1[s] && k <= src.hi1[s];
+        if (in) {
+            const T v = T(src.sJ[s]);
+            if (src.pc[s] == 0) Jx += v;
+            else if (src.pc[s] == 1) Jy += v;
+            else Jz += v;
+        }
+    }
 }
 
 // Plain-vector updates: no CPML slab, gain cell or source in the W cells, every cell
@@ -504,8 +540,9 @@ k_update_H(const StepArgs<S, T> a, const int kchunk, const SweepGeom g) {
 
 // ---------------------------------------------------------------------------------
 // CG: H is read through L2 only -- the slab-ordered step (k_step_slabs) reads H that other
-// SMs wrote in the same launch, which a stale L1 line could hide.
-template <typename S, typename T, bool EDGE, bool CG = false>
+// SMs wrote in the same launch, which a stale L1 line could hide.  SH: the step has
+// plane-wave sheets (a separate instantiation keeps the sheet tests out of the common case).
+template <typename S, typename T, bool EDGE, bool CG = false, bool SH = false>
 __device__ __forceinline__ void e_column(const StepArgs<S, T>& a, const SweepGeom& g, const ESrc& src, const int j,
                                          const int i0, const bool act, const int kb, const int ke, const int lane) {
     auto ldH = [](const S* p, T (&v)[Vec<T>::W]) {
@@ -592,7 +629,7 @@ __device__ __forceinline__ void e_column(const StepArgs<S, T>& a, const SweepGeo
             if (!pload) { hzp = sz; hyp = sy; }
         }
         const bool gplane = grow && k >= a.gk0 && k < a.gk0 + a.gZ;
-        if (plain_row && !zpml && !gplane && !src_in_vector(src, i0, j, k, W)) {
+        if (plain_row && !zpml && !gplane && !src_in_vector<SH>(src, i0, j, k, W)) {
             e_plain<S, T>(a, c, ex, ey, ez, bx, by, bz, hx, hy, hz, hzj, hxj, hxm, hym, hzp, hyp, idx, idy, idz);
 #pragma unroll
             for (int e = 0; e < W; ++e) { hxm[e] = hx[e]; hym[e] = hy[e]; }
@@ -634,6 +671,7 @@ __device__ __forceinline__ void e_column(const StepArgs<S, T>& a, const SweepGeo
                     else Jz += v;
                 }
             }
+            if constexpr (SH) sheet_J(src, i, j, k, Jx, Jy, Jz);
             ex[e] = ex[e] + bx[e] * ((dHz_dy - dHy_dz) - Jx);
             ey[e] = ey[e] + by[e] * ((dHx_dz - dHz_dx) - Jy);
             // Two-level gain: polarization with E^n, E update with -dP/dt, populations with E^{n+1}.
@@ -687,7 +725,7 @@ __device__ __forceinline__ void e_column(const StepArgs<S, T>& a, const SweepGeo
     }
 }
 
-template <typename S, typename T, bool CG = false>
+template <typename S, typename T, bool CG = false, bool SH = false>
 __device__ __forceinline__ void update_E_block(const StepArgs<S, T>& a, const int kchunk, const ESrc& src,
                                                const SweepGeom& g, const int bx, const int by, const int bz) {
     constexpr int W = Vec<T>::W;
@@ -700,7 +738,7 @@ __device__ __forceinline__ void update_E_block(const StepArgs<S, T>& a, const in
         const int j = by * kBlockY + threadIdx.y;
         if (j < 1 || j >= a.NyT) return;  // E is updated for j >= 1 only; whole warp
         const int i0 = g.xi0 + (bx * 32 + lane) * W;
-        e_column<S, T, false, CG>(a, g, src, j, i0, i0 < g.xi1, kb, ke, lane);
+        e_column<S, T, false, CG, SH>(a, g, src, j, i0, i0 < g.xi1, kb, ke, lane);
     } else {
         const int t = threadIdx.y * 32 + lane;
         const int rr = t / g.ne, v = t - rr * g.ne;
@@ -708,14 +746,14 @@ __device__ __forceinline__ void update_E_block(const StepArgs<S, T>& a, const in
         if (rr >= g.er || j < 1 || j >= a.NyT) return;
         const int i0 = v < g.nl ? v * W : g.xi1 + (v - g.nl) * W;
         if (i0 >= a.NxT) return;
-        e_column<S, T, true, CG>(a, g, src, j, i0, true, kb, ke, lane);
+        e_column<S, T, true, CG, SH>(a, g, src, j, i0, true, kb, ke, lane);
     }
 }
 
-template <typename S, typename T>
+template <typename S, typename T, bool SH = false>
 __global__ void __launch_bounds__(32 * kBlockY, 2)
 k_update_E(const StepArgs<S, T> a, const int kchunk, const ESrc src, const SweepGeom g) {
-    update_E_block<S, T>(a, kchunk, src, g, blockIdx.x, blockIdx.y, blockIdx.z);
+    update_E_block<S, T, false, SH>(a, kchunk, src, g, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 
 // ---------------------------------------------------------------------------------
@@ -741,7 +779,7 @@ __device__ __forceinline__ unsigned ld_acquire(const unsigned* p) {
     return v;
 }
 
-template <typename S, typename T>
+template <typename S, typename T, bool SH = false>
 __global__ void __launch_bounds__(32 * kBlockY, 2)
 k_step_slabs(const StepArgs<S, T> a, const ESrc src, const SweepGeom g, const SlabPlan p, unsigned* ctr,
              unsigned* status_w) {
@@ -782,7 +820,7 @@ k_step_slabs(const StepArgs<S, T> a, const ESrc src, const SweepGeom g, const Sl
                 if (tid == 0) atomicOr(status_w, kStatusTimeout);
                 return;
             }
-            update_E_block<S, T, true>(a, p.P, src, g, r % p.gxE, r / p.gxE, slab);
+            update_E_block<S, T, true, SH>(a, p.P, src, g, r % p.gxE, r / p.gxE, slab);
             __syncthreads();
         }
     }

@@ -344,16 +344,22 @@ struct BatchTick {
 __constant__ StepArgs<float> c_bargs[kMaxBatch];
 __constant__ BatchSolve c_bsolve[kMaxBatch];
 __constant__ BatchTick c_btick[kMaxBatch];
+// The 64 KB constant bank also holds the monitor's and DFT kernels' few constants.
+static_assert((sizeof(StepArgs<float>) + sizeof(BatchSolve) + sizeof(BatchTick)) * kMaxBatch <= 60 * 1024,
+              "per-solve constant records exceed the constant bank");
 
 __global__ void __launch_bounds__(32 * kBlockY, 2) k_update_H_multi(const int4* __restrict__ tab) {
     const int4 e = tab[blockIdx.x];
     update_H_block<float, float>(c_bargs[e.x], c_bsolve[e.x].kchunkH, c_bsolve[e.x].g, e.y, e.z, e.w);
 }
 
+// SH: the blocks of solves with plane-wave sheets, listed after all others in the table, so a
+// solve runs the same code whatever else is resident.
+template <bool SH>
 __global__ void __launch_bounds__(32 * kBlockY, 2) k_update_E_multi(const int4* __restrict__ tab) {
     const int4 e = tab[blockIdx.x];
-    update_E_block<float, float>(c_bargs[e.x], c_bsolve[e.x].kchunkE, c_btick[e.x].src, c_bsolve[e.x].g, e.y, e.z,
-                                 e.w);
+    update_E_block<float, float, false, SH>(c_bargs[e.x], c_bsolve[e.x].kchunkE, c_btick[e.x].src, c_bsolve[e.x].g,
+                                            e.y, e.z, e.w);
 }
 
 // one block per solve
@@ -499,6 +505,35 @@ private:
     double dt_;
     // sources
     std::vector<fdtd_dipole_v1> dip_;
+    std::vector<fdtd_sheet_v1> sheets_;
+    // Point sources and sheet geometry of the per-step source record, then this step's J.
+    void src_static(ESrc& src) const {
+        src.n = int(dip_.size());
+        for (int q = 0; q < src.n; ++q) {
+            src.si[q] = int(dip_[q].i); src.sj[q] = int(dip_[q].j); src.sk[q] = int(dip_[q].k);
+            src.sc[q] = dip_[q].polarization % 3;
+        }
+        src.ns = int(sheets_.size());
+        for (int q = 0; q < src.ns; ++q) {
+            const fdtd_sheet_v1& w = sheets_[q];
+            src.ax[q] = w.axis; src.pc[q] = w.comp; src.pl[q] = int(w.plane);
+            src.lo0[q] = int(w.lo0); src.hi0[q] = int(w.hi0); src.lo1[q] = int(w.lo1); src.hi1[q] = int(w.hi1);
+        }
+    }
+    void src_step(ESrc& src, uint64_t s) const {
+        src.parity = int(s & 1);
+        for (int q = 0; q < src.n; ++q) {
+            const fdtd_dipole_v1& d = dip_[q];
+            src.J[q] = fdtd::current_density(d.waveform, s, dt_, d.I0, d.f0, d.tau, d.t0, d.t_shift, d.cell_area) *
+                       (1.0 / sH_);
+        }
+        const double t_half = (double(s) + 0.5) * dt_;
+        for (int q = 0; q < src.ns; ++q) {  // PlaneWaveSource::inject_*_plane
+            const fdtd_sheet_v1& w = sheets_[q];
+            const double Et = fdtd::waveform_value(w.waveform, t_half, w.E0, w.f0, w.tau, w.t0, w.t_shift);
+            src.sJ[q] = 2.0 * Et / (376.730313668 * w.d) * w.sign * (1.0 / sH_);
+        }
+    }
     // detectors
     uint32_t save_every_ = 1, nprobes_ = 0, nf_ = 0;
     ProbeDev* d_probes_ = nullptr;
@@ -551,6 +586,7 @@ Solver<S, T>::Solver(const fdtd_setup_v1& s, int dev) {
         // its normal numbers at 6e-5): the estimate tau |I0| / (eps0 cell_area) -- the field a
         // dipole's current would build in its cell over one pulse width without radiating --
         // overshoots the peak by one to two decades, so sE is that over 64, as a power of two.
+        // A plane-wave soft source launches a wave of its own amplitude E0: it counts as 64 |E0|.
         // BF16 has FP32's range: sE = 1.
         double sE = s.field_scale;
         if (!(sE > 0.0)) {
@@ -561,6 +597,7 @@ Solver<S, T>::Solver(const fdtd_setup_v1& s, int dev) {
                     const fdtd_dipole_v1& d = s.dipoles[q];
                     if (d.cell_area > 0) est = std::max(est, d.tau * std::fabs(d.I0) / (8.8541878128e-12 * d.cell_area));
                 }
+                for (uint32_t q = 0; q < s.n_sheets; ++q) est = std::max(est, 64.0 * std::fabs(s.sheets[q].E0));
                 if (est > 0) sE = std::exp2(std::round(std::log2(est / 64.0)));
             }
         }
@@ -716,6 +753,16 @@ Solver<S, T>::Solver(const fdtd_setup_v1& s, int dev) {
     }
 
 
+    if (s.n_sheets > uint32_t(kMaxSheets)) throw Failure(FDTD_ERR_UNSUPPORTED, "more than 2 plane-wave sources");
+    for (uint32_t q = 0; q < s.n_sheets; ++q) {
+        const fdtd_sheet_v1& w = s.sheets[q];
+        const uint64_t N[3] = {s.NxT, s.NyT, s.NzT};
+        if (w.axis < 0 || w.axis > 2 || w.comp < 0 || w.comp > 2 || w.comp == w.axis || w.plane >= N[w.axis] ||
+            !(w.d > 0))
+            throw Failure(FDTD_ERR_INVALID, "bad plane-wave source");
+        sheets_.push_back(w);
+    }
+
     // probes / DFT
     save_every_ = std::max<uint32_t>(1, s.save_every);
     nprobes_ = s.n_probes;
@@ -791,7 +838,9 @@ void Solver<S, T>::setup_slabs() {
     d_ctr_ = alloc<unsigned>(size_t(plan_.nslab) + 1);
     int sms = 148, per = 0;
     ck(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device), "cudaDeviceGetAttribute");
-    ck(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_step_slabs<S, T>, 32 * kBlockY, 0),
+    ck(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, sheets_.empty() ? k_step_slabs<S, T, false>
+                                                                          : k_step_slabs<S, T, true>,
+                                                    32 * kBlockY, 0),
        "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
     if (per < 1) throw Failure(FDTD_ERR_CUDA, "slab-ordered step kernel does not fit on an SM");
     gridS_ = dim3(unsigned(sms * per));
@@ -1110,21 +1159,12 @@ void Solver<S, T>::run(uint64_t n) {
     ensure_series((last + save_every_ - 1) / save_every_);
     const dim3 blk(32, kBlockY);
     ESrc src{};
-    src.n = int(dip_.size());
-    for (int q = 0; q < src.n; ++q) {
-        src.si[q] = int(dip_[q].i); src.sj[q] = int(dip_[q].j); src.sk[q] = int(dip_[q].k);
-        src.sc[q] = dip_[q].polarization % 3;
-    }
+    src_static(src);
     const int pthreads = int(nprobes_ * std::max<uint32_t>(nf_, 1));
     const bool per_kernel = timing_ == FDTD_TIMING_KERNELS;
     if (timing_ == FDTD_TIMING_RUN) ck(cudaEventRecord(ev_[0], st_), "cudaEventRecord");
     for (uint64_t s = n0; s < last; ++s) {
-        src.parity = int(s & 1);
-        for (int q = 0; q < src.n; ++q) {
-            const fdtd_dipole_v1& d = dip_[q];
-            src.J[q] = fdtd::current_density(d.waveform, s, dt_, d.I0, d.f0, d.tau, d.t0, d.t_shift, d.cell_area) *
-                       (1.0 / sH_);
-        }
+        src_step(src, s);
         if (per_kernel) ck(cudaEventRecord(ev_[0], st_), "cudaEventRecord");
         bool fused_step = false;
         if constexpr (std::is_same_v<S, T>) fused_step = path_ == 0;
@@ -1147,13 +1187,15 @@ void Solver<S, T>::run(uint64_t n) {
         } else if (path_ == 2) {
             ck(cudaMemsetAsync(d_ctr_, 0, (size_t(plan_.nslab) + 1) * sizeof(unsigned), st_), "cudaMemsetAsync");
             if (per_kernel) ck(cudaEventRecord(ev_[0], st_), "cudaEventRecord");
-            k_step_slabs<S, T><<<gridS_, blk, 0, st_>>>(a_, src, geom_, plan_, d_ctr_, d_status_);
+            if (src.ns) k_step_slabs<S, T, true><<<gridS_, blk, 0, st_>>>(a_, src, geom_, plan_, d_ctr_, d_status_);
+            else k_step_slabs<S, T><<<gridS_, blk, 0, st_>>>(a_, src, geom_, plan_, d_ctr_, d_status_);
             if (per_kernel) ck(cudaEventRecord(ev_[1], st_), "cudaEventRecord");
             launches += 1;
         } else {
             k_update_H<S, T><<<gridH_, blk, 0, st_>>>(a_, kchunkH_, geom_);
             if (per_kernel) ck(cudaEventRecord(ev_[1], st_), "cudaEventRecord");
-            k_update_E<S, T><<<gridE_, blk, 0, st_>>>(a_, kchunkE_, src, geom_);
+            if (src.ns) k_update_E<S, T, true><<<gridE_, blk, 0, st_>>>(a_, kchunkE_, src, geom_);
+            else k_update_E<S, T><<<gridE_, blk, 0, st_>>>(a_, kchunkE_, src, geom_);
             launches += 2;
         }
         if (per_kernel) ck(cudaEventRecord(ev_[2], st_), "cudaEventRecord");
@@ -1370,7 +1412,7 @@ private:
         std::vector<StepArgs<float>> args(n);
         std::vector<BatchSolve> bs(n);
         std::vector<int4> tab;
-        nH_ = nE_ = 0;
+        nH_ = nE_ = nE0_ = 0;
         for (int r = 0; r < n; ++r) {
             Solver<float, float>& v = *jobs_.at(res_[r]).sol;
             args[r] = v.a_;
@@ -1398,11 +1440,16 @@ private:
                     for (unsigned x = 0; x < g.x; ++x) tab.push_back(make_int4(r, int(x), int(y), int(z)));
         }
         nH_ = tab.size();
-        for (int r = 0; r < n; ++r) {
-            const dim3 g = jobs_.at(res_[r]).sol->gridE_;
-            for (unsigned z = 0; z < g.z; ++z)
-                for (unsigned y = 0; y < g.y; ++y)
-                    for (unsigned x = 0; x < g.x; ++x) tab.push_back(make_int4(r, int(x), int(y), int(z)));
+        for (int pass = 0; pass < 2; ++pass) {  // E blocks of solves without sheets, then with
+            for (int r = 0; r < n; ++r) {
+                const Solver<float, float>& v = *jobs_.at(res_[r]).sol;
+                if (v.sheets_.empty() == (pass == 1)) continue;
+                const dim3 g = v.gridE_;
+                for (unsigned z = 0; z < g.z; ++z)
+                    for (unsigned y = 0; y < g.y; ++y)
+                        for (unsigned x = 0; x < g.x; ++x) tab.push_back(make_int4(r, int(x), int(y), int(z)));
+            }
+            if (pass == 0) nE0_ = tab.size() - nH_;
         }
         nE_ = tab.size() - nH_;
         ck(cudaStreamSynchronize(st_), "rebuild");  // no step may read the old tables
@@ -1429,14 +1476,8 @@ private:
             const uint64_t s = v.steps;
             BatchTick& k = tk[r];
             k = BatchTick{};
-            k.src.n = int(v.dip_.size());
-            k.src.parity = int(s & 1);
-            for (int q = 0; q < k.src.n; ++q) {
-                const fdtd_dipole_v1& d = v.dip_[q];
-                k.src.si[q] = int(d.i); k.src.sj[q] = int(d.j); k.src.sk[q] = int(d.k);
-                k.src.sc[q] = d.polarization % 3;
-                k.src.J[q] = fdtd::current_density(d.waveform, s, v.dt_, d.I0, d.f0, d.tau, d.t0, d.t_shift, d.cell_area);
-            }
+            v.src_static(k.src);
+            v.src_step(k.src, s);
             k.sample = (s % v.save_every_ == 0) ? (long long)(s / v.save_every_) : -1;
             if (k.sample >= 0) v.series_count_ = uint64_t(k.sample) + 1;
             k.t = double(s + 1) * v.dt_;
@@ -1449,7 +1490,8 @@ private:
         ck(cudaEventRecord(ring_ev_[slot], st_), "cudaEventRecord");
         const dim3 blk(32, kBlockY);
         k_update_H_multi<<<unsigned(nH_), blk, 0, st_>>>(d_tab_);
-        k_update_E_multi<<<unsigned(nE_), blk, 0, st_>>>(d_tab_ + nH_);
+        if (nE0_) k_update_E_multi<false><<<unsigned(nE0_), blk, 0, st_>>>(d_tab_ + nH_);
+        if (nE_ > nE0_) k_update_E_multi<true><<<unsigned(nE_ - nE0_), blk, 0, st_>>>(d_tab_ + nH_ + nE0_);
         k_probe_multi<<<n, 128, 0, st_>>>();
         if (monitor) {
             k_monitor_reduce_multi<<<n * kMonBlocks, 256, 0, st_>>>();
@@ -1502,7 +1544,7 @@ private:
     std::deque<uint64_t> queue_;
     std::vector<uint64_t> res_;  // resident tickets in slot order
     int4* d_tab_ = nullptr;
-    size_t tab_cap_ = 0, nH_ = 0, nE_ = 0;
+    size_t tab_cap_ = 0, nH_ = 0, nE_ = 0, nE0_ = 0;
     BatchTick* ticks_ = nullptr;
     cudaEvent_t ring_ev_[kRing] = {};
     uint64_t ring_ = 0;

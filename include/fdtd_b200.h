@@ -76,6 +76,22 @@ typedef struct fdtd_dipole_v1 {
     double cell_area, I0, f0, tau, t0, t_shift;
 } fdtd_dipole_v1;
 
+/* One plane-wave soft source: PlaneWaveSource after make_plane_wave_source
+ * (src/sources/plane_wave_source.hpp:19-312).  Each step it adds
+ * J = 2 E(t) / (eta0 d) * sign, t = (n + 1/2) dt, E(t) = compute_waveform(waveform, t, E0, f0,
+ * tau, t0, t_shift), to J component `comp` of the cells of plane `plane` (normal to `axis`)
+ * whose in-plane indices lie in [lo0, hi0] x [lo1, hi1] (axis 2: i, j; axis 0: j, k;
+ * axis 1: i, k), d = the spacing along `axis` at `plane`. */
+typedef struct fdtd_sheet_v1 {
+    int32_t axis;      /* 0 x, 1 y, 2 z: the propagation axis */
+    int32_t comp;      /* 0 Jx, 1 Jy, 2 Jz */
+    uint64_t plane, lo0, hi0, lo1, hi1;
+    double d, sign;    /* spacing at the plane; +1 / -1 for + / - propagation */
+    int32_t waveform;  /* Sources::Waveform */
+    int32_t reserved;
+    double E0, f0, tau, t0, t_shift;
+} fdtd_sheet_v1;
+
 /* One gain region: TwoLevelParams after finalize()/finalize_with_dt()
  * (src/two_level_system.hpp:17-110). */
 typedef struct fdtd_tls_region_v1 {
@@ -141,6 +157,9 @@ typedef struct fdtd_setup_v1 {
     /* FP16 / BF16 storage: the E field scale sE (stored E' = E / sE); 0 = automatic (FP16: the
      * dipoles' tau |I0| / (eps0 cell_area) rounded up to a power of two; BF16: 1) */
     double field_scale;
+    /* plane-wave soft sources (at most 2) */
+    uint32_t n_sheets;
+    const fdtd_sheet_v1 *sheets;
 } fdtd_setup_v1;
 
 /* Diagnostics of the most recent monitor step, FP64 device reductions
@@ -219,7 +238,8 @@ int fdtd_kernel_launches(const fdtd_handle *h, uint64_t *n);
 int fdtd_set_timing(fdtd_handle *h, int mode);
 int fdtd_get_timing(fdtd_handle *h, fdtd_timing_v1 *out);
 /* Kernel path, before the first step only: 0 = one fused H+E launch per step with
- * TMA-staged planes, 1 = separate H and E sweeps (default).  Results agree to rounding. */
+ * TMA-staged planes, 1 = separate H and E sweeps (default), 2 = one persistent launch that
+ * runs the H and E sweeps slab by slab in dependency order.  Results agree to rounding. */
 int fdtd_set_kernel_path(fdtd_handle *h, int path);
 /* Block until all device work of the handle is complete. */
 int fdtd_synchronize(fdtd_handle *h);

@@ -27,6 +27,18 @@ typedef struct oracle_source {
     double cell_area, I0, f0, tau, t0, t_shift;
 } oracle_source;
 
+/* A plane-wave soft source (src/sources/plane_wave_source.hpp:77-98): every step adds
+ * J = 2 E(t_half) / (eta0 d) * sign to component comp over the cells lo0..hi0 x lo1..hi1
+ * (inclusive) of the plane index `plane` along `axis`; the in-plane axes are (x, y) for a
+ * z plane, (y, z) for an x plane and (x, z) for a y plane. */
+typedef struct oracle_sheet {
+    int32_t axis, comp;
+    uint64_t plane, lo0, hi0, lo1, hi1;
+    double d, sign;
+    int32_t waveform, reserved;
+    double E0, f0, tau, t0, t_shift;
+} oracle_sheet;
+
 typedef struct oracle_region {
     double kapa_coeff, pa2, pa3, inv_dt, tau, hbar, omega_a, N0, pump_rate;
     int32_t clamp, reserved;
@@ -46,6 +58,8 @@ typedef struct oracle_case {
     uint64_t probe_idx[16];    /* idx3 offsets */
     int32_t probe_comp[16];
     uint32_t save_every;
+    int32_t n_sheets;
+    oracle_sheet sheets[2];
 } oracle_case;
 
 /* Mutable state (FP64 caller-owned arrays, idx3).  Gain arrays may be NULL without gain. */

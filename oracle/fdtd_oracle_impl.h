@@ -76,6 +76,21 @@ static int64_t FN(oracle_run)(const oracle_case *c, oracle_state *s, uint64_t n0
                                 sr->cell_area;
             J[sr->comp][IDX3(sr->i, sr->j, sr->k, NyT, NzT)] += (REAL)Jval;
         }
+        /* PlaneWaveSource::inject_half_step (src/sources/plane_wave_source.hpp:77-176),
+         * registered after the dipoles */
+        for (int q = 0; q < c->n_sheets; ++q) {
+            const oracle_sheet *w = &c->sheets[q];
+            const double t_half = ((double)n + 0.5) * dt;
+            const double Et = waveform_value(w->waveform, t_half, w->E0, w->f0, w->tau, w->t0, w->t_shift);
+            const double Jamp = 2.0 * Et / (376.730313668 * w->d) * w->sign;
+            for (uint64_t a = w->lo0; a <= w->hi0; ++a)
+                for (uint64_t b = w->lo1; b <= w->hi1; ++b) {
+                    const uint64_t i = w->axis == 0 ? w->plane : a;
+                    const uint64_t j = w->axis == 1 ? w->plane : w->axis == 0 ? a : b;
+                    const uint64_t k = w->axis == 2 ? w->plane : b;
+                    J[w->comp][IDX3(i, j, k, NyT, NzT)] += (REAL)Jamp;
+                }
+        }
         /* update_polarization_multi_region (src/two_level_system.hpp:574-609) */
         if (gain) {
 #pragma omp parallel for

@@ -36,6 +36,13 @@ class OSource(C.Structure):
                 ("tau", C.c_double), ("t0", C.c_double), ("t_shift", C.c_double)]
 
 
+class OSheet(C.Structure):
+    _fields_ = [("axis", C.c_int32), ("comp", C.c_int32), ("plane", C.c_uint64), ("lo0", C.c_uint64),
+                ("hi0", C.c_uint64), ("lo1", C.c_uint64), ("hi1", C.c_uint64), ("d", C.c_double),
+                ("sign", C.c_double), ("waveform", C.c_int32), ("reserved", C.c_int32), ("E0", C.c_double),
+                ("f0", C.c_double), ("tau", C.c_double), ("t0", C.c_double), ("t_shift", C.c_double)]
+
+
 class ORegion(C.Structure):
     _fields_ = [("kapa_coeff", C.c_double), ("pa2", C.c_double), ("pa3", C.c_double), ("inv_dt", C.c_double),
                 ("tau", C.c_double), ("hbar", C.c_double), ("omega_a", C.c_double), ("N0", C.c_double),
@@ -50,7 +57,8 @@ class OCase(C.Structure):
                 ("kappa", _dp * 3), ("bEp", _dp * 3), ("cEp", _dp * 3), ("bHp", _dp * 3), ("cHp", _dp * 3),
                 ("bE", _dp * 3), ("src", OSource * 8), ("regions", ORegion * 16),
                 ("region_map", C.POINTER(C.c_int32)), ("probe_idx", C.c_uint64 * 16),
-                ("probe_comp", C.c_int32 * 16), ("save_every", C.c_uint32)]
+                ("probe_comp", C.c_int32 * 16), ("save_every", C.c_uint32), ("n_sheets", C.c_int32),
+                ("sheets", OSheet * 2)]
 
 
 class OState(C.Structure):
@@ -120,6 +128,11 @@ class OracleSolve:
             d = v.dipoles[q]
             c.src[q] = OSource(d.i, d.j, d.k, d.polarization % 3, d.waveform, d.cell_area, d.I0, d.f0, d.tau, d.t0,
                                d.t_shift)
+        c.n_sheets = int(v.n_sheets)
+        for q in range(c.n_sheets):
+            w = v.sheets[q]
+            c.sheets[q] = OSheet(w.axis, w.comp, w.plane, w.lo0, w.hi0, w.lo1, w.hi1, w.d, w.sign, w.waveform, 0,
+                                 w.E0, w.f0, w.tau, w.t0, w.t_shift)
         c.n_regions = int(v.n_tls_regions)
         for q in range(c.n_regions):
             r = v.tls_regions[q]

@@ -317,7 +317,7 @@ int main(int argc, char** argv) {
         write_f64(od, "n_grid", n_grid);
     }
 
-    // ---- sources (register_default_sources, src/params.hpp:594-678; dipoles only) ----
+    // ---- sources (register_default_sources, src/params.hpp:594-678: dipoles, then plane waves) ----
     Config::Runtime rt;
     meta << "  \"sources\": [";
     bool first_src = true;
@@ -346,6 +346,28 @@ int main(int argc, char** argv) {
         rt.sources.push_back(std::move(src));
     }
     meta << "],\n";
+    for (const auto& s : pf.list("PLANE_WAVE_SOURCES")) {  // src/params.hpp:643-679
+        if (!to_bool(s.at(0))) continue;
+        Sources::PlaneWaveConfig cfg;
+        cfg.injection_position = d(s, 1);
+        cfg.amplitude = d(s, 2); cfg.frequency = d(s, 3); cfg.wavelength = d(s, 4);
+        cfg.tau = d(s, 5); cfg.df_fwhm = d(s, 6); cfg.t0_factor = d(s, 7);
+        switch (int(d(s, 8))) {
+            case 1: cfg.waveform = Sources::Waveform::GaussianModulatedSine; break;
+            case 2: cfg.waveform = Sources::Waveform::RickerLikeGaussian2nd; break;
+            case 3: cfg.waveform = Sources::Waveform::ContinuousWave; break;
+            default: cfg.waveform = Sources::Waveform::Ricker; break;
+        }
+        const int dir = int(d(s, 9));
+        cfg.direction = static_cast<Sources::PlaneWaveDirection>((dir >= 0 && dir <= 5) ? dir : 4);
+        const int pol = int(d(s, 10));
+        cfg.polarization = static_cast<Sources::Polarization>((pol >= 0 && pol <= 5) ? pol : 2);
+        cfg.x_min = d(s, 11); cfg.x_max = d(s, 12); cfg.y_min = d(s, 13);
+        cfg.y_max = d(s, 14); cfg.z_min = d(s, 15); cfg.z_max = d(s, 16);
+        rt.sources.push_back(Sources::make_plane_wave_source(cfg, ctx.grid_spacing, ctx.NxT, ctx.NyT, ctx.NzT,
+                                                             ctx.npml, ctx.dt, P.domain_x_min, P.domain_y_min,
+                                                             P.domain_z_min));
+    }
 
     std::vector<real> Ex(NxT * NyT * NzT, 0), Ey(Ex), Ez(Ex), Hx(Ex), Hy(Ex), Hz(Ex), Jx(Ex), Jy(Ex), Jz(Ex);
     if (!init_dir.empty()) {

@@ -12,8 +12,8 @@ shipped configs, and stores what it produced:
   configs.json mesh lines and SHA-256 digests of the material arrays of the shipped
                configs (their full arrays are too large to commit)
 
-Usage: python tests/golden/make_golden.py   (needs the reference checkout; the GPU box
-only reads the .npz/.json files this writes)
+Usage: python tests/golden/make_golden.py [case stem ...]   (needs the reference checkout;
+the GPU box only reads the .npz/.json files this writes; with stems, only those cases)
 """
 from __future__ import annotations
 
@@ -105,14 +105,17 @@ def configs() -> None:
     (HERE / "configs.json").write_text(json.dumps(out, indent=1))
 
 
-def main() -> None:
+def main(only=()) -> None:
     oracle.build(ref=True)
     for path in sorted((HERE / "cases").glob("mesh_*.params")):
-        mesh_case(path)
+        if not only or path.stem in only:
+            mesh_case(path)
     for path in sorted((HERE / "cases").glob("step_*.params")):
-        step_case(path)
-    configs()
+        if not only or path.stem in only:
+            step_case(path)
+    if not only:
+        configs()
 
 
 if __name__ == "__main__":
-    main()
+    main(tuple(sys.argv[1:]))

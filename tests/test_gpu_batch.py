@@ -10,6 +10,7 @@ pytestmark = pytest.mark.gpu
 CASES = [  # (setup source, overrides, steps)
     (GOLDEN / "cases" / "step_g0_sphere.params", {}, 150),
     (GOLDEN / "cases" / "step_g1_gain.params", {"PUMP_RATE": "1e11"}, 120),
+    (GOLDEN / "cases" / "step_g2_planewave.params", {}, 100),
     ("c0_dipole_sphere.params", {}, 300),
     ("c1_gain_slab.params", {"PUMP_RATE": "1e9"}, 210),
 ]

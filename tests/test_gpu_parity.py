@@ -72,6 +72,59 @@ def test_gain_case_matches_reference(pkg, precision, tol):
     assert rel(series, g["probe_series"].reshape(series.shape)) <= tol
 
 
+@pytest.mark.parametrize("path", [0, 1, 2])
+@pytest.mark.parametrize("precision,tol", [(1, 1e-12), (0, 1e-5)])
+def test_plane_wave_case_matches_reference(pkg, precision, tol, path):
+    """Two plane-wave soft sources (a full +Z / Ex plane and a -Y / Ez sub-rectangle) and a
+    dipole, against the reference's own fields and probe series."""
+    g, s, _ = golden_solver(pkg, "step_g2_planewave", precision)
+    assert s.view.n_sheets == 2
+    sol = pkg.Solver(s, precision=precision, kernel_path=path)
+    sol.run(g["meta"]["steps"])
+    ref = ref_fields(g, sol.shape)
+    mine = fields(sol)
+    assert field_rel_l2(mine, ref, "E") <= tol and field_rel_l2(mine, ref, "H") <= tol
+    series = sol.probe_series()
+    assert rel(series, g["probe_series"].reshape(series.shape)) <= tol
+
+
+PLANE_WAVE_PAIRS = [
+    # (+X / Ey full plane, -Z / Ex sub-rectangle), (+Y / Ez, -X / Ez), (-Y / Ex, +Z / Ey)
+    ("true, 400e-9, 1.0, 193.4e12, 0, 2e-15, 0, 1.0, 1, 0, 1, 0, 0, 0, 0, 0, 0",
+     "true, 700e-9, 0.7, 0, 1400e-9, 0, 30e12, 1.2, 2, 5, 0, 300e-9, 1200e-9, 100e-9, 800e-9, 0, 0"),
+    ("true, 300e-9, 1.0, 193.4e12, 0, 2e-15, 0, 1.0, 1, 2, 2, 0, 0, 0, 0, 0, 0",
+     "true, 1300e-9, 2.0, 193.4e12, 0, 3e-15, 0, 1.0, 0, 1, 5, 0, 0, 200e-9, 500e-9, 400e-9, 900e-9"),
+    ("true, 500e-9, 1.0, 193.4e12, 0, 2e-15, 0, 1.0, 1, 3, 0, 0, 0, 0, 0, 0, 0",
+     "true, 600e-9, 1.0, 193.4e12, 0, 2e-15, 0, 1.0, 1, 4, 4, 0, 0, 0, 0, 0, 0"),
+]
+
+
+@pytest.mark.parametrize("pair", range(len(PLANE_WAVE_PAIRS)))
+def test_plane_waves_on_odd_grid(pkg, oracle, pair):
+    """Sheets along every axis and both signs, full planes and sub-rectangles, on a grid that
+    is not a multiple of any tile or slab; every kernel path against the oracle."""
+    text = (GOLDEN / "cases" / "step_g0_sphere.params").read_text()
+    text = text.replace("NX = 10", "NX = 71").replace("NY = 9", "NY = 37").replace("NZ = 8", "NZ = 45")
+    text = text.replace("DOMAIN_X_MAX = 250e-9", "DOMAIN_X_MAX = 1775e-9").replace("DOMAIN_Y_MAX = 225e-9", "DOMAIN_Y_MAX = 925e-9")
+    text = text.replace("DOMAIN_Z_MAX = 200e-9", "DOMAIN_Z_MAX = 1125e-9")
+    text = "\n".join(ln for ln in text.splitlines() if not ln.startswith("DIPOLE_SOURCES"))
+    for w in PLANE_WAVE_PAIRS[pair]:
+        text += "\nPLANE_WAVE_SOURCES += " + w
+    s = pkg.Setup.from_text(text)
+    assert s.view.n_sheets == 2 and s.view.n_dipoles == 0
+    o = oracle.OracleSolve(s, 0)
+    o.run(70)
+    ref = {c: o.field(c) for c in FIELDS}
+    for path in (0, 1, 2):
+        for precision, tol in ((1, 1e-12), (0, 1e-5)):
+            sol = pkg.Solver(s, precision=precision, kernel_path=path)
+            sol.run(70)
+            mine = fields(sol)
+            assert field_rel_l2(mine, ref, "E") <= tol, (path, precision)
+            assert field_rel_l2(mine, ref, "H") <= tol, (path, precision)
+            sol.close()
+
+
 def test_c0_fp32_active_field_within_1e5(pkg, oracle):
     s = pkg.Setup.from_file(pkg.config_path("c0_dipole_sphere.params"))
     o = oracle.OracleSolve(s, 0)

@@ -153,7 +153,7 @@ def test_shipped_configs_match_reference_setup(pkg, cfg):
         assert (v.probes[q].i, v.probes[q].j, v.probes[q].k) == (p["i"], p["j"], p["k"])
 
 
-@pytest.mark.parametrize("case", ["step_g0_sphere", "step_g1_gain"])
+@pytest.mark.parametrize("case", ["step_g0_sphere", "step_g1_gain", "step_g2_planewave"])
 def test_step_case_setup_matches_reference(pkg, case):
     g = golden(case)
     s = pkg.Setup.from_file(GOLDEN / "cases" / (case + ".params"))
@@ -179,3 +179,25 @@ def test_live_reference_harness_setup(pkg, oracle):
     for k in ("x_bounds", "dz", "inv_dy", "bEx", "bEz", "cpml_cHz", "n_grid"):
         assert bits_equal(s.array(k), r[k]), k
     assert np.array_equal(s.array("tls_region_map"), r["tls_region_map"].astype(np.float64))
+
+
+def test_plane_wave_sheet_geometry(pkg):
+    """make_plane_wave_source's plane clamp and compute_bounds, and the component rule of
+    inject_*_plane: an Ez plane wave along z drives nothing and is dropped."""
+    text = (GOLDEN / "cases" / "step_g2_planewave.params").read_text()
+    s = pkg.Setup.from_text(text)
+    v = s.view
+    assert v.n_sheets == 2
+    a, b = v.sheets[0], v.sheets[1]
+    # +Z / Ex over the whole non-PML plane; z = 80 nm -> core index 3 + npml
+    assert (a.axis, a.comp, a.sign, a.plane) == (2, 0, 1.0, 6)
+    assert (a.lo0, a.hi0, a.lo1, a.hi1) == (3, 14, 3, 12)
+    assert abs(a.d - 25e-9) < 1e-20 and a.E0 == 1.0
+    # -Y / Ez over x 50..200 nm, z 100..250 nm (in-plane axes x, z)
+    assert (b.axis, b.comp, b.sign, b.plane) == (1, 2, -1.0, 9)
+    assert (b.lo0, b.hi0, b.lo1, b.hi1) == (5, 11, 7, 13)
+    ez_along_z = text + "\nPLANE_WAVE_SOURCES += true, 80e-9, 1.0, 193.4e12, 0, 2e-15, 0, 1.0, 1, 5, 2, 0, 0, 0, 0, 0, 0"
+    s2 = pkg.Setup.from_text(ez_along_z)
+    assert s2.view.n_sheets == 2
+    with pytest.raises(pkg.FdtdError):
+        pkg.Setup.from_text(ez_along_z.replace(", 1, 5, 2, 0, 0,", ", 1, 5, 1, 0, 0,"))  # a third sheet
