@@ -108,6 +108,7 @@ class SetupV1(C.Structure):
         ("conservation_err", C.c_double), ("growth_rate", C.c_double),
         ("field_scale", C.c_double),
         ("n_sheets", C.c_uint32), ("sheets", C.POINTER(SheetV1)),
+        ("pec_boundary", C.c_uint32), ("reserved1", C.c_uint32),
     ]
 
 

@@ -147,6 +147,7 @@ int fdtd_setup_view(const fdtd_setup* s, fdtd_setup_v1* v) {
     v->bH_uniform = s->uniform_ah ? S.mats.bH[0][0] : S.dt / fdtd::phys::MU0;
     v->n_sheets = uint32_t(s->sheets.size());
     v->sheets = s->sheets.data();
+    v->pec_boundary = S.boundary_pec ? 1 : 0;
     v->n_dipoles = uint32_t(s->dipoles.size());
     v->dipoles = s->dipoles.data();
     v->n_tls_regions = uint32_t(s->regions.size());

@@ -471,8 +471,6 @@ SimSetup SimSetup::from_params(const ParamFile& pf, bool bake) {
     S.cpml_cfg.kappa_max = pf.num("CPML_KAPPA_MAX", 10.0);
     S.cpml_cfg.alpha_linear = pf.flag("CPML_ALPHA_LINEAR", true);
     require(S.cpml_cfg.npml >= 0, "CPML_NPML must be >= 0");
-    if (S.boundary_pec)
-        throw std::runtime_error("BOUNDARY_TYPE = 0 (PEC) is not supported by the stepper; use 1 (CPML)");
     const bool tls_enabled_cfg = pf.flag("TLS_ENABLED", true);
     const bool tls_clamp = pf.flag("TLS_ENABLE_CLAMP", false);
     const real background_n = pf.num("BACKGROUND_N", 1.0);
@@ -590,16 +588,28 @@ SimSetup SimSetup::from_params(const ParamFile& pf, bool bake) {
     S.Ny_core = S.NyT - 2 * npml;
     S.Nz_core = S.NzT - 2 * npml;
     S.npml = npml;
-    S.grid.npml = npml;
-    S.cpml = build_cpml_profiles(S.grid, S.cpml_cfg, S.dt);
+    if (S.boundary_pec) {
+        // PECBoundary(NxCore, NyCore, NzCore) reports the core sizes as the totals and no PML
+        // layer (src/boundary.hpp:51-79, src/params.hpp:271-294): the fields cover the first
+        // Nx_core cells of the padded mesh, whose arrays keep their padded length, and every
+        // position is taken from the mesh origin.
+        S.NxT = S.Nx_core; S.NyT = S.Ny_core; S.NzT = S.Nz_core;
+        S.npml = 0;
+        require(S.NxT >= 3 && S.NyT >= 3 && S.NzT >= 3, "PEC grid must have at least 3 core cells per axis");
+    }
+    S.grid.npml = S.npml;
+    CpmlConfig cc = S.cpml_cfg;
+    cc.npml = int(S.npml);
+    S.cpml = build_cpml_profiles(S.grid, cc, S.dt);
     if (!bake) return S;
 
     // apply_structure_packages (register_default_structures, src/params.hpp:557-592)
     Scene& sc = S.scene;
-    sc.NxT = S.NxT; sc.NyT = S.NyT; sc.NzT = S.NzT; sc.npml_cells = npml;
+    sc.NxT = S.NxT; sc.NyT = S.NyT; sc.NzT = S.NzT; sc.npml_cells = S.npml;
     sc.grid = S.grid;
     sc.bg = make_nk(background_n);
-    const real pml_x = S.grid.x_bounds[npml], pml_y = S.grid.y_bounds[npml], pml_z = S.grid.z_bounds[npml];
+    const std::size_t np0 = S.npml;
+    const real pml_x = S.grid.x_bounds[np0], pml_y = S.grid.y_bounds[np0], pml_z = S.grid.z_bounds[np0];
     for (const auto& d : defs) {
         StructureItem it;
         it.mat = make_nk(d.n);
@@ -644,6 +654,9 @@ SimSetup SimSetup::from_params(const ParamFile& pf, bool bake) {
         src.i = S.grid.physical_to_index(0, x - S.domain_min[0]);
         src.j = S.grid.physical_to_index(1, y - S.domain_min[1]);
         src.k = S.grid.physical_to_index(2, z - S.domain_min[2]);
+        // Only reachable with PEC, whose field grid is shorter than the mesh: the reference
+        // would write past its J arrays.
+        require(src.i < S.NxT && src.j < S.NyT && src.k < S.NzT, "dipole source lies outside the field grid");
         const real c0 = 299792458.0;
         real f = frequency > 0.0 ? frequency : (wavelength > 0.0 ? c0 / wavelength : c0 / 500e-9);
         real tau_eff = tau > 0.0 ? tau

@@ -52,6 +52,39 @@ __global__ void k_from_idx3(const double* __restrict__ src, D* __restrict__ dst,
     }
 }
 
+// PECBoundary::apply_after_E (src/boundary.hpp:55-74): Ex = Ey = Ez = 0 on the six outer
+// faces, after the E update.  One thread per face cell, the z faces first, then y, then x,
+// so that consecutive threads write consecutive i where the layout allows.
+template <typename D>
+__global__ void k_pec_faces(D* __restrict__ Ex, D* __restrict__ Ey, D* __restrict__ Ez, int NxT, int NyT, int NzT,
+                            int NxP) {
+    const long long nz = (long long)NxT * NyT, ny = (long long)NxT * NzT, nx = (long long)NyT * NzT;
+    const long long total = 2 * (nx + ny + nz);
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+         t += (long long)gridDim.x * blockDim.x) {
+        long long u = t;
+        int i, j, k;
+        if (u < 2 * nz) {
+            const int side = int(u / nz);
+            u -= side * nz;
+            i = int(u % NxT); j = int(u / NxT); k = side ? NzT - 1 : 0;
+        } else if ((u -= 2 * nz) < 2 * ny) {
+            const int side = int(u / ny);
+            u -= side * ny;
+            i = int(u % NxT); k = int(u / NxT); j = side ? NyT - 1 : 0;
+        } else {
+            u -= 2 * ny;
+            const int side = int(u / nx);
+            u -= side * nx;
+            j = int(u % NyT); k = int(u / NyT); i = side ? NxT - 1 : 0;
+        }
+        const size_t q = (size_t(k) * NyT + j) * NxP + i;
+        Ex[q] = from_d<D>(0.0);
+        Ey[q] = from_d<D>(0.0);
+        Ez[q] = from_d<D>(0.0);
+    }
+}
+
 template <typename D>
 __global__ void k_to_idx3(const D* __restrict__ src, double* __restrict__ dst, int NxT, int NyT, int NzT, int NxP,
                           double scale) {
@@ -454,6 +487,7 @@ public:
         if (path < 0 || path > 2)
             throw Failure(FDTD_ERR_INVALID, "kernel path must be 0 (fused), 1 (two sweeps) or 2 (slab-ordered step)");
         if (path == 0 && !std::is_same_v<S, T>) throw Failure(FDTD_ERR_UNSUPPORTED, "the fused path needs FP32 or FP64 storage");
+        if (path == 0 && pec_) throw Failure(FDTD_ERR_UNSUPPORTED, "the fused path needs a CPML boundary");
         if (steps != 0) throw Failure(FDTD_ERR_INVALID, "the kernel path can only change before the first step");
         path_ = path;
     }
@@ -547,6 +581,7 @@ private:
     unsigned* d_status_ = nullptr;
     double* d_stage_ = nullptr;
     bool has_gain_ = false;
+    bool pec_ = false;  // PECBoundary: zero E on the outer faces after every E update
     // event timing: ev_[0..3] bracket H, E and the auxiliary kernels of one step
     // kernel path 0: k_step_fused (fields and psi_H double-buffered, cur_ = buffer holding
     // the latest state); path 1 (default, measured faster on B200): k_update_H +
@@ -579,6 +614,8 @@ Solver<S, T>::Solver(const fdtd_setup_v1& s, int dev) {
     constexpr int W = Vec<T>::W;
     NxT_ = int(s.NxT); NyT_ = int(s.NyT); NzT_ = int(s.NzT);
     np_ = int(s.npml);
+    pec_ = s.pec_boundary != 0;
+    if (pec_ && np_ != 0) throw Failure(FDTD_ERR_INVALID, "a PEC boundary has no CPML layer: npml must be 0");
     NxP_ = int(round_up(size_t(NxT_), 128 / sizeof(S)));
     if constexpr (!std::is_same_v<S, T>) {
         // 16-bit storage: E' = E / sE, H' = H / sH with sH = sE / eta0 so that E' and H' have
@@ -699,13 +736,16 @@ Solver<S, T>::Solver(const fdtd_setup_v1& s, int dev) {
                     const int32_t r = s.tls_region_map[(size_t(i) * NyT_ + j) * NzT_ + k];
                     if (r < 0) continue;
                     out_of_range += r >= nreg;
-                    on_boundary += (i == 0 || j == 0 || k == 0);
+                    on_boundary += (i == 0 || j == 0 || k == 0) ||
+                                   (pec_ && (i == NxT_ - 1 || j == NyT_ - 1 || k == NzT_ - 1));
                     lo0 = std::min(lo0, i); hi0 = std::max(hi0, i);
                     lo1 = std::min(lo1, j); hi1 = std::max(hi1, j);
                     lo2 = std::min(lo2, k); hi2 = std::max(hi2, k);
                 }
         if (out_of_range) throw Failure(FDTD_ERR_INVALID, "region map entry out of range");
-        if (on_boundary) throw Failure(FDTD_ERR_UNSUPPORTED, "gain cells on the i=0/j=0/k=0 boundary planes");
+        if (on_boundary)
+            throw Failure(FDTD_ERR_UNSUPPORTED, pec_ ? "gain cells on the outer faces of a PEC grid"
+                                                     : "gain cells on the i=0/j=0/k=0 boundary planes");
         const int lo[3] = {lo0, lo1, lo2}, hi[3] = {hi0, hi1, hi2};
         if (hi[0] >= 0) {
             has_gain_ = true;
@@ -1198,6 +1238,12 @@ void Solver<S, T>::run(uint64_t n) {
             else k_update_E<S, T><<<gridE_, blk, 0, st_>>>(a_, kchunkE_, src, geom_);
             launches += 2;
         }
+        if (pec_) {
+            const long long faces = 2ll * ((long long)NxT_ * NyT_ + (long long)NxT_ * NzT_ + (long long)NyT_ * NzT_);
+            const unsigned nb = unsigned(std::min<long long>((faces + 255) / 256, 148 * 8));
+            k_pec_faces<S><<<nb, 256, 0, st_>>>(a_.Ex, a_.Ey, a_.Ez, NxT_, NyT_, NzT_, NxP_);
+            ++launches;
+        }
         if (per_kernel) ck(cudaEventRecord(ev_[2], st_), "cudaEventRecord");
         if (nprobes_) {
             const long long sample = (s % save_every_ == 0) ? (long long)(s / save_every_) : -1;
@@ -1326,6 +1372,7 @@ public:
 
     uint64_t submit(const fdtd_setup_v1& s, uint64_t nsteps) {
         if (s.precision != FDTD_PREC_FP32) throw Failure(FDTD_ERR_UNSUPPORTED, "the packed engine steps FP32 solves");
+        if (s.pec_boundary) throw Failure(FDTD_ERR_UNSUPPORTED, "the packed engine steps CPML solves");
         if (nsteps == 0) throw Failure(FDTD_ERR_INVALID, "a job needs at least one step");
         Job j;
         j.setup = &s;

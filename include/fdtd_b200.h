@@ -160,6 +160,10 @@ typedef struct fdtd_setup_v1 {
     /* plane-wave soft sources (at most 2) */
     uint32_t n_sheets;
     const fdtd_sheet_v1 *sheets;
+    /* 1: PECBoundary (src/boundary.hpp:51-79): npml must be 0, and after every E update
+     * Ex, Ey, Ez are zeroed on the six outer faces.  0: CPML. */
+    uint32_t pec_boundary;
+    uint32_t reserved1;
 } fdtd_setup_v1;
 
 /* Diagnostics of the most recent monitor step, FP64 device reductions

@@ -60,6 +60,7 @@ typedef struct oracle_case {
     uint32_t save_every;
     int32_t n_sheets;
     oracle_sheet sheets[2];
+    int32_t pec; /* PECBoundary instead of CPML (npml = 0) */
 } oracle_case;
 
 /* Mutable state (FP64 caller-owned arrays, idx3).  Gain arrays may be NULL without gain. */

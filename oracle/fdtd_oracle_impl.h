@@ -225,6 +225,18 @@ static int64_t FN(oracle_run)(const oracle_case *c, oracle_state *s, uint64_t n0
                         }
                     }
         }
+        /* PECBoundary::apply_after_E (src/boundary.hpp:55-74): E = 0 on the six faces */
+        if (c->pec) {
+            for (size_t j = 0; j < NyT; ++j)
+                for (size_t k = 0; k < NzT; ++k)
+                    for (int q = 0; q < 3; ++q) E[q][IDX3(0, j, k, NyT, NzT)] = E[q][IDX3(NxT - 1, j, k, NyT, NzT)] = 0;
+            for (size_t i = 0; i < NxT; ++i)
+                for (size_t k = 0; k < NzT; ++k)
+                    for (int q = 0; q < 3; ++q) E[q][IDX3(i, 0, k, NyT, NzT)] = E[q][IDX3(i, NyT - 1, k, NyT, NzT)] = 0;
+            for (size_t i = 0; i < NxT; ++i)
+                for (size_t j = 0; j < NyT; ++j)
+                    for (int q = 0; q < 3; ++q) E[q][IDX3(i, j, 0, NyT, NzT)] = E[q][IDX3(i, j, NzT - 1, NyT, NzT)] = 0;
+        }
         /* PointFieldDetector::record_after_E (src/detectors/point_field_detector.hpp:242-255) */
         if (n % c->save_every == 0) {
             if (probe_out)

@@ -58,7 +58,7 @@ class OCase(C.Structure):
                 ("bE", _dp * 3), ("src", OSource * 8), ("regions", ORegion * 16),
                 ("region_map", C.POINTER(C.c_int32)), ("probe_idx", C.c_uint64 * 16),
                 ("probe_comp", C.c_int32 * 16), ("save_every", C.c_uint32), ("n_sheets", C.c_int32),
-                ("sheets", OSheet * 2)]
+                ("sheets", OSheet * 2), ("pec", C.c_int32)]
 
 
 class OState(C.Structure):
@@ -128,6 +128,7 @@ class OracleSolve:
             d = v.dipoles[q]
             c.src[q] = OSource(d.i, d.j, d.k, d.polarization % 3, d.waveform, d.cell_area, d.I0, d.f0, d.tau, d.t0,
                                d.t_shift)
+        c.pec = int(v.pec_boundary)
         c.n_sheets = int(v.n_sheets)
         for q in range(c.n_sheets):
             w = v.sheets[q]

@@ -32,8 +32,10 @@ def test_parse_error_reports_message(pkg):
     assert e.value.code == 6
     with pytest.raises(pkg.FdtdError):
         pkg.Setup.from_text("MESH_MODE = 0\nSTRUCTURES += prism, 2.0, 0, 1, 0, 1, 0, 1\n")
-    with pytest.raises(pkg.FdtdError):
-        pkg.Setup.from_text("MESH_MODE = 0\nBOUNDARY_TYPE = 0\n")  # PEC: not handled by the stepper
+    with pytest.raises(pkg.FdtdError) as e:  # PEC: the field grid ends 2 npml cells before the mesh
+        pkg.Setup.from_text("MESH_MODE = 0\nNX = 20\nNY = 20\nNZ = 20\nBOUNDARY_TYPE = 0\n"
+                            "DIPOLE_SOURCES += true, 210e-9, 50e-9, 50e-9, 1e-7, 193.4e12, 0, 2e-15, 0, 1.0, 1, 2\n")
+    assert "outside the field grid" in str(e.value)
 
 
 def test_unknown_setup_array_is_an_error(pkg):

@@ -88,6 +88,42 @@ def test_plane_wave_case_matches_reference(pkg, precision, tol, path):
     assert rel(series, g["probe_series"].reshape(series.shape)) <= tol
 
 
+@pytest.mark.parametrize("path", [1, 2])
+@pytest.mark.parametrize("precision,tol", [(1, 1e-12), (0, 1e-5)])
+def test_pec_case_matches_reference(pkg, precision, tol, path):
+    """PECBoundary (E zeroed on the six faces after every E update, no CPML) with a gain core,
+    a dipole and a plane-wave sheet that reaches the faces, against the reference's state."""
+    g, s, _ = golden_solver(pkg, "step_g3_pec", precision)
+    assert s.view.pec_boundary == 1
+    sol = pkg.Solver(s, precision=precision, kernel_path=path)
+    sol.run(g["meta"]["steps"])
+    ref = ref_fields(g, sol.shape)
+    mine = fields(sol)
+    assert field_rel_l2(mine, ref, "E") <= tol and field_rel_l2(mine, ref, "H") <= tol
+    for c in ("Ex", "Ey", "Ez"):
+        f = mine[c]
+        assert not (f[0].any() or f[-1].any() or f[:, 0].any() or f[:, -1].any() or f[:, :, 0].any() or f[:, :, -1].any())
+    gain = g["tls_region_map"].reshape(sol.shape) >= 0
+    for c in ("Pz", "Nu", "Ng"):
+        assert rel(sol.tls_state(c)[gain], g[c].reshape(sol.shape)[gain]) <= max(tol, 1e-6), c
+    series = sol.probe_series()
+    assert rel(series, g["probe_series"].reshape(series.shape)) <= tol
+
+
+def test_pec_refuses_fused_path_and_packed_engine(pkg):
+    s = pkg.Setup.from_file(GOLDEN / "cases" / "step_g3_pec.params")
+    sol = pkg.Solver(s)
+    with pytest.raises(pkg.FdtdError) as e:
+        sol.set_kernel_path(0)
+    assert e.value.code == 7
+    sol.close()
+    b = pkg.Batch(budget_bytes=1 << 30)
+    with pytest.raises(pkg.FdtdError) as e:
+        b.submit(s, 10)
+    assert e.value.code == 7
+    b.close()
+
+
 PLANE_WAVE_PAIRS = [
     # (+X / Ey full plane, -Z / Ex sub-rectangle), (+Y / Ez, -X / Ez), (-Y / Ex, +Z / Ey)
     ("true, 400e-9, 1.0, 193.4e12, 0, 2e-15, 0, 1.0, 1, 0, 1, 0, 0, 0, 0, 0, 0",

@@ -33,7 +33,7 @@ def oracle_sha(a):
     return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
 
 
-@pytest.mark.parametrize("case", ["step_g0_sphere", "step_g1_gain", "step_g2_planewave"])
+@pytest.mark.parametrize("case", ["step_g0_sphere", "step_g1_gain", "step_g2_planewave", "step_g3_pec"])
 def test_oracle_reproduces_reference_bit_for_bit(pkg, oracle, case):
     g, o, series = run_oracle(pkg, oracle, case)
     for c in FIELDS:

@@ -153,7 +153,7 @@ def test_shipped_configs_match_reference_setup(pkg, cfg):
         assert (v.probes[q].i, v.probes[q].j, v.probes[q].k) == (p["i"], p["j"], p["k"])
 
 
-@pytest.mark.parametrize("case", ["step_g0_sphere", "step_g1_gain", "step_g2_planewave"])
+@pytest.mark.parametrize("case", ["step_g0_sphere", "step_g1_gain", "step_g2_planewave", "step_g3_pec"])
 def test_step_case_setup_matches_reference(pkg, case):
     g = golden(case)
     s = pkg.Setup.from_file(GOLDEN / "cases" / (case + ".params"))
@@ -201,3 +201,17 @@ def test_plane_wave_sheet_geometry(pkg):
     assert s2.view.n_sheets == 2
     with pytest.raises(pkg.FdtdError):
         pkg.Setup.from_text(ez_along_z.replace(", 1, 5, 2, 0, 0,", ", 1, 5, 1, 0, 0,"))  # a third sheet
+
+
+def test_pec_grid_is_the_padded_mesh_origin(pkg):
+    """PECBoundary's context: the field grid is the core size, taken from the start of the
+    padded mesh, with no PML layer; the mesh arrays keep their padded length."""
+    s = pkg.Setup.from_file(GOLDEN / "cases" / "step_g3_pec.params")
+    v = s.view
+    g = golden("step_g3_pec")
+    assert v.pec_boundary == 1 and v.npml == 0
+    assert (v.NxT, v.NyT, v.NzT) == tuple(g["meta"][k] for k in ("NxT", "NyT", "NzT"))
+    assert len(s.array("dx")) == v.NxT + 2 * 3 and len(s.array("x_bounds")) == v.NxT + 2 * 3 + 1
+    c = pkg.Setup.from_text((GOLDEN / "cases" / "step_g3_pec.params").read_text().replace("BOUNDARY_TYPE = 0",
+                                                                                            "BOUNDARY_TYPE = 1"))
+    assert c.view.pec_boundary == 0 and c.view.npml == 3 and c.view.NxT == v.NxT + 6
