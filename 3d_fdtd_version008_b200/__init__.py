@@ -29,7 +29,7 @@ FDTD_OK = 0
 STATUS_NAMES = {
     0: "FDTD_OK", 1: "FDTD_ERR_INVALID", 2: "FDTD_ERR_OOM", 3: "FDTD_ERR_CUDA",
     4: "FDTD_ERR_UNSTABLE", 5: "FDTD_ERR_TIMEOUT", 6: "FDTD_ERR_PARSE",
-    7: "FDTD_ERR_UNSUPPORTED", 8: "FDTD_ERR_NO_DEVICE",
+    7: "FDTD_ERR_UNSUPPORTED", 8: "FDTD_ERR_NO_DEVICE", 9: "FDTD_ERR_IO",
 }
 FDTD_ERR_INVALID = 1
 FDTD_ERR_UNSTABLE = 4
@@ -43,11 +43,11 @@ TLS_STATE = {"Pz": 0, "Pz_prev": 1, "Nu": 2, "Ng": 3}
 # Every exported symbol of include/fdtd_b200.h.
 EXPORTED_SYMBOLS = (
     "fdtd_setup_parse", "fdtd_setup_view", "fdtd_setup_array_len", "fdtd_setup_array",
-    "fdtd_setup_destroy", "fdtd_create", "fdtd_set_field", "fdtd_get_field",
+    "fdtd_setup_destroy", "fdtd_setup_write_outputs", "fdtd_create", "fdtd_set_field", "fdtd_get_field",
     "fdtd_set_tls_state", "fdtd_get_tls_state", "fdtd_run", "fdtd_steps_done",
     "fdtd_get_probe_series", "fdtd_get_dft", "fdtd_get_diagnostics", "fdtd_device_bytes",
     "fdtd_kernel_launches", "fdtd_set_timing", "fdtd_get_timing", "fdtd_set_kernel_path", "fdtd_synchronize", "fdtd_last_error",
-    "fdtd_destroy", "fdtd_field_scan_noalloc",
+    "fdtd_destroy", "fdtd_field_scan_noalloc", "fdtd_attach_outputs", "fdtd_flush_outputs",
     "fdtd_batch_create", "fdtd_batch_submit", "fdtd_batch_run", "fdtd_batch_job_state",
     "fdtd_batch_probe_series", "fdtd_batch_dft", "fdtd_batch_diagnostics", "fdtd_batch_release",
     "fdtd_batch_last_error", "fdtd_batch_destroy",
@@ -151,6 +151,9 @@ def load_library() -> C.CDLL:
         "fdtd_setup_array_len": (C.c_int, [vp, C.c_char_p, C.POINTER(C.c_uint64)]),
         "fdtd_setup_array": (C.c_int, [vp, C.c_char_p, _dptr, C.c_uint64]),
         "fdtd_setup_destroy": (None, [vp]),
+        "fdtd_setup_write_outputs": (C.c_int, [vp, C.c_char_p, C.c_char_p, C.c_size_t]),
+        "fdtd_attach_outputs": (C.c_int, [vp, vp, C.c_char_p]),
+        "fdtd_flush_outputs": (C.c_int, [vp]),
         "fdtd_create": (C.c_int, [C.POINTER(SetupV1), C.c_int, C.POINTER(vp)]),
         "fdtd_set_field": (C.c_int, [vp, C.c_int, _dptr]),
         "fdtd_get_field": (C.c_int, [vp, C.c_int, _dptr]),
@@ -244,6 +247,14 @@ class Setup:
 
     def array3(self, name: str) -> np.ndarray:
         return self.array(name).reshape(self.shape)
+
+    def write_outputs(self, out_dir) -> pathlib.Path:
+        """The files the reference writes before its time loop, under out_dir/frames/<RUN_TAG>/."""
+        err = C.create_string_buffer(1024)
+        rc = load_library().fdtd_setup_write_outputs(self._h, str(out_dir).encode(), err, len(err))
+        if rc != FDTD_OK:
+            raise FdtdError(rc, err.value.decode())
+        return pathlib.Path(out_dir)
 
     def __del__(self):
         if getattr(self, "_h", None) is not None and self._h.value and _lib is not None:
@@ -355,6 +366,15 @@ class Solver:
 
     def synchronize(self) -> None:
         self._check(load_library().fdtd_synchronize(self._h), "fdtd_synchronize")
+
+    def attach_outputs(self, out_dir, setup: Optional[Setup] = None) -> None:
+        """Stream the reference's detector files (movie frames, point time series) to
+        out_dir/frames/<RUN_TAG>/ while the solve steps; before the first step."""
+        s = setup if setup is not None else self.setup
+        self._check(load_library().fdtd_attach_outputs(self._h, s._h, str(out_dir).encode()), "fdtd_attach_outputs")
+
+    def flush_outputs(self) -> None:
+        self._check(load_library().fdtd_flush_outputs(self._h), "fdtd_flush_outputs")
 
     def close(self) -> None:
         if getattr(self, "_h", None) is not None and self._h.value:

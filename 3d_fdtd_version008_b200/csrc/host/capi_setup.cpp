@@ -1,5 +1,6 @@
 // capi_setup.cpp -- extern "C" entry points of the host setup API (include/fdtd_b200.h).
 #include "../../../include/fdtd_b200.h"
+#include "outputs.hpp"
 #include "setup.hpp"
 
 #include <cstring>
@@ -82,6 +83,9 @@ const std::vector<double>* find_array(const fdtd_setup* s, const std::string& na
 }
 
 }  // namespace
+
+// The parsed setup behind a handle, for the stepper's output attachment (solver.cu).
+const fdtd::SimSetup* fdtd_internal_setup(const fdtd_setup* s) { return s ? &s->S : nullptr; }
 
 extern "C" {
 
@@ -182,6 +186,27 @@ int fdtd_setup_array(const fdtd_setup* s, const char* name, double* out, uint64_
     const std::vector<double>* a = find_array(s, name, scratch);
     if (!a || a->size() != len) return FDTD_ERR_INVALID;
     std::memcpy(out, a->data(), len * sizeof(double));
+    return FDTD_OK;
+}
+
+int fdtd_setup_write_outputs(const fdtd_setup* s, const char* out_dir, char* err, size_t errlen) {
+    if (!s || !out_dir) {
+        write_err(err, errlen, "null argument");
+        return FDTD_ERR_INVALID;
+    }
+    fdtd::OutputPlan plan;
+    try {
+        plan = fdtd::make_output_plan(s->S);
+    } catch (const std::exception& e) {
+        write_err(err, errlen, e.what());
+        return FDTD_ERR_INVALID;
+    }
+    try {
+        fdtd::write_setup_outputs(s->S, plan, out_dir);
+    } catch (const std::exception& e) {
+        write_err(err, errlen, e.what());
+        return FDTD_ERR_IO;
+    }
     return FDTD_OK;
 }
 

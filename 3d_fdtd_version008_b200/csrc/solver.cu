@@ -8,6 +8,7 @@
 // the FP64 diagnostic reduction, on the handle's stream.  All device memory comes from
 // cudaMalloc at create time (staging for layout transposes on first use).
 #include "../../include/fdtd_b200.h"
+#include "host/outputs.hpp"
 #include "host/waveform.hpp"
 #include "kernels.cuh"
 #include "fused.cuh"
@@ -17,7 +18,9 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <condition_variable>
 #include <map>
+#include <mutex>
 #include <deque>
 #include <type_traits>
 #include <cmath>
@@ -123,30 +126,59 @@ struct ProbeDev {
 };
 
 // Probe value in physical units: stored E and H times their field scales es, hs.
+// get_field_value (src/detectors/idetector.hpp:79-110) on one cell's six FP64 values, with
+// every product and sum rounded on its own (no contraction), as the reference computes it.
+__device__ __forceinline__ double component_value(int comp, double ex, double ey, double ez, double hx, double hy,
+                                                  double hz) {
+    auto cross = [](double a, double b, double c, double d) { return __dsub_rn(__dmul_rn(a, b), __dmul_rn(c, d)); };
+    auto norm = [](double x, double y, double z) {
+        return sqrt(__dadd_rn(__dadd_rn(__dmul_rn(x, x), __dmul_rn(y, y)), __dmul_rn(z, z)));
+    };
+    switch (comp) {
+        case 0: return ex;
+        case 1: return ey;
+        case 2: return ez;
+        case 3: return hx;
+        case 4: return hy;
+        case 5: return hz;
+        case 6: return norm(ex, ey, ez);
+        case 7: return norm(hx, hy, hz);
+        case 8: return cross(ey, hz, ez, hy);
+        case 9: return cross(ez, hx, ex, hz);
+        case 10: return cross(ex, hy, ey, hx);
+        case 11: return norm(cross(ey, hz, ez, hy), cross(ez, hx, ex, hz), cross(ex, hy, ey, hx));
+    }
+    return 0.0;
+}
+
+// FieldMovie2D::record_after_E (src/detectors/field_movie_2d.hpp:107-148): one component on
+// one slice plane, in the reference's order -- XY: (i, j), XZ: (i, k), YZ: (j, k), the
+// second index fastest -- as FP64 or FP32.  One thread per output value.
+template <typename S>
+__global__ void k_slice(const S* __restrict__ Ex, const S* __restrict__ Ey, const S* __restrict__ Ez,
+                        const S* __restrict__ Hx, const S* __restrict__ Hy, const S* __restrict__ Hz, int NyT, int NxP,
+                        int plane, int index, int comp, long long d2, long long count, double es, double hs,
+                        void* __restrict__ out, int f64) {
+    for (long long o = blockIdx.x * (long long)blockDim.x + threadIdx.x; o < count;
+         o += (long long)gridDim.x * blockDim.x) {
+        const int a = int(o / d2), b = int(o - (o / d2) * d2);
+        const int i = plane == 2 ? index : a;
+        const int j = plane == 0 ? b : plane == 1 ? index : a;
+        const int k = plane == 0 ? index : b;
+        const size_t q = (size_t(k) * NyT + j) * NxP + i;
+        const double v = component_value(comp, double(to_c(Ex[q])) * es, double(to_c(Ey[q])) * es,
+                                         double(to_c(Ez[q])) * es, double(to_c(Hx[q])) * hs, double(to_c(Hy[q])) * hs,
+                                         double(to_c(Hz[q])) * hs);
+        if (f64) static_cast<double*>(out)[o] = v;
+        else static_cast<float*>(out)[o] = float(v);
+    }
+}
+
 template <typename S, typename T>
 __device__ double probe_value(const StepArgs<S, T>& a, const ProbeDev& p, double es, double hs) {
     const size_t o = size_t(p.off);
-    auto v = [&](const S* f) { return double(to_c(f[o])) * ((f == a.Ex || f == a.Ey || f == a.Ez) ? es : hs); };
-    switch (p.comp) {
-        case 0: return v(a.Ex);
-        case 1: return v(a.Ey);
-        case 2: return v(a.Ez);
-        case 3: return v(a.Hx);
-        case 4: return v(a.Hy);
-        case 5: return v(a.Hz);
-        case 6: return sqrt(v(a.Ex) * v(a.Ex) + v(a.Ey) * v(a.Ey) + v(a.Ez) * v(a.Ez));
-        case 7: return sqrt(v(a.Hx) * v(a.Hx) + v(a.Hy) * v(a.Hy) + v(a.Hz) * v(a.Hz));
-        case 8: return v(a.Ey) * v(a.Hz) - v(a.Ez) * v(a.Hy);
-        case 9: return v(a.Ez) * v(a.Hx) - v(a.Ex) * v(a.Hz);
-        case 10: return v(a.Ex) * v(a.Hy) - v(a.Ey) * v(a.Hx);
-        case 11: {
-            double sx = v(a.Ey) * v(a.Hz) - v(a.Ez) * v(a.Hy);
-            double sy = v(a.Ez) * v(a.Hx) - v(a.Ex) * v(a.Hz);
-            double sz = v(a.Ex) * v(a.Hy) - v(a.Ey) * v(a.Hx);
-            return sqrt(sx * sx + sy * sy + sz * sz);
-        }
-    }
-    return 0.0;
+    return component_value(p.comp, double(to_c(a.Ex[o])) * es, double(to_c(a.Ey[o])) * es, double(to_c(a.Ez[o])) * es,
+                           double(to_c(a.Hx[o])) * hs, double(to_c(a.Hy[o])) * hs, double(to_c(a.Hz[o])) * hs);
 }
 
 // Point probes after the E update of step n: sample (every save_every steps) and the
@@ -457,6 +489,8 @@ public:
     virtual void set_timing(int mode) = 0;
     virtual void set_path(int path) = 0;
     virtual void timing(fdtd_timing_v1* t) = 0;
+    virtual void attach_outputs(const fdtd::SimSetup& setup, const std::string& root) = 0;
+    virtual void flush_outputs() = 0;
     uint64_t steps = 0, launches = 0, dev_bytes = 0;
     int device = 0;
 };
@@ -509,6 +543,10 @@ private:
         return d;
     }
     double* staging();
+    void attach_outputs(const fdtd::SimSetup& setup, const std::string& root) override;
+    void flush_outputs() override;
+    void capture_movies();
+    void write_point_samples();
     // Host <-> device copies of FP64 arrays through two pinned chunks: the host-side copy of
     // one chunk (OpenMP) overlaps the DMA of the other.
     static constexpr size_t kPinBytes = size_t(32) << 20;
@@ -570,6 +608,25 @@ private:
     }
     // detectors
     uint32_t save_every_ = 1, nprobes_ = 0, nf_ = 0;
+
+    // The reference's detector files (fdtd_attach_outputs): movie slices are captured into
+    // one of kOutSlots device buffers, copied to the matching pinned buffer on the stream,
+    // and written by the writer thread once the copy's event has completed; a slot is
+    // reused after the writer has finished with it.  Point samples are appended to their
+    // _ts.bin files after every run() call.
+    static constexpr int kOutSlots = 4;
+    std::unique_ptr<fdtd::OutputWriter> writer_;
+    fdtd::OutputPlan oplan_;
+    std::string oroot_;
+    std::vector<size_t> mov_off_, mov_bytes_;
+    size_t oslot_bytes_ = 0;
+    char* d_oslot_[kOutSlots] = {};
+    char* h_oslot_[kOutSlots] = {};
+    cudaEvent_t oslot_ev_[kOutSlots] = {};
+    std::mutex oslot_mu_;
+    std::condition_variable oslot_cv_;
+    int oslot_busy_[kOutSlots] = {};
+    uint64_t oframe_ = 0, ots_written_ = 0;
     ProbeDev* d_probes_ = nullptr;
     double *d_freqs_ = nullptr, *d_dft_ = nullptr, *d_series_ = nullptr;
     uint64_t series_cap_ = 0, series_count_ = 0;
@@ -993,6 +1050,17 @@ template <typename S, typename T>
 Solver<S, T>::~Solver() {
     cudaSetDevice(device);
     if (st_) cudaStreamSynchronize(st_);
+    if (writer_) {
+        try {
+            writer_->drain();
+        } catch (const std::exception&) {
+        }
+        writer_.reset();
+    }
+    for (int q = 0; q < kOutSlots; ++q) {
+        if (h_oslot_[q]) cudaFreeHost(h_oslot_[q]);
+        if (oslot_ev_[q]) cudaEventDestroy(oslot_ev_[q]);
+    }
     for (auto& e : ev_) if (e) cudaEventDestroy(e);
     for (void* p : ptrs_) cudaFreeAsync(p, st_);
     if (d_stage_) cudaFreeAsync(d_stage_, st_);
@@ -1253,6 +1321,7 @@ void Solver<S, T>::run(uint64_t n) {
             ++launches;
             if (sample >= 0) series_count_ = uint64_t(sample) + 1;
         }
+        if (writer_ && !oplan_.movies.empty() && s % save_every_ == 0) capture_movies();
         if (interval_ && s % interval_ == 0) {
             k_monitor_reduce<S, T><<<8 * 148, 256, 0, st_>>>(a_, nflat_, d_dx_, d_dy_, d_dz_, int((s + 1) & 1), d_acc_, sE_);
             k_monitor_eval<<<1, 1, 0, st_>>>(d_acc_, d_ms_, d_status_, s);
@@ -1287,9 +1356,139 @@ void Solver<S, T>::run(uint64_t n) {
         ck(cudaMemcpy(&ms, d_ms_, sizeof(ms), cudaMemcpyDeviceToHost), "monitor state");
         steps = ms.step + 1;
         series_count_ = std::min<uint64_t>(series_count_, (steps + save_every_ - 1) / save_every_);
+        if (writer_) write_point_samples();
         throw Failure(FDTD_ERR_UNSTABLE, "stability monitor stopped the solve at step " + std::to_string(ms.step));
     }
     steps = last;
+    if (writer_) write_point_samples();
+}
+
+template <typename S, typename T>
+void Solver<S, T>::attach_outputs(const fdtd::SimSetup& Sp, const std::string& root) {
+    if (writer_) throw Failure(FDTD_ERR_INVALID, "outputs are already attached");
+    if (steps != 0) throw Failure(FDTD_ERR_INVALID, "outputs can only be attached before the first step");
+    if (Sp.NxT != size_t(NxT_) || Sp.NyT != size_t(NyT_) || Sp.NzT != size_t(NzT_) || Sp.save_every != save_every_)
+        throw Failure(FDTD_ERR_INVALID, "the setup does not match the handle (grid or SAVE_EVERY)");
+    fdtd::OutputPlan plan;
+    try {
+        plan = fdtd::make_output_plan(Sp);
+    } catch (const std::exception& e) {
+        throw Failure(FDTD_ERR_INVALID, e.what());
+    }
+    size_t comps = 0;
+    for (const auto& p : plan.points) comps += p.components.size();
+    if (comps != nprobes_) throw Failure(FDTD_ERR_INVALID, "the setup's point detectors do not match the handle's probes");
+    try {
+        fdtd::write_setup_outputs(Sp, plan, root);
+    } catch (const std::exception& e) {
+        throw Failure(FDTD_ERR_IO, e.what());
+    }
+    ck(cudaSetDevice(device), "cudaSetDevice");
+    const size_t word = plan.float64 ? sizeof(double) : sizeof(float);
+    oslot_bytes_ = 0;
+    for (const auto& m : plan.movies) {
+        mov_off_.push_back(oslot_bytes_);
+        mov_bytes_.push_back(m.dim1 * m.dim2 * word);
+        oslot_bytes_ += round_up(m.dim1 * m.dim2 * word, 256);
+    }
+    if (oslot_bytes_) {
+        for (int q = 0; q < kOutSlots; ++q) {
+            d_oslot_[q] = alloc<char>(oslot_bytes_, false);
+            ck(cudaHostAlloc(reinterpret_cast<void**>(&h_oslot_[q]), oslot_bytes_, cudaHostAllocDefault), "cudaHostAlloc");
+            ck(cudaEventCreateWithFlags(&oslot_ev_[q], cudaEventDisableTiming), "cudaEventCreate");
+        }
+    }
+    oplan_ = std::move(plan);
+    oroot_ = root;
+    writer_ = std::make_unique<fdtd::OutputWriter>();
+}
+
+template <typename S, typename T>
+void Solver<S, T>::capture_movies() {
+    const int sl = int(oframe_ % kOutSlots);
+    {
+        std::unique_lock<std::mutex> l(oslot_mu_);
+        oslot_cv_.wait(l, [&] { return oslot_busy_[sl] == 0; });
+        oslot_busy_[sl] = int(oplan_.movies.size());
+    }
+    for (size_t m = 0; m < oplan_.movies.size(); ++m) {
+        const fdtd::MoviePlan& v = oplan_.movies[m];
+        const long long count = (long long)(v.dim1 * v.dim2);
+        const unsigned nb = unsigned(std::min<long long>((count + 255) / 256, 148 * 4));
+        k_slice<S><<<nb, 256, 0, st_>>>(a_.Ex, a_.Ey, a_.Ez, a_.Hx, a_.Hy, a_.Hz, NyT_, NxP_, v.plane, int(v.index),
+                                        v.component, (long long)v.dim2, count, sE_, sH_, d_oslot_[sl] + mov_off_[m],
+                                        oplan_.float64 ? 1 : 0);
+        ++launches;
+    }
+    ck(cudaMemcpyAsync(h_oslot_[sl], d_oslot_[sl], oslot_bytes_, cudaMemcpyDeviceToHost, st_), "movie frame D2H");
+    ck(cudaEventRecord(oslot_ev_[sl], st_), "cudaEventRecord");
+    const cudaEvent_t ev = oslot_ev_[sl];
+    const int dev = device;
+    for (size_t m = 0; m < oplan_.movies.size(); ++m) {
+        fdtd::OutputWriter::Job j;
+        if (m == 0)
+            j.wait = [ev, dev] {
+                cudaSetDevice(dev);
+                if (cudaEventSynchronize(ev) != cudaSuccess) throw std::runtime_error("movie frame copy failed");
+            };
+        j.done = [this, sl] {
+            {
+                std::lock_guard<std::mutex> l(oslot_mu_);
+                --oslot_busy_[sl];
+            }
+            oslot_cv_.notify_all();
+        };
+        j.path = fdtd::frame_path(oplan_, oroot_, m, oframe_);
+        j.data = h_oslot_[sl] + mov_off_[m];
+        j.bytes = mov_bytes_[m];
+        writer_->submit(std::move(j));
+    }
+    ++oframe_;
+}
+
+template <typename S, typename T>
+void Solver<S, T>::write_point_samples() {
+    if (oplan_.points.empty() || series_count_ <= ots_written_) return;
+    const uint64_t n0 = ots_written_, n = series_count_ - ots_written_;
+    std::vector<double> v(size_t(n) * nprobes_);
+    ck(cudaMemcpy(v.data(), d_series_ + size_t(n0) * nprobes_, v.size() * sizeof(double), cudaMemcpyDeviceToHost),
+       "probe samples D2H");
+    const std::string dir = fdtd::run_dir(oplan_, oroot_);
+    size_t col = 0;
+    for (const auto& p : oplan_.points) {
+        for (int c : p.components) {
+            auto buf = std::make_shared<std::vector<char>>();
+            if (oplan_.float64) {
+                buf->resize(n * sizeof(double));
+                for (uint64_t t = 0; t < n; ++t) std::memcpy(buf->data() + t * 8, &v[t * nprobes_ + col], 8);
+            } else {
+                buf->resize(n * sizeof(float));
+                for (uint64_t t = 0; t < n; ++t) {
+                    const float f = float(v[t * nprobes_ + col]);
+                    std::memcpy(buf->data() + t * 4, &f, 4);
+                }
+            }
+            fdtd::OutputWriter::Job j;
+            j.path = dir + "/" + p.name + "/" + fdtd::component_name(c) + "_ts.bin";
+            j.data = buf->data();
+            j.bytes = buf->size();
+            j.append = true;
+            j.done = [buf] {};
+            writer_->submit(std::move(j));
+            ++col;
+        }
+    }
+    ots_written_ = series_count_;
+}
+
+template <typename S, typename T>
+void Solver<S, T>::flush_outputs() {
+    if (!writer_) return;
+    try {
+        writer_->drain();
+    } catch (const std::exception& e) {
+        throw Failure(FDTD_ERR_IO, e.what());
+    }
 }
 
 template <typename S, typename T>
@@ -1641,6 +1840,8 @@ const char* setup_problem(const fdtd_setup_v1* s) {
 }
 }  // namespace
 
+const fdtd::SimSetup* fdtd_internal_setup(const fdtd_setup* s);  // capi_setup.cpp
+
 extern "C" {
 
 int fdtd_create(const fdtd_setup_v1* s, int device, fdtd_handle** out) {
@@ -1681,6 +1882,11 @@ int fdtd_kernel_launches(const fdtd_handle* h, uint64_t* n) { if (!h || !n) retu
 int fdtd_set_timing(fdtd_handle* h, int mode) { if (!h) return FDTD_ERR_INVALID; return guarded(h, [&] { h->s->set_timing(mode); }); }
 int fdtd_get_timing(fdtd_handle* h, fdtd_timing_v1* t) { if (!h || !t) return FDTD_ERR_INVALID; return guarded(h, [&] { h->s->timing(t); }); }
 int fdtd_set_kernel_path(fdtd_handle* h, int path) { if (!h) return FDTD_ERR_INVALID; return guarded(h, [&] { h->s->set_path(path); }); }
+int fdtd_attach_outputs(fdtd_handle* h, const fdtd_setup* s, const char* out_dir) {
+    if (!h || !s || !out_dir) return FDTD_ERR_INVALID;
+    return guarded(h, [&] { h->s->attach_outputs(*fdtd_internal_setup(s), out_dir); });
+}
+int fdtd_flush_outputs(fdtd_handle* h) { if (!h) return FDTD_ERR_INVALID; return guarded(h, [&] { h->s->flush_outputs(); }); }
 int fdtd_synchronize(fdtd_handle* h) { if (!h) return FDTD_ERR_INVALID; return guarded(h, [&] { h->s->sync(); }); }
 const char* fdtd_last_error(const fdtd_handle* h) { return h ? h->err.c_str() : g_err.c_str(); }
 void fdtd_destroy(fdtd_handle* h) { delete h; }

@@ -43,7 +43,8 @@ enum {
     FDTD_ERR_TIMEOUT = 5,     /* a bounded device wait gave up */
     FDTD_ERR_PARSE = 6,       /* parameter file could not be parsed / set up */
     FDTD_ERR_UNSUPPORTED = 7, /* valid for the reference, not handled by this stepper */
-    FDTD_ERR_NO_DEVICE = 8    /* no CUDA device available */
+    FDTD_ERR_NO_DEVICE = 8,   /* no CUDA device available */
+    FDTD_ERR_IO = 9           /* an output file could not be written */
 };
 
 /* ------------------------------------------------------------ enums */
@@ -212,6 +213,15 @@ int fdtd_setup_view(const fdtd_setup *s, fdtd_setup_v1 *out);
  * "bEx", "aHz", "n_grid", "tls_region_map", ...): length query, then copy as FP64. */
 int fdtd_setup_array_len(const fdtd_setup *s, const char *name, uint64_t *len);
 int fdtd_setup_array(const fdtd_setup *s, const char *name, double *out, uint64_t len);
+
+/* Writes the files the reference writes before its time loop, under
+ * out_dir/frames/<RUN_TAG>/ (out_dir plays the reference's working directory):
+ * grid_spacing.txt, coordinate_mapping.txt, mesh_info.json (make_context,
+ * src/params.hpp:296-505), the MESH_DETECTORS' files (MeshDetector,
+ * src/detectors/mesh_detector.hpp), the metadata.json of every FIELD_MOVIE_2D_DETECTORS
+ * and POINT_FIELD_DETECTORS entry and their empty <component>_ts.bin files.  Needs a baked
+ * setup (mesh_only = 0).  FDTD_ERR_IO when a file cannot be written. */
+int fdtd_setup_write_outputs(const fdtd_setup *s, const char *out_dir, char *err, size_t errlen);
 void fdtd_setup_destroy(fdtd_setup *s);
 
 /* ------------------------------------------------------------ stepper */
@@ -245,6 +255,17 @@ int fdtd_get_timing(fdtd_handle *h, fdtd_timing_v1 *out);
  * TMA-staged planes, 1 = separate H and E sweeps (default), 2 = one persistent launch that
  * runs the H and E sweeps slab by slab in dependency order.  Results agree to rounding. */
 int fdtd_set_kernel_path(fdtd_handle *h, int path);
+/* Streams the reference's detector files of the parsed setup `s` -- the one whose view
+ * created h -- while the handle steps (FieldMovie2D and PointFieldDetector,
+ * src/detectors/field_movie_2d.hpp, point_field_detector.hpp): first writes everything
+ * fdtd_setup_write_outputs writes, then every SAVE_EVERY-th step each
+ * FIELD_MOVIE_2D_DETECTORS slice is captured on the device, copied out and written as its
+ * own frame file by a background thread, and after every fdtd_run call the new point
+ * samples are appended to the <component>_ts.bin files.  Before the first step only. */
+int fdtd_attach_outputs(fdtd_handle *h, const fdtd_setup *s, const char *out_dir);
+/* Waits until every frame and sample captured so far is on disk; FDTD_ERR_IO if a write
+ * failed.  fdtd_destroy also waits. */
+int fdtd_flush_outputs(fdtd_handle *h);
 /* Block until all device work of the handle is complete. */
 int fdtd_synchronize(fdtd_handle *h);
 /* Message of the last failing call on h (or of the last global failure when h is NULL). */

@@ -15,6 +15,7 @@ import ctypes as C
 import json
 import os
 import pathlib
+import shutil
 import subprocess
 import tempfile
 from typing import Dict, Optional
@@ -199,11 +200,17 @@ def dft(series: np.ndarray, dt: float, freqs: np.ndarray, n0: int = 0, every: in
 
 def run_harness(params_path, steps: int, *flags: str, native: bool = False, init_dir: Optional[str] = None,
                 outdir: Optional[str] = None, env: Optional[Dict[str, str]] = None) -> Dict[str, object]:
-    """Run the reference harness; returns meta plus every array it wrote (name -> ndarray)."""
+    """Run the reference harness; returns meta plus every array it wrote (name -> ndarray)
+    and, under "frames", every file of its frames/ directory (relative path -> bytes).
+    Without outdir it runs in a scratch directory under oracle/_ref/runs that is removed
+    afterwards."""
     exe = REF_HARNESS_NATIVE if native else REF_HARNESS
     if not exe.exists():
         raise FileNotFoundError(f"{exe} is missing: build it with make -C oracle ref")
-    out = outdir or tempfile.mkdtemp(prefix="refh_")
+    scratch = outdir is None
+    if scratch:
+        (ORACLE_DIR / "_ref" / "runs").mkdir(parents=True, exist_ok=True)
+    out = outdir or tempfile.mkdtemp(prefix="refh_", dir=str(ORACLE_DIR / "_ref" / "runs"))
     cmd = [str(exe), str(params_path), out, "--steps", str(steps), *flags]
     if init_dir:
         cmd += ["--init", init_dir]
@@ -218,6 +225,11 @@ def run_harness(params_path, steps: int, *flags: str, native: bool = False, init
             res[f[:-4]] = np.fromfile(os.path.join(out, f), dtype=np.float64)
         elif f.endswith(".i32"):
             res[f[:-4]] = np.fromfile(os.path.join(out, f), dtype=np.int32)
+    frames = pathlib.Path(out) / "frames"
+    res["frames"] = {str(f.relative_to(frames)): f.read_bytes() for f in sorted(frames.rglob("*")) if f.is_file()}
+    if scratch:
+        shutil.rmtree(out, ignore_errors=True)
+        del res["dir"]
     return res
 
 

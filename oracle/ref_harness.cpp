@@ -129,13 +129,13 @@ bool read_f64(const std::string& path, std::vector<double>& v) {
 
 int main(int argc, char** argv) {
     if (argc < 3) {
-        std::fprintf(stderr, "usage: %s PARAMS OUTDIR [--steps N] [--mesh-only] [--dump-materials] [--init DIR] [--no-fields]\n", argv[0]);
+        std::fprintf(stderr, "usage: %s PARAMS OUTDIR [--steps N] [--mesh-only] [--dump-materials] [--init DIR] [--no-fields] [--detectors]\n", argv[0]);
         return 2;
     }
     const std::string params_path = fs::absolute(argv[1]).string();
     const std::string outdir = fs::absolute(argv[2]).string();
     long long steps_override = -1;
-    bool mesh_only = false, dump_materials = false, dump_fields = true;
+    bool mesh_only = false, dump_materials = false, dump_fields = true, with_detectors = false;
     std::string init_dir;
     for (int a = 3; a < argc; ++a) {
         std::string s = argv[a];
@@ -143,6 +143,7 @@ int main(int argc, char** argv) {
         else if (s == "--mesh-only") mesh_only = true;
         else if (s == "--dump-materials") dump_materials = true;
         else if (s == "--no-fields") dump_fields = false;
+        else if (s == "--detectors") with_detectors = true;
         else if (s == "--init" && a + 1 < argc) init_dir = fs::absolute(argv[++a]).string();
     }
     fs::create_directories(outdir);
@@ -172,6 +173,8 @@ int main(int argc, char** argv) {
     P.probe_y = pf.num("PROBE_Y", UserConfig::PROBE_Y);
     P.probe_z = pf.num("PROBE_Z", UserConfig::PROBE_Z);
     P.bp.type = (int(pf.num("BOUNDARY_TYPE", UserConfig::BOUNDARY_TYPE)) == 0) ? BcType::PEC : BcType::CPML_RC;
+    if (pf.scalars.count("RUN_TAG")) P.run_tag = pf.scalars.at("RUN_TAG");
+    P.writeFloat64 = pf.flag("WRITE_FLOAT64", UserConfig::WRITE_FLOAT64);
     P.bp.cpml.npml = int(pf.num("CPML_NPML", UserConfig::CPML_NPML));
     P.bp.cpml.m = pf.num("CPML_M", UserConfig::CPML_M);
     P.bp.cpml.Rerr = pf.num("CPML_RERR", UserConfig::CPML_RERR);
@@ -442,6 +445,52 @@ int main(int argc, char** argv) {
     }
     meta << "],\n";
 
+    // ---- detectors (register_default_detectors, src/params.hpp:681-790, lists from the file) ----
+    std::vector<std::unique_ptr<Detectors::IDetector>> dets;
+    if (with_detectors) {
+        const fs::path out_root = fs::path("frames") / P.run_tag;
+        std::vector<real> n_grid;
+        make_n_grid_from_scene(ctx.scene, n_grid);
+        auto comp = [](int fc) {
+            return (fc >= 0 && fc <= 11) ? static_cast<Detectors::FieldComponent>(fc) : Detectors::FieldComponent::Ez;
+        };
+        for (const auto& m : pf.list("MESH_DETECTORS")) {
+            if (!to_bool(m.at(0))) continue;
+            Detectors::MeshDetectorConfig cfg;
+            cfg.name = m.at(1); cfg.slice_position = d(m, 2); cfg.slice_plane = int(d(m, 3));
+            cfg.export_mesh_lines = to_bool(m.at(4)); cfg.export_spacing_arrays = to_bool(m.at(5));
+            auto det = Detectors::make_mesh_detector(out_root, cfg, NxT, NyT, NzT, ctx.Nx_core, ctx.Ny_core,
+                                                     ctx.Nz_core, ctx.npml, ctx.grid_spacing, P.domain_size_x(),
+                                                     P.domain_size_y(), P.domain_size_z(), P.domain_x_min,
+                                                     P.domain_y_min, P.domain_z_min);
+            det->save_index_slice(n_grid);
+            det->save_mesh_info();
+            dets.push_back(std::move(det));
+        }
+        for (const auto& m : pf.list("FIELD_MOVIE_2D_DETECTORS")) {
+            if (!to_bool(m.at(0))) continue;
+            Detectors::FieldMovie2DConfig cfg;
+            cfg.name = m.at(1); cfg.component = comp(int(d(m, 2))); cfg.slice_plane = int(d(m, 3));
+            cfg.slice_position = d(m, 4); cfg.frame_pattern = m.at(5);
+            cfg.save_every = P.saveEvery; cfg.n_steps = P.nSteps; cfg.write_float64 = P.writeFloat64;
+            dets.push_back(Detectors::make_field_movie_2d(out_root, cfg, NxT, NyT, NzT, ctx.Nx_core, ctx.Ny_core,
+                                                          ctx.Nz_core, ctx.npml, ctx.grid_spacing, P.domain_size_x(),
+                                                          P.domain_size_y(), P.domain_size_z(), P.domain_x_min,
+                                                          P.domain_y_min, P.domain_z_min));
+        }
+        for (const auto& m : pf.list("POINT_FIELD_DETECTORS")) {
+            if (!to_bool(m.at(0))) continue;
+            Detectors::PointFieldDetectorConfig cfg;
+            cfg.name = m.at(1); cfg.x = d(m, 2); cfg.y = d(m, 3); cfg.z = d(m, 4);
+            cfg.save_every = P.saveEvery; cfg.n_steps = P.nSteps; cfg.write_float64 = P.writeFloat64;
+            cfg.components.clear();
+            for (size_t c = 5; c < m.size(); ++c) cfg.components.push_back(comp(int(d(m, c))));
+            dets.push_back(Detectors::make_point_field_detector(out_root, cfg, NxT, NyT, NzT, ctx.npml,
+                                                                ctx.grid_spacing, ctx.dt, P.domain_x_min,
+                                                                P.domain_y_min, P.domain_z_min));
+        }
+    }
+
     // ---- time loop (src/3D_FDTD_version008.cpp:269-328, serial path) ----
     const size_t nsteps = steps_override >= 0 ? size_t(steps_override) : P.nSteps;
     std::vector<double> probe_series;
@@ -475,6 +524,7 @@ int main(int argc, char** argv) {
                           Jz.data());
         }
         ctx.bc->apply_after_E(Ex, Ey, Ez, Hx, Hy, Hz);
+        for (auto& det : dets) det->record_after_E(n, ctx.dt, Ex, Ey, Ez, Hx, Hy, Hz);
         if (n % P.saveEvery == 0) {
             for (const auto& pr : probes)
                 for (int c : pr.comps)
@@ -484,6 +534,7 @@ int main(int argc, char** argv) {
         if (any_tls) update_populations_multi_region(NxT, NyT, NzT, ctx.dt, tls_manager, Ez, tls_state);
     }
     auto t_end = std::chrono::steady_clock::now();
+    for (auto& det : dets) det->finalize();
     const double loop_s = std::chrono::duration<double>(t_end - t_begin).count();
     meta << "  \"steps\": " << nsteps << ", \"loop_seconds\": " << loop_s << ", \"threads\": "
          << omp_get_max_threads() << ",\n";

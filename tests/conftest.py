@@ -32,6 +32,18 @@ def oracle():
     return o
 
 
+@pytest.fixture
+def outdir():
+    """A scratch directory inside the repository's build area, removed afterwards."""
+    import shutil
+    import tempfile
+    base = ROOT / "_build" / "test_out"
+    base.mkdir(parents=True, exist_ok=True)
+    d = pathlib.Path(tempfile.mkdtemp(dir=str(base)))
+    yield d
+    shutil.rmtree(d, ignore_errors=True)
+
+
 def golden(name: str):
     d = np.load(GOLDEN / (name + ".npz"))
     out = {k: d[k] for k in d.files}

@@ -9,6 +9,8 @@ shipped configs, and stores what it produced:
   step_*.npz   setup arrays (mesh lines, CPML profiles, gain map; SHA-256 digests of the
                bE arrays and of the seeded initial fields), and the reference's state and
                probe series after N_STEPS steps
+  det_*.npz    every file the reference's detectors wrote (frames/<RUN_TAG>/..., as bytes
+               keyed by relative path) over N_STEPS steps
   configs.json mesh lines and SHA-256 digests of the material arrays of the shipped
                configs (their full arrays are too large to commit)
 
@@ -21,6 +23,7 @@ import hashlib
 import json
 import os
 import pathlib
+import shutil
 import sys
 import tempfile
 
@@ -59,13 +62,16 @@ def step_case(path: pathlib.Path) -> None:
     init_dir = None
     init = {}
     if path.stem in NOISE_SEED:
-        init_dir = tempfile.mkdtemp(prefix="golden_init_")
+        (oracle.ORACLE_DIR / "_ref" / "runs").mkdir(parents=True, exist_ok=True)
+        init_dir = tempfile.mkdtemp(prefix="golden_init_", dir=str(oracle.ORACLE_DIR / "_ref" / "runs"))
         for c, v in initial_noise(path.stem, n).items():
             init["init_" + c] = v
             v.tofile(os.path.join(init_dir, c + ".f64"))
     text = path.read_text()
     steps = int([ln.split("=")[1] for ln in text.splitlines() if ln.strip().startswith("N_STEPS")][0])
     r = oracle.run_harness(path, steps, "--dump-materials", init_dir=init_dir)
+    if init_dir:
+        shutil.rmtree(init_dir, ignore_errors=True)
     keep = {k: r[k] for k in ("x_bounds", "y_bounds", "z_bounds", "probe_series") + FIELDS}
     digests = {"sha256_" + k: sha(r[k]) for k in ("bEx", "bEy", "bEz", "n_grid")}
     for k in list(r):
@@ -82,6 +88,15 @@ def step_case(path: pathlib.Path) -> None:
     keep["meta_json"] = np.frombuffer(json.dumps(meta).encode(), dtype=np.uint8)
     np.savez_compressed(HERE / (path.stem + ".npz"), **keep)
     print(path.stem, shape, steps, "steps")
+
+
+def detector_case(path: pathlib.Path) -> None:
+    text = path.read_text()
+    steps = int([ln.split("=")[1] for ln in text.splitlines() if ln.strip().startswith("N_STEPS")][0])
+    r = oracle.run_harness(path, steps, "--detectors", "--no-fields")
+    files = {k: np.frombuffer(v, dtype=np.uint8) for k, v in r["frames"].items()}
+    np.savez_compressed(HERE / (path.stem + ".npz"), **files)
+    print(path.stem, len(files), "files")
 
 
 def configs() -> None:
@@ -113,6 +128,9 @@ def main(only=()) -> None:
     for path in sorted((HERE / "cases").glob("step_*.params")):
         if not only or path.stem in only:
             step_case(path)
+    for path in sorted((HERE / "cases").glob("det_*.params")):
+        if not only or path.stem in only:
+            detector_case(path)
     if not only:
         configs()
 
