@@ -48,6 +48,7 @@ EXPORTED_SYMBOLS = (
     "fdtd_get_probe_series", "fdtd_get_dft", "fdtd_get_diagnostics", "fdtd_device_bytes",
     "fdtd_kernel_launches", "fdtd_set_timing", "fdtd_get_timing", "fdtd_set_kernel_path", "fdtd_synchronize", "fdtd_last_error",
     "fdtd_destroy", "fdtd_field_scan_noalloc", "fdtd_attach_outputs", "fdtd_flush_outputs",
+    "fdtd_close_outputs",
     "fdtd_batch_create", "fdtd_batch_submit", "fdtd_batch_run", "fdtd_batch_job_state",
     "fdtd_batch_probe_series", "fdtd_batch_dft", "fdtd_batch_diagnostics", "fdtd_batch_release",
     "fdtd_batch_last_error", "fdtd_batch_destroy",
@@ -154,6 +155,7 @@ def load_library() -> C.CDLL:
         "fdtd_setup_write_outputs": (C.c_int, [vp, C.c_char_p, C.c_char_p, C.c_size_t]),
         "fdtd_attach_outputs": (C.c_int, [vp, vp, C.c_char_p]),
         "fdtd_flush_outputs": (C.c_int, [vp]),
+        "fdtd_close_outputs": (C.c_int, [vp]),
         "fdtd_create": (C.c_int, [C.POINTER(SetupV1), C.c_int, C.POINTER(vp)]),
         "fdtd_set_field": (C.c_int, [vp, C.c_int, _dptr]),
         "fdtd_get_field": (C.c_int, [vp, C.c_int, _dptr]),
@@ -375,6 +377,10 @@ class Solver:
 
     def flush_outputs(self) -> None:
         self._check(load_library().fdtd_flush_outputs(self._h), "fdtd_flush_outputs")
+
+    def close_outputs(self) -> None:
+        """End-of-run files (last population frame, its metadata), then detach."""
+        self._check(load_library().fdtd_close_outputs(self._h), "fdtd_close_outputs")
 
     def close(self) -> None:
         if getattr(self, "_h", None) is not None and self._h.value:

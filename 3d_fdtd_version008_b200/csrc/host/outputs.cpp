@@ -147,7 +147,71 @@ OutputPlan make_output_plan(const SimSetup& S) {
         q.pz = S.grid.cell_center_physical(2, p.k);
         plan.points.push_back(q);
     }
+    plan.NxT = S.NxT; plan.NyT = S.NyT; plan.NzT = S.NzT;
+    plan.save_every = S.save_every; plan.n_steps = S.n_steps; plan.dt = S.dt;
+    plan.tls = S.tls.enabled();
+    if (plan.tls) {  // src/3D_FDTD_version008.cpp:175-180 (P.probe_* from PROBE_X/Y/Z)
+        const real pr[3] = {pf.num("PROBE_X", 2000e-9), pf.num("PROBE_Y", 2000e-9), pf.num("PROBE_Z", 500e-9)};
+        std::size_t ix[3];
+        for (int a = 0; a < 3; ++a) ix[a] = S.grid.physical_to_index(a, pr[a] - S.domain_min[a]);
+        plan.mon_i = ix[0]; plan.mon_j = ix[1]; plan.mon_k = ix[2];
+        plan.mon_valid = ix[0] < S.NxT && ix[1] < S.NyT && ix[2] < S.NzT;
+    }
     return plan;
+}
+
+std::string inversion_line(uint64_t n, double dt, double total_Nu, double total_Ng) {
+    const double inversion = total_Nu - total_Ng, denom = total_Nu + total_Ng;
+    const double inv_fraction = (denom > 1e-30) ? (inversion / denom) : 0.0;
+    const real t = real(n) * dt;
+    std::ostringstream o;
+    o << std::setprecision(18) << t << "," << total_Nu << "," << total_Ng << "," << inversion << "," << inv_fraction
+      << "\n";
+    return o.str();
+}
+
+std::string polarization_line(uint64_t n, double dt, double Pz_center, double dPz_dt_center, double P_energy) {
+    const real t = real(n) * dt;
+    std::ostringstream o;
+    o << std::setprecision(18) << t << "," << Pz_center << "," << dPz_dt_center << "," << P_energy << "\n";
+    return o.str();
+}
+
+std::string global_history_line(uint64_t n, double dt, double Nu_total, double Ng_total) {
+    const double Ntotal = Nu_total + Ng_total, inversion_total = Nu_total - Ng_total;
+    double Nu_percent = 0.0, Ng_percent = 0.0, inv_norm = 0.5;
+    if (Ntotal > 1e-30) {
+        Nu_percent = Nu_total / Ntotal;
+        Ng_percent = Ng_total / Ntotal;
+        inv_norm = (inversion_total / Ntotal + 1.0) / 2.0;
+    }
+    const double t_fs = double(n) * dt * 1e15;
+    std::ostringstream o;
+    o << n << "," << std::setprecision(6) << std::fixed << t_fs << "," << std::setprecision(12) << std::scientific
+      << Nu_total << "," << Ng_total << "," << inversion_total << "," << std::setprecision(8) << std::fixed
+      << Nu_percent << "," << Ng_percent << "," << inv_norm << "\n";
+    return o.str();
+}
+
+void write_population_metadata(const OutputPlan& S, const std::string& root) {
+    const OutputPlan& plan = S;
+    const fs::path p = fs::path(run_dir(plan, root)) / "populations" / "metadata_populations.json";
+    std::ofstream meta(p);
+    if (!meta) throw std::runtime_error("cannot write " + p.string());
+    meta << "{\n"
+         << "  \"NxT\": " << S.NxT << ",\n"
+         << "  \"NyT\": " << S.NyT << ",\n"
+         << "  \"NzT\": " << S.NzT << ",\n"
+         << "  \"saveEvery\": " << S.save_every << ",\n"
+         << "  \"nSteps\": " << S.n_steps << ",\n"
+         << "  \"dt\": " << std::setprecision(18) << S.dt << ",\n"
+         << "  \"dtype\": \"float64\",\n"
+         << "  \"binary_frames\": 2,\n"
+         << "  \"binary_mode\": \"first_and_last\",\n"
+         << "  \"binary_data_units\": \"m^-3 (density)\",\n"
+         << "  \"csv_total_units\": \"atoms (integrated)\",\n"
+         << "  \"what\": \"population_densities_Nu_and_Ng_vs_time\"\n"
+         << "}\n";
 }
 
 std::string run_dir(const OutputPlan& plan, const std::string& root) {
@@ -434,6 +498,22 @@ void write_setup_outputs(const SimSetup& S, const OutputPlan& plan, const std::s
         f << "  \"note\": \"time series of field components at single point\"\n";
         f << "}\n";
     }
+
+    if (plan.tls) {  // the constructors of the two-level detectors (src/two_level_detectors.hpp)
+        const fs::path pop = dir / "populations", pol = dir / "polarization";
+        for (const fs::path& d : {pop, pol}) {
+            fs::create_directories(d, ec);
+            if (ec) throw std::runtime_error("cannot create " + d.string());
+        }
+        for (const char* b : {"populations_Nu.bin", "populations_Ng.bin"}) {
+            std::ofstream t(pop / b, std::ios::binary | std::ios::trunc);
+            if (!t) throw std::runtime_error("cannot write " + (pop / b).string());
+        }
+        open_text(pop / "inversion_time.csv") << "t, total_Nu, total_Ng, inversion, inv_fraction\n";
+        open_text(pol / "polarization_time.csv") << "t, Pz_center, dPz_dt_center, total_P_energy\n";
+        open_text(dir / "tls_global_history.csv")
+            << "step,t_fs,Nu_total,Ng_total,inversion_total,Nu_percent,Ng_percent,inv_norm\n";
+    }
 }
 
 // ---------------------------------------------------------------- writer thread
@@ -482,7 +562,12 @@ void OutputWriter::loop() {
             if (j.wait) j.wait();
             std::ofstream f(j.path, std::ios::binary | (j.append ? std::ios::app : std::ios::trunc));
             if (!f) throw std::runtime_error("cannot write " + j.path);
-            f.write(static_cast<const char*>(j.data), std::streamsize(j.bytes));
+            if (j.text) {
+                const std::string t = j.text();
+                f.write(t.data(), std::streamsize(t.size()));
+            } else {
+                f.write(static_cast<const char*>(j.data), std::streamsize(j.bytes));
+            }
             if (!f) throw std::runtime_error("write failed: " + j.path);
         } catch (const std::exception& e) {
             err = e.what();

@@ -3,6 +3,11 @@
 // detectors of register_default_detectors (src/params.hpp:681-790): MeshDetector,
 // FieldMovie2D and PointFieldDetector (src/detectors/*.hpp), same names, layout and text.
 //
+// With gain, the two-level detectors main() creates (src/3D_FDTD_version008.cpp:174-198,
+// src/two_level_detectors.hpp): populations/ (first and last Nu/Ng frames, inversion_time.csv,
+// metadata_populations.json), polarization/polarization_time.csv and tls_global_history.csv.
+// (TLSGlobalHistory's plotting script is not written: it is not an output format.)
+//
 // This part is host-only: the plan (which files, which slices), the text files and the
 // writer thread.  The stepper captures movie slices and probe samples on the device and
 // hands them to an OutputWriter (solver.cu).
@@ -52,7 +57,23 @@ struct OutputPlan {
     std::vector<MeshDetectorPlan> meshes;
     std::vector<MoviePlan> movies;
     std::vector<PointPlan> points;
+    bool tls = false;  // the setup has gain: write the two-level detectors' files
+    // PolarizationDiagnostics' cell: PROBE_X/Y/Z mapped like main() does (no clamp);
+    // mon_valid is false when that cell lies outside the field grid.
+    bool mon_valid = false;
+    std::size_t mon_i = 0, mon_j = 0, mon_k = 0;
+    // what the end-of-run metadata needs
+    std::size_t NxT = 0, NyT = 0, NzT = 0, save_every = 1, n_steps = 0;
+    double dt = 0;
 };
+
+// One line of each two-level CSV at step n (the record() functions of
+// PopulationTimeSeriesDetector, PolarizationDiagnostics and TLSGlobalHistory).
+std::string inversion_line(uint64_t n, double dt, double total_Nu, double total_Ng);
+std::string polarization_line(uint64_t n, double dt, double Pz_center, double dPz_dt_center, double P_energy);
+std::string global_history_line(uint64_t n, double dt, double Nu_total, double Ng_total);
+// PopulationTimeSeriesDetector::finalize's metadata_populations.json.
+void write_population_metadata(const OutputPlan& plan, const std::string& root);
 
 // Reads RUN_TAG, WRITE_FLOAT64, MESH_DETECTORS and FIELD_MOVIE_2D_DETECTORS from the
 // setup's parameter file and takes the point detectors from the setup.  Throws
@@ -80,6 +101,7 @@ class OutputWriter {
 public:
     struct Job {
         std::function<void()> wait, done;
+        std::function<std::string()> text;  // when set: the bytes to write, made after wait()
         std::string path;
         const void* data = nullptr;
         std::size_t bytes = 0;

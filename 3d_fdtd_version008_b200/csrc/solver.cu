@@ -279,7 +279,7 @@ __device__ void block_commit(DiagAccum* acc, double mE, double mP, unsigned fl, 
 // calculate_conservation_error (:155-170), compute_integrated_Nu/Ng and
 // compute_polarization_energy (src/two_level_system.hpp:344-418) over the fields after
 // the step.  Field arrays are scanned as flat padded arrays (padding holds zeros).
-template <typename S, typename T>
+template <typename S, typename T, bool FIELDS = true>
 __device__ void monitor_reduce_blocks(const StepArgs<S, T>& a, size_t nflat, const double* __restrict__ dxs,
                                       const double* __restrict__ dys, const double* __restrict__ dzs, int parity_next,
                                       DiagAccum* acc, double es, unsigned bid, unsigned nblk) {
@@ -289,7 +289,7 @@ __device__ void monitor_reduce_blocks(const StepArgs<S, T>& a, size_t nflat, con
     const size_t stride = size_t(nblk) * blockDim.x;
     // 16-byte vectors: nflat is a multiple of the padded row, itself a multiple of W
     constexpr int W = Vec<T>::W;
-    for (size_t v = bid * size_t(blockDim.x) + threadIdx.x; v < nflat / W; v += stride) {
+    for (size_t v = bid * size_t(blockDim.x) + threadIdx.x; FIELDS && v < nflat / W; v += stride) {
         const size_t t = v * W;
         T ex[W], ey[W], ez[W], hx[W], hy[W], hz[W];
         Fld<S, T>::ldg(a.Ex + t, ex); Fld<S, T>::ldg(a.Ey + t, ey); Fld<S, T>::ldg(a.Ez + t, ez);
@@ -327,6 +327,31 @@ __device__ void monitor_reduce_blocks(const StepArgs<S, T>& a, size_t nflat, con
         }
     }
     block_commit(acc, mE, mP, fl, s0, s1, s2, s3, s4);
+}
+
+// The two-level detectors' record at one step: the gain integrals (as the monitor computes
+// them, without the field scan) and, at the PolarizationDiagnostics cell (gain-box offset
+// mon_t, or -1), Pz^{n+1} and dPz/dt = (Pz^{n+1} - Pz^n) inv_dt (src/two_level_system.hpp:600-604).
+struct TlsRecord {
+    DiagAccum acc;
+    double P_center, dP_dt;
+};
+
+template <typename S, typename T>
+__global__ void k_tls_reduce(const StepArgs<S, T> a, const double* __restrict__ dxs, const double* __restrict__ dys,
+                             const double* __restrict__ dzs, int parity_next, double es, TlsRecord* rec,
+                             long long mon_t) {
+    monitor_reduce_blocks<S, T, false>(a, 0, dxs, dys, dzs, parity_next, &rec->acc, es, blockIdx.x, gridDim.x);
+    if (blockIdx.x == 0 && threadIdx.x == 0 && mon_t >= 0) {
+        const int r = a.greg[mon_t];
+        if (r >= 0 && a.gcoef[r].active) {
+            const T* Pn = parity_next ? a.P1 : a.P0;
+            const T* Po = parity_next ? a.P0 : a.P1;
+            const double pn = double(Pn[mon_t]), po = double(Po[mon_t]);
+            rec->P_center = pn;
+            rec->dP_dt = __dmul_rn(__dsub_rn(pn, po), double(a.gcoef[r].inv_dt));
+        }
+    }
 }
 
 // One thread: the StabilityMonitor decision for monitor step `step`; sets the abort
@@ -491,6 +516,7 @@ public:
     virtual void timing(fdtd_timing_v1* t) = 0;
     virtual void attach_outputs(const fdtd::SimSetup& setup, const std::string& root) = 0;
     virtual void flush_outputs() = 0;
+    virtual void close_outputs() = 0;
     uint64_t steps = 0, launches = 0, dev_bytes = 0;
     int device = 0;
 };
@@ -547,6 +573,9 @@ private:
     void flush_outputs() override;
     void capture_movies();
     void write_point_samples();
+    void capture_tls(uint64_t s);
+    void write_population_frame();
+    void close_outputs() override;
     // Host <-> device copies of FP64 arrays through two pinned chunks: the host-side copy of
     // one chunk (OpenMP) overlaps the DMA of the other.
     static constexpr size_t kPinBytes = size_t(32) << 20;
@@ -627,6 +656,15 @@ private:
     std::condition_variable oslot_cv_;
     int oslot_busy_[kOutSlots] = {};
     uint64_t oframe_ = 0, ots_written_ = 0;
+    // two-level detector records: kTlsSlots device records and pinned copies, same reuse rule
+    static constexpr int kTlsSlots = 16;
+    TlsRecord* d_trec_ = nullptr;
+    TlsRecord* h_trec_ = nullptr;
+    cudaEvent_t trec_ev_[kTlsSlots] = {};
+    int trec_busy_[kTlsSlots] = {};
+    uint64_t tls_count_ = 0;
+    long long mon_t_ = -1;
+    bool pop_first_done_ = false;
     ProbeDev* d_probes_ = nullptr;
     double *d_freqs_ = nullptr, *d_dft_ = nullptr, *d_series_ = nullptr;
     uint64_t series_cap_ = 0, series_count_ = 0;
@@ -1061,6 +1099,9 @@ Solver<S, T>::~Solver() {
         if (h_oslot_[q]) cudaFreeHost(h_oslot_[q]);
         if (oslot_ev_[q]) cudaEventDestroy(oslot_ev_[q]);
     }
+    if (h_trec_) cudaFreeHost(h_trec_);
+    for (int q = 0; q < kTlsSlots; ++q)
+        if (trec_ev_[q]) cudaEventDestroy(trec_ev_[q]);
     for (auto& e : ev_) if (e) cudaEventDestroy(e);
     for (void* p : ptrs_) cudaFreeAsync(p, st_);
     if (d_stage_) cudaFreeAsync(d_stage_, st_);
@@ -1322,6 +1363,7 @@ void Solver<S, T>::run(uint64_t n) {
             if (sample >= 0) series_count_ = uint64_t(sample) + 1;
         }
         if (writer_ && !oplan_.movies.empty() && s % save_every_ == 0) capture_movies();
+        if (writer_ && oplan_.tls && s % save_every_ == 0) capture_tls(s);
         if (interval_ && s % interval_ == 0) {
             k_monitor_reduce<S, T><<<8 * 148, 256, 0, st_>>>(a_, nflat_, d_dx_, d_dy_, d_dz_, int((s + 1) & 1), d_acc_, sE_);
             k_monitor_eval<<<1, 1, 0, st_>>>(d_acc_, d_ms_, d_status_, s);
@@ -1398,9 +1440,107 @@ void Solver<S, T>::attach_outputs(const fdtd::SimSetup& Sp, const std::string& r
             ck(cudaEventCreateWithFlags(&oslot_ev_[q], cudaEventDisableTiming), "cudaEventCreate");
         }
     }
+    if (plan.tls) {
+        d_trec_ = alloc<TlsRecord>(kTlsSlots);
+        ck(cudaHostAlloc(reinterpret_cast<void**>(&h_trec_), kTlsSlots * sizeof(TlsRecord), cudaHostAllocDefault),
+           "cudaHostAlloc");
+        for (int q = 0; q < kTlsSlots; ++q)
+            ck(cudaEventCreateWithFlags(&trec_ev_[q], cudaEventDisableTiming), "cudaEventCreate");
+        const StepArgs<S, T>& a = a_;
+        if (has_gain_ && plan.mon_valid) {
+            const long long i = (long long)plan.mon_i - a.gi0, j = (long long)plan.mon_j - a.gj0,
+                            k = (long long)plan.mon_k - a.gk0;
+            if (i >= 0 && i < a.gX && j >= 0 && j < a.gY && k >= 0 && k < a.gZ) mon_t_ = (k * a.gY + j) * a.gX + i;
+        }
+    }
     oplan_ = std::move(plan);
     oroot_ = root;
     writer_ = std::make_unique<fdtd::OutputWriter>();
+}
+
+template <typename S, typename T>
+void Solver<S, T>::write_population_frame() {
+    // PopulationTimeSeriesDetector::write_binary_frame: the full-grid Nu and Ng, FP64, idx3.
+    const size_t N = size_t(NxT_) * NyT_ * NzT_;
+    const std::string dir = fdtd::run_dir(oplan_, oroot_) + "/populations/";
+    for (int w : {int(FDTD_TLS_NU), int(FDTD_TLS_NG)}) {
+        auto buf = std::make_shared<std::vector<double>>(N);
+        get_tls(w, buf->data());
+        fdtd::OutputWriter::Job j;
+        j.path = dir + (w == FDTD_TLS_NU ? "populations_Nu.bin" : "populations_Ng.bin");
+        j.data = buf->data();
+        j.bytes = N * sizeof(double);
+        j.append = true;
+        j.done = [buf] {};
+        writer_->submit(std::move(j));
+    }
+}
+
+template <typename S, typename T>
+void Solver<S, T>::capture_tls(uint64_t s) {
+    if (!pop_first_done_) {
+        write_population_frame();
+        pop_first_done_ = true;
+    }
+    const int sl = int(tls_count_++ % kTlsSlots);
+    {
+        std::unique_lock<std::mutex> l(oslot_mu_);
+        oslot_cv_.wait(l, [&] { return trec_busy_[sl] == 0; });
+        trec_busy_[sl] = 3;
+    }
+    ck(cudaMemsetAsync(d_trec_ + sl, 0, sizeof(TlsRecord), st_), "cudaMemsetAsync");
+    if (has_gain_) {
+        const size_t ng = size_t(a_.gX) * a_.gY * a_.gZ;
+        const unsigned nb = unsigned(std::max<size_t>(1, std::min<size_t>((ng + 255) / 256, 148 * 4)));
+        k_tls_reduce<S, T><<<nb, 256, 0, st_>>>(a_, d_dx_, d_dy_, d_dz_, int((s + 1) & 1), sE_, d_trec_ + sl, mon_t_);
+        ++launches;
+    }
+    ck(cudaMemcpyAsync(h_trec_ + sl, d_trec_ + sl, sizeof(TlsRecord), cudaMemcpyDeviceToHost, st_), "TLS record D2H");
+    ck(cudaEventRecord(trec_ev_[sl], st_), "cudaEventRecord");
+    const cudaEvent_t ev = trec_ev_[sl];
+    const int dev = device;
+    const TlsRecord* r = h_trec_ + sl;
+    const double dt = dt_;
+    const std::string dir = fdtd::run_dir(oplan_, oroot_);
+    auto release = [this, sl] {
+        {
+            std::lock_guard<std::mutex> l(oslot_mu_);
+            --trec_busy_[sl];
+        }
+        oslot_cv_.notify_all();
+    };
+    fdtd::OutputWriter::Job a, b, c;
+    a.wait = [ev, dev] {
+        cudaSetDevice(dev);
+        if (cudaEventSynchronize(ev) != cudaSuccess) throw std::runtime_error("two-level record copy failed");
+    };
+    a.text = [r, s, dt] { return fdtd::inversion_line(s, dt, r->acc.int_Nu, r->acc.int_Ng); };
+    a.path = dir + "/populations/inversion_time.csv";
+    b.text = [r, s, dt] { return fdtd::polarization_line(s, dt, r->P_center, r->dP_dt, r->acc.p_energy); };
+    b.path = dir + "/polarization/polarization_time.csv";
+    c.text = [r, s, dt] { return fdtd::global_history_line(s, dt, r->acc.int_Nu, r->acc.int_Ng); };
+    c.path = dir + "/tls_global_history.csv";
+    for (fdtd::OutputWriter::Job* j : {&a, &b, &c}) {
+        j->append = true;
+        j->done = release;
+        writer_->submit(std::move(*j));
+    }
+}
+
+template <typename S, typename T>
+void Solver<S, T>::close_outputs() {
+    if (!writer_) return;
+    ck(cudaSetDevice(device), "cudaSetDevice");
+    if (oplan_.tls) {  // PopulationTimeSeriesDetector::finalize: the last frame and the metadata
+        write_population_frame();
+        try {
+            fdtd::write_population_metadata(oplan_, oroot_);
+        } catch (const std::exception& e) {
+            throw Failure(FDTD_ERR_IO, e.what());
+        }
+    }
+    flush_outputs();
+    writer_.reset();
 }
 
 template <typename S, typename T>
@@ -1887,6 +2027,7 @@ int fdtd_attach_outputs(fdtd_handle* h, const fdtd_setup* s, const char* out_dir
     return guarded(h, [&] { h->s->attach_outputs(*fdtd_internal_setup(s), out_dir); });
 }
 int fdtd_flush_outputs(fdtd_handle* h) { if (!h) return FDTD_ERR_INVALID; return guarded(h, [&] { h->s->flush_outputs(); }); }
+int fdtd_close_outputs(fdtd_handle* h) { if (!h) return FDTD_ERR_INVALID; return guarded(h, [&] { h->s->close_outputs(); }); }
 int fdtd_synchronize(fdtd_handle* h) { if (!h) return FDTD_ERR_INVALID; return guarded(h, [&] { h->s->sync(); }); }
 const char* fdtd_last_error(const fdtd_handle* h) { return h ? h->err.c_str() : g_err.c_str(); }
 void fdtd_destroy(fdtd_handle* h) { delete h; }

@@ -261,11 +261,19 @@ int fdtd_set_kernel_path(fdtd_handle *h, int path);
  * fdtd_setup_write_outputs writes, then every SAVE_EVERY-th step each
  * FIELD_MOVIE_2D_DETECTORS slice is captured on the device, copied out and written as its
  * own frame file by a background thread, and after every fdtd_run call the new point
- * samples are appended to the <component>_ts.bin files.  Before the first step only. */
+ * samples are appended to the <component>_ts.bin files.  With gain, the two-level
+ * detectors of main() (src/two_level_detectors.hpp) record at the same steps:
+ * populations/inversion_time.csv, polarization/polarization_time.csv and
+ * tls_global_history.csv from device reductions, and the first Nu/Ng frame.  Before the
+ * first step only. */
 int fdtd_attach_outputs(fdtd_handle *h, const fdtd_setup *s, const char *out_dir);
 /* Waits until every frame and sample captured so far is on disk; FDTD_ERR_IO if a write
  * failed.  fdtd_destroy also waits. */
 int fdtd_flush_outputs(fdtd_handle *h);
+/* Ends the outputs as the reference ends its run (PopulationTimeSeriesDetector::finalize:
+ * the last Nu/Ng frame and metadata_populations.json), waits for every write and detaches;
+ * later steps write nothing. */
+int fdtd_close_outputs(fdtd_handle *h);
 /* Block until all device work of the handle is complete. */
 int fdtd_synchronize(fdtd_handle *h);
 /* Message of the last failing call on h (or of the last global failure when h is NULL). */

@@ -26,6 +26,7 @@
 #include "structure_material.hpp"
 #include "two_level_system.hpp"
 #include "stability_monitor.hpp"
+#include "two_level_detectors.hpp"
 
 #include <chrono>
 #include <cstdio>
@@ -402,6 +403,18 @@ int main(int argc, char** argv) {
         }
         tls_manager.initialize(tls_state, ctx.grid_spacing);
         tls_manager.finalize_with_dt(ctx.dt);
+        if (tls_manager.num_regions() > 0) {  // gain bounding box (src/3D_FDTD_version008.cpp:146-163)
+            const auto& r0 = tls_manager.regions[0];
+            tls_state.gain_i0 = r0.i0; tls_state.gain_i1 = r0.i1;
+            tls_state.gain_j0 = r0.j0; tls_state.gain_j1 = r0.j1;
+            tls_state.gain_k0 = r0.k0; tls_state.gain_k1 = r0.k1;
+            for (size_t r = 1; r < tls_manager.num_regions(); ++r) {
+                const auto& rg = tls_manager.regions[r];
+                tls_state.gain_i0 = std::min(tls_state.gain_i0, rg.i0); tls_state.gain_i1 = std::max(tls_state.gain_i1, rg.i1);
+                tls_state.gain_j0 = std::min(tls_state.gain_j0, rg.j0); tls_state.gain_j1 = std::max(tls_state.gain_j1, rg.j1);
+                tls_state.gain_k0 = std::min(tls_state.gain_k0, rg.k0); tls_state.gain_k1 = std::max(tls_state.gain_k1, rg.k1);
+            }
+        }
         write_i32(od, "tls_region_map", tls_manager.cell_region_map);
         write_f64(od, "tls_Ndip", tls_state.Ndip);
         if (!init_dir.empty()) {
@@ -491,6 +504,23 @@ int main(int argc, char** argv) {
         }
     }
 
+    // ---- two-level detectors (src/3D_FDTD_version008.cpp:174-198), with the gain ----
+    std::unique_ptr<PopulationTimeSeriesDetector> pop_detector;
+    std::unique_ptr<PolarizationDiagnostics> pol_diagnostics;
+    std::unique_ptr<TLSGlobalHistory> tls_global_history;
+    if (with_detectors && any_tls) {
+        const fs::path out_root = fs::path("frames") / P.run_tag;
+        const size_t ic = ctx.grid_spacing.physical_to_index_x(P.probe_x - P.domain_x_min);
+        const size_t jc = ctx.grid_spacing.physical_to_index_y(P.probe_y - P.domain_y_min);
+        const size_t kc = ctx.grid_spacing.physical_to_index_z(P.probe_z - P.domain_z_min);
+        pop_detector = std::make_unique<PopulationTimeSeriesDetector>(out_root, "populations", NxT, NyT, NzT,
+                                                                      P.saveEvery, P.nSteps, P.dt, ctx.grid_spacing);
+        pol_diagnostics = std::make_unique<PolarizationDiagnostics>(out_root, "polarization", NxT, NyT, NzT, ic, jc,
+                                                                    kc, P.saveEvery, P.dt);
+        tls_global_history = std::make_unique<TLSGlobalHistory>(out_root, tls_state, ctx.grid_spacing, P.saveEvery,
+                                                                P.dt, false);
+    }
+
     // ---- time loop (src/3D_FDTD_version008.cpp:269-328, serial path) ----
     const size_t nsteps = steps_override >= 0 ? size_t(steps_override) : P.nSteps;
     std::vector<double> probe_series;
@@ -532,7 +562,12 @@ int main(int argc, char** argv) {
                                                                       pr.id, Ex, Ey, Ez, Hx, Hy, Hz));
         }
         if (any_tls) update_populations_multi_region(NxT, NyT, NzT, ctx.dt, tls_manager, Ez, tls_state);
+        if (pop_detector) pop_detector->record(n, tls_state);
+        if (pol_diagnostics) pol_diagnostics->record(n, tls_state, Ez, ctx.grid_spacing);
+        if (tls_global_history) tls_global_history->record(n, tls_state);
     }
+    if (pop_detector) pop_detector->finalize(tls_state);
+    if (tls_global_history) tls_global_history->finalize();
     auto t_end = std::chrono::steady_clock::now();
     for (auto& det : dets) det->finalize();
     const double loop_s = std::chrono::duration<double>(t_end - t_begin).count();

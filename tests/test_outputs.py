@@ -26,6 +26,17 @@ def is_frame(name: str) -> bool:
     return name.endswith(".raw") and "refractive_index" not in name
 
 
+def is_run_time(name: str) -> bool:
+    """Written while the solve steps (or at its end), not at setup."""
+    return is_frame(name) or name.endswith(("_ts.bin", "populations_Nu.bin", "populations_Ng.bin", ".csv",
+                                            "metadata_populations.json"))
+
+
+def csv_rows(data: bytes):
+    lines = data.decode().splitlines()
+    return lines[0], np.array([[float(x) for x in ln.split(",")] for ln in lines[1:]])
+
+
 def config_line(line: str) -> bool:
     t = line.strip()
     return t.startswith('"source_') or t.startswith('"num_structures') or t.startswith('"structures') or \
@@ -38,9 +49,14 @@ def test_setup_outputs_match_reference(pkg, outdir):
     ref = ref_files()
     root = pathlib.Path(outdir) / "frames"
     mine = {str(f.relative_to(root)): f.read_bytes() for f in root.rglob("*") if f.is_file()}
-    setup_time = {k for k in ref if not is_frame(k) and not k.endswith("_ts.bin")}
+    setup_time = {k for k in ref if not is_run_time(k)}
     assert setup_time <= set(mine), sorted(setup_time - set(mine))
     assert {k for k in mine if k.endswith("_ts.bin")} == {k for k in ref if k.endswith("_ts.bin")}
+    for k in ref:  # the two-level CSVs start with the reference's header line
+        if k.endswith(".csv"):
+            assert mine[k] == ref[k].split(b"\n")[0] + b"\n", k
+        if k.endswith(("populations_Nu.bin", "populations_Ng.bin")):
+            assert mine[k] == b""
     for k in sorted(setup_time):
         if k.endswith("mesh_info.json"):
             a = [ln for ln in mine[k].decode().splitlines() if not config_line(ln)]
@@ -51,6 +67,7 @@ def test_setup_outputs_match_reference(pkg, outdir):
     for k in mine:
         if k.endswith("_ts.bin"):
             assert mine[k] == b""
+    assert not any(k.endswith("metadata_populations.json") for k in mine)
 
 
 def test_mesh_info_uses_this_setups_dipole_and_structures(pkg, outdir):
@@ -85,13 +102,27 @@ def test_streamed_outputs_match_reference(pkg, outdir, precision, tol):
     sol.attach_outputs(outdir)
     sol.run(17)
     sol.run(13)
-    sol.flush_outputs()
+    sol.close_outputs()
     ref = ref_files()
     root = pathlib.Path(outdir) / "frames"
     mine = {str(f.relative_to(root)): f.read_bytes() for f in root.rglob("*") if f.is_file()}
     assert set(mine) == set(ref), sorted(set(mine) ^ set(ref))
     for k in sorted(ref):
-        if is_frame(k) or k.endswith("_ts.bin"):
+        if k.endswith(".csv"):
+            h1, a = csv_rows(mine[k])
+            h2, b = csv_rows(ref[k])
+            assert h1 == h2 and a.shape == b.shape, k
+            scale = np.maximum(np.abs(b).max(axis=0), 1e-300)
+            # tls_global_history.csv prints 6-12 significant digits: its own rounding dominates
+            ctol = max(tol, 2e-8) if "tls_global" in k else tol
+            assert np.all(np.abs(a - b) <= ctol * scale + 1e-300), (k, np.abs(a - b).max(axis=0) / scale)
+            if "tls_global" in k:
+                assert np.array_equal(a[:, 0], b[:, 0])
+        elif k.endswith(("populations_Nu.bin", "populations_Ng.bin")):
+            a = np.frombuffer(mine[k], dtype=np.float64)
+            b = np.frombuffer(ref[k], dtype=np.float64)
+            assert a.shape == b.shape and np.linalg.norm(a - b) <= max(tol, 1e-6) * np.linalg.norm(b), k
+        elif is_frame(k) or k.endswith("_ts.bin"):
             a = np.frombuffer(mine[k], dtype=np.float64)
             b = np.frombuffer(ref[k], dtype=np.float64)
             assert a.shape == b.shape, k
