@@ -47,7 +47,7 @@ EXPORTED_SYMBOLS = (
     "fdtd_set_tls_state", "fdtd_get_tls_state", "fdtd_run", "fdtd_steps_done",
     "fdtd_get_probe_series", "fdtd_get_dft", "fdtd_get_diagnostics", "fdtd_device_bytes",
     "fdtd_kernel_launches", "fdtd_set_timing", "fdtd_get_timing", "fdtd_set_kernel_path", "fdtd_synchronize", "fdtd_last_error",
-    "fdtd_destroy", "fdtd_field_scan_noalloc", "fdtd_attach_outputs", "fdtd_flush_outputs",
+    "fdtd_destroy", "fdtd_field_scan_noalloc", "fdtd_attach_outputs", "fdtd_flush_outputs", "fdtd_material_rows",
     "fdtd_close_outputs",
     "fdtd_batch_create", "fdtd_batch_submit", "fdtd_batch_run", "fdtd_batch_job_state",
     "fdtd_batch_probe_series", "fdtd_batch_dft", "fdtd_batch_diagnostics", "fdtd_batch_release",
@@ -109,7 +109,8 @@ class SetupV1(C.Structure):
         ("conservation_err", C.c_double), ("growth_rate", C.c_double),
         ("field_scale", C.c_double),
         ("n_sheets", C.c_uint32), ("sheets", C.POINTER(SheetV1)),
-        ("pec_boundary", C.c_uint32), ("reserved1", C.c_uint32),
+        ("pec_boundary", C.c_uint32), ("n_bE_rows", C.c_uint32),
+        ("bE_rows", C.POINTER(C.c_double)), ("bE_index", C.POINTER(C.c_uint16)),
     ]
 
 
@@ -155,6 +156,7 @@ def load_library() -> C.CDLL:
         "fdtd_setup_write_outputs": (C.c_int, [vp, C.c_char_p, C.c_char_p, C.c_size_t]),
         "fdtd_attach_outputs": (C.c_int, [vp, vp, C.c_char_p]),
         "fdtd_flush_outputs": (C.c_int, [vp]),
+        "fdtd_material_rows": (C.c_int, [vp, C.POINTER(C.c_uint64)]),
         "fdtd_close_outputs": (C.c_int, [vp]),
         "fdtd_create": (C.c_int, [C.POINTER(SetupV1), C.c_int, C.POINTER(vp)]),
         "fdtd_set_field": (C.c_int, [vp, C.c_int, _dptr]),
@@ -345,6 +347,13 @@ class Solver:
     def device_bytes(self) -> int:
         n = C.c_uint64()
         self._check(load_library().fdtd_device_bytes(self._h, C.byref(n)), "fdtd_device_bytes")
+        return n.value
+
+    @property
+    def material_rows(self) -> int:
+        """Distinct bE rows when the material is held as a row index per cell, else 0."""
+        n = C.c_uint64()
+        self._check(load_library().fdtd_material_rows(self._h, C.byref(n)), "fdtd_material_rows")
         return n.value
 
     @property

@@ -19,6 +19,9 @@ struct fdtd_setup {
     // aE = aH = 1 and bH uniform everywhere (lossless, mu_r = 1 -- what make_nk gives): the
     // view then passes those arrays as NULL and the stepper skips scanning them
     bool uniform_ah = false;
+    // distinct bE rows and each cell's row number (empty when there are more than 65535)
+    std::vector<double> bE_rows;
+    std::vector<uint16_t> bE_index;
 };
 
 namespace {
@@ -116,6 +119,15 @@ int fdtd_setup_parse(const char* params_text, int mesh_only, fdtd_setup** out, c
             u = !S.mats.aE[a].empty() && !S.mats.aH[a].empty() && !S.mats.bH[a].empty() && all_equal(S.mats.aE[a], 1.0) &&
                 all_equal(S.mats.aH[a], 1.0) && all_equal(S.mats.bH[a], S.mats.bH[0][0]);
         s->uniform_ah = u;
+        if (!S.mats.bE[0].empty()) {
+            const double* bE[3] = {S.mats.bE[0].data(), S.mats.bE[1].data(), S.mats.bE[2].data()};
+            std::vector<std::array<double, 3>> rows;
+            if (fdtd::distinct_rows(bE, S.mats.bE[0].size(), rows, s->bE_index)) {
+                for (const auto& r : rows) s->bE_rows.insert(s->bE_rows.end(), r.begin(), r.end());
+            } else {
+                s->bE_index.clear();
+            }
+        }
         *out = s;
         return FDTD_OK;
     } catch (const std::exception& e) {
@@ -152,6 +164,11 @@ int fdtd_setup_view(const fdtd_setup* s, fdtd_setup_v1* v) {
     v->n_sheets = uint32_t(s->sheets.size());
     v->sheets = s->sheets.data();
     v->pec_boundary = S.boundary_pec ? 1 : 0;
+    if (!s->bE_index.empty()) {
+        v->n_bE_rows = uint32_t(s->bE_rows.size() / 3);
+        v->bE_rows = s->bE_rows.data();
+        v->bE_index = s->bE_index.data();
+    }
     v->n_dipoles = uint32_t(s->dipoles.size());
     v->dipoles = s->dipoles.data();
     v->n_tls_regions = uint32_t(s->regions.size());

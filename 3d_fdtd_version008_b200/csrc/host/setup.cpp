@@ -7,11 +7,15 @@
 #include "setup.hpp"
 #include "waveform.hpp"
 
+#include <omp.h>
+
 #include <algorithm>
 #include <cmath>
+#include <cstring>
 #include <numbers>
 #include <sstream>
 #include <stdexcept>
+#include <unordered_map>
 
 namespace fdtd {
 
@@ -799,5 +803,87 @@ SimSetup SimSetup::from_params(const ParamFile& pf, bool bake) {
     }
     return S;
 }
+
+// ================================================================ material rows
+// Each thread numbers the rows of its chunk (a cell equal to the previous one costs one
+// compare, which is nearly every cell: materials are piecewise constant), then the chunk
+// tables are merged in chunk order.
+namespace {
+struct RowKey {
+    uint64_t b[3];
+    bool operator==(const RowKey& o) const { return b[0] == o.b[0] && b[1] == o.b[1] && b[2] == o.b[2]; }
+};
+struct RowHash {
+    size_t operator()(const RowKey& k) const {
+        uint64_t h = k.b[0] * 0x9E3779B97F4A7C15ull;
+        h ^= (k.b[1] + 0x632BE59BD9B4E019ull) * 0xC2B2AE3D27D4EB4Full;
+        h ^= (k.b[2] + 0x165667B19E3779F9ull) * 0x85EBCA77C2B2AE63ull;
+        return size_t(h ^ (h >> 29));
+    }
+};
+
+}  // namespace
+
+bool distinct_rows(const double* const bE[3], size_t N, std::vector<std::array<double, 3>>& rows,
+                    std::vector<uint16_t>& idx) {
+    constexpr size_t kMaxRows = 65535;
+    const int P = std::max(1, omp_get_max_threads());
+    idx.resize(N);
+    std::vector<std::vector<RowKey>> local(P);
+    int over = 0, used = 1;
+#pragma omp parallel num_threads(P) reduction(| : over)
+    {
+        const int t = omp_get_thread_num(), nt = omp_get_num_threads();
+        if (t == 0) used = nt;
+        const size_t lo = N * size_t(t) / size_t(nt), hi = N * size_t(t + 1) / size_t(nt);
+        std::unordered_map<RowKey, uint16_t, RowHash> map;
+        RowKey prev{};
+        unsigned prev_id = ~0u;
+        for (size_t q = lo; q < hi; ++q) {
+            RowKey k;
+            std::memcpy(&k.b[0], bE[0] + q, 8);
+            std::memcpy(&k.b[1], bE[1] + q, 8);
+            std::memcpy(&k.b[2], bE[2] + q, 8);
+            if (prev_id != ~0u && k == prev) { idx[q] = uint16_t(prev_id); continue; }
+            auto it = map.find(k);
+            unsigned id;
+            if (it == map.end()) {
+                if (local[t].size() >= kMaxRows) { over = 1; break; }
+                id = unsigned(local[t].size());
+                map.emplace(k, uint16_t(id));
+                local[t].push_back(k);
+            } else {
+                id = it->second;
+            }
+            idx[q] = uint16_t(id);
+            prev = k;
+            prev_id = id;
+        }
+    }
+    if (over) return false;
+    std::unordered_map<RowKey, uint16_t, RowHash> global;
+    std::vector<std::vector<uint16_t>> remap(P);
+    rows.clear();
+    for (int t = 0; t < P; ++t) {
+        for (const RowKey& k : local[t]) {
+            auto it = global.find(k);
+            if (it == global.end()) {
+                if (rows.size() >= kMaxRows) return false;
+                it = global.emplace(k, uint16_t(rows.size())).first;
+                std::array<double, 3> r;
+                std::memcpy(r.data(), k.b, 24);
+                rows.push_back(r);
+            }
+            remap[t].push_back(it->second);
+        }
+    }
+#pragma omp parallel for schedule(static)
+    for (int t = 0; t < used; ++t) {  // the chunks of the first pass
+        const size_t lo = N * size_t(t) / size_t(used), hi = N * size_t(t + 1) / size_t(used);
+        for (size_t q = lo; q < hi; ++q) idx[q] = remap[t][idx[q]];
+    }
+    return true;
+}
+
 
 }  // namespace fdtd

@@ -14,6 +14,7 @@
 #include <cstddef>
 #include <cstdint>
 #include <map>
+#include <array>
 #include <string>
 #include <vector>
 
@@ -65,6 +66,11 @@ struct GridSpacing {
 };
 
 void build_cumulative_bounds(const std::vector<real>& spacing, std::vector<real>& bounds);
+
+// The distinct (bEx, bEy, bEz) rows of N cells and each cell's row number (idx3 order), rows
+// compared bit for bit; false when there are more than 65535 rows.
+bool distinct_rows(const double* const bE[3], std::size_t N, std::vector<std::array<double, 3>>& rows,
+                   std::vector<uint16_t>& idx);
 
 // ---------------------------------------------------------------- auto mesher
 // Mirrors of MeshOverrideRegion / AutoMeshConfig / AutoMeshStructureBounds

@@ -200,6 +200,10 @@ struct StepArgs {
     long long plane;  // NxP * NyT
     S *Ex, *Ey, *Ez, *Hx, *Hy, *Hz;
     const T *bEx, *bEy, *bEz;
+    // Indexed material (the E kernels' MAT instantiation): per cell a uint16 index into a table
+    // of distinct (bEx, bEy, bEz, 0) rows; bEx/bEy/bEz are then unused.
+    const uint16_t* bidx;
+    const T* btab;
     T bH;
     const T *idx, *idy, *idz;         // 1/dx (padded to NxP), 1/dy, 1/dz
     const T *ik[3];                   // 1/kappa per axis
@@ -265,6 +269,51 @@ __device__ __forceinline__ void xpsi_store(S* p3, S* p4, const StepArgs<S, T>& a
             put(p3[q], x3[e]);
             put(p4[q], x4[e]);
         }
+    }
+}
+
+// One row (bEx, bEy, bEz) of the indexed material's table.
+template <typename T>
+__device__ __forceinline__ void table_row(const T* tab, unsigned id, T& x, T& y, T& z) {
+    if constexpr (sizeof(T) == 4) {
+        const float4 r = __ldg(reinterpret_cast<const float4*>(tab) + id);
+        x = r.x; y = r.y; z = r.z;
+    } else {
+        const double2 r0 = __ldg(reinterpret_cast<const double2*>(tab) + 2 * id);
+        x = r0.x; y = r0.y;
+        z = __ldg(tab + 4 * size_t(id) + 2);
+    }
+}
+
+// The W row numbers at p, packed two per word (W = 4: 8 bytes, W = 2: 4 bytes).
+template <int W>
+struct RowIds {
+    unsigned w[W / 2];
+    __device__ __forceinline__ void load(const uint16_t* p) {
+        if constexpr (W == 4) {
+            const uint2 v = __ldg(reinterpret_cast<const uint2*>(p));
+            w[0] = v.x; w[1] = v.y;
+        } else {
+            w[0] = __ldg(reinterpret_cast<const unsigned*>(p));
+        }
+    }
+    __device__ __forceinline__ unsigned operator[](int e) const { return (w[e >> 1] >> (16 * (e & 1))) & 0xffffu; }
+};
+
+// bEx, bEy, bEz of the W cells at offset c: from the three arrays, or (MAT) the table rows of
+// the ids the caller loaded one plane ahead (so the table reads, which hit L1, do not wait
+// for an HBM load of the same iteration).
+template <bool MAT, typename S, typename T>
+__device__ __forceinline__ void load_bE(const StepArgs<S, T>& a, size_t c, const RowIds<Vec<T>::W>& ids,
+                                        T (&bx)[Vec<T>::W], T (&by)[Vec<T>::W], T (&bz)[Vec<T>::W]) {
+    constexpr int W = Vec<T>::W;
+    if constexpr (MAT) {
+#pragma unroll
+        for (int e = 0; e < W; ++e) table_row(a.btab, ids[e], bx[e], by[e], bz[e]);
+    } else {
+        Vec<T>::ldg(a.bEx + c, bx);
+        Vec<T>::ldg(a.bEy + c, by);
+        Vec<T>::ldg(a.bEz + c, bz);
     }
 }
 
@@ -542,7 +591,7 @@ k_update_H(const StepArgs<S, T> a, const int kchunk, const SweepGeom g) {
 // CG: H is read through L2 only -- the slab-ordered step (k_step_slabs) reads H that other
 // SMs wrote in the same launch, which a stale L1 line could hide.  SH: the step has
 // plane-wave sheets (a separate instantiation keeps the sheet tests out of the common case).
-template <typename S, typename T, bool EDGE, bool CG = false, bool SH = false>
+template <typename S, typename T, bool EDGE, bool CG = false, bool SH = false, bool MAT = false>
 __device__ __forceinline__ void e_column(const StepArgs<S, T>& a, const SweepGeom& g, const ESrc& src, const int j,
                                          const int i0, const bool act, const int kb, const int ke, const int lane) {
     auto ldH = [](const S* p, T (&v)[Vec<T>::W]) {
@@ -575,9 +624,11 @@ __device__ __forceinline__ void e_column(const StepArgs<S, T>& a, const SweepGeo
 
     const size_t row = size_t(j) * a.NxP + i0;
     T hxm[W], hym[W];  // Hx, Hy at k-1
+    RowIds<W> ids{};   // (MAT) material rows of the current plane, loaded one plane ahead
     if (act) {
         ldH(a.Hx + size_t(kb - 1) * a.plane + row, hxm);
         ldH(a.Hy + size_t(kb - 1) * a.plane + row, hym);
+        if constexpr (MAT) ids.load(a.bidx + size_t(kb) * a.plane + row);
     } else {
 #pragma unroll
         for (int e = 0; e < W; ++e) hxm[e] = hym[e] = T(0);
@@ -590,9 +641,10 @@ __device__ __forceinline__ void e_column(const StepArgs<S, T>& a, const SweepGeo
             Fld<S, T>::ld(a.Ex + c, ex);
             Fld<S, T>::ld(a.Ey + c, ey);
             Fld<S, T>::ld(a.Ez + c, ez);
-            Vec<T>::ldg(a.bEx + c, bx);
-            Vec<T>::ldg(a.bEy + c, by);
-            Vec<T>::ldg(a.bEz + c, bz);
+            load_bE<MAT>(a, c, ids, bx, by, bz);
+            if constexpr (MAT) {
+                if (k + 1 < ke) ids.load(a.bidx + c + a.plane);
+            }
             ldH(a.Hx + c, hx);
             ldH(a.Hy + c, hy);
             ldH(a.Hz + c, hz);
@@ -725,7 +777,7 @@ __device__ __forceinline__ void e_column(const StepArgs<S, T>& a, const SweepGeo
     }
 }
 
-template <typename S, typename T, bool CG = false, bool SH = false>
+template <typename S, typename T, bool CG = false, bool SH = false, bool MAT = false>
 __device__ __forceinline__ void update_E_block(const StepArgs<S, T>& a, const int kchunk, const ESrc& src,
                                                const SweepGeom& g, const int bx, const int by, const int bz) {
     constexpr int W = Vec<T>::W;
@@ -738,7 +790,7 @@ __device__ __forceinline__ void update_E_block(const StepArgs<S, T>& a, const in
         const int j = by * kBlockY + threadIdx.y;
         if (j < 1 || j >= a.NyT) return;  // E is updated for j >= 1 only; whole warp
         const int i0 = g.xi0 + (bx * 32 + lane) * W;
-        e_column<S, T, false, CG, SH>(a, g, src, j, i0, i0 < g.xi1, kb, ke, lane);
+        e_column<S, T, false, CG, SH, MAT>(a, g, src, j, i0, i0 < g.xi1, kb, ke, lane);
     } else {
         const int t = threadIdx.y * 32 + lane;
         const int rr = t / g.ne, v = t - rr * g.ne;
@@ -746,14 +798,14 @@ __device__ __forceinline__ void update_E_block(const StepArgs<S, T>& a, const in
         if (rr >= g.er || j < 1 || j >= a.NyT) return;
         const int i0 = v < g.nl ? v * W : g.xi1 + (v - g.nl) * W;
         if (i0 >= a.NxT) return;
-        e_column<S, T, true, CG, SH>(a, g, src, j, i0, true, kb, ke, lane);
+        e_column<S, T, true, CG, SH, MAT>(a, g, src, j, i0, true, kb, ke, lane);
     }
 }
 
-template <typename S, typename T, bool SH = false>
+template <typename S, typename T, bool SH = false, bool MAT = false>
 __global__ void __launch_bounds__(32 * kBlockY, 2)
 k_update_E(const StepArgs<S, T> a, const int kchunk, const ESrc src, const SweepGeom g) {
-    update_E_block<S, T, false, SH>(a, kchunk, src, g, blockIdx.x, blockIdx.y, blockIdx.z);
+    update_E_block<S, T, false, SH, MAT>(a, kchunk, src, g, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 
 // ---------------------------------------------------------------------------------
@@ -779,7 +831,7 @@ __device__ __forceinline__ unsigned ld_acquire(const unsigned* p) {
     return v;
 }
 
-template <typename S, typename T, bool SH = false>
+template <typename S, typename T, bool SH = false, bool MAT = false>
 __global__ void __launch_bounds__(32 * kBlockY, 2)
 k_step_slabs(const StepArgs<S, T> a, const ESrc src, const SweepGeom g, const SlabPlan p, unsigned* ctr,
              unsigned* status_w) {
@@ -820,7 +872,7 @@ k_step_slabs(const StepArgs<S, T> a, const ESrc src, const SweepGeom g, const Sl
                 if (tid == 0) atomicOr(status_w, kStatusTimeout);
                 return;
             }
-            update_E_block<S, T, true, SH>(a, p.P, src, g, r % p.gxE, r / p.gxE, slab);
+            update_E_block<S, T, true, SH, MAT>(a, p.P, src, g, r % p.gxE, r / p.gxE, slab);
             __syncthreads();
         }
     }

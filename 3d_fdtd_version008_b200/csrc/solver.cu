@@ -18,6 +18,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <array>
 #include <condition_variable>
 #include <map>
 #include <mutex>
@@ -52,6 +53,35 @@ __global__ void k_from_idx3(const double* __restrict__ src, D* __restrict__ dst,
     for (int r = threadIdx.y; r < 32; r += blockDim.y) {
         const int k = k0 + r, i = i0 + threadIdx.x;
         if (i < NxT && k < NzT) dst[(size_t(k) * NyT + j) * NxP + i] = from_d<D>(tile[threadIdx.x][r] * scale);
+    }
+}
+
+// The per-cell material index, idx3 (uint16) -> device layout, 32x32 tiles over (k, i).
+__global__ void k_index_from_idx3(const uint16_t* __restrict__ src, uint16_t* __restrict__ dst, int NxT, int NyT,
+                                  int NzT, int NxP) {
+    __shared__ uint16_t tile[32][33];
+    const int j = blockIdx.z;
+    const int k0 = blockIdx.x * 32, i0 = blockIdx.y * 32;
+    for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+        const int i = i0 + r, k = k0 + threadIdx.x;
+        tile[r][threadIdx.x] = (i < NxT && k < NzT) ? src[(size_t(i) * NyT + j) * NzT + k] : uint16_t(0);
+    }
+    __syncthreads();
+    for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+        const int k = k0 + r, i = i0 + threadIdx.x;
+        if (i < NxT && k < NzT) dst[(size_t(k) * NyT + j) * NxP + i] = tile[threadIdx.x][r];
+    }
+}
+
+// Full bE arrays from the index and the table (for the fused path, which streams them by TMA).
+template <typename T>
+__global__ void k_expand_material(const uint16_t* __restrict__ idx, const T* __restrict__ tab, size_t n, T* bx, T* by,
+                                  T* bz) {
+    for (size_t q = blockIdx.x * size_t(blockDim.x) + threadIdx.x; q < n; q += size_t(gridDim.x) * blockDim.x) {
+        const size_t r = 4 * size_t(idx[q]);
+        bx[q] = tab[r];
+        by[q] = tab[r + 1];
+        bz[q] = tab[r + 2];
     }
 }
 
@@ -443,13 +473,13 @@ __global__ void __launch_bounds__(32 * kBlockY, 2) k_update_H_multi(const int4* 
     update_H_block<float, float>(c_bargs[e.x], c_bsolve[e.x].kchunkH, c_bsolve[e.x].g, e.y, e.z, e.w);
 }
 
-// SH: the blocks of solves with plane-wave sheets, listed after all others in the table, so a
-// solve runs the same code whatever else is resident.
-template <bool SH>
+// SH / MAT: the blocks of solves with plane-wave sheets / an indexed material; the table lists
+// the four kinds in separate runs, so a solve runs the same code whatever else is resident.
+template <bool SH, bool MAT>
 __global__ void __launch_bounds__(32 * kBlockY, 2) k_update_E_multi(const int4* __restrict__ tab) {
     const int4 e = tab[blockIdx.x];
-    update_E_block<float, float, false, SH>(c_bargs[e.x], c_bsolve[e.x].kchunkE, c_btick[e.x].src, c_bsolve[e.x].g,
-                                            e.y, e.z, e.w);
+    update_E_block<float, float, false, SH, MAT>(c_bargs[e.x], c_bsolve[e.x].kchunkE, c_btick[e.x].src,
+                                                 c_bsolve[e.x].g, e.y, e.z, e.w);
 }
 
 // one block per solve
@@ -517,7 +547,7 @@ public:
     virtual void attach_outputs(const fdtd::SimSetup& setup, const std::string& root) = 0;
     virtual void flush_outputs() = 0;
     virtual void close_outputs() = 0;
-    uint64_t steps = 0, launches = 0, dev_bytes = 0;
+    uint64_t steps = 0, launches = 0, dev_bytes = 0, material_rows = 0;
     int device = 0;
 };
 
@@ -677,6 +707,7 @@ private:
     double* d_stage_ = nullptr;
     bool has_gain_ = false;
     bool pec_ = false;  // PECBoundary: zero E on the outer faces after every E update
+    size_t mat_rows_ = 0;  // > 0: indexed material (a_.bidx / a_.btab)
     // event timing: ev_[0..3] bracket H, E and the auxiliary kernels of one step
     // kernel path 0: k_step_fused (fields and psi_H double-buffered, cur_ = buffer holding
     // the latest state); path 1 (default, measured faster on B200): k_update_H +
@@ -763,12 +794,55 @@ Solver<S, T>::Solver(const fdtd_setup_v1& s, int dev) {
         if (s.bH[c] && !all_equal(s.bH[c], bH)) throw Failure(FDTD_ERR_UNSUPPORTED, "non-uniform bH (mu_r != 1) is not supported");
     }
     a.bH = T(bH * (sE_ / sH_));
-    T* be[3];
-    for (int c = 0; c < 3; ++c) {
-        be[c] = alloc<T>(nflat_);
-        to_device(s.bE[c], be[c], sH_ / sE_);
+    // Material: a uint16 row index per cell and a table of the distinct rows when the solve
+    // has at most 65535 of them (2 bytes per cell per step instead of 3 words), else the
+    // three arrays.  FDTD_B200_MATERIAL_INDEX=0 forces the arrays.
+    // The setup view may bring the rows and the index (fdtd_setup_parse makes them); else they
+    // are made here from the arrays.
+    std::vector<std::array<double, 3>> rows;
+    std::vector<uint16_t> rid;
+    const char* mi = std::getenv("FDTD_B200_MATERIAL_INDEX");
+    const bool want_index = !(mi && std::string(mi) == "0");
+    bool have_index = false;
+    if (want_index && s.bE_index && s.bE_rows && s.n_bE_rows > 0 && s.n_bE_rows <= 65535) {
+        rows.resize(s.n_bE_rows);
+        for (uint32_t r = 0; r < s.n_bE_rows; ++r)
+            for (int c = 0; c < 3; ++c) rows[r][c] = s.bE_rows[3 * size_t(r) + c];
+        rid.resize((N + 3) / 4 * 4, 0);
+        std::memcpy(rid.data(), s.bE_index, N * sizeof(uint16_t));
+        uint16_t bad = 0;
+#pragma omp parallel for reduction(| : bad) schedule(static)
+        for (long long q = 0; q < (long long)N; ++q) bad |= uint16_t(rid[q] >= s.n_bE_rows);
+        if (bad) throw Failure(FDTD_ERR_INVALID, "bE_index holds a row number >= n_bE_rows");
+        have_index = true;
+    } else if (want_index) {
+        have_index = fdtd::distinct_rows(s.bE, N, rows, rid);
     }
-    a.bEx = be[0]; a.bEy = be[1]; a.bEz = be[2];
+    if (have_index) {
+        std::vector<T> tab(4 * rows.size(), T(0));
+        for (size_t r = 0; r < rows.size(); ++r)
+            for (int c = 0; c < 3; ++c) tab[4 * r + c] = T(rows[r][c] * (sH_ / sE_));
+        a.btab = upload(tab);
+        uint16_t* d_idx = alloc<uint16_t>(nflat_);
+        rid.resize((N + 3) / 4 * 4, 0);  // whole doubles for the staged copy
+        double* sbuf = staging();
+        h2d(reinterpret_cast<const double*>(rid.data()), sbuf, rid.size() / 4);
+        dim3 g((NzT_ + 31) / 32, (NxT_ + 31) / 32, NyT_), b(32, 8);
+        k_index_from_idx3<<<g, b, 0, st_>>>(reinterpret_cast<const uint16_t*>(sbuf), d_idx, NxT_, NyT_, NzT_, NxP_);
+        ++launches;
+        ck(cudaGetLastError(), "k_index_from_idx3");
+        ck(cudaStreamSynchronize(st_), "material index upload");
+        a.bidx = d_idx;
+        mat_rows_ = rows.size();
+        material_rows = rows.size();
+    } else {
+        T* be[3];
+        for (int c = 0; c < 3; ++c) {
+            be[c] = alloc<T>(nflat_);
+            to_device(s.bE[c], be[c], sH_ / sE_);
+        }
+        a.bEx = be[0]; a.bEy = be[1]; a.bEz = be[2];
+    }
 
     // 1-D arrays
     std::vector<T> idx(NxP_, T(0)), idy(NyT_), idz(NzT_);
@@ -973,9 +1047,9 @@ void Solver<S, T>::setup_slabs() {
     d_ctr_ = alloc<unsigned>(size_t(plan_.nslab) + 1);
     int sms = 148, per = 0;
     ck(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device), "cudaDeviceGetAttribute");
-    ck(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, sheets_.empty() ? k_step_slabs<S, T, false>
-                                                                          : k_step_slabs<S, T, true>,
-                                                    32 * kBlockY, 0),
+    const auto slabs_fn = sheets_.empty() ? (a_.bidx ? k_step_slabs<S, T, false, true> : k_step_slabs<S, T, false, false>)
+                                          : (a_.bidx ? k_step_slabs<S, T, true, true> : k_step_slabs<S, T, true, false>);
+    ck(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, slabs_fn, 32 * kBlockY, 0),
        "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
     if (per < 1) throw Failure(FDTD_ERR_CUDA, "slab-ordered step kernel does not fit on an SM");
     gridS_ = dim3(unsigned(sms * per));
@@ -1007,6 +1081,14 @@ PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
 template <typename S, typename T>
 void Solver<S, T>::ensure_fused() {
     if (fused_ready_) return;
+    if (a_.bidx && !a_.bEx) {  // the fused path streams the three arrays
+        T* be[3];
+        for (int c = 0; c < 3; ++c) be[c] = alloc<T>(nflat_, false);
+        k_expand_material<T><<<148 * 8, 256, 0, st_>>>(a_.bidx, a_.btab, nflat_, be[0], be[1], be[2]);
+        ++launches;
+        ck(cudaGetLastError(), "k_expand_material");
+        a_.bEx = be[0]; a_.bEy = be[1]; a_.bEz = be[2];
+    }
     for (int c = 0; c < 6; ++c) {
         fld_[1][c] = alloc<S>(nflat_, false);
         ck(cudaMemcpyAsync(fld_[1][c], fld_[0][c], nflat_ * sizeof(S), cudaMemcpyDeviceToDevice, st_), "field copy");
@@ -1336,15 +1418,17 @@ void Solver<S, T>::run(uint64_t n) {
         } else if (path_ == 2) {
             ck(cudaMemsetAsync(d_ctr_, 0, (size_t(plan_.nslab) + 1) * sizeof(unsigned), st_), "cudaMemsetAsync");
             if (per_kernel) ck(cudaEventRecord(ev_[0], st_), "cudaEventRecord");
-            if (src.ns) k_step_slabs<S, T, true><<<gridS_, blk, 0, st_>>>(a_, src, geom_, plan_, d_ctr_, d_status_);
-            else k_step_slabs<S, T><<<gridS_, blk, 0, st_>>>(a_, src, geom_, plan_, d_ctr_, d_status_);
+            const auto slabs = src.ns ? (a_.bidx ? k_step_slabs<S, T, true, true> : k_step_slabs<S, T, true, false>)
+                                      : (a_.bidx ? k_step_slabs<S, T, false, true> : k_step_slabs<S, T, false, false>);
+            slabs<<<gridS_, blk, 0, st_>>>(a_, src, geom_, plan_, d_ctr_, d_status_);
             if (per_kernel) ck(cudaEventRecord(ev_[1], st_), "cudaEventRecord");
             launches += 1;
         } else {
             k_update_H<S, T><<<gridH_, blk, 0, st_>>>(a_, kchunkH_, geom_);
             if (per_kernel) ck(cudaEventRecord(ev_[1], st_), "cudaEventRecord");
-            if (src.ns) k_update_E<S, T, true><<<gridE_, blk, 0, st_>>>(a_, kchunkE_, src, geom_);
-            else k_update_E<S, T><<<gridE_, blk, 0, st_>>>(a_, kchunkE_, src, geom_);
+            const auto upd = src.ns ? (a_.bidx ? k_update_E<S, T, true, true> : k_update_E<S, T, true, false>)
+                                    : (a_.bidx ? k_update_E<S, T, false, true> : k_update_E<S, T, false, false>);
+            upd<<<gridE_, blk, 0, st_>>>(a_, kchunkE_, src, geom_);
             launches += 2;
         }
         if (pec_) {
@@ -1798,7 +1882,7 @@ private:
         std::vector<StepArgs<float>> args(n);
         std::vector<BatchSolve> bs(n);
         std::vector<int4> tab;
-        nH_ = nE_ = nE0_ = 0;
+        nH_ = nE_ = 0;
         for (int r = 0; r < n; ++r) {
             Solver<float, float>& v = *jobs_.at(res_[r]).sol;
             args[r] = v.a_;
@@ -1826,16 +1910,17 @@ private:
                     for (unsigned x = 0; x < g.x; ++x) tab.push_back(make_int4(r, int(x), int(y), int(z)));
         }
         nH_ = tab.size();
-        for (int pass = 0; pass < 2; ++pass) {  // E blocks of solves without sheets, then with
+        nEk_[0] = 0;
+        for (int kind = 0; kind < 4; ++kind) {  // E blocks by kind: 2 * has sheets + indexed material
             for (int r = 0; r < n; ++r) {
                 const Solver<float, float>& v = *jobs_.at(res_[r]).sol;
-                if (v.sheets_.empty() == (pass == 1)) continue;
+                if (2 * int(!v.sheets_.empty()) + int(v.a_.bidx != nullptr) != kind) continue;
                 const dim3 g = v.gridE_;
                 for (unsigned z = 0; z < g.z; ++z)
                     for (unsigned y = 0; y < g.y; ++y)
                         for (unsigned x = 0; x < g.x; ++x) tab.push_back(make_int4(r, int(x), int(y), int(z)));
             }
-            if (pass == 0) nE0_ = tab.size() - nH_;
+            nEk_[kind + 1] = tab.size() - nH_;
         }
         nE_ = tab.size() - nH_;
         ck(cudaStreamSynchronize(st_), "rebuild");  // no step may read the old tables
@@ -1876,8 +1961,11 @@ private:
         ck(cudaEventRecord(ring_ev_[slot], st_), "cudaEventRecord");
         const dim3 blk(32, kBlockY);
         k_update_H_multi<<<unsigned(nH_), blk, 0, st_>>>(d_tab_);
-        if (nE0_) k_update_E_multi<false><<<unsigned(nE0_), blk, 0, st_>>>(d_tab_ + nH_);
-        if (nE_ > nE0_) k_update_E_multi<true><<<unsigned(nE_ - nE0_), blk, 0, st_>>>(d_tab_ + nH_ + nE0_);
+        static constexpr void (*kinds[4])(const int4*) = {k_update_E_multi<false, false>, k_update_E_multi<false, true>,
+                                                          k_update_E_multi<true, false>, k_update_E_multi<true, true>};
+        for (int q = 0; q < 4; ++q)
+            if (nEk_[q + 1] > nEk_[q])
+                kinds[q]<<<unsigned(nEk_[q + 1] - nEk_[q]), blk, 0, st_>>>(d_tab_ + nH_ + nEk_[q]);
         k_probe_multi<<<n, 128, 0, st_>>>();
         if (monitor) {
             k_monitor_reduce_multi<<<n * kMonBlocks, 256, 0, st_>>>();
@@ -1930,7 +2018,8 @@ private:
     std::deque<uint64_t> queue_;
     std::vector<uint64_t> res_;  // resident tickets in slot order
     int4* d_tab_ = nullptr;
-    size_t tab_cap_ = 0, nH_ = 0, nE_ = 0, nE0_ = 0;
+    size_t tab_cap_ = 0, nH_ = 0, nE_ = 0;
+    size_t nEk_[5] = {};  // E blocks of kind q are table entries [nEk_[q], nEk_[q + 1]) after the H ones
     BatchTick* ticks_ = nullptr;
     cudaEvent_t ring_ev_[kRing] = {};
     uint64_t ring_ = 0;
@@ -2019,6 +2108,7 @@ int fdtd_get_dft(fdtd_handle* h, uint32_t p, double* re, double* im) { if (!h ||
 int fdtd_get_diagnostics(fdtd_handle* h, fdtd_diagnostics_v1* d) { if (!h || !d) return FDTD_ERR_INVALID; return guarded(h, [&] { h->s->diagnostics(d); }); }
 int fdtd_device_bytes(const fdtd_handle* h, uint64_t* b) { if (!h || !b) return FDTD_ERR_INVALID; *b = h->s->dev_bytes; return FDTD_OK; }
 int fdtd_kernel_launches(const fdtd_handle* h, uint64_t* n) { if (!h || !n) return FDTD_ERR_INVALID; *n = h->s->launches; return FDTD_OK; }
+int fdtd_material_rows(const fdtd_handle* h, uint64_t* rows) { if (!h || !rows) return FDTD_ERR_INVALID; *rows = h->s->material_rows; return FDTD_OK; }
 int fdtd_set_timing(fdtd_handle* h, int mode) { if (!h) return FDTD_ERR_INVALID; return guarded(h, [&] { h->s->set_timing(mode); }); }
 int fdtd_get_timing(fdtd_handle* h, fdtd_timing_v1* t) { if (!h || !t) return FDTD_ERR_INVALID; return guarded(h, [&] { h->s->timing(t); }); }
 int fdtd_set_kernel_path(fdtd_handle* h, int path) { if (!h) return FDTD_ERR_INVALID; return guarded(h, [&] { h->s->set_path(path); }); }

@@ -119,22 +119,24 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def algorithmic_bytes(setup, word: int, coef_word: int = 0):
+def algorithmic_bytes(setup, word: int, coef_word: int = 0, material_bytes: int = 0):
     """Compulsory bytes per step of the two-sweep algorithm: fields and psi stored in `word`
     bytes, bE and gain state in `coef_word` bytes (default: the same).
 
     H sweep: read E(3) H(3), write H(3) = 9 field words/cell; E sweep: read H(3) E(3), write
-    E(3) = 9 field words + bE(3) coefficient words; + 2 field words per active CPML psi (4 per
-    axis, 2 per sweep) in that axis' slab; + gain cells: read P^n, P^{n-1}, Nu, Ng and write
-    P^{n+1}, Nu, Ng = 7 coefficient words."""
+    E(3) = 9 field words + the material (bE: 3 coefficient words per cell, or `material_bytes`
+    per cell when the stepper holds it as a row index -- the small row table stays on chip);
+    + 2 field words per active CPML psi (4 per axis, 2 per sweep) in that axis' slab; + gain
+    cells: read P^n, P^{n-1}, Nu, Ng and write P^{n+1}, Nu, Ng = 7 coefficient words."""
     cw = coef_word or word
+    mat = material_bytes or 3 * cw
     NxT, NyT, NzT = setup.shape
     npml = int(setup.view.npml)
     cells = NxT * NyT * NzT
     slab = sum(2 * npml * (cells // n) for n in (NxT, NyT, NzT))  # cells inside each axis' slab, summed
     gain = int((setup.array("tls_region_map") >= 0).sum()) if setup.view.n_tls_regions else 0
     h = 9 * word * cells + 2 * 2 * word * slab
-    e = 9 * word * cells + 3 * cw * cells + 2 * 2 * word * slab + 7 * cw * gain
+    e = 9 * word * cells + mat * cells + 2 * 2 * word * slab + 7 * cw * gain
     return {"cells": cells, "h_bytes": h, "e_bytes": e, "step_bytes": h + e,
             "per_cell": (h + e) / cells, "slab_cells": slab, "gain_cells": gain}
 
@@ -423,10 +425,9 @@ def main():
     coef_word = 8 if prec == PKG.PREC_FP64 else 4
     setup = PKG.Setup.from_file(PKG.config_path(cfg))
     cells = setup.shape[0] * setup.shape[1] * setup.shape[2]
-    alg = algorithmic_bytes(setup, word, coef_word)
-
     # ---------------------------------------------------------------- device-resident value
     sol = PKG.Solver(setup, device=local, precision=prec)
+    alg = algorithmic_bytes(setup, word, coef_word, 2 if sol.material_rows else 0)
     for _ in range(W):
         sol.run(S)
     sol.synchronize()
@@ -474,9 +475,11 @@ def main():
     e2e = None
     if not args.no_e2e:
         import numpy as np
-        # bytes fdtd_create copies host -> device: bE (FP64 idx3, transposed on the device),
-        # 1-D spacing / CPML arrays, gain box (counted before the timed region)
-        h2d = 3 * cells * 8 + sum(8 * n for n in setup.shape) * 16
+        # bytes fdtd_create copies host -> device: the material (the setup's row index, 2 bytes
+        # per cell, and its row table -- or bE as three FP64 idx3 arrays), 1-D spacing / CPML
+        # arrays, gain box (counted before the timed region)
+        nrows = int(setup.view.n_bE_rows)
+        h2d = (2 * cells + 24 * nrows if nrows else 3 * cells * 8) + sum(8 * n for n in setup.shape) * 16
         if setup.view.n_tls_regions:
             m = setup.array("tls_region_map").reshape(setup.shape) >= 0
             box = int(np.prod([np.ptp(np.nonzero(m.any(axis=tuple(x for x in range(3) if x != ax)))[0]) + 1

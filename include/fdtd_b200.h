@@ -164,7 +164,14 @@ typedef struct fdtd_setup_v1 {
     /* 1: PECBoundary (src/boundary.hpp:51-79): npml must be 0, and after every E update
      * Ex, Ey, Ez are zeroed on the six outer faces.  0: CPML. */
     uint32_t pec_boundary;
-    uint32_t reserved1;
+    /* Optional compact material: n_bE_rows distinct (bEx, bEy, bEz) rows (bE_rows, row-major,
+     * FP64) and each cell's row number (bE_index, idx3).  When given (n_bE_rows <= 65535) the
+     * stepper uploads these instead of reading bE[0..2]; fdtd_setup_view fills them.  NULL / 0:
+     * the stepper derives them from bE[0..2] itself.  No counterpart in the reference, whose
+     * material is the three arrays. */
+    uint32_t n_bE_rows;
+    const double *bE_rows;
+    const uint16_t *bE_index;
 } fdtd_setup_v1;
 
 /* Diagnostics of the most recent monitor step, FP64 device reductions
@@ -248,6 +255,10 @@ int fdtd_get_diagnostics(fdtd_handle *h, fdtd_diagnostics_v1 *out);
 int fdtd_device_bytes(const fdtd_handle *h, uint64_t *bytes);
 /* Number of CUDA kernel launches issued by the handle since creation. */
 int fdtd_kernel_launches(const fdtd_handle *h, uint64_t *n);
+/* How the handle holds bE: *rows = the number of distinct (bEx, bEy, bEz) rows when it keeps a
+ * 2-byte row index per cell and a table of the rows (at most 65535 rows), 0 when it keeps the
+ * three arrays.  Results are the same either way. */
+int fdtd_material_rows(const fdtd_handle *h, uint64_t *rows);
 /* Select FDTD_TIMING_OFF / _RUN / _KERNELS; any call resets the totals. */
 int fdtd_set_timing(fdtd_handle *h, int mode);
 int fdtd_get_timing(fdtd_handle *h, fdtd_timing_v1 *out);

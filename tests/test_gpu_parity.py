@@ -428,3 +428,26 @@ def test_16bit_storage_rejects_fused_path(pkg):
     sol = pkg.Solver(s, precision=2)
     with pytest.raises(pkg.FdtdError):
         sol.set_kernel_path(0)
+
+
+@pytest.mark.parametrize("precision,path", [(0, 1), (1, 1), (3, 1), (0, 2), (0, 0), (1, 0)])
+def test_material_index_matches_arrays(pkg, precision, path, monkeypatch):
+    """The indexed material (a uint16 row number per cell and a table of distinct rows), as the
+    setup view brings it or as the stepper derives it from the arrays, gives bit-identical
+    fields to the three bE arrays: the same values reach the same arithmetic."""
+    s = pkg.Setup.from_file(GOLDEN / "cases" / "step_g2_planewave.params")
+    assert s.view.n_bE_rows > 0
+    bare = pkg.SetupV1.from_buffer_copy(s.view)
+    bare.n_bE_rows = 0
+    bare.bE_rows = None
+    bare.bE_index = None
+    out = []
+    for mode, view in (("1", None), ("1", bare), ("0", None)):
+        monkeypatch.setenv("FDTD_B200_MATERIAL_INDEX", mode)
+        sol = pkg.Solver(s, precision=precision, kernel_path=path, view=view)
+        assert (sol.material_rows == s.view.n_bE_rows) == (mode == "1")
+        sol.run(45)
+        out.append(fields(sol))
+        sol.close()
+    for c in FIELDS:
+        assert np.array_equal(out[0][c], out[2][c]) and np.array_equal(out[1][c], out[2][c]), c
