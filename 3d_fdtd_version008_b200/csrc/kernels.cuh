@@ -317,6 +317,32 @@ __device__ __forceinline__ void load_bE(const StepArgs<S, T>& a, size_t c, const
     }
 }
 
+// ---------------------------------------------------------------------------------
+// Asynchronous copies into shared memory (cp.async): the loads of the next plane are in
+// flight while the current one is computed, without registers held for them.
+// L1: keep the line in L1 (data another warp of the block reads too: H, whose row j is the
+// next warp's row j-1); else 16-byte copies go through L2 only.
+template <int BYTES, bool L1 = true>
+__device__ __forceinline__ void cp_async(void* smem, const void* g) {
+    const unsigned s = unsigned(__cvta_generic_to_shared(smem));
+    if constexpr (BYTES == 16 && !L1) asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(s), "l"(g) : "memory");
+    else asm volatile("cp.async.ca.shared.global [%0], [%1], %2;" ::"r"(s), "l"(g), "n"(BYTES) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+
+// Shared-memory staging of the E sweep's interior columns: two planes (stages) of kSlots
+// 16-byte slots per thread, slot-major so that a warp's slots are consecutive.  Slots: 0-2 E,
+// 3-5 H, 6 Hz(j-1), 7 Hx(j-1), 8 the material (row ids or bEx), 9-10 bEy/bEz (arrays only),
+// last: Hz and Hy at i0-1 for the warp's first lane.
+template <bool MAT>
+struct EPipe {
+    static constexpr int kSlots = MAT ? 10 : 12;
+    static constexpr int kX = kSlots - 1;
+    static constexpr size_t bytes() { return size_t(2) * kSlots * (32 * kBlockY) * 16; }
+};
+
 // True when a point source or (SH) a plane-wave sheet touches one of the W cells (i0.., j, k).
 template <bool SH>
 __device__ __forceinline__ bool src_in_vector(const ESrc& src, int i0, int j, int k, int W) {
@@ -432,7 +458,14 @@ struct SweepGeom {
 // 1/dz, the CPML psi of the vector) is issued before the first use of any of them, so a
 // vector costs one memory round trip per plane whatever slab it lies in.  EDGE columns
 // read the x-neighbour from memory (lanes hold other rows); interior columns shuffle it.
-template <typename S, typename T, bool EDGE>
+// Shared-memory staging of the H sweep's interior columns (as EPipe): slots 0-1 Ex, Ey at k+1,
+// 2 Ez, 3 Ex(j+1), 4 Ez(j+1), 5-7 H, 8 Ey and Ez at i0+W for the lanes that load it.
+struct HPipe {
+    static constexpr int kSlots = 9;
+    static constexpr size_t bytes() { return size_t(2) * kSlots * (32 * kBlockY) * 16; }
+};
+
+template <typename S, typename T, bool EDGE, bool PIPE = false>
 __device__ __forceinline__ void h_column(const StepArgs<S, T>& a, const SweepGeom& g, const int j, const int i0,
                                          const bool act, const int kb, const int ke, const int lane) {
     constexpr int W = Vec<T>::W;
@@ -463,10 +496,58 @@ __device__ __forceinline__ void h_column(const StepArgs<S, T>& a, const SweepGeo
         for (int e = 0; e < W; ++e) ex0[e] = ey0[e] = T(0);
     }
 
+    // PIPE (interior columns of k_update_H): this thread's planes come from shared memory,
+    // filled by cp.async one plane ahead.
+    extern __shared__ uint4 pipe_smem[];
+    constexpr int NT = 32 * kBlockY, NV = HPipe::kSlots;
+    constexpr int VB = W * int(sizeof(S));
+    constexpr int NB = sizeof(S) < 4 ? 4 : int(sizeof(S));
+    const int tid = threadIdx.y * 32 + threadIdx.x;
+    const bool xn = nload && i0 + W < a.NxT;
+    auto issue = [&](int kk, int stg) {
+        const size_t cc = size_t(kk) * a.plane + row;
+        uint4* b = pipe_smem + size_t(stg) * NV * NT + tid;
+        cp_async<VB>(b + 0 * NT, a.Ex + cc + a.plane);
+        cp_async<VB>(b + 1 * NT, a.Ey + cc + a.plane);
+        cp_async<VB>(b + 2 * NT, a.Ez + cc);
+        cp_async<VB>(b + 3 * NT, a.Ex + cc + a.NxP);
+        cp_async<VB>(b + 4 * NT, a.Ez + cc + a.NxP);
+        cp_async<VB, false>(b + 5 * NT, a.Hx + cc);
+        cp_async<VB, false>(b + 6 * NT, a.Hy + cc);
+        cp_async<VB, false>(b + 7 * NT, a.Hz + cc);
+        if (xn) {
+            cp_async<NB>(b + 8 * NT, a.Ey + cc + W);
+            cp_async<NB>(reinterpret_cast<char*>(b + 8 * NT) + 8, a.Ez + cc + W);
+        }
+    };
+    if constexpr (PIPE) {
+        if (act) issue(kb, 0);
+        cp_async_commit();
+    }
+
     for (int k = kb; k < ke; ++k) {
         const size_t c = size_t(k) * a.plane + row;
         T ex1[W], ey1[W], ez[W], exj[W], ezj[W], hx[W], hy[W], hz[W];
-        if (act) {
+        T eye = T(0), eze = T(0);
+        if (PIPE && act) {
+            if (k + 1 < ke) issue(k + 1, (k + 1 - kb) & 1);
+            cp_async_commit();
+            cp_async_wait<1>();
+            const uint4* b = pipe_smem + size_t((k - kb) & 1) * NV * NT + tid;
+            Fld<S, T>::ld(reinterpret_cast<const S*>(b + 0 * NT), ex1);
+            Fld<S, T>::ld(reinterpret_cast<const S*>(b + 1 * NT), ey1);
+            Fld<S, T>::ld(reinterpret_cast<const S*>(b + 2 * NT), ez);
+            Fld<S, T>::ld(reinterpret_cast<const S*>(b + 3 * NT), exj);
+            Fld<S, T>::ld(reinterpret_cast<const S*>(b + 4 * NT), ezj);
+            Fld<S, T>::ld(reinterpret_cast<const S*>(b + 5 * NT), hx);
+            Fld<S, T>::ld(reinterpret_cast<const S*>(b + 6 * NT), hy);
+            Fld<S, T>::ld(reinterpret_cast<const S*>(b + 7 * NT), hz);
+            if (xn) {
+                const S* xs = reinterpret_cast<const S*>(b + 8 * NT);
+                eye = T(to_c(xs[0]));
+                eze = T(to_c(reinterpret_cast<const S*>(reinterpret_cast<const char*>(xs) + 8)[0]));
+            }
+        } else if (act) {
             Fld<S, T>::ldg(a.Ex + c + a.plane, ex1);
             Fld<S, T>::ldg(a.Ey + c + a.plane, ey1);
             Fld<S, T>::ldg(a.Ez + c, ez);
@@ -479,8 +560,7 @@ __device__ __forceinline__ void h_column(const StepArgs<S, T>& a, const SweepGeo
 #pragma unroll
             for (int e = 0; e < W; ++e) ex1[e] = ey1[e] = ez[e] = exj[e] = ezj[e] = hx[e] = hy[e] = hz[e] = T(0);
         }
-        T eye = T(0), eze = T(0);
-        if (nload && act && i0 + W < a.NxT) { eye = to_c(a.Ey[c + W]); eze = to_c(a.Ez[c + W]); }
+        if (!PIPE && xn && act) { eye = to_c(a.Ey[c + W]); eze = to_c(a.Ez[c + W]); }
         const T idz = __ldg(a.idz + k);
         const bool zpml = in_pml(k, a.NzT, np);
         T zb = 1, zc = 0, zik = 1;
@@ -555,7 +635,7 @@ __device__ __forceinline__ void h_column(const StepArgs<S, T>& a, const SweepGeo
 }
 
 // One block of the H sweep: block (bx, by, bz) of the solve's launch grid.
-template <typename S, typename T>
+template <typename S, typename T, bool PIPE = false>
 __device__ __forceinline__ void update_H_block(const StepArgs<S, T>& a, const int kchunk, const SweepGeom& g,
                                                const int bx, const int by, const int bz) {
     constexpr int W = Vec<T>::W;
@@ -568,7 +648,7 @@ __device__ __forceinline__ void update_H_block(const StepArgs<S, T>& a, const in
         const int j = by * kBlockY + threadIdx.y;
         if (j >= a.NyT - 1) return;  // whole warp: a warp is one row
         const int i0 = g.xi0 + (bx * 32 + lane) * W;
-        h_column<S, T, false>(a, g, j, i0, i0 < g.xi1, kb, ke, lane);
+        h_column<S, T, false, PIPE>(a, g, j, i0, i0 < g.xi1, kb, ke, lane);
     } else {
         const int t = threadIdx.y * 32 + lane;
         const int rr = t / g.ne, v = t - rr * g.ne;
@@ -581,17 +661,18 @@ __device__ __forceinline__ void update_H_block(const StepArgs<S, T>& a, const in
 }
 
 // Two resident blocks per SM (at most 128 registers; a third block would spill).
-template <typename S, typename T>
+// PIPE: interior columns stage their planes in shared memory (HPipe::bytes() dynamic).
+template <typename S, typename T, bool PIPE = false>
 __global__ void __launch_bounds__(32 * kBlockY, 2)
 k_update_H(const StepArgs<S, T> a, const int kchunk, const SweepGeom g) {
-    update_H_block<S, T>(a, kchunk, g, blockIdx.x, blockIdx.y, blockIdx.z);
+    update_H_block<S, T, PIPE>(a, kchunk, g, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 
 // ---------------------------------------------------------------------------------
 // CG: H is read through L2 only -- the slab-ordered step (k_step_slabs) reads H that other
 // SMs wrote in the same launch, which a stale L1 line could hide.  SH: the step has
 // plane-wave sheets (a separate instantiation keeps the sheet tests out of the common case).
-template <typename S, typename T, bool EDGE, bool CG = false, bool SH = false, bool MAT = false>
+template <typename S, typename T, bool EDGE, bool CG = false, bool SH = false, bool MAT = false, bool PIPE = false>
 __device__ __forceinline__ void e_column(const StepArgs<S, T>& a, const SweepGeom& g, const ESrc& src, const int j,
                                          const int i0, const bool act, const int kb, const int ke, const int lane) {
     auto ldH = [](const S* p, T (&v)[Vec<T>::W]) {
@@ -628,16 +709,84 @@ __device__ __forceinline__ void e_column(const StepArgs<S, T>& a, const SweepGeo
     if (act) {
         ldH(a.Hx + size_t(kb - 1) * a.plane + row, hxm);
         ldH(a.Hy + size_t(kb - 1) * a.plane + row, hym);
-        if constexpr (MAT) ids.load(a.bidx + size_t(kb) * a.plane + row);
+        if constexpr (MAT && !PIPE) ids.load(a.bidx + size_t(kb) * a.plane + row);
     } else {
 #pragma unroll
         for (int e = 0; e < W; ++e) hxm[e] = hym[e] = T(0);
     }
 
+    // PIPE (interior columns of k_update_E): the plane's vectors come from this thread's
+    // shared-memory slots, filled by cp.async one plane ahead.
+    extern __shared__ uint4 pipe_smem[];
+    constexpr int NT = 32 * kBlockY, NV = EPipe<MAT>::kSlots, XS = EPipe<MAT>::kX;
+    constexpr int VB = W * int(sizeof(S));                 // bytes of one field vector
+    constexpr int NB = sizeof(S) < 4 ? 4 : int(sizeof(S));  // x-neighbour copy (>= 4 bytes)
+    constexpr int NE = NB / int(sizeof(S));                 // elements in it; the neighbour is the last
+    const int tid = threadIdx.y * 32 + threadIdx.x;
+    auto issue = [&](int kk, int stg) {
+        const size_t cc = size_t(kk) * a.plane + row;
+        uint4* b = pipe_smem + size_t(stg) * NV * NT + tid;
+        cp_async<VB, false>(b + 0 * NT, a.Ex + cc);
+        cp_async<VB, false>(b + 1 * NT, a.Ey + cc);
+        cp_async<VB, false>(b + 2 * NT, a.Ez + cc);
+        cp_async<VB>(b + 3 * NT, a.Hx + cc);
+        cp_async<VB>(b + 4 * NT, a.Hy + cc);
+        cp_async<VB>(b + 5 * NT, a.Hz + cc);
+        cp_async<VB>(b + 6 * NT, a.Hz + cc - a.NxP);
+        cp_async<VB>(b + 7 * NT, a.Hx + cc - a.NxP);
+        if constexpr (MAT) {
+            cp_async<2 * W>(b + 8 * NT, a.bidx + cc);
+        } else {
+            cp_async<W * int(sizeof(T)), false>(b + 8 * NT, a.bEx + cc);
+            cp_async<W * int(sizeof(T)), false>(b + 9 * NT, a.bEy + cc);
+            cp_async<W * int(sizeof(T)), false>(b + 10 * NT, a.bEz + cc);
+        }
+        if (pload && i0 > 0) {
+            cp_async<NB>(b + XS * NT, a.Hz + cc - NE);
+            cp_async<NB>(reinterpret_cast<char*>(b + XS * NT) + 8, a.Hy + cc - NE);
+        }
+    };
+    if constexpr (PIPE) {
+        if (act) issue(kb, 0);
+        cp_async_commit();
+    }
+
     for (int k = kb; k < ke; ++k) {
         const size_t c = size_t(k) * a.plane + row;
         T ex[W], ey[W], ez[W], bx[W], by[W], bz[W], hx[W], hy[W], hz[W], hzj[W], hxj[W];
-        if (act) {
+        T hze = T(0), hye = T(0);
+        if (PIPE && act) {
+            // the next plane into the other stage (its contents were used last iteration),
+            // then wait for this plane's copies
+            if (k + 1 < ke) issue(k + 1, (k + 1 - kb) & 1);
+            cp_async_commit();
+            cp_async_wait<1>();
+            const uint4* b = pipe_smem + size_t((k - kb) & 1) * NV * NT + tid;
+            Fld<S, T>::ld(reinterpret_cast<const S*>(b + 0 * NT), ex);
+            Fld<S, T>::ld(reinterpret_cast<const S*>(b + 1 * NT), ey);
+            Fld<S, T>::ld(reinterpret_cast<const S*>(b + 2 * NT), ez);
+            Fld<S, T>::ld(reinterpret_cast<const S*>(b + 3 * NT), hx);
+            Fld<S, T>::ld(reinterpret_cast<const S*>(b + 4 * NT), hy);
+            Fld<S, T>::ld(reinterpret_cast<const S*>(b + 5 * NT), hz);
+            Fld<S, T>::ld(reinterpret_cast<const S*>(b + 6 * NT), hzj);
+            Fld<S, T>::ld(reinterpret_cast<const S*>(b + 7 * NT), hxj);
+            if constexpr (MAT) {
+                RowIds<W> idk;
+                const unsigned* w = reinterpret_cast<const unsigned*>(b + 8 * NT);
+#pragma unroll
+                for (int q = 0; q < W / 2; ++q) idk.w[q] = w[q];
+                load_bE<MAT>(a, c, idk, bx, by, bz);
+            } else {
+                Vec<T>::ld(reinterpret_cast<const T*>(b + 8 * NT), bx);
+                Vec<T>::ld(reinterpret_cast<const T*>(b + 9 * NT), by);
+                Vec<T>::ld(reinterpret_cast<const T*>(b + 10 * NT), bz);
+            }
+            if (pload && i0 > 0) {
+                const S* xs = reinterpret_cast<const S*>(b + XS * NT);
+                hze = T(to_c(xs[NE - 1]));
+                hye = T(to_c(reinterpret_cast<const S*>(reinterpret_cast<const char*>(xs) + 8)[NE - 1]));
+            }
+        } else if (act) {
             Fld<S, T>::ld(a.Ex + c, ex);
             Fld<S, T>::ld(a.Ey + c, ey);
             Fld<S, T>::ld(a.Ez + c, ez);
@@ -650,13 +799,12 @@ __device__ __forceinline__ void e_column(const StepArgs<S, T>& a, const SweepGeo
             ldH(a.Hz + c, hz);
             ldH(a.Hz + c - a.NxP, hzj);
             ldH(a.Hx + c - a.NxP, hxj);
+            if (pload && i0 > 0) { hze = ldH1(a.Hz + c - 1); hye = ldH1(a.Hy + c - 1); }
         } else {
 #pragma unroll
             for (int e = 0; e < W; ++e)
                 ex[e] = ey[e] = ez[e] = bx[e] = by[e] = bz[e] = hx[e] = hy[e] = hz[e] = hzj[e] = hxj[e] = T(0);
         }
-        T hze = T(0), hye = T(0);
-        if (pload && act && i0 > 0) { hze = ldH1(a.Hz + c - 1); hye = ldH1(a.Hy + c - 1); }
         const T idz = __ldg(a.idz + k);
         const bool zpml = in_pml(k, a.NzT, np);
         T zb = 1, zc = 0, zik = 1;
@@ -777,7 +925,7 @@ __device__ __forceinline__ void e_column(const StepArgs<S, T>& a, const SweepGeo
     }
 }
 
-template <typename S, typename T, bool CG = false, bool SH = false, bool MAT = false>
+template <typename S, typename T, bool CG = false, bool SH = false, bool MAT = false, bool PIPE = false>
 __device__ __forceinline__ void update_E_block(const StepArgs<S, T>& a, const int kchunk, const ESrc& src,
                                                const SweepGeom& g, const int bx, const int by, const int bz) {
     constexpr int W = Vec<T>::W;
@@ -790,7 +938,7 @@ __device__ __forceinline__ void update_E_block(const StepArgs<S, T>& a, const in
         const int j = by * kBlockY + threadIdx.y;
         if (j < 1 || j >= a.NyT) return;  // E is updated for j >= 1 only; whole warp
         const int i0 = g.xi0 + (bx * 32 + lane) * W;
-        e_column<S, T, false, CG, SH, MAT>(a, g, src, j, i0, i0 < g.xi1, kb, ke, lane);
+        e_column<S, T, false, CG, SH, MAT, PIPE>(a, g, src, j, i0, i0 < g.xi1, kb, ke, lane);
     } else {
         const int t = threadIdx.y * 32 + lane;
         const int rr = t / g.ne, v = t - rr * g.ne;
@@ -802,10 +950,11 @@ __device__ __forceinline__ void update_E_block(const StepArgs<S, T>& a, const in
     }
 }
 
-template <typename S, typename T, bool SH = false, bool MAT = false>
+// PIPE: interior columns stage their planes in shared memory (EPipe<MAT>::bytes() dynamic).
+template <typename S, typename T, bool SH = false, bool MAT = false, bool PIPE = false>
 __global__ void __launch_bounds__(32 * kBlockY, 2)
 k_update_E(const StepArgs<S, T> a, const int kchunk, const ESrc src, const SweepGeom g) {
-    update_E_block<S, T, false, SH, MAT>(a, kchunk, src, g, blockIdx.x, blockIdx.y, blockIdx.z);
+    update_E_block<S, T, false, SH, MAT, PIPE>(a, kchunk, src, g, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 
 // ---------------------------------------------------------------------------------

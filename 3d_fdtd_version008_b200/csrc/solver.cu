@@ -708,6 +708,18 @@ private:
     bool has_gain_ = false;
     bool pec_ = false;  // PECBoundary: zero E on the outer faces after every E update
     size_t mat_rows_ = 0;  // > 0: indexed material (a_.bidx / a_.btab)
+    // The sweeps' interior columns stage their planes in shared memory through cp.async
+    // (FDTD_B200_E_PIPE / FDTD_B200_H_PIPE = 0 / 1 override the defaults set in the constructor).
+    bool pipe_ = false, hpipe_ = false;
+    using EKernel = void (*)(const StepArgs<S, T>, const int, const ESrc, const SweepGeom);
+    EKernel e_kernel(bool sheets) const {
+        static constexpr EKernel k[8] = {
+            k_update_E<S, T, false, false, false>, k_update_E<S, T, false, false, true>,
+            k_update_E<S, T, false, true, false>,  k_update_E<S, T, false, true, true>,
+            k_update_E<S, T, true, false, false>,  k_update_E<S, T, true, false, true>,
+            k_update_E<S, T, true, true, false>,   k_update_E<S, T, true, true, true>};
+        return k[4 * int(sheets) + 2 * int(a_.bidx != nullptr) + int(pipe_)];
+    }
     // event timing: ev_[0..3] bracket H, E and the auxiliary kernels of one step
     // kernel path 0: k_step_fused (fields and psi_H double-buffered, cur_ = buffer holding
     // the latest state); path 1 (default, measured faster on B200): k_update_H +
@@ -732,10 +744,27 @@ private:
     fdtd_timing_v1 tm_{};
 };
 
+// The device's default memory pool (which cudaMallocAsync draws from) keeps what solves give
+// back instead of returning it to the driver at the next synchronisation: a retired solve's
+// memory is then reused by the next one without new mappings, and retiring does not unmap
+// gigabytes.  Set once per device.
+void keep_pool_memory(int dev) {
+    static std::mutex mu;
+    static std::vector<int> done;
+    std::lock_guard<std::mutex> l(mu);
+    if (std::find(done.begin(), done.end(), dev) != done.end()) return;
+    cudaMemPool_t pool;
+    ck(cudaDeviceGetDefaultMemPool(&pool, dev), "cudaDeviceGetDefaultMemPool");
+    uint64_t keep = ~uint64_t(0);
+    ck(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep), "cudaMemPoolSetAttribute");
+    done.push_back(dev);
+}
+
 template <typename S, typename T>
 Solver<S, T>::Solver(const fdtd_setup_v1& s, int dev) {
     device = dev;
     ck(cudaSetDevice(dev), "cudaSetDevice");
+    keep_pool_memory(dev);
     ck(cudaStreamCreateWithFlags(&st_, cudaStreamNonBlocking), "cudaStreamCreate");
     constexpr int W = Vec<T>::W;
     NxT_ = int(s.NxT); NyT_ = int(s.NyT); NzT_ = int(s.NzT);
@@ -842,6 +871,23 @@ Solver<S, T>::Solver(const fdtd_setup_v1& s, int dev) {
             to_device(s.bE[c], be[c], sH_ / sE_);
         }
         a.bEx = be[0]; a.bEy = be[1]; a.bEz = be[2];
+    }
+    // Where the staging pays (536^3 slab case, one B200): the E sweep with the row-indexed
+    // material in FP32 (-2 %) and 16-bit storage (-10 %); the H sweep with 16-bit storage only
+    // (-8 %; FP32 and FP64 +4 %).  With the three bE arrays the E staging takes 96 KB of shared
+    // memory per block, leaves L1 too small for the neighbour rows, and is 15 % slower.
+    pipe_ = a.bidx != nullptr && sizeof(S) <= 4;
+    hpipe_ = sizeof(S) == 2;
+    if (const char* e = std::getenv("FDTD_B200_H_PIPE")) hpipe_ = std::string(e) != "0";
+    if (const char* e = std::getenv("FDTD_B200_E_PIPE")) pipe_ = a.bidx != nullptr && std::string(e) != "0";
+    if (hpipe_)
+        ck(cudaFuncSetAttribute(k_update_H<S, T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(HPipe::bytes())),
+           "cudaFuncSetAttribute");
+    if (pipe_) {
+        const int smem = int(a.bidx ? EPipe<true>::bytes() : EPipe<false>::bytes());
+        for (bool sh : {false, true})
+            ck(cudaFuncSetAttribute(e_kernel(sh), cudaFuncAttributeMaxDynamicSharedMemorySize, smem),
+               "cudaFuncSetAttribute");
     }
 
     // 1-D arrays
@@ -1424,11 +1470,11 @@ void Solver<S, T>::run(uint64_t n) {
             if (per_kernel) ck(cudaEventRecord(ev_[1], st_), "cudaEventRecord");
             launches += 1;
         } else {
-            k_update_H<S, T><<<gridH_, blk, 0, st_>>>(a_, kchunkH_, geom_);
+            if (hpipe_) k_update_H<S, T, true><<<gridH_, blk, HPipe::bytes(), st_>>>(a_, kchunkH_, geom_);
+            else k_update_H<S, T><<<gridH_, blk, 0, st_>>>(a_, kchunkH_, geom_);
             if (per_kernel) ck(cudaEventRecord(ev_[1], st_), "cudaEventRecord");
-            const auto upd = src.ns ? (a_.bidx ? k_update_E<S, T, true, true> : k_update_E<S, T, true, false>)
-                                    : (a_.bidx ? k_update_E<S, T, false, true> : k_update_E<S, T, false, false>);
-            upd<<<gridE_, blk, 0, st_>>>(a_, kchunkE_, src, geom_);
+            const size_t smem = pipe_ ? (a_.bidx ? EPipe<true>::bytes() : EPipe<false>::bytes()) : 0;
+            e_kernel(src.ns != 0)<<<gridE_, blk, smem, st_>>>(a_, kchunkE_, src, geom_);
             launches += 2;
         }
         if (pec_) {
@@ -1778,6 +1824,7 @@ public:
 
     Batch(int dev, uint64_t budget) : device_(dev), budget_(budget) {
         ck(cudaSetDevice(dev), "cudaSetDevice");
+        keep_pool_memory(dev);
         ck(cudaStreamCreateWithFlags(&st_, cudaStreamNonBlocking), "cudaStreamCreate");
         ck(cudaHostAlloc(reinterpret_cast<void**>(&ticks_), sizeof(BatchTick) * kMaxBatch * kRing, cudaHostAllocDefault),
            "cudaHostAlloc");

@@ -434,7 +434,10 @@ def test_16bit_storage_rejects_fused_path(pkg):
 def test_material_index_matches_arrays(pkg, precision, path, monkeypatch):
     """The indexed material (a uint16 row number per cell and a table of distinct rows), as the
     setup view brings it or as the stepper derives it from the arrays, gives bit-identical
-    fields to the three bE arrays: the same values reach the same arithmetic."""
+    fields to the three bE arrays: the same values reach the same arithmetic.  (The E sweep's
+    shared-memory staging, used with the index only, is a different compilation of the same
+    update and is compared to rounding in test_staged_sweeps_match_direct_loads.)"""
+    monkeypatch.setenv("FDTD_B200_E_PIPE", "0")
     s = pkg.Setup.from_file(GOLDEN / "cases" / "step_g2_planewave.params")
     assert s.view.n_bE_rows > 0
     bare = pkg.SetupV1.from_buffer_copy(s.view)
@@ -451,3 +454,26 @@ def test_material_index_matches_arrays(pkg, precision, path, monkeypatch):
         sol.close()
     for c in FIELDS:
         assert np.array_equal(out[0][c], out[2][c]) and np.array_equal(out[1][c], out[2][c]), c
+
+
+# Tolerances: the parity bars of each storage (FP64 1e-12, FP32 1e-5); BF16 2e-2, since one
+# fused multiply-add rounded differently can move a stored value by a BF16 step (2^-8).
+@pytest.mark.parametrize("precision,tol", [(1, 1e-12), (0, 1e-5), (3, 2e-2)])
+@pytest.mark.parametrize("case", ["step_g2_planewave", "step_g1_gain", "step_g3_pec"])
+def test_staged_sweeps_match_direct_loads(pkg, precision, tol, case, monkeypatch):
+    """The sweeps whose interior columns stage the next plane in shared memory (cp.async)
+    against the same sweeps loading straight from global memory: the same update compiled
+    twice, equal to rounding (the compiler may fuse a multiply-add differently)."""
+    s = pkg.Setup.from_file(GOLDEN / "cases" / (case + ".params"))
+    out = []
+    for mode in ("1", "0"):
+        monkeypatch.setenv("FDTD_B200_E_PIPE", mode)
+        monkeypatch.setenv("FDTD_B200_H_PIPE", mode)
+        sol = pkg.Solver(s, precision=precision, kernel_path=1)
+        rng = np.random.default_rng(5)
+        for c in ("Ex", "Ey", "Ez"):
+            sol.set_field(c, rng.normal(0, 1e-3, sol.shape))
+        sol.run(40)
+        out.append(fields(sol))
+        sol.close()
+    assert field_rel_l2(out[0], out[1], "E") <= tol and field_rel_l2(out[0], out[1], "H") <= tol
