@@ -114,8 +114,8 @@ int fdtd_setup_parse(const char* params_text, int mesh_only, fdtd_setup** out, c
         for (const auto& w : S.plane_waves)
             s->sheets.push_back({w.axis, w.comp, w.plane, w.lo0, w.hi0, w.lo1, w.hi1, w.d, w.sign, int32_t(w.waveform), 0,
                                  w.E0, w.f0, w.tau, w.t0, w.t_shift});
-        bool u = !S.mats.bH[0].empty();
-        for (int a = 0; a < 3 && u; ++a)
+        bool u = S.mats.uniform_ah || !S.mats.bH[0].empty();
+        for (int a = 0; a < 3 && u && !S.mats.uniform_ah; ++a)
             u = !S.mats.aE[a].empty() && !S.mats.aH[a].empty() && !S.mats.bH[a].empty() && all_equal(S.mats.aE[a], 1.0) &&
                 all_equal(S.mats.aH[a], 1.0) && all_equal(S.mats.bH[a], S.mats.bH[0][0]);
         s->uniform_ah = u;
@@ -160,7 +160,7 @@ int fdtd_setup_view(const fdtd_setup* s, fdtd_setup_v1* v) {
         v->aH[a] = (s->uniform_ah || S.mats.aH[a].empty()) ? nullptr : S.mats.aH[a].data();
         v->bH[a] = (s->uniform_ah || S.mats.bH[a].empty()) ? nullptr : S.mats.bH[a].data();
     }
-    v->bH_uniform = s->uniform_ah ? S.mats.bH[0][0] : S.dt / fdtd::phys::MU0;
+    v->bH_uniform = S.mats.uniform_ah ? S.mats.bH_value : s->uniform_ah ? S.mats.bH[0][0] : S.dt / fdtd::phys::MU0;
     v->n_sheets = uint32_t(s->sheets.size());
     v->sheets = s->sheets.data();
     v->pec_boundary = S.boundary_pec ? 1 : 0;

@@ -266,56 +266,58 @@ void Shape::bounding_box(real bb[6]) const {
     }
 }
 
-namespace {
-
 // Spatial bins over the scene items so that "the last item containing the point wins"
 // (src/structure_material.hpp:214-220) is answered by scanning, newest first, only the
 // items whose bounding box overlaps the point's bin.  Same winner as the full scan.
+ItemBins make_item_bins(const std::vector<StructureItem>& items, const GridSpacing& g) {
+    ItemBins B;
+    for (int a = 0; a < 3; ++a) {
+        const auto& b = g.bounds(a);
+        B.lo[a] = b.front();
+        const real hi = b.back();
+        B.nb[a] = std::max<std::size_t>(1, std::min<std::size_t>(64, (b.size() + 7) / 8));
+        B.w[a] = (hi - B.lo[a]) / real(B.nb[a]);
+        if (!(B.w[a] > 0)) B.w[a] = 1.0;
+    }
+    std::vector<std::vector<uint32_t>> bins(B.nb[0] * B.nb[1] * B.nb[2]);
+    for (std::size_t it = items.size(); it-- > 0;) {
+        real bb[6];
+        items[it].shape.bounding_box(bb);
+        std::size_t b0[3], b1[3];
+        for (int a = 0; a < 3; ++a) {
+            b0[a] = B.bin(a, bb[2 * a]);
+            b1[a] = B.bin(a, bb[2 * a + 1]);
+        }
+        for (std::size_t x = b0[0]; x <= b1[0]; ++x)
+            for (std::size_t y = b0[1]; y <= b1[1]; ++y)
+                for (std::size_t z = b0[2]; z <= b1[2]; ++z)
+                    bins[(x * B.nb[1] + y) * B.nb[2] + z].push_back(uint32_t(it));
+    }
+    B.start.push_back(0);
+    for (const auto& l : bins) {
+        B.ids.insert(B.ids.end(), l.begin(), l.end());
+        B.start.push_back(uint32_t(B.ids.size()));
+    }
+    return B;
+}
+
+namespace {
+
 class ItemIndex {
 public:
-    ItemIndex(const std::vector<StructureItem>& items, const GridSpacing& g) : items_(items) {
-        for (int a = 0; a < 3; ++a) {
-            const auto& b = g.bounds(a);
-            lo_[a] = b.front();
-            hi_[a] = b.back();
-            nb_[a] = std::max<std::size_t>(1, std::min<std::size_t>(64, (b.size() + 7) / 8));
-            w_[a] = (hi_[a] - lo_[a]) / real(nb_[a]);
-            if (!(w_[a] > 0)) w_[a] = 1.0;
-        }
-        bins_.resize(nb_[0] * nb_[1] * nb_[2]);
-        for (std::size_t it = items.size(); it-- > 0;) {
-            real bb[6];
-            items[it].shape.bounding_box(bb);
-            std::size_t b0[3], b1[3];
-            for (int a = 0; a < 3; ++a) {
-                b0[a] = bin_of(a, bb[2 * a]);
-                b1[a] = bin_of(a, bb[2 * a + 1]);
-            }
-            for (std::size_t x = b0[0]; x <= b1[0]; ++x)
-                for (std::size_t y = b0[1]; y <= b1[1]; ++y)
-                    for (std::size_t z = b0[2]; z <= b1[2]; ++z)
-                        bins_[(x * nb_[1] + y) * nb_[2] + z].push_back(uint32_t(it));
-        }
-    }
+    ItemIndex(const std::vector<StructureItem>& items, const GridSpacing& g)
+        : items_(items), B_(make_item_bins(items, g)) {}
 
     const Material& sample(real x, real y, real z, const Material& bg) const {
-        const auto& list = bins_[(bin_of(0, x) * nb_[1] + bin_of(1, y)) * nb_[2] + bin_of(2, z)];
-        for (uint32_t it : list)
-            if (items_[it].shape.contains(x, y, z)) return items_[it].mat;
+        const std::size_t b = (B_.bin(0, x) * B_.nb[1] + B_.bin(1, y)) * B_.nb[2] + B_.bin(2, z);
+        for (uint32_t q = B_.start[b]; q < B_.start[b + 1]; ++q)
+            if (items_[B_.ids[q]].shape.contains(x, y, z)) return items_[B_.ids[q]].mat;
         return bg;
     }
 
 private:
-    std::size_t bin_of(int a, real v) const {
-        real t = (v - lo_[a]) / w_[a];
-        if (!(t > 0)) return 0;  // also catches NaN
-        std::size_t b = std::size_t(t);
-        return b >= nb_[a] ? nb_[a] - 1 : b;
-    }
     const std::vector<StructureItem>& items_;
-    real lo_[3], hi_[3], w_[3];
-    std::size_t nb_[3];
-    std::vector<std::vector<uint32_t>> bins_;
+    ItemBins B_;
 };
 
 }  // namespace
@@ -641,8 +643,13 @@ SimSetup SimSetup::from_params(const ParamFile& pf, bool bake) {
         }
         sc.items.push_back(it);
     }
-    // bake_and_bind (src/params.hpp:512-516), 8 subpixel samples as main() passes.
-    sc.bake(S.mats, S.dt, phys::EPS0, phys::MU0, 8);
+    // bake_and_bind (src/params.hpp:512-516), 8 subpixel samples as main() passes.  BAKE = gpu
+    // (a build-only key) bakes bE on the CUDA device instead, bit-identical, when the items
+    // allow it.
+    const std::string bake_on = pf.str("BAKE", "host");
+    require(bake_on == "host" || bake_on == "gpu", "BAKE must be host or gpu");
+    if (!(bake_on == "gpu" && gpu_bake(sc, S.mats, S.dt, phys::EPS0, phys::MU0)))
+        sc.bake(S.mats, S.dt, phys::EPS0, phys::MU0, 8);
 
     // Dipole sources (register_default_sources / make_dipole_source,
     // src/params.hpp:594-647, src/sources/dipole_source.hpp:90-153).

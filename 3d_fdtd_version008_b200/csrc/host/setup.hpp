@@ -163,6 +163,24 @@ struct StructureItem {
 struct MaterialGrids {
     std::size_t NxT = 0, NyT = 0, NzT = 0;
     std::vector<real> aE[3], bE[3], aH[3], bH[3];
+    // Set by the GPU bake, which only makes bE: aE = aH = 1 everywhere and bH = bH_value
+    // everywhere (the aE/aH/bH arrays are then left empty).
+    bool uniform_ah = false;
+    real bH_value = 0;
+};
+
+// Spatial bins over the scene items (CSR): the items whose bounding box overlaps a bin,
+// newest first, so the first one containing a point is the last-defined one.
+struct ItemBins {
+    real lo[3], w[3];
+    std::size_t nb[3];
+    std::vector<uint32_t> start, ids;  // bin b holds ids[start[b] .. start[b+1])
+    std::size_t bin(int a, real v) const {
+        const real t = (v - lo[a]) / w[a];
+        if (!(t > 0)) return 0;  // also catches NaN
+        const std::size_t b = std::size_t(t);
+        return b >= nb[a] ? nb[a] - 1 : b;
+    }
 };
 
 struct Scene {
@@ -176,6 +194,15 @@ struct Scene {
     void bake(MaterialGrids& mg, real dt, real eps0, real mu0, int subpixel_samples) const;
     void n_grid(std::vector<real>& out) const;  // make_n_grid_from_scene (:291-310)
 };
+
+ItemBins make_item_bins(const std::vector<StructureItem>& items, const GridSpacing& g);
+
+// The same bake for bE on the current CUDA device, bit-identical to Scene::bake with 8
+// samples (every product and sum rounded on its own, in the same order).  Only for
+// lossless, non-magnetic items (sigma = sigma_m = 0, mu_r = 1, what make_nk gives): returns
+// false otherwise, and the caller bakes on the host.  Throws std::runtime_error when no
+// CUDA device can be used.
+bool gpu_bake(const Scene& sc, MaterialGrids& mg, real dt, real eps0, real mu0);
 
 // ---------------------------------------------------------------- sources
 enum class Waveform { Ricker = 0, GaussianModulatedSine = 1, RickerLikeGaussian2nd = 2, ContinuousWave = 3 };

@@ -110,7 +110,7 @@ class OracleSolve:
         c.NxT, c.NyT, c.NzT = self.shape
         c.npml = int(v.npml)
         c.dt = float(v.dt)
-        c.bH = float(setup.array("bHx")[0])
+        c.bH = float(setup.array("bHx")[0]) if v.bH[0] else float(v.bH_uniform)
         arrays = {}
         for n in ("inv_dx", "inv_dy", "inv_dz", "dx", "dy", "dz"):
             arrays[n] = np.ascontiguousarray(setup.array(n))

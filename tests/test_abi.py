@@ -65,3 +65,14 @@ def test_create_validates_view(pkg):
     with pytest.raises(pkg.FdtdError) as e:
         pkg.Solver(s, view=v)
     assert e.value.code == 1
+
+
+def test_gpu_bake_fails_loudly_without_a_device(pkg):
+    """BAKE = gpu bakes on a CUDA device or reports that it cannot; it never falls back silently."""
+    text = (pkg.config_path("c0_dipole_sphere.params")).read_text() + "\nBAKE = gpu\n"
+    try:
+        s = pkg.Setup.from_text(text)
+    except pkg.FdtdError as e:
+        assert "CUDA device" in str(e)
+    else:
+        assert s.view.n_bE_rows > 0
