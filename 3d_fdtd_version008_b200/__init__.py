@@ -48,6 +48,7 @@ EXPORTED_SYMBOLS = (
     "fdtd_get_probe_series", "fdtd_get_dft", "fdtd_get_diagnostics", "fdtd_device_bytes",
     "fdtd_kernel_launches", "fdtd_set_timing", "fdtd_get_timing", "fdtd_set_kernel_path", "fdtd_synchronize", "fdtd_last_error",
     "fdtd_destroy", "fdtd_field_scan_noalloc", "fdtd_attach_outputs", "fdtd_flush_outputs", "fdtd_material_rows",
+    "fdtd_create_sharded",
     "fdtd_close_outputs",
     "fdtd_batch_create", "fdtd_batch_submit", "fdtd_batch_run", "fdtd_batch_job_state",
     "fdtd_batch_probe_series", "fdtd_batch_dft", "fdtd_batch_diagnostics", "fdtd_batch_release",
@@ -157,6 +158,7 @@ def load_library() -> C.CDLL:
         "fdtd_attach_outputs": (C.c_int, [vp, vp, C.c_char_p]),
         "fdtd_flush_outputs": (C.c_int, [vp]),
         "fdtd_material_rows": (C.c_int, [vp, C.POINTER(C.c_uint64)]),
+        "fdtd_create_sharded": (C.c_int, [C.POINTER(SetupV1), C.c_int, C.POINTER(C.c_int), C.POINTER(vp)]),
         "fdtd_close_outputs": (C.c_int, [vp]),
         "fdtd_create": (C.c_int, [C.POINTER(SetupV1), C.c_int, C.POINTER(vp)]),
         "fdtd_set_field": (C.c_int, [vp, C.c_int, _dptr]),
@@ -270,7 +272,10 @@ class Solver:
     """One resident solve on one GPU (fdtd_create ... fdtd_destroy)."""
 
     def __init__(self, setup: Setup, device: int = 0, precision: Optional[int] = None,
-                 view: Optional[SetupV1] = None, kernel_path: Optional[int] = None):
+                 view: Optional[SetupV1] = None, kernel_path: Optional[int] = None, shards: int = 1,
+                 devices=None):
+        """shards > 1: the solve split along z (fdtd_create_sharded), shard r on devices[r]
+        (default: all on `device`)."""
         lib = load_library()
         v = view if view is not None else setup.view
         if precision is not None:
@@ -279,7 +284,11 @@ class Solver:
         self.setup = setup
         self.view = v
         h = C.c_void_p()
-        rc = lib.fdtd_create(C.byref(v), int(device), C.byref(h))
+        if shards > 1:
+            devs = (C.c_int * shards)(*(devices if devices is not None else [device] * shards))
+            rc = lib.fdtd_create_sharded(C.byref(v), int(shards), devs, C.byref(h))
+        else:
+            rc = lib.fdtd_create(C.byref(v), int(device), C.byref(h))
         if rc != FDTD_OK:
             raise FdtdError(rc, lib.fdtd_last_error(None).decode())
         self._h = h

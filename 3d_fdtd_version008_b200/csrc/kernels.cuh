@@ -198,6 +198,9 @@ template <typename S, typename T = S>
 struct StepArgs {
     int NxT, NyT, NzT, NxP, np;
     long long plane;  // NxP * NyT
+    // z sharding: local plane k is global plane k + kz0 of NzG; the H sweep updates local planes
+    // [kH0, kH1), the E sweep [kE0, kE1).  A whole solve: kz0 = 0, NzG = NzT, [0, NzT-1), [1, NzT).
+    int kz0, NzG, kH0, kH1, kE0, kE1;
     S *Ex, *Ey, *Ez, *Hx, *Hy, *Hz;
     const T *bEx, *bEy, *bEz;
     // Indexed material (the E kernels' MAT instantiation): per cell a uint16 index into a table
@@ -562,13 +565,13 @@ __device__ __forceinline__ void h_column(const StepArgs<S, T>& a, const SweepGeo
         }
         if (!PIPE && xn && act) { eye = to_c(a.Ey[c + W]); eze = to_c(a.Ez[c + W]); }
         const T idz = __ldg(a.idz + k);
-        const bool zpml = in_pml(k, a.NzT, np);
+        const bool zpml = in_pml(k + a.kz0, a.NzG, np);
         T zb = 1, zc = 0, zik = 1;
         size_t zs = 0, ys = 0;
         T pxy[W], pzy[W], pxz[W], pyz[W];  // psi Hx_y, Hz_y, Hx_z, Hy_z
         if (zpml) {
             zb = __ldg(a.pbH[2] + k); zc = __ldg(a.pcH[2] + k); zik = __ldg(a.ik[2] + k);
-            zs = (size_t(slab_index(k, a.NzT, np)) * a.NyT + j) * a.NxP + i0;
+            zs = (size_t(slab_index(k + a.kz0, a.NzG, np)) * a.NyT + j) * a.NxP + i0;
             if (act) { Fld<S, T>::ld(a.psiH[1] + zs, pxz); Fld<S, T>::ld(a.psiH[2] + zs, pyz); }
         }
         if (ypml) {
@@ -641,8 +644,8 @@ __device__ __forceinline__ void update_H_block(const StepArgs<S, T>& a, const in
     constexpr int W = Vec<T>::W;
     if (*a.status) return;
     const int lane = threadIdx.x;
-    const int kb = bz * kchunk;
-    const int ke = min(kb + kchunk, a.NzT - 1);
+    const int kb = max(bz * kchunk, a.kH0);
+    const int ke = min(bz * kchunk + kchunk, a.kH1);
     if (kb >= ke) return;
     if (bx < g.gxi) {
         const int j = by * kBlockY + threadIdx.y;
@@ -806,13 +809,13 @@ __device__ __forceinline__ void e_column(const StepArgs<S, T>& a, const SweepGeo
                 ex[e] = ey[e] = ez[e] = bx[e] = by[e] = bz[e] = hx[e] = hy[e] = hz[e] = hzj[e] = hxj[e] = T(0);
         }
         const T idz = __ldg(a.idz + k);
-        const bool zpml = in_pml(k, a.NzT, np);
+        const bool zpml = in_pml(k + a.kz0, a.NzG, np);
         T zb = 1, zc = 0, zik = 1;
         size_t zs = 0, ys = 0;
         T pxy[W], pzy[W], pxz[W], pyz[W];  // psi Ex_y, Ez_y, Ex_z, Ey_z
         if (zpml) {
             zb = __ldg(a.pbE[2] + k); zc = __ldg(a.pcE[2] + k); zik = __ldg(a.ik[2] + k);
-            zs = (size_t(slab_index(k, a.NzT, np)) * a.NyT + j) * a.NxP + i0;
+            zs = (size_t(slab_index(k + a.kz0, a.NzG, np)) * a.NyT + j) * a.NxP + i0;
             if (act) { Fld<S, T>::ld(a.psiE[1] + zs, pxz); Fld<S, T>::ld(a.psiE[2] + zs, pyz); }
         }
         if (ypml) {
@@ -931,8 +934,8 @@ __device__ __forceinline__ void update_E_block(const StepArgs<S, T>& a, const in
     constexpr int W = Vec<T>::W;
     if (*a.status) return;
     const int lane = threadIdx.x;
-    const int kb = max(bz * kchunk, 1);
-    const int ke = min(bz * kchunk + kchunk, a.NzT);
+    const int kb = max(bz * kchunk, a.kE0);
+    const int ke = min(bz * kchunk + kchunk, a.kE1);
     if (kb >= ke) return;
     if (bx < g.gxi) {
         const int j = by * kBlockY + threadIdx.y;

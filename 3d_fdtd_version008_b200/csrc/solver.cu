@@ -310,7 +310,7 @@ __device__ void block_commit(DiagAccum* acc, double mE, double mP, unsigned fl, 
 // compute_polarization_energy (src/two_level_system.hpp:344-418) over the fields after
 // the step.  Field arrays are scanned as flat padded arrays (padding holds zeros).
 template <typename S, typename T, bool FIELDS = true>
-__device__ void monitor_reduce_blocks(const StepArgs<S, T>& a, size_t nflat, const double* __restrict__ dxs,
+__device__ void monitor_reduce_blocks(const StepArgs<S, T>& a, size_t f0, size_t nflat, const double* __restrict__ dxs,
                                       const double* __restrict__ dys, const double* __restrict__ dzs, int parity_next,
                                       DiagAccum* acc, double es, unsigned bid, unsigned nblk) {
     if (*a.status) return;
@@ -319,7 +319,7 @@ __device__ void monitor_reduce_blocks(const StepArgs<S, T>& a, size_t nflat, con
     const size_t stride = size_t(nblk) * blockDim.x;
     // 16-byte vectors: nflat is a multiple of the padded row, itself a multiple of W
     constexpr int W = Vec<T>::W;
-    for (size_t v = bid * size_t(blockDim.x) + threadIdx.x; FIELDS && v < nflat / W; v += stride) {
+    for (size_t v = f0 / W + bid * size_t(blockDim.x) + threadIdx.x; FIELDS && v < nflat / W; v += stride) {
         const size_t t = v * W;
         T ex[W], ey[W], ez[W], hx[W], hy[W], hz[W];
         Fld<S, T>::ldg(a.Ex + t, ex); Fld<S, T>::ldg(a.Ey + t, ey); Fld<S, T>::ldg(a.Ez + t, ez);
@@ -371,7 +371,7 @@ template <typename S, typename T>
 __global__ void k_tls_reduce(const StepArgs<S, T> a, const double* __restrict__ dxs, const double* __restrict__ dys,
                              const double* __restrict__ dzs, int parity_next, double es, TlsRecord* rec,
                              long long mon_t) {
-    monitor_reduce_blocks<S, T, false>(a, 0, dxs, dys, dzs, parity_next, &rec->acc, es, blockIdx.x, gridDim.x);
+    monitor_reduce_blocks<S, T, false>(a, 0, 0, dxs, dys, dzs, parity_next, &rec->acc, es, blockIdx.x, gridDim.x);
     if (blockIdx.x == 0 && threadIdx.x == 0 && mon_t >= 0) {
         const int r = a.greg[mon_t];
         if (r >= 0 && a.gcoef[r].active) {
@@ -387,10 +387,10 @@ __global__ void k_tls_reduce(const StepArgs<S, T> a, const double* __restrict__ 
 // One thread: the StabilityMonitor decision for monitor step `step`; sets the abort
 // word when the reference would terminate (NaN/Inf anywhere, or > 10 threshold warnings).
 template <typename S, typename T>
-__global__ void k_monitor_reduce(const StepArgs<S, T> a, size_t nflat, const double* __restrict__ dxs,
+__global__ void k_monitor_reduce(const StepArgs<S, T> a, size_t f0, size_t nflat, const double* __restrict__ dxs,
                                  const double* __restrict__ dys, const double* __restrict__ dzs, int parity_next,
                                  DiagAccum* acc, double es) {
-    monitor_reduce_blocks(a, nflat, dxs, dys, dzs, parity_next, acc, es, blockIdx.x, gridDim.x);
+    monitor_reduce_blocks(a, f0, nflat, dxs, dys, dzs, parity_next, acc, es, blockIdx.x, gridDim.x);
 }
 
 __device__ void monitor_eval(DiagAccum* acc, MonitorState* ms, unsigned* status, unsigned long long step) {
@@ -426,6 +426,22 @@ __device__ void monitor_eval(DiagAccum* acc, MonitorState* ms, unsigned* status,
 
 __global__ void k_monitor_eval(DiagAccum* acc, MonitorState* ms, unsigned* status, unsigned long long step) {
     monitor_eval(acc, ms, status, step);
+}
+
+// The monitor of a sharded solve: the other shards' accumulators, copied next to shard 0's,
+// folded into it (max, or, sums) before the one evaluation.
+__global__ void k_acc_combine(DiagAccum* dst, const DiagAccum* parts, int n) {
+    for (int r = 0; r < n; ++r) {
+        const DiagAccum& p = parts[r];
+        dst->maxE = dst->maxE > p.maxE ? dst->maxE : p.maxE;
+        dst->maxP = dst->maxP > p.maxP ? dst->maxP : p.maxP;
+        dst->flags |= p.flags;
+        dst->sum_pop += p.sum_pop;
+        dst->sum_N0 += p.sum_N0;
+        dst->int_Nu += p.int_Nu;
+        dst->int_Ng += p.int_Ng;
+        dst->p_energy += p.p_energy;
+    }
 }
 
 // ================================================================ packed multi-solve step
@@ -499,7 +515,7 @@ __global__ void k_monitor_reduce_multi() {
     const int r = blockIdx.x / kMonBlocks;
     if (!c_btick[r].monitor || *c_bargs[r].status) return;
     const BatchSolve& b = c_bsolve[r];
-    monitor_reduce_blocks(c_bargs[r], size_t(b.nflat), b.dx, b.dy, b.dz, int((c_btick[r].step + 1) & 1), b.acc, 1.0,
+    monitor_reduce_blocks(c_bargs[r], 0, size_t(b.nflat), b.dx, b.dy, b.dz, int((c_btick[r].step + 1) & 1), b.acc, 1.0,
                           blockIdx.x % kMonBlocks, kMonBlocks);
 }
 
@@ -529,6 +545,31 @@ void ck(cudaError_t e, const char* what) {
 
 size_t round_up(size_t v, size_t m) { return (v + m - 1) / m * m; }
 
+// The E field scale of 16-bit storage (see the Solver constructor).
+double field_scale_of(const fdtd_setup_v1& s, bool fp16) {
+    double sE = s.field_scale;
+    if (!(sE > 0.0)) {
+        sE = 1.0;
+        if (fp16) {
+            double est = 0.0;
+            for (uint32_t q = 0; q < s.n_dipoles; ++q) {
+                const fdtd_dipole_v1& d = s.dipoles[q];
+                if (d.cell_area > 0) est = std::max(est, d.tau * std::fabs(d.I0) / (8.8541878128e-12 * d.cell_area));
+            }
+            for (uint32_t q = 0; q < s.n_sheets; ++q) est = std::max(est, 64.0 * std::fabs(s.sheets[q].E0));
+            if (est > 0) sE = std::exp2(std::round(std::log2(est / 64.0)));
+        }
+    }
+    return sE;
+}
+
+// One z shard of a solve: the shard's grid holds global planes [kz0, kz0 + NzT) of NzG, of
+// which it updates (owns) the local planes [own0, own1); the planes around them are halo copies
+// of the neighbours' planes.  A whole solve: kz0 = 0, NzG = NzT, own = [0, NzT).
+struct ShardSpec {
+    int kz0 = 0, NzG = 0, own0 = 0, own1 = 0;
+};
+
 class SolverBase {
 public:
     virtual ~SolverBase() = default;
@@ -555,13 +596,16 @@ public:
 // __nv_bfloat16 with T = float for the 16-bit storage forms, whose stored values are
 // E' = E / sE and H' = H / sH).
 class Batch;
+template <typename S, typename T>
+class Sharded;
 
 template <typename S, typename T>
 class Solver final : public SolverBase {
     friend class Batch;
+    friend class Sharded<S, T>;
 
 public:
-    explicit Solver(const fdtd_setup_v1& s, int dev);
+    explicit Solver(const fdtd_setup_v1& s, int dev, const ShardSpec* shard = nullptr);
     ~Solver() override;
     void run(uint64_t n) override;
     void set_field(int comp, const double* h) override;
@@ -604,6 +648,8 @@ private:
     void capture_movies();
     void write_point_samples();
     void capture_tls(uint64_t s);
+    void phase_H();
+    void phase_E(uint64_t s, ESrc& src, bool monitor);
     void write_population_frame();
     void close_outputs() override;
     // Host <-> device copies of FP64 arrays through two pinned chunks: the host-side copy of
@@ -708,6 +754,7 @@ private:
     bool has_gain_ = false;
     bool pec_ = false;  // PECBoundary: zero E on the outer faces after every E update
     size_t mat_rows_ = 0;  // > 0: indexed material (a_.bidx / a_.btab)
+    ShardSpec shard_{};
     // The sweeps' interior columns stage their planes in shared memory through cp.async
     // (FDTD_B200_E_PIPE / FDTD_B200_H_PIPE = 0 / 1 override the defaults set in the constructor).
     bool pipe_ = false, hpipe_ = false;
@@ -761,7 +808,7 @@ void keep_pool_memory(int dev) {
 }
 
 template <typename S, typename T>
-Solver<S, T>::Solver(const fdtd_setup_v1& s, int dev) {
+Solver<S, T>::Solver(const fdtd_setup_v1& s, int dev, const ShardSpec* shard) {
     device = dev;
     ck(cudaSetDevice(dev), "cudaSetDevice");
     keep_pool_memory(dev);
@@ -780,19 +827,7 @@ Solver<S, T>::Solver(const fdtd_setup_v1& s, int dev) {
         // overshoots the peak by one to two decades, so sE is that over 64, as a power of two.
         // A plane-wave soft source launches a wave of its own amplitude E0: it counts as 64 |E0|.
         // BF16 has FP32's range: sE = 1.
-        double sE = s.field_scale;
-        if (!(sE > 0.0)) {
-            sE = 1.0;
-            if (std::is_same_v<S, __half>) {
-                double est = 0.0;
-                for (uint32_t q = 0; q < s.n_dipoles; ++q) {
-                    const fdtd_dipole_v1& d = s.dipoles[q];
-                    if (d.cell_area > 0) est = std::max(est, d.tau * std::fabs(d.I0) / (8.8541878128e-12 * d.cell_area));
-                }
-                for (uint32_t q = 0; q < s.n_sheets; ++q) est = std::max(est, 64.0 * std::fabs(s.sheets[q].E0));
-                if (est > 0) sE = std::exp2(std::round(std::log2(est / 64.0)));
-            }
-        }
+        const double sE = field_scale_of(s, std::is_same_v<S, __half>);
         sE_ = sE;
         sH_ = sE / 376.730313668;
     }
@@ -804,6 +839,14 @@ Solver<S, T>::Solver(const fdtd_setup_v1& s, int dev) {
     StepArgs<S, T>& a = a_;
     a.NxT = NxT_; a.NyT = NyT_; a.NzT = NzT_; a.NxP = NxP_; a.np = np_;
     a.plane = (long long)plane_;
+    // plane ranges: H is updated for global k < NzG - 1, E for global k >= 1, each on the owned planes
+    shard_ = shard ? *shard : ShardSpec{0, NzT_, 0, NzT_};
+    a.kz0 = shard_.kz0;
+    a.NzG = shard_.NzG;
+    a.kH0 = shard_.own0;
+    a.kH1 = std::min(shard_.own1, shard_.NzG - 1 - shard_.kz0);
+    a.kE0 = std::max(shard_.own0, 1 - shard_.kz0);
+    a.kE1 = shard_.own1;
     // buffer 1 (fields and psi_H) exists only for the fused path, made at its first step
     for (int c = 0; c < 6; ++c) fld_[0][c] = alloc<S>(nflat_);
     point_args_at(0);
@@ -1073,8 +1116,8 @@ Solver<S, T>::Solver(const fdtd_setup_v1& s, int dev) {
     kchunkH_ = chunk(NyT_ - 1, NzT_ - 1);
     kchunkE_ = chunk(NyT_, NzT_);
     if (gyE > 65535) throw Failure(FDTD_ERR_INVALID, "grid too large for the sweep launch shape (NyT)");
-    gridH_ = dim3(gx, gyE, (NzT_ - 1 + kchunkH_ - 1) / kchunkH_);
-    gridE_ = dim3(gx, gyE, (NzT_ + kchunkE_ - 1) / kchunkE_);
+    gridH_ = dim3(gx, gyE, std::max(1, (a.kH1 + kchunkH_ - 1) / kchunkH_));
+    gridE_ = dim3(gx, gyE, std::max(1, (a.kE1 + kchunkE_ - 1) / kchunkE_));
     if (const char* p = std::getenv("FDTD_B200_KERNEL_PATH")) set_path(std::atoi(p));
     ck(cudaStreamSynchronize(st_), "setup upload");
 }
@@ -1495,7 +1538,8 @@ void Solver<S, T>::run(uint64_t n) {
         if (writer_ && !oplan_.movies.empty() && s % save_every_ == 0) capture_movies();
         if (writer_ && oplan_.tls && s % save_every_ == 0) capture_tls(s);
         if (interval_ && s % interval_ == 0) {
-            k_monitor_reduce<S, T><<<8 * 148, 256, 0, st_>>>(a_, nflat_, d_dx_, d_dy_, d_dz_, int((s + 1) & 1), d_acc_, sE_);
+            k_monitor_reduce<S, T><<<8 * 148, 256, 0, st_>>>(a_, size_t(shard_.own0) * plane_, size_t(shard_.own1) * plane_,
+                                                             d_dx_, d_dy_, d_dz_, int((s + 1) & 1), d_acc_, sE_);
             k_monitor_eval<<<1, 1, 0, st_>>>(d_acc_, d_ms_, d_status_, s);
             launches += 2;
         }
@@ -1533,6 +1577,40 @@ void Solver<S, T>::run(uint64_t n) {
     }
     steps = last;
     if (writer_) write_point_samples();
+}
+
+// ---- the phases of one step, for the sharded stepper (run() keeps its own loop)
+template <typename S, typename T>
+void Solver<S, T>::phase_H() {
+    const dim3 blk(32, kBlockY);
+    if (hpipe_) k_update_H<S, T, true><<<gridH_, blk, HPipe::bytes(), st_>>>(a_, kchunkH_, geom_);
+    else k_update_H<S, T><<<gridH_, blk, 0, st_>>>(a_, kchunkH_, geom_);
+    ++launches;
+}
+
+// E sweep, probes / DFT and, on monitor steps, this shard's part of the monitor reduction
+// (the evaluation is made once, on the combined accumulators).
+template <typename S, typename T>
+void Solver<S, T>::phase_E(uint64_t s, ESrc& src, bool monitor) {
+    const dim3 blk(32, kBlockY);
+    src_step(src, s);
+    const size_t smem = pipe_ ? (a_.bidx ? EPipe<true>::bytes() : EPipe<false>::bytes()) : 0;
+    e_kernel(src.ns != 0)<<<gridE_, blk, smem, st_>>>(a_, kchunkE_, src, geom_);
+    ++launches;
+    if (nprobes_) {
+        const int pthreads = int(nprobes_ * std::max<uint32_t>(nf_, 1));
+        const long long sample = (s % save_every_ == 0) ? (long long)(s / save_every_) : -1;
+        k_probe_dft<S, T><<<(pthreads + 127) / 128, 128, 0, st_>>>(a_, d_probes_, int(nprobes_), d_freqs_, int(nf_),
+                                                                     d_dft_, d_series_, sample, double(s + 1) * dt_, dt_,
+                                                                     sE_, sH_);
+        ++launches;
+        if (sample >= 0) series_count_ = uint64_t(sample) + 1;
+    }
+    if (monitor) {
+        k_monitor_reduce<S, T><<<8 * 148, 256, 0, st_>>>(a_, size_t(shard_.own0) * plane_, size_t(shard_.own1) * plane_,
+                                                         d_dx_, d_dy_, d_dz_, int((s + 1) & 1), d_acc_, sE_);
+        ++launches;
+    }
 }
 
 template <typename S, typename T>
@@ -2072,6 +2150,432 @@ private:
     uint64_t ring_ = 0;
     int since_check_ = 0;
 };
+
+// ==================================================================== sharded solve
+// One solve split into z slabs, one Solver per shard (on one device or several).  A shard's
+// grid is its owned planes plus one halo plane on each side that has a neighbour; every step
+// the neighbours exchange one plane of E (Ex, Ey: the H sweep reads E at k+1) and one plane of
+// H (Hx, Hy: the E sweep reads H at k-1), as device-to-device (peer) copies ordered by events
+// between the shards' streams; no kernel waits on another GPU.  The kernels take the shard's
+// global z offset for the z CPML and the global plane ranges they update, so a sharded solve
+// computes the same values, cell for cell, as the whole solve.  The stability monitor reduces
+// each shard's owned planes and is evaluated once, on shard 0, which then hands its status
+// word to the others.  Kernel path 1 only, CPML only, no detector files.
+template <typename S, typename T>
+class Sharded final : public SolverBase {
+public:
+    Sharded(const fdtd_setup_v1& s, int n, const int* devices);
+    ~Sharded() override;
+    void run(uint64_t n) override;
+    void set_field(int comp, const double* h) override { scatter(h, [&](Solver<S, T>& p, const double* l) { p.set_field(comp, l); }); }
+    void get_field(int comp, double* h) override { gather(h, [&](Solver<S, T>& p, double* l) { p.get_field(comp, l); }); }
+    void set_tls(int which, const double* h) override { scatter(h, [&](Solver<S, T>& p, const double* l) { p.set_tls(which, l); }); }
+    void get_tls(int which, double* h) override {
+        // the P slots by parity of the shard's own step count, which run() keeps in step
+        gather(h, [&](Solver<S, T>& p, double* l) { p.get_tls(which, l); });
+    }
+    void probe_series(double* out, uint64_t max, uint64_t* n) override;
+    void dft(uint32_t p, double* re, double* im) override;
+    void diagnostics(fdtd_diagnostics_v1* d) override {
+        part_[0]->diagnostics(d);
+        d->steps_done = steps;
+    }
+    void sync() override {
+        for (auto& p : part_) p->sync();
+    }
+    // FDTD_TIMING_RUN: one event pair per run() on shard 0's stream, the other shards' work
+    // fenced between them; per-kernel timing is a whole solve's mode.
+    void set_timing(int mode) override {
+        if (mode == FDTD_TIMING_KERNELS) throw Failure(FDTD_ERR_UNSUPPORTED, "a sharded solve times whole runs only");
+        if (mode != FDTD_TIMING_OFF && mode != FDTD_TIMING_RUN) throw Failure(FDTD_ERR_INVALID, "bad timing mode");
+        timing_ = mode;
+        run_ms_ = 0;
+        tsteps_ = 0;
+        if (mode == FDTD_TIMING_RUN && !tev_[0]) {
+            ck(cudaSetDevice(part_[0]->device), "cudaSetDevice");
+            for (auto& e : tev_) ck(cudaEventCreate(&e), "cudaEventCreate");
+        }
+    }
+    void set_path(int path) override {
+        if (path != 1) throw Failure(FDTD_ERR_UNSUPPORTED, "a sharded solve steps with kernel path 1");
+    }
+    void timing(fdtd_timing_v1* t) override {
+        std::memset(t, 0, sizeof(*t));
+        t->steps = tsteps_;
+        t->run_ms = run_ms_;
+    }
+    void attach_outputs(const fdtd::SimSetup&, const std::string&) override {
+        throw Failure(FDTD_ERR_UNSUPPORTED, "detector files are written by a whole solve only");
+    }
+    void flush_outputs() override {}
+    void close_outputs() override {}
+
+private:
+    // A shard's slice of the setup view: the arrays it needs, copied out of the whole view.
+    struct Slice {
+        fdtd_setup_v1 v{};
+        std::vector<double> dz, inv_dz, kz[5], bE[3], freqs;
+        std::unique_ptr<double[]> Nu, Ng;  // valid in the gain cells' columns only
+        std::vector<uint16_t> bidx;
+        std::vector<int32_t> reg;
+        std::vector<fdtd_dipole_v1> dip;
+        std::vector<fdtd_probe_v1> probes;
+        std::vector<fdtd_sheet_v1> sheets;
+    };
+    template <typename F> void scatter(const double* h, F&& f);
+    template <typename F> void gather(double* h, F&& f);
+    void copy_planes(int dst, int dst_plane, int src, int src_plane, int c0, int c1);
+
+    std::vector<std::unique_ptr<Slice>> slice_;
+    std::vector<std::unique_ptr<Solver<S, T>>> part_;
+    std::vector<int> z0_, z1_, lo_;   // owned global planes [z0, z1); local plane 0 is global lo
+    std::vector<std::pair<int, int>> probe_at_;  // global probe -> (shard, local probe)
+    uint64_t NxT_, NyT_, NzT_;
+    uint32_t interval_ = 0;
+    std::vector<cudaEvent_t> evE_, evH_, evCpE_, evCpH_, evMon_;
+    DiagAccum* d_parts_ = nullptr;  // shard 0's device: the other shards' accumulators
+    int timing_ = FDTD_TIMING_OFF;
+    cudaEvent_t tev_[2] = {};
+    double run_ms_ = 0;
+    uint64_t tsteps_ = 0;
+};
+
+template <typename S, typename T>
+Sharded<S, T>::Sharded(const fdtd_setup_v1& s, int n, const int* devices) {
+    NxT_ = s.NxT; NyT_ = s.NyT; NzT_ = s.NzT;
+    if (n < 2) throw Failure(FDTD_ERR_INVALID, "a sharded solve needs at least 2 shards");
+    if (s.pec_boundary) throw Failure(FDTD_ERR_UNSUPPORTED, "a sharded solve needs a CPML boundary");
+    for (int c = 0; c < 3; ++c)
+        if (s.aE[c] || s.aH[c] || s.bH[c])
+            throw Failure(FDTD_ERR_UNSUPPORTED, "a sharded solve takes uniform aE/aH/bH (passed as NULL)");
+    if (int64_t(NzT_) < 3 * n) throw Failure(FDTD_ERR_INVALID, "fewer than 3 z planes per shard");
+    const size_t N = NxT_ * NyT_ * NzT_;
+    device = devices ? devices[0] : 0;
+    const bool fp16 = std::is_same_v<S, __half>;
+    const double sE = field_scale_of(s, fp16);  // one scale for all shards
+    interval_ = s.monitor_interval;
+    probe_at_.assign(s.n_probes, {-1, -1});
+    for (int r = 0; r < n; ++r) {
+        const int z0 = int(NzT_ * uint64_t(r) / uint64_t(n)), z1 = int(NzT_ * uint64_t(r + 1) / uint64_t(n));
+        const int lo = std::max(0, z0 - 1), hi = std::min(int(NzT_), z1 + 1), nz = hi - lo;
+        z0_.push_back(z0); z1_.push_back(z1); lo_.push_back(lo);
+        auto sl = std::make_unique<Slice>();
+        fdtd_setup_v1& v = sl->v;
+        v = s;
+        v.NzT = uint64_t(nz);
+        v.field_scale = sE;
+        auto cut1 = [&](const double* a, std::vector<double>& out) -> const double* {
+            if (!a) return nullptr;
+            out.assign(a + lo, a + hi);
+            return out.data();
+        };
+        auto cut3 = [&](auto* a, auto& out) {
+            using E = std::remove_cv_t<std::remove_pointer_t<decltype(a)>>;
+            if (!a) return (const E*)nullptr;
+            out.resize(NxT_ * NyT_ * size_t(nz));
+#pragma omp parallel for schedule(static)
+            for (long long ij = 0; ij < (long long)(NxT_ * NyT_); ++ij)
+                std::memcpy(out.data() + size_t(ij) * nz, a + size_t(ij) * NzT_ + lo, size_t(nz) * sizeof(E));
+            return (const E*)out.data();
+        };
+        v.dz = cut1(s.dz, sl->dz);
+        v.inv_dz = cut1(s.inv_dz, sl->inv_dz);
+        v.cpml_kappa[2] = cut1(s.cpml_kappa[2], sl->kz[0]);
+        v.cpml_bE[2] = cut1(s.cpml_bE[2], sl->kz[1]);
+        v.cpml_cE[2] = cut1(s.cpml_cE[2], sl->kz[2]);
+        v.cpml_bH[2] = cut1(s.cpml_bH[2], sl->kz[3]);
+        v.cpml_cH[2] = cut1(s.cpml_cH[2], sl->kz[4]);
+        const char* mi = std::getenv("FDTD_B200_MATERIAL_INDEX");
+        const bool use_index = s.bE_index && s.n_bE_rows && !(mi && std::string(mi) == "0");
+        if (use_index) {  // the shard reads the row index; the arrays are not copied
+            v.bE_index = cut3(s.bE_index, sl->bidx);
+            for (int c = 0; c < 3; ++c) v.bE[c] = nullptr;
+        } else {
+            v.bE_index = nullptr;
+            v.n_bE_rows = 0;
+            for (int c = 0; c < 3; ++c) v.bE[c] = cut3(s.bE[c], sl->bE[c]);
+        }
+        if (s.tls_region_map) {
+            v.tls_region_map = cut3(s.tls_region_map, sl->reg);
+            // gain cells only where this shard updates E: none in the halo planes
+            for (size_t ij = 0; ij < NxT_ * NyT_; ++ij)
+                for (int k = 0; k < nz; ++k)
+                    if (lo + k < z0 || lo + k >= z1) sl->reg[ij * nz + k] = -1;
+        }
+        // initial Nu, Ng: the stepper reads them at gain cells only, so only the (i, j) columns
+        // that hold one are copied (the rest of the buffer is never read)
+        v.tls_Nu = v.tls_Ng = nullptr;
+        if (s.tls_Nu || s.tls_Ng) {
+            const size_t nl = NxT_ * NyT_ * size_t(nz);
+            if (s.tls_Nu) sl->Nu.reset(new double[nl]);
+            if (s.tls_Ng) sl->Ng.reset(new double[nl]);
+#pragma omp parallel for schedule(static)
+            for (long long ij = 0; ij < (long long)(NxT_ * NyT_); ++ij) {
+                bool any = false;
+                for (int k = 0; k < nz && v.tls_region_map; ++k) any |= sl->reg[size_t(ij) * nz + k] >= 0;
+                if (!any) continue;
+                if (s.tls_Nu) std::memcpy(sl->Nu.get() + size_t(ij) * nz, s.tls_Nu + size_t(ij) * NzT_ + lo, size_t(nz) * 8);
+                if (s.tls_Ng) std::memcpy(sl->Ng.get() + size_t(ij) * nz, s.tls_Ng + size_t(ij) * NzT_ + lo, size_t(nz) * 8);
+            }
+            v.tls_Nu = sl->Nu.get();
+            v.tls_Ng = sl->Ng.get();
+        }
+        for (uint32_t q = 0; q < s.n_dipoles; ++q) {
+            fdtd_dipole_v1 d = s.dipoles[q];
+            if (int(d.k) < z0 || int(d.k) >= z1) continue;
+            d.k -= uint64_t(lo);
+            sl->dip.push_back(d);
+        }
+        v.n_dipoles = uint32_t(sl->dip.size());
+        v.dipoles = sl->dip.data();
+        for (uint32_t q = 0; q < s.n_sheets; ++q) {
+            fdtd_sheet_v1 w = s.sheets[q];
+            if (w.axis == 2) {
+                if (int(w.plane) < z0 || int(w.plane) >= z1) continue;
+                w.plane -= uint64_t(lo);
+            } else {  // z is the second in-plane axis
+                const int a = std::max(int(w.lo1), z0), b = std::min(int(w.hi1), z1 - 1);
+                if (a > b) continue;
+                w.lo1 = uint64_t(a - lo);
+                w.hi1 = uint64_t(b - lo);
+            }
+            sl->sheets.push_back(w);
+        }
+        v.n_sheets = uint32_t(sl->sheets.size());
+        v.sheets = sl->sheets.data();
+        for (uint32_t q = 0; q < s.n_probes; ++q) {
+            fdtd_probe_v1 pr = s.probes[q];
+            if (int(pr.k) < z0 || int(pr.k) >= z1) continue;
+            probe_at_[q] = {r, int(sl->probes.size())};
+            pr.k -= uint64_t(lo);
+            sl->probes.push_back(pr);
+        }
+        v.n_probes = uint32_t(sl->probes.size());
+        v.probes = sl->probes.data();
+        ShardSpec spec{lo, int(NzT_), z0 - lo, z1 - lo};
+        part_.push_back(std::make_unique<Solver<S, T>>(v, devices ? devices[r] : 0, &spec));
+        slice_.push_back(std::move(sl));
+    }
+    (void)N;
+    // the monitor is evaluated on shard 0 for the whole solve
+    bool gain = false;
+    for (auto& p : part_) gain |= p->has_gain_;
+    {
+        Solver<S, T>& p0 = *part_[0];
+        ck(cudaSetDevice(p0.device), "cudaSetDevice");
+        MonitorState ms{};
+        ck(cudaMemcpy(&ms, p0.d_ms_, sizeof(ms), cudaMemcpyDeviceToHost), "monitor state");
+        ms.has_gain = gain ? 1 : 0;
+        ck(cudaMemcpy(p0.d_ms_, &ms, sizeof(ms), cudaMemcpyHostToDevice), "monitor state");
+        ck(cudaMalloc(&d_parts_, std::max<size_t>(1, part_.size()) * sizeof(DiagAccum)), "cudaMalloc");
+    }
+    for (auto* evs : {&evE_, &evH_, &evCpE_, &evCpH_, &evMon_}) {
+        evs->resize(part_.size());
+        for (size_t r = 0; r < part_.size(); ++r) {
+            ck(cudaSetDevice(part_[r]->device), "cudaSetDevice");
+            ck(cudaEventCreateWithFlags(&(*evs)[r], cudaEventDisableTiming), "cudaEventCreate");
+        }
+    }
+    for (auto& p : part_) dev_bytes += p->dev_bytes;
+}
+
+template <typename S, typename T>
+Sharded<S, T>::~Sharded() {
+    for (auto& p : part_) p->sync();
+    for (auto* evs : {&evE_, &evH_, &evCpE_, &evCpH_, &evMon_})
+        for (cudaEvent_t e : *evs) if (e) cudaEventDestroy(e);
+    for (cudaEvent_t e : tev_) if (e) cudaEventDestroy(e);
+    if (d_parts_) {
+        cudaSetDevice(part_[0]->device);
+        cudaFree(d_parts_);
+    }
+}
+
+// Planes [c0, c1) components of one local plane of shard src into a local plane of shard dst,
+// on dst's stream (components 0-2 E, 3-5 H).
+template <typename S, typename T>
+void Sharded<S, T>::copy_planes(int dst, int dst_plane, int src, int src_plane, int c0, int c1) {
+    Solver<S, T>& a = *part_[dst];
+    const Solver<S, T>& b = *part_[src];
+    S* const da[6] = {a.a_.Ex, a.a_.Ey, a.a_.Ez, a.a_.Hx, a.a_.Hy, a.a_.Hz};
+    const S* const sb[6] = {b.a_.Ex, b.a_.Ey, b.a_.Ez, b.a_.Hx, b.a_.Hy, b.a_.Hz};
+    for (int c = c0; c < c1; ++c)
+        ck(cudaMemcpyPeerAsync(da[c] + size_t(dst_plane) * a.plane_, a.device, sb[c] + size_t(src_plane) * b.plane_,
+                               b.device, a.plane_ * sizeof(S), a.st_),
+           "halo copy");
+}
+
+template <typename S, typename T>
+void Sharded<S, T>::run(uint64_t n) {
+    const int R = int(part_.size());
+    const uint64_t n0 = steps, last = n0 + n;
+    std::vector<ESrc> src(R);
+    for (int r = 0; r < R; ++r) {
+        ck(cudaSetDevice(part_[r]->device), "cudaSetDevice");
+        part_[r]->ensure_series((last + part_[r]->save_every_ - 1) / part_[r]->save_every_);
+        src[r] = ESrc{};
+        part_[r]->src_static(src[r]);
+    }
+    auto loc = [&](int r, int g) { return g - lo_[r]; };  // global plane -> shard r's local plane
+    const bool timed = timing_ == FDTD_TIMING_RUN;
+    if (timed) {  // every shard starts after the start event
+        ck(cudaSetDevice(part_[0]->device), "cudaSetDevice");
+        ck(cudaEventRecord(tev_[0], part_[0]->st_), "cudaEventRecord");
+        for (int r = 1; r < R; ++r) {
+            ck(cudaSetDevice(part_[r]->device), "cudaSetDevice");
+            ck(cudaStreamWaitEvent(part_[r]->st_, tev_[0], 0), "cudaStreamWaitEvent");
+        }
+    }
+    for (uint64_t s = n0; s < last; ++s) {
+        // E of shard r+1's first plane -> shard r's top halo, after r+1's last E sweep
+        for (int r = 0; r + 1 < R; ++r) {
+            ck(cudaSetDevice(part_[r]->device), "cudaSetDevice");
+            ck(cudaStreamWaitEvent(part_[r]->st_, evE_[r + 1], 0), "cudaStreamWaitEvent");
+            copy_planes(r, loc(r, z1_[r]), r + 1, loc(r + 1, z0_[r + 1]), 0, 2);
+            ck(cudaEventRecord(evCpE_[r], part_[r]->st_), "cudaEventRecord");
+        }
+        for (int r = 0; r < R; ++r) {  // H, once shard r-1 has read r's H plane of the last step
+            ck(cudaSetDevice(part_[r]->device), "cudaSetDevice");
+            if (r + 1 < R) ck(cudaStreamWaitEvent(part_[r]->st_, evCpH_[r], 0), "cudaStreamWaitEvent");
+            ck(cudaStreamWaitEvent(part_[r]->st_, evMon_[r], 0), "cudaStreamWaitEvent");
+            part_[r]->phase_H();
+            ck(cudaEventRecord(evH_[r], part_[r]->st_), "cudaEventRecord");
+        }
+        // H of shard r's last plane -> shard r+1's bottom halo
+        for (int r = 0; r + 1 < R; ++r) {
+            ck(cudaSetDevice(part_[r + 1]->device), "cudaSetDevice");
+            ck(cudaStreamWaitEvent(part_[r + 1]->st_, evH_[r], 0), "cudaStreamWaitEvent");
+            copy_planes(r + 1, loc(r + 1, z0_[r + 1] - 1), r, loc(r, z1_[r] - 1), 3, 5);
+            ck(cudaEventRecord(evCpH_[r], part_[r + 1]->st_), "cudaEventRecord");
+        }
+        const bool mon = interval_ && s % interval_ == 0;
+        for (int r = 0; r < R; ++r) {  // E, once shard r-1 has read r's E plane
+            ck(cudaSetDevice(part_[r]->device), "cudaSetDevice");
+            if (r > 0) ck(cudaStreamWaitEvent(part_[r]->st_, evCpE_[r - 1], 0), "cudaStreamWaitEvent");
+            part_[r]->phase_E(s, src[r], mon);
+            ck(cudaEventRecord(evE_[r], part_[r]->st_), "cudaEventRecord");
+        }
+        if (mon) {
+            Solver<S, T>& p0 = *part_[0];
+            ck(cudaSetDevice(p0.device), "cudaSetDevice");
+            for (int r = 1; r < R; ++r) {
+                ck(cudaStreamWaitEvent(p0.st_, evE_[r], 0), "cudaStreamWaitEvent");
+                ck(cudaMemcpyPeerAsync(d_parts_ + (r - 1), p0.device, part_[r]->d_acc_, part_[r]->device,
+                                       sizeof(DiagAccum), p0.st_),
+                   "monitor copy");
+            }
+            k_acc_combine<<<1, 1, 0, p0.st_>>>(p0.d_acc_, d_parts_, R - 1);
+            k_monitor_eval<<<1, 1, 0, p0.st_>>>(p0.d_acc_, p0.d_ms_, p0.d_status_, s);
+            p0.launches += 2;
+            for (int r = 1; r < R; ++r)
+                ck(cudaMemcpyPeerAsync(part_[r]->d_status_, part_[r]->device, p0.d_status_, p0.device,
+                                       sizeof(unsigned), p0.st_),
+                   "status copy");
+            ck(cudaEventRecord(evMon_[0], p0.st_), "cudaEventRecord");
+            for (int r = 1; r < R; ++r) {  // the shard's accumulator restarts once it was read
+                ck(cudaSetDevice(part_[r]->device), "cudaSetDevice");
+                ck(cudaStreamWaitEvent(part_[r]->st_, evMon_[0], 0), "cudaStreamWaitEvent");
+                ck(cudaMemsetAsync(part_[r]->d_acc_, 0, sizeof(DiagAccum), part_[r]->st_), "cudaMemsetAsync");
+                ck(cudaEventRecord(evMon_[r], part_[r]->st_), "cudaEventRecord");
+            }
+        }
+    }
+    if (timed) {  // the end event after every shard's last work
+        for (int r = 1; r < R; ++r) {
+            ck(cudaSetDevice(part_[r]->device), "cudaSetDevice");
+            ck(cudaEventRecord(evE_[r], part_[r]->st_), "cudaEventRecord");
+        }
+        ck(cudaSetDevice(part_[0]->device), "cudaSetDevice");
+        for (int r = 1; r < R; ++r) ck(cudaStreamWaitEvent(part_[0]->st_, evE_[r], 0), "cudaStreamWaitEvent");
+        ck(cudaEventRecord(tev_[1], part_[0]->st_), "cudaEventRecord");
+    }
+    unsigned status = 0;
+    for (auto& p : part_) {
+        ck(cudaSetDevice(p->device), "cudaSetDevice");
+        ck(cudaStreamSynchronize(p->st_), "run");
+        ck(cudaGetLastError(), "step kernels");
+    }
+    if (timed) {
+        float ms = 0;
+        ck(cudaEventElapsedTime(&ms, tev_[0], tev_[1]), "cudaEventElapsedTime");
+        run_ms_ += ms;
+        tsteps_ += n;
+    }
+    Solver<S, T>& p0 = *part_[0];
+    ck(cudaSetDevice(p0.device), "cudaSetDevice");
+    ck(cudaMemcpy(&status, p0.d_status_, sizeof(unsigned), cudaMemcpyDeviceToHost), "status");
+    uint64_t done = last;
+    if (status) {
+        MonitorState ms{};
+        ck(cudaMemcpy(&ms, p0.d_ms_, sizeof(ms), cudaMemcpyDeviceToHost), "monitor state");
+        done = ms.step + 1;
+    }
+    launches = 0;
+    for (auto& p : part_) {
+        p->steps = done;
+        p->series_count_ = std::min<uint64_t>(p->series_count_, (done + p->save_every_ - 1) / p->save_every_);
+        launches += p->launches;
+    }
+    steps = done;
+    if (status) throw Failure(FDTD_ERR_UNSTABLE, "stability monitor stopped the solve at step " + std::to_string(done - 1));
+}
+
+// Whole-grid idx3 array -> each shard's planes (halos included), and back (owned planes).
+template <typename S, typename T>
+template <typename F>
+void Sharded<S, T>::scatter(const double* h, F&& f) {
+    if (!h) throw Failure(FDTD_ERR_INVALID, "null host array");
+    for (size_t r = 0; r < part_.size(); ++r) {
+        const int nz = int(slice_[r]->v.NzT), lo = lo_[r];
+        std::vector<double> l(NxT_ * NyT_ * size_t(nz));
+#pragma omp parallel for schedule(static)
+        for (long long ij = 0; ij < (long long)(NxT_ * NyT_); ++ij)
+            std::memcpy(l.data() + size_t(ij) * nz, h + size_t(ij) * NzT_ + lo, size_t(nz) * sizeof(double));
+        f(*part_[r], l.data());
+    }
+}
+
+template <typename S, typename T>
+template <typename F>
+void Sharded<S, T>::gather(double* h, F&& f) {
+    if (!h) throw Failure(FDTD_ERR_INVALID, "null host array");
+    for (size_t r = 0; r < part_.size(); ++r) {
+        const int nz = int(slice_[r]->v.NzT), lo = lo_[r], z0 = z0_[r], z1 = z1_[r];
+        std::vector<double> l(NxT_ * NyT_ * size_t(nz));
+        f(*part_[r], l.data());
+#pragma omp parallel for schedule(static)
+        for (long long ij = 0; ij < (long long)(NxT_ * NyT_); ++ij)
+            std::memcpy(h + size_t(ij) * NzT_ + z0, l.data() + size_t(ij) * nz + (z0 - lo), size_t(z1 - z0) * sizeof(double));
+    }
+}
+
+template <typename S, typename T>
+void Sharded<S, T>::probe_series(double* out, uint64_t max, uint64_t* n) {
+    const size_t np = probe_at_.size();
+    uint64_t count = 0;
+    std::vector<std::vector<double>> col(part_.size());
+    for (size_t r = 0; r < part_.size(); ++r) {
+        Solver<S, T>& p = *part_[r];
+        if (!p.nprobes_) continue;
+        count = std::max(count, p.series_count_);
+        col[r].resize(p.series_count_ * p.nprobes_);
+        if (!col[r].empty()) p.probe_series(col[r].data(), p.series_count_, nullptr);
+    }
+    if (n) *n = count;
+    if (!out || !np) return;
+    const uint64_t cnt = std::min(count, max);
+    for (size_t q = 0; q < np; ++q) {
+        const auto [r, lq] = probe_at_[q];
+        const uint32_t pn = part_[r]->nprobes_;
+        for (uint64_t t = 0; t < cnt; ++t) out[t * np + q] = col[r][t * pn + size_t(lq)];
+    }
+}
+
+template <typename S, typename T>
+void Sharded<S, T>::dft(uint32_t p, double* re, double* im) {
+    if (p >= probe_at_.size()) throw Failure(FDTD_ERR_INVALID, "no DFT for this probe");
+    part_[probe_at_[p].first]->dft(uint32_t(probe_at_[p].second), re, im);
+}
 }  // namespace
 
 // ==================================================================== C ABI
@@ -2137,6 +2641,32 @@ int fdtd_create(const fdtd_setup_v1* s, int device, fdtd_handle** out) {
         else if (s->precision == FDTD_PREC_FP32) h->s = std::make_unique<Solver<float, float>>(*s, device);
         else if (s->precision == FDTD_PREC_FP16) h->s = std::make_unique<Solver<__half, float>>(*s, device);
         else if (s->precision == FDTD_PREC_BF16) h->s = std::make_unique<Solver<__nv_bfloat16, float>>(*s, device);
+        else throw Failure(FDTD_ERR_UNSUPPORTED, "precision must be FDTD_PREC_FP32, _FP64, _FP16 or _BF16");
+    });
+    if (rc != FDTD_OK) { delete h; return rc; }
+    *out = h;
+    return FDTD_OK;
+}
+
+int fdtd_create_sharded(const fdtd_setup_v1* s, int nshards, const int* devices, fdtd_handle** out) {
+    if (!s || !out) { g_err = "null argument"; return FDTD_ERR_INVALID; }
+    *out = nullptr;
+    if (const char* why = setup_problem(s)) { g_err = why; return FDTD_ERR_INVALID; }
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        g_err = "no CUDA device available";
+        return FDTD_ERR_NO_DEVICE;
+    }
+    if (nshards < 2 || nshards > 64) { g_err = "nshards must be 2..64"; return FDTD_ERR_INVALID; }
+    for (int r = 0; devices && r < nshards; ++r)
+        if (devices[r] < 0 || devices[r] >= ndev) { g_err = "device index out of range"; return FDTD_ERR_INVALID; }
+    auto* h = new fdtd_handle();
+    const int rc = guarded(nullptr, [&] {
+        if (s->precision == FDTD_PREC_FP64) h->s = std::make_unique<Sharded<double, double>>(*s, nshards, devices);
+        else if (s->precision == FDTD_PREC_FP32) h->s = std::make_unique<Sharded<float, float>>(*s, nshards, devices);
+        else if (s->precision == FDTD_PREC_FP16) h->s = std::make_unique<Sharded<__half, float>>(*s, nshards, devices);
+        else if (s->precision == FDTD_PREC_BF16) h->s = std::make_unique<Sharded<__nv_bfloat16, float>>(*s, nshards, devices);
         else throw Failure(FDTD_ERR_UNSUPPORTED, "precision must be FDTD_PREC_FP32, _FP64, _FP16 or _BF16");
     });
     if (rc != FDTD_OK) { delete h; return rc; }

@@ -285,6 +285,14 @@ int fdtd_flush_outputs(fdtd_handle *h);
  * the last Nu/Ng frame and metadata_populations.json), waits for every write and detaches;
  * later steps write nothing. */
 int fdtd_close_outputs(fdtd_handle *h);
+/* One solve split along z into nshards slabs, shard r on devices[r] (NULL: all on device 0),
+ * each stepped by the same kernels with its global z offset; neighbouring shards exchange one
+ * plane of E and one of H per step by device-to-device (peer) copies, and the stability
+ * monitor is evaluated once for the whole solve.  The handle answers the same calls as a
+ * whole solve (fields, gain state, probes, DFT, diagnostics) with identical values; kernel
+ * path 1 only, CPML only, no detector files, timing off.  No counterpart in the reference's
+ * time loop; its slab-parallel variant (src/parallel_domain.hpp) splits one process's loop. */
+int fdtd_create_sharded(const fdtd_setup_v1 *setup, int nshards, const int *devices, fdtd_handle **out);
 /* Block until all device work of the handle is complete. */
 int fdtd_synchronize(fdtd_handle *h);
 /* Message of the last failing call on h (or of the last global failure when h is NULL). */
