@@ -2377,6 +2377,20 @@ Sharded<S, T>::Sharded(const fdtd_setup_v1& s, int n, const int* devices) {
         }
     }
     for (auto& p : part_) dev_bytes += p->dev_bytes;
+    // neighbours on different GPUs copy their halo planes directly over NVLink
+    for (size_t r = 0; r + 1 < part_.size(); ++r) {
+        const int a = part_[r]->device, b = part_[r + 1]->device;
+        if (a == b) continue;
+        for (auto [x, y] : {std::pair<int, int>{a, b}, std::pair<int, int>{b, a}}) {
+            int can = 0;
+            ck(cudaDeviceCanAccessPeer(&can, x, y), "cudaDeviceCanAccessPeer");
+            if (!can) continue;
+            ck(cudaSetDevice(x), "cudaSetDevice");
+            const cudaError_t e = cudaDeviceEnablePeerAccess(y, 0);
+            if (e == cudaErrorPeerAccessAlreadyEnabled) cudaGetLastError();
+            else ck(e, "cudaDeviceEnablePeerAccess");
+        }
+    }
 }
 
 template <typename S, typename T>
