@@ -2377,6 +2377,7 @@ Sharded<S, T>::Sharded(const fdtd_setup_v1& s, int n, const int* devices) {
         }
     }
     for (auto& p : part_) dev_bytes += p->dev_bytes;
+    material_rows = part_[0]->material_rows;
     // neighbours on different GPUs copy their halo planes directly over NVLink
     for (size_t r = 0; r + 1 < part_.size(); ++r) {
         const int a = part_[r]->device, b = part_[r + 1]->device;
