@@ -413,8 +413,9 @@ class Solver:
 
 
 class Batch:
-    """Packed multi-solve engine (fdtd_batch_*): FP32 solves queued on one GPU, admitted by
-    device footprint under `budget_bytes`, stepped together with one launch per sweep."""
+    """Packed multi-solve engine (fdtd_batch_*): FP32, FP16 and BF16 solves queued on one GPU,
+    admitted by device footprint under `budget_bytes`, stepped together with one launch per
+    sweep and storage form.  One engine per device at a time in a process."""
 
     def __init__(self, device: int = 0, budget_bytes: int = 150 << 30):
         self._h = C.c_void_p()
@@ -478,6 +479,12 @@ class Batch:
         if getattr(self, "_h", None) and self._h.value:
             load_library().fdtd_batch_destroy(self._h)
             self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
         self._keep.clear()
 
     def __del__(self):

@@ -445,11 +445,12 @@ __global__ void k_acc_combine(DiagAccum* dst, const DiagAccum* parts, int n) {
 }
 
 // ================================================================ packed multi-solve step
-// Up to kMaxBatch resident FP32 solves advance together: every sweep is ONE launch whose
-// blocks are listed in a table (solve, bx, by, bz), each block running the same block code
-// as the single-solve kernels on its solve's arguments, read from constant memory with a
-// block-uniform index.  Per-solve step data (sources, probe sample, monitor flag) is
-// rewritten in constant memory before every step.
+// Up to kMaxBatch resident solves (FP32, or FP16/BF16 storage with FP32 arithmetic) advance
+// together: every sweep is one launch per storage form present, whose blocks are listed in a
+// table (solve, bx, by, bz), each block running the same block code as the single-solve
+// kernels on its solve's arguments, read from constant memory with a block-uniform index.
+// Per-solve step data (sources, probe sample, monitor flag) is rewritten in constant memory
+// before every step.
 constexpr int kMaxBatch = 64;
 constexpr int kMonBlocks = 64;  // monitor blocks per solve
 
@@ -466,6 +467,9 @@ struct BatchSolve {
     unsigned* status;
     unsigned long long nflat;
     double dt;
+    double sE, sH;  // stored fields are E / sE and H / sH (1 for FP32)
+    int storage;    // 0 FP32, 1 FP16, 2 BF16
+    int pad;
 };
 
 struct BatchTick {
@@ -477,46 +481,83 @@ struct BatchTick {
     int pad;
 };
 
-__constant__ StepArgs<float> c_bargs[kMaxBatch];
+// A resident solve's sweep arguments, whichever its storage form (the three forms differ
+// only in the element type of the field and psi pointers).
+union BatchArgs {
+    StepArgs<float, float> f32;
+    StepArgs<__half, float> f16;
+    StepArgs<__nv_bfloat16, float> bf16;
+};
+static_assert(sizeof(StepArgs<float, float>) == sizeof(StepArgs<__nv_bfloat16, float>) &&
+                  sizeof(StepArgs<float, float>) == sizeof(StepArgs<__half, float>),
+              "storage forms share one argument layout");
+
+__constant__ BatchArgs c_bargs[kMaxBatch];
 __constant__ BatchSolve c_bsolve[kMaxBatch];
 __constant__ BatchTick c_btick[kMaxBatch];
 // The 64 KB constant bank also holds the monitor's and DFT kernels' few constants.
-static_assert((sizeof(StepArgs<float>) + sizeof(BatchSolve) + sizeof(BatchTick)) * kMaxBatch <= 60 * 1024,
+static_assert((sizeof(BatchArgs) + sizeof(BatchSolve) + sizeof(BatchTick)) * kMaxBatch <= 60 * 1024,
               "per-solve constant records exceed the constant bank");
 
+template <typename S>
+__device__ __forceinline__ const StepArgs<S, float>& bargs(int r) {
+    if constexpr (std::is_same_v<S, float>) return c_bargs[r].f32;
+    else if constexpr (std::is_same_v<S, __half>) return c_bargs[r].f16;
+    else return c_bargs[r].bf16;
+}
+
+// The blocks of the solves stored as S.
+template <typename S>
 __global__ void __launch_bounds__(32 * kBlockY, 2) k_update_H_multi(const int4* __restrict__ tab) {
     const int4 e = tab[blockIdx.x];
-    update_H_block<float, float>(c_bargs[e.x], c_bsolve[e.x].kchunkH, c_bsolve[e.x].g, e.y, e.z, e.w);
+    update_H_block<S, float>(bargs<S>(e.x), c_bsolve[e.x].kchunkH, c_bsolve[e.x].g, e.y, e.z, e.w);
 }
 
 // SH / MAT: the blocks of solves with plane-wave sheets / an indexed material; the table lists
-// the four kinds in separate runs, so a solve runs the same code whatever else is resident.
-template <bool SH, bool MAT>
+// each (storage, SH, MAT) kind in a separate run, so a solve runs the same code whatever else
+// is resident.
+template <typename S, bool SH, bool MAT>
 __global__ void __launch_bounds__(32 * kBlockY, 2) k_update_E_multi(const int4* __restrict__ tab) {
     const int4 e = tab[blockIdx.x];
-    update_E_block<float, float, false, SH, MAT>(c_bargs[e.x], c_bsolve[e.x].kchunkE, c_btick[e.x].src,
-                                                 c_bsolve[e.x].g, e.y, e.z, e.w);
+    update_E_block<S, float, false, SH, MAT>(bargs<S>(e.x), c_bsolve[e.x].kchunkE, c_btick[e.x].src,
+                                             c_bsolve[e.x].g, e.y, e.z, e.w);
 }
 
-// one block per solve
-__global__ void k_probe_multi() {
-    const int r = blockIdx.x;
-    const StepArgs<float>& a = c_bargs[r];
+template <typename S>
+__device__ __forceinline__ void probe_multi_block(int r) {
+    const StepArgs<S, float>& a = bargs<S>(r);
     const BatchSolve& b = c_bsolve[r];
     const BatchTick& tk = c_btick[r];
     if (*a.status || b.nprobes == 0) return;
     const int n = b.nprobes * (b.nf > 0 ? b.nf : 1);
     for (int tid = threadIdx.x; tid < n; tid += blockDim.x)
-        probe_dft_thread(a, b.probes, b.nprobes, b.freqs, b.nf, b.dft, b.series, tk.sample, tk.t, b.dt, 1.0, 1.0, tid);
+        probe_dft_thread(a, b.probes, b.nprobes, b.freqs, b.nf, b.dft, b.series, tk.sample, tk.t, b.dt, b.sE, b.sH, tid);
+}
+
+// one block per solve
+__global__ void k_probe_multi() {
+    const int r = blockIdx.x;
+    const int st = c_bsolve[r].storage;
+    if (st == 0) probe_multi_block<float>(r);
+    else if (st == 1) probe_multi_block<__half>(r);
+    else probe_multi_block<__nv_bfloat16>(r);
+}
+
+template <typename S>
+__device__ __forceinline__ void monitor_multi_block(int r) {
+    const BatchSolve& b = c_bsolve[r];
+    monitor_reduce_blocks(bargs<S>(r), 0, size_t(b.nflat), b.dx, b.dy, b.dz, int((c_btick[r].step + 1) & 1), b.acc,
+                          b.sE, blockIdx.x % kMonBlocks, kMonBlocks);
 }
 
 // kMonBlocks blocks per solve; solves without a monitor step this step return at once
 __global__ void k_monitor_reduce_multi() {
     const int r = blockIdx.x / kMonBlocks;
-    if (!c_btick[r].monitor || *c_bargs[r].status) return;
-    const BatchSolve& b = c_bsolve[r];
-    monitor_reduce_blocks(c_bargs[r], 0, size_t(b.nflat), b.dx, b.dy, b.dz, int((c_btick[r].step + 1) & 1), b.acc, 1.0,
-                          blockIdx.x % kMonBlocks, kMonBlocks);
+    if (!c_btick[r].monitor) return;
+    const int st = c_bsolve[r].storage;
+    if (st == 0) monitor_multi_block<float>(r);
+    else if (st == 1) monitor_multi_block<__half>(r);
+    else monitor_multi_block<__nv_bfloat16>(r);
 }
 
 __global__ void k_monitor_eval_multi(int nres) {
@@ -1887,44 +1928,62 @@ namespace {
 class Batch {
 public:
     enum { QUEUED = 0, RESIDENT = 1, DONE = 2, FAILED = 3 };
+    // A resident solve: one of the three storage forms (storage = BatchSolve::storage).
     struct Job {
         const fdtd_setup_v1* setup = nullptr;
         uint64_t target = 0;
         int state = QUEUED;
+        int storage = 0;
         uint64_t bytes = 0;
-        std::unique_ptr<Solver<float, float>> sol;
+        std::unique_ptr<Solver<float, float>> f32;
+        std::unique_ptr<Solver<__half, float>> f16;
+        std::unique_ptr<Solver<__nv_bfloat16, float>> bf16;
         std::vector<double> series, dft;
         uint64_t samples = 0;
         uint32_t nprobes = 0, nf = 0;
         fdtd_diagnostics_v1 diag{};
         std::string err;
+        uint64_t steps() const { return f32 ? f32->steps : f16 ? f16->steps : bf16 ? bf16->steps : 0; }
+        bool live() const { return f32 || f16 || bf16; }
+        void drop() { f32.reset(); f16.reset(); bf16.reset(); }
     };
+    // f(solver) on the job's solver, whatever its storage form.
+    template <typename F>
+    static void with(Job& j, F&& f) {
+        if (j.f32) f(*j.f32);
+        else if (j.f16) f(*j.f16);
+        else f(*j.bf16);
+    }
 
     Batch(int dev, uint64_t budget) : device_(dev), budget_(budget) {
         ck(cudaSetDevice(dev), "cudaSetDevice");
-        keep_pool_memory(dev);
-        ck(cudaStreamCreateWithFlags(&st_, cudaStreamNonBlocking), "cudaStreamCreate");
-        ck(cudaHostAlloc(reinterpret_cast<void**>(&ticks_), sizeof(BatchTick) * kMaxBatch * kRing, cudaHostAllocDefault),
-           "cudaHostAlloc");
-        for (auto& e : ring_ev_) ck(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "cudaEventCreate");
+        claim(dev, true);
+        try {
+            keep_pool_memory(dev);
+            ck(cudaStreamCreateWithFlags(&st_, cudaStreamNonBlocking), "cudaStreamCreate");
+            ck(cudaHostAlloc(reinterpret_cast<void**>(&ticks_), sizeof(BatchTick) * kMaxBatch * kRing,
+                             cudaHostAllocDefault),
+               "cudaHostAlloc");
+            for (auto& e : ring_ev_) ck(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "cudaEventCreate");
+        } catch (...) {
+            release_all();
+            throw;
+        }
     }
-    ~Batch() {
-        cudaSetDevice(device_);
-        if (st_) cudaStreamSynchronize(st_);
-        jobs_.clear();
-        if (d_tab_) cudaFree(d_tab_);
-        if (ticks_) cudaFreeHost(ticks_);
-        for (auto& e : ring_ev_) if (e) cudaEventDestroy(e);
-        if (st_) cudaStreamDestroy(st_);
-    }
+    ~Batch() { release_all(); }
 
     uint64_t submit(const fdtd_setup_v1& s, uint64_t nsteps) {
-        if (s.precision != FDTD_PREC_FP32) throw Failure(FDTD_ERR_UNSUPPORTED, "the packed engine steps FP32 solves");
+        int storage = 0;
+        if (s.precision == FDTD_PREC_FP32) storage = 0;
+        else if (s.precision == FDTD_PREC_FP16) storage = 1;
+        else if (s.precision == FDTD_PREC_BF16) storage = 2;
+        else throw Failure(FDTD_ERR_UNSUPPORTED, "the packed engine steps FP32, FP16 and BF16 solves");
         if (s.pec_boundary) throw Failure(FDTD_ERR_UNSUPPORTED, "the packed engine steps CPML solves");
         if (nsteps == 0) throw Failure(FDTD_ERR_INVALID, "a job needs at least one step");
         Job j;
         j.setup = &s;
         j.target = nsteps;
+        j.storage = storage;
         j.bytes = footprint(s);
         if (j.bytes > budget_) throw Failure(FDTD_ERR_OOM, "job footprint exceeds the batch memory budget");
         const uint64_t t = next_++;
@@ -1941,7 +2000,7 @@ public:
         for (uint64_t t = 0; t < max_steps && !res_.empty(); ++t) {
             step();
             bool finished = false;
-            for (uint64_t r : res_) finished |= jobs_.at(r).sol->steps >= jobs_.at(r).target;
+            for (uint64_t r : res_) finished |= jobs_.at(r).steps() >= jobs_.at(r).target;
             if (finished || ++since_check_ >= kCheckEvery) {
                 check_and_retire();
                 admit();
@@ -1967,8 +2026,39 @@ public:
 private:
     static constexpr int kRing = 64;        // pinned per-step records in flight
     static constexpr int kCheckEvery = 16;  // steps between status checks
+    // E kernel kinds: storage (3) x plane-wave sheets x indexed material
+    static constexpr int kEKinds = 12;
 
-    // Device bytes a solve will hold: fields, bE, psi slabs, gain box (upper bound).
+    // The per-solve records live in the module's constant memory, one set per device: a
+    // second engine on the same device would overwrite the first one's, so it is refused.
+    static void claim(int dev, bool take) {
+        static std::mutex mu;
+        static std::vector<int> owned;
+        std::lock_guard<std::mutex> l(mu);
+        auto it = std::find(owned.begin(), owned.end(), dev);
+        if (!take) {
+            if (it != owned.end()) owned.erase(it);
+            return;
+        }
+        if (it != owned.end())
+            throw Failure(FDTD_ERR_INVALID, "device " + std::to_string(dev) + " already has a packed engine in this process");
+        owned.push_back(dev);
+    }
+    void release_all() {
+        cudaSetDevice(device_);
+        if (st_) cudaStreamSynchronize(st_);
+        jobs_.clear();
+        if (d_tab_) cudaFree(d_tab_);
+        if (ticks_) cudaFreeHost(ticks_);
+        for (auto& e : ring_ev_) if (e) cudaEventDestroy(e);
+        if (st_) cudaStreamDestroy(st_);
+        d_tab_ = nullptr; ticks_ = nullptr; st_ = nullptr;
+        for (auto& e : ring_ev_) e = nullptr;
+        claim(device_, false);
+    }
+
+    // Device bytes a solve will hold: fields, bE, psi slabs, gain box (upper bound; the FP32
+    // figure bounds the 16-bit forms too).
     static uint64_t footprint(const fdtd_setup_v1& s) {
         const uint64_t NxP = (s.NxT + 31) / 32 * 32, NyT = s.NyT, NzT = s.NzT, np2 = 2ull * s.npml;
         uint64_t b = 9ull * NxP * NyT * NzT * 4;
@@ -1985,15 +2075,19 @@ private:
             if (used_ + j.bytes > budget_) break;  // first come, first served
             queue_.pop_front();
             try {
-                j.sol = std::make_unique<Solver<float, float>>(*j.setup, device_);
-                j.sol->ensure_series((j.target + j.sol->save_every_ - 1) / j.sol->save_every_);
-                ck(cudaStreamSynchronize(j.sol->st_), "admit");
+                if (j.storage == 0) j.f32 = std::make_unique<Solver<float, float>>(*j.setup, device_);
+                else if (j.storage == 1) j.f16 = std::make_unique<Solver<__half, float>>(*j.setup, device_);
+                else j.bf16 = std::make_unique<Solver<__nv_bfloat16, float>>(*j.setup, device_);
+                with(j, [&](auto& v) {
+                    v.ensure_series((j.target + v.save_every_ - 1) / v.save_every_);
+                    ck(cudaStreamSynchronize(v.st_), "admit");
+                });
                 j.state = RESIDENT;
                 used_ += j.bytes;
                 res_.push_back(t);
                 changed = true;
             } catch (const std::exception& e) {
-                j.sol.reset();
+                j.drop();
                 j.state = FAILED;
                 j.err = e.what();
             }
@@ -2004,59 +2098,70 @@ private:
     // Per-solve constants and the packed block tables.
     void rebuild() {
         const int n = int(res_.size());
-        std::vector<StepArgs<float>> args(n);
+        std::vector<BatchArgs> args(n);
         std::vector<BatchSolve> bs(n);
         std::vector<int4> tab;
-        nH_ = nE_ = 0;
+        std::vector<int> ekind(n);
         for (int r = 0; r < n; ++r) {
-            Solver<float, float>& v = *jobs_.at(res_[r]).sol;
-            args[r] = v.a_;
+            Job& j = jobs_.at(res_[r]);
             BatchSolve& b = bs[r];
-            b.g = v.geom_;
-            b.kchunkH = v.kchunkH_;
-            b.kchunkE = v.kchunkE_;
-            b.probes = v.d_probes_;
-            b.nprobes = int(v.nprobes_);
-            b.nf = int(v.nf_);
-            b.freqs = v.d_freqs_;
-            b.dft = v.d_dft_;
-            b.series = v.d_series_;
-            b.dx = v.d_dx_; b.dy = v.d_dy_; b.dz = v.d_dz_;
-            b.acc = v.d_acc_;
-            b.ms = v.d_ms_;
-            b.status = v.d_status_;
-            b.nflat = v.nflat_;
-            b.dt = v.dt_;
+            std::memset(&args[r], 0, sizeof(BatchArgs));
+            if (j.f32) args[r].f32 = j.f32->a_;
+            else if (j.f16) args[r].f16 = j.f16->a_;
+            else args[r].bf16 = j.bf16->a_;
+            with(j, [&](auto& v) {
+                b.g = v.geom_;
+                b.kchunkH = v.kchunkH_;
+                b.kchunkE = v.kchunkE_;
+                b.probes = v.d_probes_;
+                b.nprobes = int(v.nprobes_);
+                b.nf = int(v.nf_);
+                b.freqs = v.d_freqs_;
+                b.dft = v.d_dft_;
+                b.series = v.d_series_;
+                b.dx = v.d_dx_; b.dy = v.d_dy_; b.dz = v.d_dz_;
+                b.acc = v.d_acc_;
+                b.ms = v.d_ms_;
+                b.status = v.d_status_;
+                b.nflat = v.nflat_;
+                b.dt = v.dt_;
+                b.sE = v.sE_;
+                b.sH = v.sH_;
+                b.storage = j.storage;
+                b.pad = 0;
+                ekind[r] = 4 * j.storage + 2 * int(!v.sheets_.empty()) + int(v.a_.bidx != nullptr);
+            });
         }
-        for (int r = 0; r < n; ++r) {  // H blocks of every solve, then E blocks
-            const dim3 g = jobs_.at(res_[r]).sol->gridH_;
+        auto add_blocks = [&](int r, dim3 g) {
             for (unsigned z = 0; z < g.z; ++z)
                 for (unsigned y = 0; y < g.y; ++y)
                     for (unsigned x = 0; x < g.x; ++x) tab.push_back(make_int4(r, int(x), int(y), int(z)));
+        };
+        nHk_[0] = 0;
+        for (int st = 0; st < 3; ++st) {  // H blocks by storage form, then E blocks by kind
+            for (int r = 0; r < n; ++r) {
+                Job& j = jobs_.at(res_[r]);
+                if (j.storage == st) with(j, [&](auto& v) { add_blocks(r, v.gridH_); });
+            }
+            nHk_[st + 1] = tab.size();
         }
         nH_ = tab.size();
         nEk_[0] = 0;
-        for (int kind = 0; kind < 4; ++kind) {  // E blocks by kind: 2 * has sheets + indexed material
-            for (int r = 0; r < n; ++r) {
-                const Solver<float, float>& v = *jobs_.at(res_[r]).sol;
-                if (2 * int(!v.sheets_.empty()) + int(v.a_.bidx != nullptr) != kind) continue;
-                const dim3 g = v.gridE_;
-                for (unsigned z = 0; z < g.z; ++z)
-                    for (unsigned y = 0; y < g.y; ++y)
-                        for (unsigned x = 0; x < g.x; ++x) tab.push_back(make_int4(r, int(x), int(y), int(z)));
-            }
+        for (int kind = 0; kind < kEKinds; ++kind) {
+            for (int r = 0; r < n; ++r)
+                if (ekind[r] == kind) with(jobs_.at(res_[r]), [&](auto& v) { add_blocks(r, v.gridE_); });
             nEk_[kind + 1] = tab.size() - nH_;
         }
-        nE_ = tab.size() - nH_;
         ck(cudaStreamSynchronize(st_), "rebuild");  // no step may read the old tables
         if (tab.size() > tab_cap_) {
             if (d_tab_) ck(cudaFree(d_tab_), "cudaFree");
+            d_tab_ = nullptr;
             tab_cap_ = std::max<size_t>(tab.size(), 2 * tab_cap_);
             ck(cudaMalloc(&d_tab_, tab_cap_ * sizeof(int4)), "cudaMalloc block table");
         }
         if (!tab.empty()) ck(cudaMemcpy(d_tab_, tab.data(), tab.size() * sizeof(int4), cudaMemcpyHostToDevice), "block table");
         if (n) {
-            ck(cudaMemcpyToSymbol(c_bargs, args.data(), n * sizeof(StepArgs<float>)), "cudaMemcpyToSymbol");
+            ck(cudaMemcpyToSymbol(c_bargs, args.data(), n * sizeof(BatchArgs)), "cudaMemcpyToSymbol");
             ck(cudaMemcpyToSymbol(c_bsolve, bs.data(), n * sizeof(BatchSolve)), "cudaMemcpyToSymbol");
         }
     }
@@ -2068,29 +2173,38 @@ private:
         BatchTick* tk = ticks_ + size_t(slot) * kMaxBatch;
         bool monitor = false;
         for (int r = 0; r < n; ++r) {
-            Solver<float, float>& v = *jobs_.at(res_[r]).sol;
-            const uint64_t s = v.steps;
-            BatchTick& k = tk[r];
-            k = BatchTick{};
-            v.src_static(k.src);
-            v.src_step(k.src, s);
-            k.sample = (s % v.save_every_ == 0) ? (long long)(s / v.save_every_) : -1;
-            if (k.sample >= 0) v.series_count_ = uint64_t(k.sample) + 1;
-            k.t = double(s + 1) * v.dt_;
-            k.step = s;
-            k.monitor = (v.interval_ && s % v.interval_ == 0) ? 1 : 0;
-            monitor |= k.monitor != 0;
-            v.steps = s + 1;
+            with(jobs_.at(res_[r]), [&](auto& v) {
+                const uint64_t s = v.steps;
+                BatchTick& k = tk[r];
+                k = BatchTick{};
+                v.src_static(k.src);
+                v.src_step(k.src, s);
+                k.sample = (s % v.save_every_ == 0) ? (long long)(s / v.save_every_) : -1;
+                if (k.sample >= 0) v.series_count_ = uint64_t(k.sample) + 1;
+                k.t = double(s + 1) * v.dt_;
+                k.step = s;
+                k.monitor = (v.interval_ && s % v.interval_ == 0) ? 1 : 0;
+                monitor |= k.monitor != 0;
+                v.steps = s + 1;
+            });
         }
         ck(cudaMemcpyToSymbolAsync(c_btick, tk, n * sizeof(BatchTick), 0, cudaMemcpyHostToDevice, st_), "step records");
         ck(cudaEventRecord(ring_ev_[slot], st_), "cudaEventRecord");
         const dim3 blk(32, kBlockY);
-        k_update_H_multi<<<unsigned(nH_), blk, 0, st_>>>(d_tab_);
-        static constexpr void (*kinds[4])(const int4*) = {k_update_E_multi<false, false>, k_update_E_multi<false, true>,
-                                                          k_update_E_multi<true, false>, k_update_E_multi<true, true>};
-        for (int q = 0; q < 4; ++q)
+        using K = void (*)(const int4*);
+        static constexpr K hk[3] = {k_update_H_multi<float>, k_update_H_multi<__half>, k_update_H_multi<__nv_bfloat16>};
+        static constexpr K ek[kEKinds] = {
+            k_update_E_multi<float, false, false>,         k_update_E_multi<float, false, true>,
+            k_update_E_multi<float, true, false>,          k_update_E_multi<float, true, true>,
+            k_update_E_multi<__half, false, false>,        k_update_E_multi<__half, false, true>,
+            k_update_E_multi<__half, true, false>,         k_update_E_multi<__half, true, true>,
+            k_update_E_multi<__nv_bfloat16, false, false>, k_update_E_multi<__nv_bfloat16, false, true>,
+            k_update_E_multi<__nv_bfloat16, true, false>,  k_update_E_multi<__nv_bfloat16, true, true>};
+        for (int q = 0; q < 3; ++q)
+            if (nHk_[q + 1] > nHk_[q]) hk[q]<<<unsigned(nHk_[q + 1] - nHk_[q]), blk, 0, st_>>>(d_tab_ + nHk_[q]);
+        for (int q = 0; q < kEKinds; ++q)
             if (nEk_[q + 1] > nEk_[q])
-                kinds[q]<<<unsigned(nEk_[q + 1] - nEk_[q]), blk, 0, st_>>>(d_tab_ + nH_ + nEk_[q]);
+                ek[q]<<<unsigned(nEk_[q + 1] - nEk_[q]), blk, 0, st_>>>(d_tab_ + nH_ + nEk_[q]);
         k_probe_multi<<<n, 128, 0, st_>>>();
         if (monitor) {
             k_monitor_reduce_multi<<<n * kMonBlocks, 256, 0, st_>>>();
@@ -2106,28 +2220,32 @@ private:
         std::vector<uint64_t> keep;
         for (uint64_t t : res_) {
             Job& j = jobs_.at(t);
-            Solver<float, float>& v = *j.sol;
-            unsigned status = 0;
-            ck(cudaMemcpy(&status, v.d_status_, sizeof(unsigned), cudaMemcpyDeviceToHost), "status");
-            if (status == 0 && v.steps < j.target) { keep.push_back(t); continue; }
-            if (status) {
-                MonitorState ms{};
-                ck(cudaMemcpy(&ms, v.d_ms_, sizeof(ms), cudaMemcpyDeviceToHost), "monitor state");
-                j.err = "stability monitor stopped the solve at step " + std::to_string(ms.step);
-                v.steps = ms.step + 1;
-                v.series_count_ = std::min<uint64_t>(v.series_count_, (v.steps + v.save_every_ - 1) / v.save_every_);
-            }
-            j.nprobes = v.nprobes_;
-            j.nf = v.nf_;
-            j.series.assign(size_t(v.series_count_) * v.nprobes_, 0.0);
-            uint64_t got = 0;
-            if (v.nprobes_) v.probe_series(j.series.data(), v.series_count_, &got);
-            j.samples = got;
-            j.dft.assign(size_t(2) * v.nprobes_ * v.nf_, 0.0);
-            if (v.nprobes_ && v.nf_) ck(cudaMemcpy(j.dft.data(), v.d_dft_, j.dft.size() * sizeof(double), cudaMemcpyDeviceToHost), "dft");
-            v.diagnostics(&j.diag);
-            j.state = status ? FAILED : DONE;
-            j.sol.reset();
+            bool stay = false;
+            with(j, [&](auto& v) {
+                unsigned status = 0;
+                ck(cudaMemcpy(&status, v.d_status_, sizeof(unsigned), cudaMemcpyDeviceToHost), "status");
+                if (status == 0 && v.steps < j.target) { stay = true; return; }
+                if (status) {
+                    MonitorState ms{};
+                    ck(cudaMemcpy(&ms, v.d_ms_, sizeof(ms), cudaMemcpyDeviceToHost), "monitor state");
+                    j.err = "stability monitor stopped the solve at step " + std::to_string(ms.step);
+                    v.steps = ms.step + 1;
+                    v.series_count_ = std::min<uint64_t>(v.series_count_, (v.steps + v.save_every_ - 1) / v.save_every_);
+                }
+                j.nprobes = v.nprobes_;
+                j.nf = v.nf_;
+                j.series.assign(size_t(v.series_count_) * v.nprobes_, 0.0);
+                uint64_t got = 0;
+                if (v.nprobes_) v.probe_series(j.series.data(), v.series_count_, &got);
+                j.samples = got;
+                j.dft.assign(size_t(2) * v.nprobes_ * v.nf_, 0.0);
+                if (v.nprobes_ && v.nf_)
+                    ck(cudaMemcpy(j.dft.data(), v.d_dft_, j.dft.size() * sizeof(double), cudaMemcpyDeviceToHost), "dft");
+                v.diagnostics(&j.diag);
+                j.state = status ? FAILED : DONE;
+            });
+            if (stay) { keep.push_back(t); continue; }
+            j.drop();
             j.setup = nullptr;
             used_ -= j.bytes;
         }
@@ -2143,8 +2261,9 @@ private:
     std::deque<uint64_t> queue_;
     std::vector<uint64_t> res_;  // resident tickets in slot order
     int4* d_tab_ = nullptr;
-    size_t tab_cap_ = 0, nH_ = 0, nE_ = 0;
-    size_t nEk_[5] = {};  // E blocks of kind q are table entries [nEk_[q], nEk_[q + 1]) after the H ones
+    size_t tab_cap_ = 0, nH_ = 0;
+    size_t nHk_[4] = {};          // H blocks of storage form q are table entries [nHk_[q], nHk_[q + 1])
+    size_t nEk_[kEKinds + 1] = {};  // E blocks of kind q are entries [nEk_[q], nEk_[q + 1]) after the H ones
     BatchTick* ticks_ = nullptr;
     cudaEvent_t ring_ev_[kRing] = {};
     uint64_t ring_ = 0;
@@ -2778,7 +2897,7 @@ int fdtd_batch_job_state(fdtd_batch* b, uint64_t ticket, int* state, uint64_t* s
     return bguard(b, [&] {
         Batch::Job& j = b->b->job(ticket);
         *state = j.state;
-        if (steps_done) *steps_done = j.sol ? j.sol->steps : j.diag.steps_done;
+        if (steps_done) *steps_done = j.live() ? j.steps() : j.diag.steps_done;
     });
 }
 

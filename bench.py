@@ -330,6 +330,75 @@ def serving_bench(args):
     print(json.dumps(line))
 
 
+def sweep_bench(args):
+    """The batched gain-laser sweep: 256 slab microcavities of 96 x 96 x 64 cells (80 x 80 x 48
+    core at 20 nm, 8-cell CPML, gain layer), pump W_p log-uniform in 1e7..1e11 1/s (seed 4),
+    BF16 field storage with FP32 arithmetic, FP32 populations, FP64 DFT, through the packed
+    engine; --sweep-steps steps each instead of 200000 (the rate is per step).  The same jobs
+    in FP32 storage are timed beside them.  Two figures per storage form: the whole sweep
+    (all jobs queued at once, admission included) and the packed step of 64 resident
+    cavities alone."""
+    import numpy as np
+    rng = np.random.default_rng(4)
+    pumps = np.exp(rng.uniform(np.log(1e7), np.log(1e11), size=args.sweep_jobs))
+    n = args.sweep_steps
+    base = serving_job_text((80, 80, 48), n)
+    setups = [PKG.Setup.from_text(base.replace("PUMP_RATE = 1e9", f"PUMP_RATE = {float(p)!r}")) for p in pumps]
+    cells = setups[0].shape[0] * setups[0].shape[1] * setups[0].shape[2]
+    out = {}
+    for name, prec in (("bf16", PKG.PREC_BF16), ("fp32", PKG.PREC_FP32)):
+        views = []
+        for s in setups:
+            v = PKG.SetupV1.from_buffer_copy(s.view)
+            v.precision = prec
+            views.append(v)
+        # warm-up: module load and one packed step of each kernel kind
+        b = PKG.Batch(budget_bytes=150 << 30)
+        t = b.submit(setups[0], 20, view=views[0])
+        while b.state(t)[0] < PKG.JOB_DONE:
+            b.run(20)
+        b.release(t)
+        # the packed step alone: 64 resident cavities
+        ts = [b.submit(s, args.sweep_probe_steps + 100, view=v) for s, v in zip(setups[:64], views[:64])]
+        b.run(3)
+        t0 = time.perf_counter()
+        b.run(args.sweep_probe_steps)
+        step_s = (time.perf_counter() - t0) / args.sweep_probe_steps
+        b.close()
+        # the whole sweep, all jobs queued at t = 0
+        b = PKG.Batch(budget_bytes=150 << 30)
+        t0 = time.perf_counter()
+        ts = [b.submit(s, n, view=v) for s, v in zip(setups, views)]
+        pending, failed = set(ts), 0
+        while pending:
+            b.run(64)
+            for t in list(pending):
+                st = b.state(t)[0]
+                if st >= PKG.JOB_DONE:
+                    failed += st == PKG.JOB_FAILED
+                    b.dft(t)
+                    b.release(t)
+                    pending.discard(t)
+        wall = time.perf_counter() - t0
+        b.close()
+        out[name] = {"sweep_seconds": round(wall, 3),
+                     "sweep_Gcell_updates_per_s": round(len(setups) * cells * n / wall / 1e9, 2),
+                     "packed_step_ms_64_cavities": round(step_s * 1e3, 4),
+                     "packed_Gcell_updates_per_s": round(64 * cells / step_s / 1e9, 2),
+                     "failed_jobs": int(failed),
+                     "projected_hours_200000_steps": round(len(setups) / 64 * 200000 * step_s / 3600, 3)}
+    line = {
+        "metric": "Gcell-updates/s (batched BF16 sweep, packed engine)", "value": out["bf16"]["sweep_Gcell_updates_per_s"],
+        "unit": "Gcell-updates/s", "n_gpus": 1, "steps": n, "warmup": 1, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "bf16 storage, f32 arithmetic", "data": "synthetic",
+        "config": {"workload": f"sweep: {len(setups)} gain-slab microcavities of 96x96x64 cells, pump log-uniform "
+                               "1e7-1e11 1/s, BF16 fields / FP32 populations / FP64 DFT", "jobs": len(setups),
+                   "cells_per_job": cells, "steps_per_job": n, "budget_GB": 150},
+        "bf16": out["bf16"], "fp32": out["fp32"],
+    }
+    print(json.dumps(line))
+
+
 def precision_study(args):
     """The 512^3 sphere solve (or --workload's) for --study-steps steps as FP64, FP32, FP16 and
     BF16 storage: field L2 (E and H), probe series, DFT and DFT-peak errors against FP64."""
@@ -383,6 +452,11 @@ def main():
     ap.add_argument("--serving", action="store_true",
                     help="serving form: a stream of small solves through the packed engine (own JSON line)")
     ap.add_argument("--serving-jobs", type=int, default=48)
+    ap.add_argument("--sweep", action="store_true",
+                    help="the batched BF16 gain-laser sweep through the packed engine (own JSON line)")
+    ap.add_argument("--sweep-jobs", type=int, default=256)
+    ap.add_argument("--sweep-steps", type=int, default=1000, help="steps per cavity (the full sweep is 200000)")
+    ap.add_argument("--sweep-probe-steps", type=int, default=200)
     ap.add_argument("--precision-study", action="store_true",
                     help="FP64 / FP32 / FP16 / BF16 errors on --workload (own JSON line)")
     ap.add_argument("--study-steps", type=int, default=5000)
@@ -403,6 +477,11 @@ def main():
     if args.precision_study and args.impl != "reference":
         if rank == 0:
             precision_study(args)
+        return
+
+    if args.sweep and args.impl != "reference":
+        if rank == 0:
+            sweep_bench(args)
         return
 
     if args.serving and args.impl != "reference":

@@ -300,17 +300,21 @@ const char *fdtd_last_error(const fdtd_handle *h);
 void fdtd_destroy(fdtd_handle *h);
 
 /* ------------------------------------------------------------ packed multi-solve engine */
-/* The serving form of the stepper: a queue of FP32 solves on one GPU.  fdtd_batch_submit
+/* The serving form of the stepper: a queue of FP32, FP16 and BF16 solves (mixed freely; FP64
+ * and PEC solves are refused with FDTD_ERR_UNSUPPORTED) on one GPU.  fdtd_batch_submit
  * queues a solve (the setup view and the arrays it points to must stay valid until the job
  * has finished); fdtd_batch_run admits queued jobs in order while their device footprint
  * fits budget_bytes and fewer than 64 are resident, then advances every resident solve by
- * up to max_steps steps, each step of all of them issued as one packed H launch, one packed
- * E launch and one probe launch (plus one monitor pair on monitor steps), and retires
+ * up to max_steps steps, each step of all of them issued as one packed H and one packed E
+ * launch per storage form present (E: per kind of solve) and one probe launch (plus one
+ * monitor pair on monitor steps), and retires
  * solves that reach their step count or that the stability monitor stops.  The per-cell
  * arithmetic is fdtd_run's, so a job's probe series, DFT and diagnostics are the same as
  * from fdtd_create + fdtd_run on the same setup.  No counterpart in the reference (it runs
  * one solve per process); it replaces running the reference once per design point.
- * A batch is driven from one host thread. */
+ * A batch is driven from one host thread.  One batch per device at a time in a process (its
+ * per-solve records live in the device's constant memory): fdtd_batch_create on a device
+ * that has one returns FDTD_ERR_INVALID. */
 typedef struct fdtd_batch fdtd_batch;
 enum { FDTD_JOB_QUEUED = 0, FDTD_JOB_RESIDENT = 1, FDTD_JOB_DONE = 2, FDTD_JOB_FAILED = 3 };
 int fdtd_batch_create(int device, uint64_t budget_bytes, fdtd_batch **out);

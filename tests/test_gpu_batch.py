@@ -110,9 +110,105 @@ def test_batch_unstable_job_fails_alone(pkg):
     b.close()
 
 
-def test_batch_rejects_non_fp32(pkg):
+def test_batch_rejects_fp64(pkg):
     s = pkg.Setup.from_file(GOLDEN / "cases" / "step_g0_sphere.params", overrides={"PRECISION": "fp64"})
     b = pkg.Batch()
-    with pytest.raises(pkg.FdtdError):
+    with pytest.raises(pkg.FdtdError) as e:
         b.submit(s, 10)
+    assert e.value.code == 7
     b.close()
+
+
+def test_one_batch_per_device(pkg):
+    """The per-solve records live in the device's constant memory: a second engine on the
+    same device is refused while the first one lives, and allowed once it is closed."""
+    b = pkg.Batch()
+    with pytest.raises(pkg.FdtdError) as e:
+        pkg.Batch()
+    assert e.value.code == 1
+    b.close()
+    pkg.Batch().close()
+
+
+def _with_precision(s, precision):
+    v = type(s.view).from_buffer_copy(s.view)
+    v.precision = precision
+    return v
+
+
+def _batch_views(pkg, jobs):
+    """jobs: (setup, view, steps); all resident at once; returns (series, dft, diagnostics)."""
+    b = pkg.Batch(budget_bytes=8 << 30)
+    tickets = [b.submit(s, n, view=v) for s, v, n in jobs]
+    r, q = b.run(1)
+    assert r == len(jobs) and q == 0
+    _drain(pkg, b, tickets, rounds=4000)
+    out = []
+    for t, (s, v, n) in zip(tickets, jobs):
+        st, done = b.state(t)
+        assert st == pkg.JOB_DONE and done == n
+        out.append((b.probe_series(t), b.dft(t), b.diagnostics(t)))
+    b.close()
+    return out
+
+
+MIXED = [  # (setup source, overrides, steps, precision): all three storage forms and E kinds
+    (GOLDEN / "cases" / "step_g0_sphere.params", {}, 150, 3),
+    (GOLDEN / "cases" / "step_g1_gain.params", {"PUMP_RATE": "1e11"}, 120, 2),
+    (GOLDEN / "cases" / "step_g2_planewave.params", {}, 100, 3),
+    (GOLDEN / "cases" / "step_g2_planewave.params", {}, 90, 2),
+    ("c0_dipole_sphere.params", {}, 300, 0),
+    ("c1_gain_slab.params", {"PUMP_RATE": "1e9"}, 210, 3),
+]
+
+
+def test_batch_mixed_storage_alone_and_in_the_mix(pkg):
+    """FP32, FP16 and BF16 solves resident together: each storage form's blocks run in their
+    own launch, and each job's results are bit-identical alone and in the mix."""
+    jobs = []
+    for src, ov, n, prec in MIXED:
+        s = _setup(pkg, src, ov)
+        jobs.append((s, _with_precision(s, prec), n))
+    mixed = _batch_views(pkg, jobs)
+    for k, job in enumerate(jobs):
+        (series, dft, diag), = _batch_views(pkg, [job])
+        assert np.array_equal(mixed[k][0], series) and np.array_equal(mixed[k][1], dft), k
+        assert mixed[k][2]["max_E"] == diag["max_E"] and diag["nan_flags"] == 0
+
+
+def _rel(a, b):
+    return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+
+
+# The bars of test_16bit_storage_spectrum (the single-solve 16-bit forms against FP64):
+# the packed 16-bit solves meet the same bars.
+@pytest.mark.parametrize("precision,cfg,tol", [(3, "c0_dipole_sphere.params", 6e-3), (2, "c0_dipole_sphere.params", 2e-3),
+                                               (3, "c1_gain_slab.params", 1e-2)])
+def test_batch_16bit_spectrum_against_fp64(pkg, precision, cfg, tol):
+    overrides = {"PUMP_RATE": "0"} if cfg.startswith("c1") else {}
+    s = _setup(pkg, cfg, overrides)
+    sol = pkg.Solver(s, precision=1)
+    sol.run(2000)
+    d64 = sol.dft(0)
+    sol.close()
+    (series, d16, diag), = _batch_views(pkg, [(s, _with_precision(s, precision), 2000)])
+    assert diag["nan_flags"] == 0 and diag["stable"] == 1 and np.all(np.isfinite(series))
+    assert np.argmax(np.abs(d16)) == np.argmax(np.abs(d64))
+    assert _rel(d16, d64) <= tol
+
+
+def test_batch_bf16_matches_single_bf16_solve(pkg, monkeypatch):
+    """Against fdtd_create + fdtd_run of the same BF16 solve with the direct-load sweeps (the
+    packed kernels' code, compiled separately): equal to BF16 rounding."""
+    monkeypatch.setenv("FDTD_B200_E_PIPE", "0")
+    monkeypatch.setenv("FDTD_B200_H_PIPE", "0")
+    s = _setup(pkg, "c1_gain_slab.params", {"PUMP_RATE": "1e9"})
+    sol = pkg.Solver(s, precision=3, kernel_path=1)
+    sol.run(300)
+    ref = (sol.probe_series(), sol.dft(0), sol.diagnostics())
+    sol.close()
+    (series, dft, diag), = _batch_views(pkg, [(s, _with_precision(s, 3), 300)])
+    assert _rel(series, ref[0]) <= 2e-2
+    assert np.abs(dft - ref[1]).max() <= 2e-2 * np.abs(ref[1]).max()
+    assert abs(diag["max_E"] - ref[2]["max_E"]) <= 2e-2 * ref[2]["max_E"]
+    assert diag["steps_done"] == 300
