@@ -162,9 +162,14 @@ MIXED = [  # (setup source, overrides, steps, precision): all three storage form
 ]
 
 
-def test_batch_mixed_storage_alone_and_in_the_mix(pkg):
+@pytest.mark.parametrize("shape", [{}, {"FDTD_B200_BATCH_KCHUNK": "0", "FDTD_B200_BATCH_H_PIPE": "0",
+                                      "FDTD_B200_BATCH_E_PIPE": "0"}])
+def test_batch_mixed_storage_alone_and_in_the_mix(pkg, shape, monkeypatch):
     """FP32, FP16 and BF16 solves resident together: each storage form's blocks run in their
-    own launch, and each job's results are bit-identical alone and in the mix."""
+    own launch, and each job's results are bit-identical alone and in the mix (default launch
+    shape: 16-plane z-chunks and staged sweeps; and each solve's own chunks, direct loads)."""
+    for k, v in shape.items():
+        monkeypatch.setenv(k, v)
     jobs = []
     for src, ov, n, prec in MIXED:
         s = _setup(pkg, src, ov)
@@ -197,11 +202,9 @@ def test_batch_16bit_spectrum_against_fp64(pkg, precision, cfg, tol):
     assert _rel(d16, d64) <= tol
 
 
-def test_batch_bf16_matches_single_bf16_solve(pkg, monkeypatch):
-    """Against fdtd_create + fdtd_run of the same BF16 solve with the direct-load sweeps (the
-    packed kernels' code, compiled separately): equal to BF16 rounding."""
-    monkeypatch.setenv("FDTD_B200_E_PIPE", "0")
-    monkeypatch.setenv("FDTD_B200_H_PIPE", "0")
+def test_batch_bf16_matches_single_bf16_solve(pkg):
+    """Against fdtd_create + fdtd_run of the same BF16 solve (both with the staged sweeps; the
+    packed kernels are a separate compilation of the same block code): equal to BF16 rounding."""
     s = _setup(pkg, "c1_gain_slab.params", {"PUMP_RATE": "1e9"})
     sol = pkg.Solver(s, precision=3, kernel_path=1)
     sol.run(300)
