@@ -112,6 +112,7 @@ class SetupV1(C.Structure):
         ("n_sheets", C.c_uint32), ("sheets", C.POINTER(SheetV1)),
         ("pec_boundary", C.c_uint32), ("n_bE_rows", C.c_uint32),
         ("bE_rows", C.POINTER(C.c_double)), ("bE_index", C.POINTER(C.c_uint16)),
+        ("rounding", C.c_uint32),
     ]
 
 

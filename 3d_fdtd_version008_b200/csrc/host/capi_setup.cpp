@@ -164,6 +164,7 @@ int fdtd_setup_view(const fdtd_setup* s, fdtd_setup_v1* v) {
     v->n_sheets = uint32_t(s->sheets.size());
     v->sheets = s->sheets.data();
     v->pec_boundary = S.boundary_pec ? 1 : 0;
+    v->rounding = S.stochastic_rounding ? FDTD_ROUND_STOCHASTIC : FDTD_ROUND_NEAREST;
     if (!s->bE_index.empty()) {
         v->n_bE_rows = uint32_t(s->bE_rows.size() / 3);
         v->bE_rows = s->bE_rows.data();

@@ -490,6 +490,9 @@ SimSetup SimSetup::from_params(const ParamFile& pf, bool bake) {
     if (S.precision != "fp32" && S.precision != "fp64" && S.precision != "fp16" && S.precision != "bf16")
         throw std::runtime_error("PRECISION must be fp32, fp64, fp16 or bf16");
     S.field_scale = pf.num("FIELD_SCALE", 0.0);
+    const std::string rounding = pf.str("ROUNDING", "nearest");
+    if (rounding != "nearest" && rounding != "stochastic") throw std::runtime_error("ROUNDING must be nearest or stochastic");
+    S.stochastic_rounding = rounding == "stochastic";
     S.noise_amplitude = pf.num("NOISE_AMPLITUDE", 0.0);
     S.seed = uint64_t(pf.num("SEED", 1));
     const real pump = pf.num("PUMP_RATE", 0.0);

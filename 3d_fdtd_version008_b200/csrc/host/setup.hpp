@@ -287,6 +287,7 @@ struct SimSetup {
     // build-only keys
     std::vector<real> dft_freqs;
     std::string precision = "fp32";  // fp32 | fp64 | fp16 | bf16
+    bool stochastic_rounding = false;  // ROUNDING = stochastic (build-only key; BF16 storage)
     real field_scale = 0;            // FP16/BF16 storage scale sE (0 = automatic)
     real noise_amplitude = 0;
     uint64_t seed = 1;

@@ -141,6 +141,26 @@ template <> struct Fld<__nv_bfloat16, float> {
     }
 };
 
+// 32-bit integer mixer (the finaliser of Austin Appleby's MurmurHash3, public domain).
+__device__ __forceinline__ unsigned mix32(unsigned x) {
+    x ^= x >> 16;
+    x *= 0x85ebca6bu;
+    x ^= x >> 13;
+    x *= 0xc2b2ae35u;
+    x ^= x >> 16;
+    return x;
+}
+
+// FP32 -> BF16 with stochastic rounding: r's low 16 bits (uniform) are added to the 16 bits
+// that the conversion drops, then the value is truncated, so it rounds away from zero with
+// probability (dropped bits) / 2^16 and the rounding error is zero on average.  Inf and NaN
+// pass unchanged.
+__device__ __forceinline__ unsigned short bf16_stochastic(float f, unsigned r) {
+    unsigned b = __float_as_uint(f);
+    if ((b & 0x7f800000u) != 0x7f800000u) b += r & 0xffffu;
+    return static_cast<unsigned short>(b >> 16);
+}
+
 // Scalar load through L2 only (no L1): values another SM wrote during this launch.
 __device__ __forceinline__ float ldcg1(const float* p) { return __ldcg(p); }
 __device__ __forceinline__ double ldcg1(const double* p) { return __ldcg(p); }
@@ -221,7 +241,31 @@ struct StepArgs {
     const GainCoef<T>* gcoef;
     const unsigned* status;           // nonzero: a monitor step failed, skip all work
     T psc;                            // psi scale (16-bit storage: 1 / dx_min; else 1)
+    int sr;                           // BF16 storage: E and H stores rounded stochastically
 };
+
+// W values of field array `arr` (Ex..Hz = 0..5) at local offset c.  With a.sr (BF16 storage)
+// they are rounded stochastically, keyed by (global cell, array, step), so a cell's rounding
+// is the same whatever the launch shape, sharding or packing; else rounded to nearest.
+template <typename S, typename T>
+__device__ __forceinline__ void st_field(const StepArgs<S, T>& a, S* p, size_t c, const T (&v)[Vec<T>::W], unsigned arr,
+                                         unsigned step) {
+    if constexpr (std::is_same_v<S, __nv_bfloat16>) {
+        if (a.sr) {
+            const unsigned cell = unsigned(c + size_t(a.kz0) * size_t(a.plane));
+            const unsigned salt = mix32(step * 0x9e3779b9u + arr);
+            unsigned short h[4];
+#pragma unroll
+            for (int e = 0; e < 4; ++e) h[e] = bf16_stochastic(v[e], mix32((cell + e) ^ salt));
+            uint2 u;
+            u.x = unsigned(h[0]) | (unsigned(h[1]) << 16);
+            u.y = unsigned(h[2]) | (unsigned(h[3]) << 16);
+            *reinterpret_cast<uint2*>(p + c) = u;
+            return;
+        }
+    }
+    Fld<S, T>::st(p + c, v);
+}
 
 constexpr int kMaxSheets = 2;
 
@@ -236,6 +280,7 @@ struct ESrc {
     int ns;
     int ax[kMaxSheets], pc[kMaxSheets], pl[kMaxSheets];
     int lo0[kMaxSheets], hi0[kMaxSheets], lo1[kMaxSheets], hi1[kMaxSheets];
+    unsigned step;         // n (low 32 bits): the stochastic rounding key of step n's stores
     double sJ[kMaxSheets];
 };
 
@@ -392,7 +437,7 @@ __device__ __forceinline__ void h_plain(const StepArgs<S, T>& a, const size_t c,
                                         const T (&ey1)[Vec<T>::W], const T (&ez)[Vec<T>::W],
                                         const T (&exj)[Vec<T>::W], const T (&ezj)[Vec<T>::W], const T eyn,
                                         const T ezn, T (&hx)[Vec<T>::W], T (&hy)[Vec<T>::W], T (&hz)[Vec<T>::W],
-                                        const T (&idx)[Vec<T>::W], const T idy, const T idz) {
+                                        const T (&idx)[Vec<T>::W], const T idy, const T idz, const unsigned step) {
     constexpr int W = Vec<T>::W;
     const T bH = a.bH;
 #pragma unroll
@@ -409,9 +454,9 @@ __device__ __forceinline__ void h_plain(const StepArgs<S, T>& a, const size_t c,
         hy[e] = hy[e] - bH * (dEx_dz - dEz_dx);
         hz[e] = hz[e] - bH * (dEy_dx - dEx_dy);
     }
-    Fld<S, T>::st(a.Hx + c, hx);
-    Fld<S, T>::st(a.Hy + c, hy);
-    Fld<S, T>::st(a.Hz + c, hz);
+    st_field(a, a.Hx, c, hx, 3, step);
+    st_field(a, a.Hy, c, hy, 4, step);
+    st_field(a, a.Hz, c, hz, 5, step);
 }
 
 template <typename S, typename T>
@@ -421,7 +466,8 @@ __device__ __forceinline__ void e_plain(const StepArgs<S, T>& a, const size_t c,
                                         const T (&hy)[Vec<T>::W], const T (&hz)[Vec<T>::W],
                                         const T (&hzj)[Vec<T>::W], const T (&hxj)[Vec<T>::W],
                                         const T (&hxm)[Vec<T>::W], const T (&hym)[Vec<T>::W], const T hzp,
-                                        const T hyp, const T (&idx)[Vec<T>::W], const T idy, const T idz) {
+                                        const T hyp, const T (&idx)[Vec<T>::W], const T idy, const T idz,
+                                        const unsigned step) {
     constexpr int W = Vec<T>::W;
 #pragma unroll
     for (int e = 0; e < W; ++e) {
@@ -437,9 +483,9 @@ __device__ __forceinline__ void e_plain(const StepArgs<S, T>& a, const size_t c,
         ey[e] = ey[e] + by[e] * (dHx_dz - dHz_dx);
         ez[e] = ez[e] + bz[e] * (dHy_dx - dHx_dy);
     }
-    Fld<S, T>::st(a.Ex + c, ex);
-    Fld<S, T>::st(a.Ey + c, ey);
-    Fld<S, T>::st(a.Ez + c, ez);
+    st_field(a, a.Ex, c, ex, 0, step);
+    st_field(a, a.Ey, c, ey, 1, step);
+    st_field(a, a.Ez, c, ez, 2, step);
 }
 
 // ---------------------------------------------------------------------------------
@@ -470,7 +516,8 @@ struct HPipe {
 
 template <typename S, typename T, bool EDGE, bool PIPE = false>
 __device__ __forceinline__ void h_column(const StepArgs<S, T>& a, const SweepGeom& g, const int j, const int i0,
-                                         const bool act, const int kb, const int ke, const int lane) {
+                                         const bool act, const int kb, const int ke, const int lane,
+                                         const unsigned step) {
     constexpr int W = Vec<T>::W;
     const int np = a.np, np2 = 2 * np;
     const T bH = a.bH;
@@ -588,7 +635,7 @@ __device__ __forceinline__ void h_column(const StepArgs<S, T>& a, const SweepGeo
             if (!nload) { eyn = sy; ezn = sz; }
         }
         if (plain_row && !zpml) {
-            h_plain<S, T>(a, c, ex0, ex1, ey0, ey1, ez, exj, ezj, eyn, ezn, hx, hy, hz, idx, idy, idz);
+            h_plain<S, T>(a, c, ex0, ex1, ey0, ey1, ez, exj, ezj, eyn, ezn, hx, hy, hz, idx, idy, idz, step);
 #pragma unroll
             for (int e = 0; e < W; ++e) { ex0[e] = ex1[e]; ey0[e] = ey1[e]; }
             continue;
@@ -625,9 +672,9 @@ __device__ __forceinline__ void h_column(const StepArgs<S, T>& a, const SweepGeo
             hz[e] = hz[e] - bH * (dEy_dx - dEx_dy);
         }
         if (act) {
-            Fld<S, T>::st(a.Hx + c, hx);
-            Fld<S, T>::st(a.Hy + c, hy);
-            Fld<S, T>::st(a.Hz + c, hz);
+            st_field(a, a.Hx, c, hx, 3, step);
+            st_field(a, a.Hy, c, hy, 4, step);
+            st_field(a, a.Hz, c, hz, 5, step);
             if (zpml) { Fld<S, T>::st(a.psiH[1] + zs, pxz); Fld<S, T>::st(a.psiH[2] + zs, pyz); }
             if (ypml) { Fld<S, T>::st(a.psiH[0] + ys, pxy); Fld<S, T>::st(a.psiH[5] + ys, pzy); }
             if (xpml) xpsi_store<S, T>(a.psiH[3], a.psiH[4], a, k, j, i0, 0, a.NxT - 1, x3, x4);
@@ -640,7 +687,7 @@ __device__ __forceinline__ void h_column(const StepArgs<S, T>& a, const SweepGeo
 // One block of the H sweep: block (bx, by, bz) of the solve's launch grid.
 template <typename S, typename T, bool PIPE = false>
 __device__ __forceinline__ void update_H_block(const StepArgs<S, T>& a, const int kchunk, const SweepGeom& g,
-                                               const int bx, const int by, const int bz) {
+                                               const int bx, const int by, const int bz, const unsigned step) {
     constexpr int W = Vec<T>::W;
     if (*a.status) return;
     const int lane = threadIdx.x;
@@ -651,7 +698,7 @@ __device__ __forceinline__ void update_H_block(const StepArgs<S, T>& a, const in
         const int j = by * kBlockY + threadIdx.y;
         if (j >= a.NyT - 1) return;  // whole warp: a warp is one row
         const int i0 = g.xi0 + (bx * 32 + lane) * W;
-        h_column<S, T, false, PIPE>(a, g, j, i0, i0 < g.xi1, kb, ke, lane);
+        h_column<S, T, false, PIPE>(a, g, j, i0, i0 < g.xi1, kb, ke, lane, step);
     } else {
         const int t = threadIdx.y * 32 + lane;
         const int rr = t / g.ne, v = t - rr * g.ne;
@@ -659,7 +706,7 @@ __device__ __forceinline__ void update_H_block(const StepArgs<S, T>& a, const in
         if (rr >= g.er || j >= a.NyT - 1) return;
         const int i0 = v < g.nl ? v * W : g.xi1 + (v - g.nl) * W;
         if (i0 >= a.NxT) return;
-        h_column<S, T, true>(a, g, j, i0, true, kb, ke, lane);
+        h_column<S, T, true>(a, g, j, i0, true, kb, ke, lane, step);
     }
 }
 
@@ -667,8 +714,8 @@ __device__ __forceinline__ void update_H_block(const StepArgs<S, T>& a, const in
 // PIPE: interior columns stage their planes in shared memory (HPipe::bytes() dynamic).
 template <typename S, typename T, bool PIPE = false>
 __global__ void __launch_bounds__(32 * kBlockY, 2)
-k_update_H(const StepArgs<S, T> a, const int kchunk, const SweepGeom g) {
-    update_H_block<S, T, PIPE>(a, kchunk, g, blockIdx.x, blockIdx.y, blockIdx.z);
+k_update_H(const StepArgs<S, T> a, const int kchunk, const SweepGeom g, const unsigned step) {
+    update_H_block<S, T, PIPE>(a, kchunk, g, blockIdx.x, blockIdx.y, blockIdx.z, step);
 }
 
 // ---------------------------------------------------------------------------------
@@ -833,7 +880,7 @@ __device__ __forceinline__ void e_column(const StepArgs<S, T>& a, const SweepGeo
         }
         const bool gplane = grow && k >= a.gk0 && k < a.gk0 + a.gZ;
         if (plain_row && !zpml && !gplane && !src_in_vector<SH>(src, i0, j, k, W)) {
-            e_plain<S, T>(a, c, ex, ey, ez, bx, by, bz, hx, hy, hz, hzj, hxj, hxm, hym, hzp, hyp, idx, idy, idz);
+            e_plain<S, T>(a, c, ex, ey, ez, bx, by, bz, hx, hy, hz, hzj, hxj, hxm, hym, hzp, hyp, idx, idy, idz, src.step);
 #pragma unroll
             for (int e = 0; e < W; ++e) { hxm[e] = hx[e]; hym[e] = hy[e]; }
             continue;
@@ -916,9 +963,9 @@ __device__ __forceinline__ void e_column(const StepArgs<S, T>& a, const SweepGeo
             }
         }
         if (act) {
-            Fld<S, T>::st(a.Ex + c, ex);
-            Fld<S, T>::st(a.Ey + c, ey);
-            Fld<S, T>::st(a.Ez + c, ez);
+            st_field(a, a.Ex, c, ex, 0, src.step);
+            st_field(a, a.Ey, c, ey, 1, src.step);
+            st_field(a, a.Ez, c, ez, 2, src.step);
             if (zpml) { Fld<S, T>::st(a.psiE[1] + zs, pxz); Fld<S, T>::st(a.psiE[2] + zs, pyz); }
             if (ypml) { Fld<S, T>::st(a.psiE[0] + ys, pxy); Fld<S, T>::st(a.psiE[5] + ys, pzy); }
             if (xpml) xpsi_store<S, T>(a.psiE[3], a.psiE[4], a, k, j, i0, 1, a.NxT, x3, x4);
@@ -1008,7 +1055,7 @@ k_step_slabs(const StepArgs<S, T> a, const ESrc src, const SweepGeom g, const Sl
             else { isH = false; slab = pair; r = pair < p.nslab - 1 ? r2 - p.nH : r2; }
         }
         if (isH) {
-            update_H_block<S, T>(a, p.P, g, r % p.gxH, r / p.gxH, slab);
+            update_H_block<S, T>(a, p.P, g, r % p.gxH, r / p.gxH, slab, src.step);
             __threadfence();  // this thread's H stores, before the block signals
             __syncthreads();
             if (tid == 0) atomicAdd(hdone + slab, 1u);

@@ -511,7 +511,8 @@ __device__ __forceinline__ const StepArgs<S, float>& bargs(int r) {
 template <typename S, bool PIPE>
 __global__ void __launch_bounds__(32 * kBlockY, 2) k_update_H_multi(const int4* __restrict__ tab) {
     const int4 e = tab[blockIdx.x];
-    update_H_block<S, float, PIPE>(bargs<S>(e.x), c_bsolve[e.x].kchunkH, c_bsolve[e.x].g, e.y, e.z, e.w);
+    update_H_block<S, float, PIPE>(bargs<S>(e.x), c_bsolve[e.x].kchunkH, c_bsolve[e.x].g, e.y, e.z, e.w,
+                                   c_btick[e.x].src.step);
 }
 
 // SH / MAT: the blocks of solves with plane-wave sheets / an indexed material; the table lists
@@ -616,6 +617,7 @@ double field_scale_of(const fdtd_setup_v1& s, bool fp16) {
 // of the neighbours' planes.  A whole solve: kz0 = 0, NzG = NzT, own = [0, NzT).
 struct ShardSpec {
     int kz0 = 0, NzG = 0, own0 = 0, own1 = 0;
+    double psi_dx = 0;  // 16-bit storage: the whole solve's smallest cell edge (0: this grid's)
 };
 
 class SolverBase {
@@ -696,7 +698,7 @@ private:
     void capture_movies();
     void write_point_samples();
     void capture_tls(uint64_t s);
-    void phase_H();
+    void phase_H(uint64_t s);
     void phase_E(uint64_t s, ESrc& src, bool monitor);
     void write_population_frame();
     void close_outputs() override;
@@ -747,6 +749,7 @@ private:
     }
     void src_step(ESrc& src, uint64_t s) const {
         src.parity = int(s & 1);
+        src.step = unsigned(s);
         for (int q = 0; q < src.n; ++q) {
             const fdtd_dipole_v1& d = dip_[q];
             src.J[q] = fdtd::current_density(d.waveform, s, dt_, d.I0, d.f0, d.tau, d.t0, d.t_shift, d.cell_area) *
@@ -993,8 +996,10 @@ Solver<S, T>::Solver(const fdtd_setup_v1& s, int dev, const ShardSpec* shard) {
         psi_dx = *std::min_element(s.dx, s.dx + NxT_);
         psi_dx = std::min(psi_dx, *std::min_element(s.dy, s.dy + NyT_));
         psi_dx = std::min(psi_dx, *std::min_element(s.dz, s.dz + NzT_));
+        if (shard_.psi_dx > 0) psi_dx = shard_.psi_dx;  // a shard scales psi as the whole solve
     }
     a.psc = T(1.0 / psi_dx);
+    a.sr = std::is_same_v<S, __nv_bfloat16> && s.rounding == FDTD_ROUND_STOCHASTIC;
     const int Ns[3] = {NxT_, NyT_, NzT_};
     for (int ax = 0; ax < 3; ++ax) {
         const int n = Ns[ax];
@@ -1561,8 +1566,8 @@ void Solver<S, T>::run(uint64_t n) {
             if (per_kernel) ck(cudaEventRecord(ev_[1], st_), "cudaEventRecord");
             launches += 1;
         } else {
-            if (hpipe_) k_update_H<S, T, true><<<gridH_, blk, HPipe::bytes(), st_>>>(a_, kchunkH_, geom_);
-            else k_update_H<S, T><<<gridH_, blk, 0, st_>>>(a_, kchunkH_, geom_);
+            if (hpipe_) k_update_H<S, T, true><<<gridH_, blk, HPipe::bytes(), st_>>>(a_, kchunkH_, geom_, src.step);
+            else k_update_H<S, T><<<gridH_, blk, 0, st_>>>(a_, kchunkH_, geom_, src.step);
             if (per_kernel) ck(cudaEventRecord(ev_[1], st_), "cudaEventRecord");
             const size_t smem = pipe_ ? (a_.bidx ? EPipe<true>::bytes() : EPipe<false>::bytes()) : 0;
             e_kernel(src.ns != 0)<<<gridE_, blk, smem, st_>>>(a_, kchunkE_, src, geom_);
@@ -1629,10 +1634,10 @@ void Solver<S, T>::run(uint64_t n) {
 
 // ---- the phases of one step, for the sharded stepper (run() keeps its own loop)
 template <typename S, typename T>
-void Solver<S, T>::phase_H() {
+void Solver<S, T>::phase_H(uint64_t s) {
     const dim3 blk(32, kBlockY);
-    if (hpipe_) k_update_H<S, T, true><<<gridH_, blk, HPipe::bytes(), st_>>>(a_, kchunkH_, geom_);
-    else k_update_H<S, T><<<gridH_, blk, 0, st_>>>(a_, kchunkH_, geom_);
+    if (hpipe_) k_update_H<S, T, true><<<gridH_, blk, HPipe::bytes(), st_>>>(a_, kchunkH_, geom_, unsigned(s));
+    else k_update_H<S, T><<<gridH_, blk, 0, st_>>>(a_, kchunkH_, geom_, unsigned(s));
     ++launches;
 }
 
@@ -2432,6 +2437,10 @@ Sharded<S, T>::Sharded(const fdtd_setup_v1& s, int n, const int* devices) {
     device = devices ? devices[0] : 0;
     const bool fp16 = std::is_same_v<S, __half>;
     const double sE = field_scale_of(s, fp16);  // one scale for all shards
+    // and one psi scale (16-bit storage): the smallest cell edge of the whole grid
+    double psi_dx = *std::min_element(s.dx, s.dx + NxT_);
+    psi_dx = std::min(psi_dx, *std::min_element(s.dy, s.dy + NyT_));
+    psi_dx = std::min(psi_dx, *std::min_element(s.dz, s.dz + NzT_));
     interval_ = s.monitor_interval;
     probe_at_.assign(s.n_probes, {-1, -1});
     for (int r = 0; r < n; ++r) {
@@ -2531,7 +2540,7 @@ Sharded<S, T>::Sharded(const fdtd_setup_v1& s, int n, const int* devices) {
         }
         v.n_probes = uint32_t(sl->probes.size());
         v.probes = sl->probes.data();
-        ShardSpec spec{lo, int(NzT_), z0 - lo, z1 - lo};
+        ShardSpec spec{lo, int(NzT_), z0 - lo, z1 - lo, psi_dx};
         part_.push_back(std::make_unique<Solver<S, T>>(v, devices ? devices[r] : 0, &spec));
         slice_.push_back(std::move(sl));
     }
@@ -2632,7 +2641,7 @@ void Sharded<S, T>::run(uint64_t n) {
             ck(cudaSetDevice(part_[r]->device), "cudaSetDevice");
             if (r + 1 < R) ck(cudaStreamWaitEvent(part_[r]->st_, evCpH_[r], 0), "cudaStreamWaitEvent");
             ck(cudaStreamWaitEvent(part_[r]->st_, evMon_[r], 0), "cudaStreamWaitEvent");
-            part_[r]->phase_H();
+            part_[r]->phase_H(s);
             ck(cudaEventRecord(evH_[r], part_[r]->st_), "cudaEventRecord");
         }
         // H of shard r's last plane -> shard r+1's bottom halo
@@ -2800,6 +2809,7 @@ namespace {
 // Why a setup view cannot be stepped, or nullptr.
 const char* setup_problem(const fdtd_setup_v1* s) {
     if (s->struct_size != sizeof(fdtd_setup_v1)) return "fdtd_setup_v1.struct_size mismatch";
+    if (s->rounding > FDTD_ROUND_STOCHASTIC) return "fdtd_setup_v1.rounding must be 0 (nearest) or 1 (stochastic)";
     // NyT is a grid dimension (z) of the layout-transpose kernels: at most 65535.
     if (s->NxT < 3 || s->NyT < 3 || s->NzT < 3 || s->NxT > (1u << 30) || s->NyT > 65535 || s->NzT > (1u << 30))
         return "grid dimensions out of range";

@@ -399,6 +399,112 @@ def sweep_bench(args):
     print(json.dumps(line))
 
 
+def ringdown(series, dt, t_from):
+    """Emission peak frequency (Hz; zero-padded FFT of the probe series after t_from, above
+    50 THz, parabolic interpolation of the peak bin), amplitude growth rate g (1/s; slope of
+    log RMS over windows of one period of the series band-passed to 0.7-1.3 f, E ~ exp(g t):
+    g < 0 decays) and Q = pi f / (-g)."""
+    import numpy as np
+    x = np.asarray(series, dtype=np.float64)[int(t_from / dt):]
+    tt = np.arange(len(x))
+    x = x - np.polyval(np.polyfit(tt, x, 1), tt)  # a static or drifting part is not the emission
+    nfft = 1 << (int(np.ceil(np.log2(len(x)))) + 3)
+    spec = np.abs(np.fft.rfft(x * np.hanning(len(x)), nfft))
+    k0 = int(np.ceil(50e12 * nfft * dt))  # the emission lies above 50 THz
+    k = int(np.argmax(spec[k0:])) + k0
+    if 1 <= k < len(spec) - 1:
+        a, b, c = np.log(spec[k - 1:k + 2] + 1e-300)
+        k = k + 0.5 * (a - c) / (a - 2 * b + c)
+    f = k / (nfft * dt)
+    # the band around the peak only (0.7 f .. 1.3 f): slow drifts and noise do not set the rate
+    X = np.fft.rfft(x)
+    fr = np.fft.rfftfreq(len(x), dt)
+    X[(fr < 0.7 * f) | (fr > 1.3 * f)] = 0
+    x = np.fft.irfft(X, len(x))
+    per = max(4, int(round(1.0 / (f * dt))))
+    nw = len(x) // per
+    rms = np.sqrt(np.mean(x[:nw * per].reshape(nw, per) ** 2, axis=1))
+    t = (np.arange(nw) + 0.5) * per * dt
+    cut = nw // 10  # the band-pass rings at both ends of the window
+    g = float(np.polyfit(t[cut:nw - cut], np.log(rms[cut:nw - cut] + 1e-300), 1)[0])
+    return float(f), g, (float(np.pi * f / -g) if g < 0 else None)
+
+
+def sweep_check(args):
+    """The sweep's fidelity check: 8 of its cavities (indices 0, 32, ..., 224 of the 256, same
+    pumps) in the packed engine, in each storage form of --check-forms, against FP64 single
+    solves, --check-steps steps each: emission peak frequency, ring-down (growth) rate, Q, and
+    the lasing threshold estimated from the growth rate's dependence on the pump (W_p where the
+    fitted growth rate reaches 0).  Forms: fp32, fp16, bf16 (round to nearest) and bf16sr
+    (BF16 with stochastic rounding of the E and H stores)."""
+    import numpy as np
+    rng = np.random.default_rng(4)
+    pumps = np.exp(rng.uniform(np.log(1e7), np.log(1e11), size=256))
+    idx = list(range(0, 256, 32))
+    n = args.check_steps
+    base = serving_job_text((80, 80, 48), n)
+    setups = [PKG.Setup.from_text(base.replace("PUMP_RATE = 1e9", f"PUMP_RATE = {float(pumps[q])!r}")) for q in idx]
+    dt = setups[0].view.dt
+    t_from = 4000 * dt  # after the source pulse (t0 + 3 tau = 64 fs)
+    t0 = time.perf_counter()
+    ref = []
+    for s in setups:
+        sol = PKG.Solver(s, precision=PKG.PREC_FP64)
+        sol.run(n)
+        ref.append((sol.probe_series()[:, 0], sol.dft(0)))
+        sol.close()
+    seconds = {"fp64_one_at_a_time": round(time.perf_counter() - t0, 2)}
+    ref_rd = [ringdown(r[0], dt, t_from) for r in ref]
+
+    def threshold(g):
+        w = np.array([float(pumps[q]) for q in idx])
+        slope, icpt = np.polyfit(w, np.asarray(g), 1)
+        th = -icpt / slope if slope > 0 else None
+        return float(th) if th is not None and w.min() <= th <= w.max() else None
+
+    forms = {}
+    for form in args.check_forms.split(","):
+        prec = {"fp32": PKG.PREC_FP32, "fp16": PKG.PREC_FP16, "bf16": PKG.PREC_BF16, "bf16sr": PKG.PREC_BF16}[form]
+        b = PKG.Batch(budget_bytes=150 << 30)
+        views = []
+        for s in setups:
+            v = PKG.SetupV1.from_buffer_copy(s.view)
+            v.precision = prec
+            v.rounding = 1 if form == "bf16sr" else 0
+            views.append(v)
+        t0 = time.perf_counter()
+        ts = [b.submit(s, n, view=v) for s, v in zip(setups, views)]
+        while any(b.state(t)[0] < PKG.JOB_DONE for t in ts):
+            b.run(256)
+        seconds[form + "_packed"] = round(time.perf_counter() - t0, 2)
+        got = [(b.probe_series(t)[:, 0], b.dft(t), b.state(t)[0]) for t in ts]
+        b.close()
+        rd = [ringdown(g[0], dt, t_from) for g in got]
+        forms[form] = {
+            "all_done": all(g[2] == PKG.JOB_DONE for g in got),
+            "max_peak_shift_THz": round(max(abs(a[0] - b_[0]) for a, b_ in zip(ref_rd, rd)) / 1e12, 5),
+            "growth_per_ps": [round(x[1] * 1e-12, 4) for x in rd],
+            "Q": [round(x[2], 1) if x[2] else None for x in rd],
+            "max_Q_rel_err": (max(abs(x[2] - r[2]) / r[2] for x, r in zip(rd, ref_rd)) if all(x[2] for x in rd) else None),
+            "max_dft_rel_err": max(float(np.linalg.norm(g[1] - r[1]) / np.linalg.norm(r[1])) for g, r in zip(got, ref)),
+            "threshold_per_s": threshold([x[1] for x in rd]),
+        }
+    line = {
+        "metric": "sweep fidelity: packed 16-bit storage vs FP64 on 8 cavities (max Q rel. error)", "unit": "rel. error",
+        "value": forms[args.check_forms.split(",")[0]]["max_Q_rel_err"], "n_gpus": 1, "steps": n, "warmup": 0,
+        "higher_is_better": False, "vs_baseline": None, "dtype": "storage forms vs f64", "data": "synthetic",
+        "config": {"workload": "8 of the sweep's 256 gain-slab microcavities of 96x96x64 cells (indices 0, 32, ..., 224)",
+                   "steps_per_job": n, "window_from_step": 4000, "pumps_per_s": [float(pumps[q]) for q in idx]},
+        "fp64": {"peak_THz": [round(r[0] / 1e12, 4) for r in ref_rd], "growth_per_ps": [round(r[1] * 1e-12, 4) for r in ref_rd],
+                 "Q": [round(r[2], 1) if r[2] else None for r in ref_rd],
+                 "threshold_per_s": threshold([r[1] for r in ref_rd])},
+        "forms": forms,
+        "threshold_note": "null: the growth rate does not reach 0 inside the swept pump range (tau21 = 1 ns >> window)",
+        "seconds": seconds,
+    }
+    print(json.dumps(line))
+
+
 def precision_study(args):
     """The 512^3 sphere solve (or --workload's) for --study-steps steps as FP64, FP32, FP16 and
     BF16 storage: field L2 (E and H), probe series, DFT and DFT-peak errors against FP64."""
@@ -457,6 +563,10 @@ def main():
     ap.add_argument("--sweep-jobs", type=int, default=256)
     ap.add_argument("--sweep-steps", type=int, default=1000, help="steps per cavity (the full sweep is 200000)")
     ap.add_argument("--sweep-probe-steps", type=int, default=200)
+    ap.add_argument("--sweep-check", action="store_true",
+                    help="the sweep's BF16 cavities against FP64 on 8 of them: peak, ring-down, Q (own JSON line)")
+    ap.add_argument("--check-steps", type=int, default=20000)
+    ap.add_argument("--check-forms", default="bf16,bf16sr,fp16,fp32")
     ap.add_argument("--precision-study", action="store_true",
                     help="FP64 / FP32 / FP16 / BF16 errors on --workload (own JSON line)")
     ap.add_argument("--study-steps", type=int, default=5000)
@@ -477,6 +587,11 @@ def main():
     if args.precision_study and args.impl != "reference":
         if rank == 0:
             precision_study(args)
+        return
+
+    if args.sweep_check and args.impl != "reference":
+        if rank == 0:
+            sweep_check(args)
         return
 
     if args.sweep and args.impl != "reference":

@@ -172,7 +172,15 @@ typedef struct fdtd_setup_v1 {
     uint32_t n_bE_rows;
     const double *bE_rows;
     const uint16_t *bE_index;
+    /* Rounding of the E and H stores with BF16 storage: FDTD_ROUND_NEAREST (0, the default) or
+     * FDTD_ROUND_STOCHASTIC (1: up or down at random, with probability given by the distance
+     * to the two neighbouring BF16 values, so the rounding error is zero on average; keyed by
+     * cell, array and step, so a solve's result does not depend on its launch shape, sharding
+     * or packing).  Other storage forms round to nearest whatever this holds.  No counterpart
+     * in the reference, which stores FP64. */
+    uint32_t rounding;
 } fdtd_setup_v1;
+enum { FDTD_ROUND_NEAREST = 0, FDTD_ROUND_STOCHASTIC = 1 };
 
 /* Diagnostics of the most recent monitor step, FP64 device reductions
  * (StabilityMonitor + compute_integrated_* + PolarizationDiagnostics). */

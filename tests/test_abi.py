@@ -38,6 +38,16 @@ def test_parse_error_reports_message(pkg):
     assert "outside the field grid" in str(e.value)
 
 
+def test_rounding_key(pkg):
+    """ROUNDING (build-only key): nearest (default) or stochastic, carried by the setup view."""
+    text = "MESH_MODE = 0\nNX = 12\nNY = 12\nNZ = 12\nCPML_NPML = 2\nPRECISION = bf16\n"
+    assert pkg.Setup.from_text(text).view.rounding == 0
+    assert pkg.Setup.from_text(text + "ROUNDING = stochastic\n").view.rounding == 1
+    with pytest.raises(pkg.FdtdError) as e:
+        pkg.Setup.from_text(text + "ROUNDING = up\n")
+    assert e.value.code == 6 and "ROUNDING" in str(e.value)
+
+
 def test_unknown_setup_array_is_an_error(pkg):
     s = pkg.Setup.from_file(pkg.config_path("c0_dipole_sphere.params"), mesh_only=True)
     with pytest.raises(pkg.FdtdError):

@@ -159,6 +159,7 @@ MIXED = [  # (setup source, overrides, steps, precision): all three storage form
     (GOLDEN / "cases" / "step_g2_planewave.params", {}, 90, 2),
     ("c0_dipole_sphere.params", {}, 300, 0),
     ("c1_gain_slab.params", {"PUMP_RATE": "1e9"}, 210, 3),
+    ("c1_gain_slab.params", {"PUMP_RATE": "1e9", "ROUNDING": "stochastic"}, 200, 3),
 ]
 
 

@@ -477,3 +477,45 @@ def test_staged_sweeps_match_direct_loads(pkg, precision, tol, case, monkeypatch
         out.append(fields(sol))
         sol.close()
     assert field_rel_l2(out[0], out[1], "E") <= tol and field_rel_l2(out[0], out[1], "H") <= tol
+
+
+def _bf16_run(pkg, s, rounding, steps, path=1):
+    v = pkg.SetupV1.from_buffer_copy(s.view)
+    v.rounding = rounding
+    sol = pkg.Solver(s, precision=3, view=v, kernel_path=path)
+    sol.run(steps)
+    out = (fields(sol), sol.dft(0), sol.diagnostics())
+    sol.close()
+    return out
+
+
+def test_bf16_stochastic_rounding_is_deterministic_and_active(pkg):
+    """ROUNDING = stochastic: the same solve twice gives the same fields (the random bits are a
+    hash of cell, array and step); the fields differ from round-to-nearest; the kernel paths
+    (two sweeps, slab-ordered step) round alike."""
+    s = pkg.Setup.from_file(GOLDEN / "cases" / "step_g1_gain.params")
+    a = _bf16_run(pkg, s, 1, 60)
+    b = _bf16_run(pkg, s, 1, 60)
+    c = _bf16_run(pkg, s, 0, 60)
+    d = _bf16_run(pkg, s, 1, 60, path=2)
+    for k in FIELDS:
+        assert np.array_equal(a[0][k], b[0][k]), k
+    assert any(not np.array_equal(a[0][k], c[0][k]) for k in FIELDS)
+    assert field_rel_l2(a[0], c[0], "E") <= 2e-2
+    assert field_rel_l2(a[0], d[0], "E") <= 2e-2 and field_rel_l2(a[0], d[0], "H") <= 2e-2
+
+
+# Measured (one B200): on the 80^3 sphere and the gain slab stochastic rounding keeps the DFT
+# within the round-to-nearest bars of test_16bit_storage_spectrum.
+@pytest.mark.parametrize("cfg,tol", [("c0_dipole_sphere.params", 6e-3), ("c1_gain_slab.params", 1e-2)])
+def test_bf16_stochastic_rounding_spectrum(pkg, cfg, tol):
+    overrides = {"PUMP_RATE": "0"} if cfg.startswith("c1") else {}
+    s = pkg.Setup.from_file(pkg.config_path(cfg), overrides=overrides)
+    sol = pkg.Solver(s, precision=1)
+    sol.run(2000)
+    d64 = sol.dft(0)
+    sol.close()
+    _, d16, g16 = _bf16_run(pkg, s, 1, 2000)
+    assert g16["nan_flags"] == 0 and g16["stable"] == 1
+    assert np.argmax(np.abs(d16)) == np.argmax(np.abs(d64))
+    assert rel(d16, d64) <= tol

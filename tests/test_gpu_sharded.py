@@ -40,7 +40,7 @@ def run(pkg, s, precision, shards, steps):
 
 @pytest.mark.parametrize("case,shards", [("step_g1_gain", 2), ("step_g1_gain", 3), ("step_g2_planewave", 2),
                                          ("step_g2_planewave", 4), ("c0_dipole_sphere.params", 3)])
-@pytest.mark.parametrize("precision", [1, 0])
+@pytest.mark.parametrize("precision", [1, 0, 3])
 def test_sharded_matches_whole_solve(pkg, case, shards, precision):
     s = setup_for(pkg, case)
     whole = run(pkg, s, precision, 1, 40)
@@ -72,3 +72,20 @@ def test_sharded_refusals(pkg):
     sol.close()
     with pytest.raises(pkg.FdtdError):
         pkg.Solver(s, shards=40)  # fewer than 3 planes per shard
+
+
+@pytest.mark.parametrize("case,shards", [("step_g1_gain", 3), ("c0_dipole_sphere.params", 2)])
+def test_sharded_bf16_stochastic_rounding_matches_whole_solve(pkg, case, shards):
+    """BF16 storage with stochastic rounding: the rounding is keyed by the global cell, so the
+    shards round every value as the whole solve does -- bit-identical fields and results."""
+    s = setup_for(pkg, case)
+    v = pkg.SetupV1.from_buffer_copy(s.view)
+    v.rounding = 1
+    out = []
+    for n in (1, shards):
+        sol = pkg.Solver(s, precision=3, shards=n, view=v)
+        sol.run(30)
+        out.append({c: sol.field(c) for c in FIELDS})
+        sol.close()
+    for c in FIELDS:
+        assert np.array_equal(out[0][c], out[1][c]), c
