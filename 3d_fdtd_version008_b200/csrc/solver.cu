@@ -924,6 +924,7 @@ Solver<S, T>::Solver(const fdtd_setup_v1& s, int dev, const ShardSpec* shard) {
     // are made here from the arrays.
     std::vector<std::array<double, 3>> rows;
     std::vector<uint16_t> rid;
+    const uint16_t* hidx = nullptr;  // the host index (the view's, or rid)
     const char* mi = std::getenv("FDTD_B200_MATERIAL_INDEX");
     const bool want_index = !(mi && std::string(mi) == "0");
     bool have_index = false;
@@ -931,15 +932,16 @@ Solver<S, T>::Solver(const fdtd_setup_v1& s, int dev, const ShardSpec* shard) {
         rows.resize(s.n_bE_rows);
         for (uint32_t r = 0; r < s.n_bE_rows; ++r)
             for (int c = 0; c < 3; ++c) rows[r][c] = s.bE_rows[3 * size_t(r) + c];
-        rid.resize((N + 3) / 4 * 4, 0);
-        std::memcpy(rid.data(), s.bE_index, N * sizeof(uint16_t));
+        hidx = s.bE_index;
+        const uint32_t nr = s.n_bE_rows;
         uint16_t bad = 0;
 #pragma omp parallel for reduction(| : bad) schedule(static)
-        for (long long q = 0; q < (long long)N; ++q) bad |= uint16_t(rid[q] >= s.n_bE_rows);
+        for (long long q = 0; q < (long long)N; ++q) bad |= uint16_t(hidx[q] >= nr);
         if (bad) throw Failure(FDTD_ERR_INVALID, "bE_index holds a row number >= n_bE_rows");
         have_index = true;
     } else if (want_index) {
         have_index = fdtd::distinct_rows(s.bE, N, rows, rid);
+        hidx = rid.data();
     }
     if (have_index) {
         std::vector<T> tab(4 * rows.size(), T(0));
@@ -947,9 +949,17 @@ Solver<S, T>::Solver(const fdtd_setup_v1& s, int dev, const ShardSpec* shard) {
             for (int c = 0; c < 3; ++c) tab[4 * r + c] = T(rows[r][c] * (sH_ / sE_));
         a.btab = upload(tab);
         uint16_t* d_idx = alloc<uint16_t>(nflat_);
-        rid.resize((N + 3) / 4 * 4, 0);  // whole doubles for the staged copy
+        // the host index straight to the staging buffer as whole doubles, then the last N % 4
+        // values through a padded double
         double* sbuf = staging();
-        h2d(reinterpret_cast<const double*>(rid.data()), sbuf, rid.size() / 4);
+        const size_t whole = N / 4;
+        if (whole) h2d(reinterpret_cast<const double*>(hidx), sbuf, whole);
+        if (N % 4) {
+            uint16_t tail[4] = {0, 0, 0, 0};
+            std::memcpy(tail, hidx + 4 * whole, (N % 4) * sizeof(uint16_t));
+            ck(cudaMemcpyAsync(sbuf + whole, tail, sizeof(tail), cudaMemcpyHostToDevice, st_), "H2D");
+            ck(cudaStreamSynchronize(st_), "H2D");
+        }
         dim3 g((NzT_ + 31) / 32, (NxT_ + 31) / 32, NyT_), b(32, 8);
         k_index_from_idx3<<<g, b, 0, st_>>>(reinterpret_cast<const uint16_t*>(sbuf), d_idx, NxT_, NyT_, NzT_, NxP_);
         ++launches;
@@ -1065,6 +1075,7 @@ Solver<S, T>::Solver(const fdtd_setup_v1& s, int dev, const ShardSpec* shard) {
             a.gX = hi[0] - lo[0] + 1; a.gY = hi[1] - lo[1] + 1; a.gZ = hi[2] - lo[2] + 1;
             const size_t ng = size_t(a.gX) * a.gY * a.gZ;
             std::vector<int8_t> reg(ng);
+#pragma omp parallel for schedule(static)
             for (int k = 0; k < a.gZ; ++k)
                 for (int j = 0; j < a.gY; ++j)
                     for (int i = 0; i < a.gX; ++i)
