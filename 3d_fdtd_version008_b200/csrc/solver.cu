@@ -1942,10 +1942,11 @@ void Solver<S, T>::diagnostics(fdtd_diagnostics_v1* d) {
 
 namespace {
 // ==================================================================== packed multi-solve engine
-// A queue of FP32 solves served by one GPU: jobs wait until their device footprint fits the
-// budget and a slot is free, then stay resident (fields, CPML psi, gain state, probes in HBM)
-// until their last step, while every step of every resident solve is issued as one packed
-// H launch, one packed E launch, one probe launch and (on monitor steps) one monitor pair.
+// A queue of solves (FP32, FP16 or BF16 storage, mixed) served by one GPU: jobs wait until
+// their device footprint fits the budget and a slot is free, then stay resident (fields, CPML
+// psi, gain state, probes in HBM) until their last step, while every step of every resident
+// solve is issued as one packed H launch per storage form, one packed E launch per kind, one
+// probe launch and (on monitor steps) one monitor pair.
 // The per-cell arithmetic is the single-solve kernels' own, so a solve's result does not
 // depend on what it shares the GPU with.
 class Batch {
