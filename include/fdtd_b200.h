@@ -50,7 +50,7 @@ enum {
 /* ------------------------------------------------------------ enums */
 typedef enum {
     FDTD_PREC_FP32 = 0, /* fields, CPML psi and gain state stored and updated in FP32 */
-    FDTD_PREC_FP64 = 1, /* everything in FP64: the accuracy judge */
+    FDTD_PREC_FP64 = 1, /* everything in FP64: the accuracy reference */
     FDTD_PREC_FP16 = 2, /* E, H, CPML psi stored in FP16 as E / sE, H / sH (sH = sE / eta0),
                            arithmetic, material, gain state in FP32 */
     FDTD_PREC_BF16 = 3  /* the same with BF16 storage */

@@ -1,10 +1,10 @@
 """GPU parity: the CUDA stepper (called through the C ABI) against the reference's golden
 state and against the oracle on the shipped configs.
 
-Tolerances: FP64 mode <= 1e-12 relative L2 (the accuracy judge).  FP32 mode <= 1e-5
+Tolerances: FP64 mode <= 1e-12 relative L2 (the accuracy reference).  FP32 mode <= 1e-5
 relative L2 while the field is active; where the pulse has left the domain the bound is
-3x the drift of the oracle's FP32 twin (same formulas, FP32 storage), the floor any FP32
-storage reaches (precision)."""
+3x the drift of the oracle's FP32 twin (same formulas, FP32 storage): the floor any FP32
+storage reaches, since the decayed field is small against the rounding of its peak."""
 import sys
 
 import numpy as np
