@@ -46,6 +46,13 @@ def test_rounding_key(pkg):
     with pytest.raises(pkg.FdtdError) as e:
         pkg.Setup.from_text(text + "ROUNDING = up\n")
     assert e.value.code == 6 and "ROUNDING" in str(e.value)
+    # fdtd_create checks the view before it looks for a device
+    s = pkg.Setup.from_text(text)
+    v = pkg.SetupV1.from_buffer_copy(s.view)
+    v.rounding = 2
+    with pytest.raises(pkg.FdtdError) as e:
+        pkg.Solver(s, view=v)
+    assert e.value.code == 1 and "rounding" in str(e.value)
 
 
 def test_unknown_setup_array_is_an_error(pkg):
