@@ -481,6 +481,13 @@ class Batch:
             load_library().fdtd_batch_destroy(self._h)
             self._h = C.c_void_p()
 
+    # `with Batch(...) as b:` releases the device's engine even when the block raises
+    def __enter__(self) -> "Batch":
+        return self
+
+    def __exit__(self, *exc) -> None:
+        self.close()
+
     def __del__(self):
         try:
             self.close()
