@@ -16,6 +16,12 @@
 // array until the process exits.  Each call writes every record that it later reads, so
 // nothing needs clearing between calls; all calls share the one array, so calls that
 // overlap on the GPU (different streams, or different host threads on one device) race.
+//
+// The scratch address of a device is looked up once, at the first call on that device, and
+// kept for the life of the process; a caller that resets the device (cudaDeviceReset)
+// reloads the module, which may move the array, so the entry point must not be used across a
+// device reset.  Only FP32 and FP64 fields are scanned (16-bit storage keeps a field scale
+// that this entry point does not take).
 #include "../../include/fdtd_b200.h"
 
 #include <cuda_runtime.h>
@@ -138,8 +144,14 @@ extern "C" int fdtd_field_scan_noalloc(int precision, const void* ex, const void
                                           " cells exceed the scratch limit of " +
                                           std::to_string((unsigned long long)FDTD_FIELD_SCAN_MAX_CELLS) +
                                           " cells per call; scan in pieces");
+    // An error left pending by earlier work of the caller is reported as such, not as a
+    // failure of this scan, and is left in place for the caller.
+    cudaError_t e = cudaPeekAtLastError();
+    if (e != cudaSuccess)
+        return fail(FDTD_ERR_CUDA, std::string("fdtd_field_scan_noalloc: a CUDA error was already pending before the "
+                                               "call (nothing launched): ") + cudaGetErrorString(e));
     int dev = -1;
-    cudaError_t e = cudaGetDevice(&dev);
+    e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return fail(FDTD_ERR_NO_DEVICE, std::string("fdtd_field_scan_noalloc: ") + cudaGetErrorString(e));
     if (dev < 0 || dev >= kMaxDevices) return fail(FDTD_ERR_UNSUPPORTED, "fdtd_field_scan_noalloc: device ordinal out of range");
     void* scratch = nullptr;
@@ -169,8 +181,12 @@ extern "C" int fdtd_field_scan_noalloc(int precision, const void* ex, const void
             static_cast<const double*>(ex), static_cast<const double*>(ey), static_cast<const double*>(ez),
             static_cast<const double*>(hx), static_cast<const double*>(hy), static_cast<const double*>(hz),
             (long long)n, part);
+    e = cudaGetLastError();
+    if (e != cudaSuccess)
+        return fail(FDTD_ERR_CUDA, std::string("fdtd_field_scan_noalloc: launch of the partial scan: ") + cudaGetErrorString(e));
     k_field_scan_finish<<<1, kScanThreads, 0, st>>>(part, nblocks, out);
     e = cudaGetLastError();
-    if (e != cudaSuccess) return fail(FDTD_ERR_CUDA, std::string("fdtd_field_scan_noalloc: launch: ") + cudaGetErrorString(e));
+    if (e != cudaSuccess)
+        return fail(FDTD_ERR_CUDA, std::string("fdtd_field_scan_noalloc: launch of the final reduction: ") + cudaGetErrorString(e));
     return FDTD_OK;
 }

@@ -350,8 +350,11 @@ void fdtd_batch_destroy(fdtd_batch *b);
  * Nothing is allocated: the scratch is a fixed 256 KiB device array inside the library,
  * held on every GPU that loads the library until the process exits, which bounds n by
  * FDTD_FIELD_SCAN_MAX_CELLS (larger n: FDTD_ERR_INVALID with a message; scan in pieces).
+ * Only FP32 and FP64 fields (precision FDTD_PREC_FP32 / FDTD_PREC_FP64) are accepted.
  * The first call on each device (with that device current) looks up the array's device
- * address; make that first call before any stream capture.  All calls share the one
+ * address and keeps it for the life of the process; make that first call before any stream
+ * capture, and do not use the entry point across a cudaDeviceReset.  A CUDA error already
+ * pending when the call starts is refused with FDTD_ERR_CUDA and left pending.  All calls share the one
  * scratch array: calls that overlap on the GPU race and give wrong results -- serialise
  * them (one stream per device, or events).  Errors: fdtd_last_error(NULL). */
 #define FDTD_FIELD_SCAN_MAX_CELLS (16384ull * 16384ull)

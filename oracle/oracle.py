@@ -26,7 +26,9 @@ ORACLE_DIR = pathlib.Path(__file__).resolve().parent
 ORACLE_LIB = ORACLE_DIR / "lib" / "libfdtd_oracle.so"
 REF_HARNESS = ORACLE_DIR / "_ref" / "ref_harness"
 REF_HARNESS_NATIVE = ORACLE_DIR / "_ref" / "ref_harness_native"
-REF_SRC = pathlib.Path("/root/reference/3D_FDTD_version008/src")
+# Where the reference's headers lie (only in the build container; the GPU hosts use the
+# prebuilt harness): FDTD_REFERENCE_SRC, else the checkout's default location.
+REF_SRC = pathlib.Path(os.environ.get("FDTD_REFERENCE_SRC", "/root/reference/3D_FDTD_version008/src"))
 
 _dp = C.POINTER(C.c_double)
 
@@ -72,7 +74,7 @@ _lib = None
 def build(ref: bool = True) -> None:
     """Build the C restatement, and the reference harness when the reference is present."""
     targets = ["oracle"] + (["ref"] if ref and REF_SRC.exists() else [])
-    subprocess.run(["make", "-C", str(ORACLE_DIR), *targets], check=True, capture_output=True)
+    subprocess.run(["make", "-C", str(ORACLE_DIR), f"REF_SRC={REF_SRC}", *targets], check=True, capture_output=True)
 
 
 def lib():

@@ -93,3 +93,19 @@ def test_gpu_bake_fails_loudly_without_a_device(pkg):
         assert "CUDA device" in str(e)
     else:
         assert s.view.n_bE_rows > 0
+
+
+def test_noalloc_scan_refusals_need_no_device(pkg):
+    """fdtd_field_scan_noalloc checks its arguments before it touches a device: a precision
+    other than FP32/FP64, a null pointer, an empty scan and a scan beyond the fixed scratch
+    (FDTD_FIELD_SCAN_MAX_CELLS = 16384 x 16384 cells) are refused with FDTD_ERR_INVALID."""
+    limit = 16384 * 16384
+    cases = [(2, [1] * 6, 10, "precision"), (3, [1] * 6, 10, "precision"), (1, [1, 1, 0, 1, 1, 1], 10, "null"),
+             (0, [1] * 6, 0, "empty"), (1, [1] * 6, limit + 1, "limit")]
+    for precision, ptrs, n, word in cases:
+        with pytest.raises(pkg.FdtdError) as e:
+            pkg.field_scan_noalloc(precision, ptrs, n, 1)
+        assert e.value.code == pkg.FDTD_ERR_INVALID and word in str(e.value), (precision, n)
+    with pytest.raises(pkg.FdtdError) as e:
+        pkg.field_scan_noalloc(1, [1] * 6, 10, 0)
+    assert e.value.code == pkg.FDTD_ERR_INVALID

@@ -45,6 +45,29 @@ def test_noalloc_scan_matches_monitor_on_two_calls(pkg, precision):
 
 
 @pytest.mark.gpu
+def test_noalloc_scan_leaves_free_memory_unchanged(pkg):
+    """The property the entry point exists for: once the inputs and the result record are on
+    the device and a first call has loaded the kernels and looked up the scratch address,
+    further calls change the device's free memory by nothing."""
+    import torch
+    rng = np.random.default_rng(3)
+    n = 5 * 16384 + 11
+    dev = [torch.from_numpy(rng.normal(0, 1.0, n)).to("cuda:0") for _ in FIELDS]
+    out = torch.zeros(2, dtype=torch.float64, device="cuda:0")
+    stream = torch.cuda.current_stream().cuda_stream
+    ptrs = [t.data_ptr() for t in dev]
+    pkg.field_scan_noalloc(1, ptrs, n, out.data_ptr(), stream)
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    for _ in range(3):
+        pkg.field_scan_noalloc(1, ptrs, n, out.data_ptr(), stream)
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    assert free1 == free0
+    assert float(out[0].item()) == max(float(t.abs().max().item()) for t in dev[:3])
+
+
+@pytest.mark.gpu
 def test_noalloc_scan_flags_and_limit(pkg):
     import torch
     rng = np.random.default_rng(9)
