@@ -33,6 +33,8 @@ STATUS_NAMES = {
 }
 FDTD_ERR_INVALID = 1
 FDTD_ERR_UNSTABLE = 4
+FDTD_ERR_TIMEOUT = 5
+FDTD_ERR_UNSUPPORTED = 7
 FDTD_ERR_NO_DEVICE = 8
 PREC_FP32, PREC_FP64, PREC_FP16, PREC_BF16 = 0, 1, 2, 3
 TIMING_OFF, TIMING_RUN, TIMING_KERNELS = 0, 1, 2
@@ -382,7 +384,7 @@ class Solver:
         return {"steps": t.steps, "run_ms": t.run_ms, "h_ms": t.h_ms, "e_ms": t.e_ms, "aux_ms": t.aux_ms}
 
     def set_kernel_path(self, path: int) -> None:
-        """0 = fused H+E step, 1 = separate H and E sweeps (default); before the first step."""
+        """1 = separate H and E sweeps (default), 2 = slab-ordered step; before the first step (0 is refused)."""
         self._check(load_library().fdtd_set_kernel_path(self._h, int(path)), "fdtd_set_kernel_path")
 
     def synchronize(self) -> None:

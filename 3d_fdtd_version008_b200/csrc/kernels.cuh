@@ -189,13 +189,37 @@ template <> __device__ __forceinline__ double from_d<double>(double v) { return 
 template <> __device__ __forceinline__ __half from_d<__half>(double v) { return __double2half(v); }
 template <> __device__ __forceinline__ __nv_bfloat16 from_d<__nv_bfloat16>(double v) { return __double2bfloat16(v); }
 
+// Explicitly rounded arithmetic of the update formulas.  Every product, difference and
+// fused multiply-add of an update goes through one of these, so the compiler can neither
+// contract nor reassociate them: every instantiation of one update (the single-solve sweeps,
+// the packed engine, staged or direct loads, the slab-ordered step, any launch shape) gives
+// the same bits.
+__device__ __forceinline__ float add_rn(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ float sub_rn(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ float fma_rn(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+__device__ __forceinline__ float div_rn(float a, float b) { return __fdiv_rn(a, b); }
+__device__ __forceinline__ double add_rn(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double sub_rn(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double fma_rn(double a, double b, double c) { return __fma_rn(a, b, c); }
+__device__ __forceinline__ double div_rn(double a, double b) { return __ddiv_rn(a, b); }
+
+// One-sided difference quotient (b - a) * inv_d.
+template <typename T>
+__device__ __forceinline__ T dq(T b, T a, T inv_d) { return mul_rn(sub_rn(b, a), inv_d); }
+
+// CPML recursion psi = b * psi + c * d.
+template <typename T>
+__device__ __forceinline__ T psi_rec(T b, T psi, T c, T d) { return fma_rn(b, psi, mul_rn(c, d)); }
+
 // CPML: d_eff = d / kappa + psi.  With 16-bit storage psi is kept as psi * dx_min (the host
 // folds dx_min into the recursion's c coefficient) so it stays in the storage's range, and
 // is scaled back here by psc = 1 / dx_min; with S = T psi is stored as is.
 template <typename S, typename T>
 __device__ __forceinline__ T psi_eff(T d, T ik, T psi, T psc) {
-    if constexpr (sizeof(S) == sizeof(T)) return d * ik + psi;
-    else return d * ik + psi * psc;
+    if constexpr (sizeof(S) == sizeof(T)) return fma_rn(d, ik, psi);
+    else return fma_rn(d, ik, mul_rn(psi, psc));
 }
 
 // Per gain region constants (TwoLevelParams after finalize_with_dt), in compute type T.
@@ -380,15 +404,26 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
 
-// Shared-memory staging of the E sweep's interior columns: two planes (stages) of kSlots
-// 16-byte slots per thread, slot-major so that a warp's slots are consecutive.  Slots: 0-2 E,
-// 3-5 H, 6 Hz(j-1), 7 Hx(j-1), 8 the material (row ids or bEx), 9-10 bEy/bEz (arrays only),
-// last: Hz and Hy at i0-1 for the warp's first lane.
-template <bool MAT>
-struct EPipe {
-    static constexpr int kSlots = MAT ? 10 : 12;
+// Shared-memory staging of the sweeps' interior columns.  A slot holds one field vector of
+// one thread (SB bytes: 16 for 32/64-bit storage, 8 for 16-bit), slots are slot-major so a
+// warp's slots are consecutive, and kStages planes of slots form a ring: the thread copies
+// plane k + kStages - 1 while it computes plane k.  16-bit storage fills half the bytes of a
+// 16-byte slot, so it runs four stages (three planes in flight) in the shared memory that
+// 32/64-bit storage spends on two.
+template <typename S>
+struct PipeShape {
+    static constexpr int SB = sizeof(S) == 2 ? 8 : 16;
+    static constexpr int kStages = sizeof(S) == 2 ? 4 : 2;
+};
+
+// E sweep slots: 0-2 E, 3-5 H, 6 Hz(j-1), 7 Hx(j-1), 8 the material row ids, last: Hz and
+// Hy at i0-1 for the warp's first lane (at byte 0 and SB/2 of the slot).  Staging is used with
+// the row-indexed material only.
+template <typename S>
+struct EPipe : PipeShape<S> {
+    static constexpr int kSlots = 10;
     static constexpr int kX = kSlots - 1;
-    static constexpr size_t bytes() { return size_t(2) * kSlots * (32 * kBlockY) * 16; }
+    static constexpr size_t bytes() { return size_t(PipeShape<S>::kStages) * kSlots * (32 * kBlockY) * PipeShape<S>::SB; }
 };
 
 // True when a point source or (SH) a plane-wave sheet touches one of the W cells (i0.., j, k).
@@ -420,9 +455,9 @@ __device__ __forceinline__ void sheet_J(const ESrc& src, int i, int j, int k, T&
         else in = i == src.pl[s] && j >= src.lo0[s] && j <= src.hi0[s] && k >= src.lo1[s] && k <= src.hi1[s];
         if (in) {
             const T v = T(src.sJ[s]);
-            if (src.pc[s] == 0) Jx += v;
-            else if (src.pc[s] == 1) Jy += v;
-            else Jz += v;
+            if (src.pc[s] == 0) Jx = add_rn(Jx, v);
+            else if (src.pc[s] == 1) Jy = add_rn(Jy, v);
+            else Jz = add_rn(Jz, v);
         }
     }
 }
@@ -439,20 +474,20 @@ __device__ __forceinline__ void h_plain(const StepArgs<S, T>& a, const size_t c,
                                         const T ezn, T (&hx)[Vec<T>::W], T (&hy)[Vec<T>::W], T (&hz)[Vec<T>::W],
                                         const T (&idx)[Vec<T>::W], const T idy, const T idz, const unsigned step) {
     constexpr int W = Vec<T>::W;
-    const T bH = a.bH;
+    const T nbH = -a.bH;
 #pragma unroll
     for (int e = 0; e < W; ++e) {
         const T eyx = (e < W - 1) ? ey0[e + 1] : eyn;
         const T ezx = (e < W - 1) ? ez[e + 1] : ezn;
-        const T dEz_dy = (ezj[e] - ez[e]) * idy;
-        const T dEy_dz = (ey1[e] - ey0[e]) * idz;
-        const T dEx_dz = (ex1[e] - ex0[e]) * idz;
-        const T dEz_dx = (ezx - ez[e]) * idx[e];
-        const T dEy_dx = (eyx - ey0[e]) * idx[e];
-        const T dEx_dy = (exj[e] - ex0[e]) * idy;
-        hx[e] = hx[e] - bH * (dEz_dy - dEy_dz);
-        hy[e] = hy[e] - bH * (dEx_dz - dEz_dx);
-        hz[e] = hz[e] - bH * (dEy_dx - dEx_dy);
+        const T dEz_dy = dq(ezj[e], ez[e], idy);
+        const T dEy_dz = dq(ey1[e], ey0[e], idz);
+        const T dEx_dz = dq(ex1[e], ex0[e], idz);
+        const T dEz_dx = dq(ezx, ez[e], idx[e]);
+        const T dEy_dx = dq(eyx, ey0[e], idx[e]);
+        const T dEx_dy = dq(exj[e], ex0[e], idy);
+        hx[e] = fma_rn(nbH, sub_rn(dEz_dy, dEy_dz), hx[e]);
+        hy[e] = fma_rn(nbH, sub_rn(dEx_dz, dEz_dx), hy[e]);
+        hz[e] = fma_rn(nbH, sub_rn(dEy_dx, dEx_dy), hz[e]);
     }
     st_field(a, a.Hx, c, hx, 3, step);
     st_field(a, a.Hy, c, hy, 4, step);
@@ -473,15 +508,16 @@ __device__ __forceinline__ void e_plain(const StepArgs<S, T>& a, const size_t c,
     for (int e = 0; e < W; ++e) {
         const T hzx = (e > 0) ? hz[e - 1] : hzp;
         const T hyx = (e > 0) ? hy[e - 1] : hyp;
-        const T dHz_dy = (hz[e] - hzj[e]) * idy;
-        const T dHy_dz = (hy[e] - hym[e]) * idz;
-        const T dHx_dz = (hx[e] - hxm[e]) * idz;
-        const T dHz_dx = (hz[e] - hzx) * idx[e];
-        const T dHy_dx = (hy[e] - hyx) * idx[e];
-        const T dHx_dy = (hx[e] - hxj[e]) * idy;
-        ex[e] = ex[e] + bx[e] * (dHz_dy - dHy_dz);
-        ey[e] = ey[e] + by[e] * (dHx_dz - dHz_dx);
-        ez[e] = ez[e] + bz[e] * (dHy_dx - dHx_dy);
+        const T dHz_dy = dq(hz[e], hzj[e], idy);
+        const T dHy_dz = dq(hy[e], hym[e], idz);
+        const T dHx_dz = dq(hx[e], hxm[e], idz);
+        const T dHz_dx = dq(hz[e], hzx, idx[e]);
+        const T dHy_dx = dq(hy[e], hyx, idx[e]);
+        const T dHx_dy = dq(hx[e], hxj[e], idy);
+        // (curl - J) with J = 0 is the curl itself, bit for bit: the general path's result
+        ex[e] = fma_rn(bx[e], sub_rn(dHz_dy, dHy_dz), ex[e]);
+        ey[e] = fma_rn(by[e], sub_rn(dHx_dz, dHz_dx), ey[e]);
+        ez[e] = fma_rn(bz[e], sub_rn(dHy_dx, dHx_dy), ez[e]);
     }
     st_field(a, a.Ex, c, ex, 0, step);
     st_field(a, a.Ey, c, ey, 1, step);
@@ -507,11 +543,12 @@ struct SweepGeom {
 // 1/dz, the CPML psi of the vector) is issued before the first use of any of them, so a
 // vector costs one memory round trip per plane whatever slab it lies in.  EDGE columns
 // read the x-neighbour from memory (lanes hold other rows); interior columns shuffle it.
-// Shared-memory staging of the H sweep's interior columns (as EPipe): slots 0-1 Ex, Ey at k+1,
-// 2 Ez, 3 Ex(j+1), 4 Ez(j+1), 5-7 H, 8 Ey and Ez at i0+W for the lanes that load it.
-struct HPipe {
+// H sweep slots (as EPipe): 0-1 Ex, Ey at k+1, 2 Ez, 3 Ex(j+1), 4 Ez(j+1), 5-7 H, 8 Ey and Ez
+// at i0+W for the lanes that load it (at byte 0 and SB/2 of the slot).
+template <typename S>
+struct HPipe : PipeShape<S> {
     static constexpr int kSlots = 9;
-    static constexpr size_t bytes() { return size_t(2) * kSlots * (32 * kBlockY) * 16; }
+    static constexpr size_t bytes() { return size_t(PipeShape<S>::kStages) * kSlots * (32 * kBlockY) * PipeShape<S>::SB; }
 };
 
 template <typename S, typename T, bool EDGE, bool PIPE = false>
@@ -520,7 +557,7 @@ __device__ __forceinline__ void h_column(const StepArgs<S, T>& a, const SweepGeo
                                          const unsigned step) {
     constexpr int W = Vec<T>::W;
     const int np = a.np, np2 = 2 * np;
-    const T bH = a.bH;
+    const T nbH = -a.bH;
 
     T idx[W];
 #pragma unroll
@@ -549,30 +586,36 @@ __device__ __forceinline__ void h_column(const StepArgs<S, T>& a, const SweepGeo
     // PIPE (interior columns of k_update_H): this thread's planes come from shared memory,
     // filled by cp.async one plane ahead.
     extern __shared__ uint4 pipe_smem[];
-    constexpr int NT = 32 * kBlockY, NV = HPipe::kSlots;
+    constexpr int NT = 32 * kBlockY, NV = HPipe<S>::kSlots, SB = HPipe<S>::SB, NS = HPipe<S>::kStages;
     constexpr int VB = W * int(sizeof(S));
+    static_assert(VB <= SB, "a field vector fills at most one slot");
     constexpr int NB = sizeof(S) < 4 ? 4 : int(sizeof(S));
     const int tid = threadIdx.y * 32 + threadIdx.x;
     const bool xn = nload && i0 + W < a.NxT;
+    char* const pipe = reinterpret_cast<char*>(pipe_smem);
+    auto slot = [&](int stg, int q) { return pipe + ((size_t(stg) * NV + q) * NT + tid) * SB; };
     auto issue = [&](int kk, int stg) {
         const size_t cc = size_t(kk) * a.plane + row;
-        uint4* b = pipe_smem + size_t(stg) * NV * NT + tid;
-        cp_async<VB>(b + 0 * NT, a.Ex + cc + a.plane);
-        cp_async<VB>(b + 1 * NT, a.Ey + cc + a.plane);
-        cp_async<VB>(b + 2 * NT, a.Ez + cc);
-        cp_async<VB>(b + 3 * NT, a.Ex + cc + a.NxP);
-        cp_async<VB>(b + 4 * NT, a.Ez + cc + a.NxP);
-        cp_async<VB, false>(b + 5 * NT, a.Hx + cc);
-        cp_async<VB, false>(b + 6 * NT, a.Hy + cc);
-        cp_async<VB, false>(b + 7 * NT, a.Hz + cc);
+        cp_async<VB>(slot(stg, 0), a.Ex + cc + a.plane);
+        cp_async<VB>(slot(stg, 1), a.Ey + cc + a.plane);
+        cp_async<VB>(slot(stg, 2), a.Ez + cc);
+        cp_async<VB>(slot(stg, 3), a.Ex + cc + a.NxP);
+        cp_async<VB>(slot(stg, 4), a.Ez + cc + a.NxP);
+        cp_async<VB, false>(slot(stg, 5), a.Hx + cc);
+        cp_async<VB, false>(slot(stg, 6), a.Hy + cc);
+        cp_async<VB, false>(slot(stg, 7), a.Hz + cc);
         if (xn) {
-            cp_async<NB>(b + 8 * NT, a.Ey + cc + W);
-            cp_async<NB>(reinterpret_cast<char*>(b + 8 * NT) + 8, a.Ez + cc + W);
+            cp_async<NB>(slot(stg, 8), a.Ey + cc + W);
+            cp_async<NB>(slot(stg, 8) + SB / 2, a.Ez + cc + W);
         }
     };
     if constexpr (PIPE) {
-        if (act) issue(kb, 0);
-        cp_async_commit();
+        // planes kb .. kb + NS - 2 in flight before the loop
+#pragma unroll
+        for (int q = 0; q < NS - 1; ++q) {
+            if (act && kb + q < ke) issue(kb + q, q);
+            cp_async_commit();
+        }
     }
 
     for (int k = kb; k < ke; ++k) {
@@ -580,22 +623,23 @@ __device__ __forceinline__ void h_column(const StepArgs<S, T>& a, const SweepGeo
         T ex1[W], ey1[W], ez[W], exj[W], ezj[W], hx[W], hy[W], hz[W];
         T eye = T(0), eze = T(0);
         if (PIPE && act) {
-            if (k + 1 < ke) issue(k + 1, (k + 1 - kb) & 1);
+            // plane k + NS - 1 into the stage read last iteration, then wait for plane k
+            if (k + NS - 1 < ke) issue(k + NS - 1, (k + NS - 1 - kb) & (NS - 1));
             cp_async_commit();
-            cp_async_wait<1>();
-            const uint4* b = pipe_smem + size_t((k - kb) & 1) * NV * NT + tid;
-            Fld<S, T>::ld(reinterpret_cast<const S*>(b + 0 * NT), ex1);
-            Fld<S, T>::ld(reinterpret_cast<const S*>(b + 1 * NT), ey1);
-            Fld<S, T>::ld(reinterpret_cast<const S*>(b + 2 * NT), ez);
-            Fld<S, T>::ld(reinterpret_cast<const S*>(b + 3 * NT), exj);
-            Fld<S, T>::ld(reinterpret_cast<const S*>(b + 4 * NT), ezj);
-            Fld<S, T>::ld(reinterpret_cast<const S*>(b + 5 * NT), hx);
-            Fld<S, T>::ld(reinterpret_cast<const S*>(b + 6 * NT), hy);
-            Fld<S, T>::ld(reinterpret_cast<const S*>(b + 7 * NT), hz);
+            cp_async_wait<NS - 1>();
+            const int stg = (k - kb) & (NS - 1);
+            Fld<S, T>::ld(reinterpret_cast<const S*>(slot(stg, 0)), ex1);
+            Fld<S, T>::ld(reinterpret_cast<const S*>(slot(stg, 1)), ey1);
+            Fld<S, T>::ld(reinterpret_cast<const S*>(slot(stg, 2)), ez);
+            Fld<S, T>::ld(reinterpret_cast<const S*>(slot(stg, 3)), exj);
+            Fld<S, T>::ld(reinterpret_cast<const S*>(slot(stg, 4)), ezj);
+            Fld<S, T>::ld(reinterpret_cast<const S*>(slot(stg, 5)), hx);
+            Fld<S, T>::ld(reinterpret_cast<const S*>(slot(stg, 6)), hy);
+            Fld<S, T>::ld(reinterpret_cast<const S*>(slot(stg, 7)), hz);
             if (xn) {
-                const S* xs = reinterpret_cast<const S*>(b + 8 * NT);
-                eye = T(to_c(xs[0]));
-                eze = T(to_c(reinterpret_cast<const S*>(reinterpret_cast<const char*>(xs) + 8)[0]));
+                const char* xs = slot(stg, 8);
+                eye = T(to_c(reinterpret_cast<const S*>(xs)[0]));
+                eze = T(to_c(reinterpret_cast<const S*>(xs + SB / 2)[0]));
             }
         } else if (act) {
             Fld<S, T>::ldg(a.Ex + c + a.plane, ex1);
@@ -646,30 +690,30 @@ __device__ __forceinline__ void h_column(const StepArgs<S, T>& a, const SweepGeo
             if (i >= a.NxT - 1) continue;  // last x plane (and padding) never updated
             const T eyx = (e < W - 1) ? ey0[e + 1] : eyn;
             const T ezx = (e < W - 1) ? ez[e + 1] : ezn;
-            T dEz_dy = (ezj[e] - ez[e]) * idy;
-            T dEy_dz = (ey1[e] - ey0[e]) * idz;
-            T dEx_dz = (ex1[e] - ex0[e]) * idz;
-            T dEz_dx = (ezx - ez[e]) * idx[e];
-            T dEy_dx = (eyx - ey0[e]) * idx[e];
-            T dEx_dy = (exj[e] - ex0[e]) * idy;
+            T dEz_dy = dq(ezj[e], ez[e], idy);
+            T dEy_dz = dq(ey1[e], ey0[e], idz);
+            T dEx_dz = dq(ex1[e], ex0[e], idz);
+            T dEz_dx = dq(ezx, ez[e], idx[e]);
+            T dEy_dx = dq(eyx, ey0[e], idx[e]);
+            T dEx_dy = dq(exj[e], ex0[e], idy);
             if (ypml) {
-                pxy[e] = yb * pxy[e] + yc * dEz_dy; dEz_dy = psi_eff<S, T>(dEz_dy, yik, pxy[e], a.psc);
-                pzy[e] = yb * pzy[e] + yc * dEx_dy; dEx_dy = psi_eff<S, T>(dEx_dy, yik, pzy[e], a.psc);
+                pxy[e] = psi_rec(yb, pxy[e], yc, dEz_dy); dEz_dy = psi_eff<S, T>(dEz_dy, yik, pxy[e], a.psc);
+                pzy[e] = psi_rec(yb, pzy[e], yc, dEx_dy); dEx_dy = psi_eff<S, T>(dEx_dy, yik, pzy[e], a.psc);
             }
             if (zpml) {
-                pxz[e] = zb * pxz[e] + zc * dEy_dz; dEy_dz = psi_eff<S, T>(dEy_dz, zik, pxz[e], a.psc);
-                pyz[e] = zb * pyz[e] + zc * dEx_dz; dEx_dz = psi_eff<S, T>(dEx_dz, zik, pyz[e], a.psc);
+                pxz[e] = psi_rec(zb, pxz[e], zc, dEy_dz); dEy_dz = psi_eff<S, T>(dEy_dz, zik, pxz[e], a.psc);
+                pyz[e] = psi_rec(zb, pyz[e], zc, dEx_dz); dEx_dz = psi_eff<S, T>(dEx_dz, zik, pyz[e], a.psc);
             }
             if (xpml && in_pml(i, a.NxT, np)) {
                 const T b = __ldg(a.pbH[0] + i), cc = __ldg(a.pcH[0] + i), ik = __ldg(a.ik[0] + i);
-                x3[e] = b * x3[e] + cc * dEz_dx;
+                x3[e] = psi_rec(b, x3[e], cc, dEz_dx);
                 dEz_dx = psi_eff<S, T>(dEz_dx, ik, x3[e], a.psc);
-                x4[e] = b * x4[e] + cc * dEy_dx;
+                x4[e] = psi_rec(b, x4[e], cc, dEy_dx);
                 dEy_dx = psi_eff<S, T>(dEy_dx, ik, x4[e], a.psc);
             }
-            hx[e] = hx[e] - bH * (dEz_dy - dEy_dz);
-            hy[e] = hy[e] - bH * (dEx_dz - dEz_dx);
-            hz[e] = hz[e] - bH * (dEy_dx - dEx_dy);
+            hx[e] = fma_rn(nbH, sub_rn(dEz_dy, dEy_dz), hx[e]);
+            hy[e] = fma_rn(nbH, sub_rn(dEx_dz, dEz_dx), hy[e]);
+            hz[e] = fma_rn(nbH, sub_rn(dEy_dx, dEx_dy), hz[e]);
         }
         if (act) {
             st_field(a, a.Hx, c, hx, 3, step);
@@ -711,7 +755,7 @@ __device__ __forceinline__ void update_H_block(const StepArgs<S, T>& a, const in
 }
 
 // Two resident blocks per SM (at most 128 registers; a third block would spill).
-// PIPE: interior columns stage their planes in shared memory (HPipe::bytes() dynamic).
+// PIPE: interior columns stage their planes in shared memory (HPipe<S>::bytes() dynamic).
 template <typename S, typename T, bool PIPE = false>
 __global__ void __launch_bounds__(32 * kBlockY, 2)
 k_update_H(const StepArgs<S, T> a, const int kchunk, const SweepGeom g, const unsigned step) {
@@ -768,37 +812,39 @@ __device__ __forceinline__ void e_column(const StepArgs<S, T>& a, const SweepGeo
     // PIPE (interior columns of k_update_E): the plane's vectors come from this thread's
     // shared-memory slots, filled by cp.async one plane ahead.
     extern __shared__ uint4 pipe_smem[];
-    constexpr int NT = 32 * kBlockY, NV = EPipe<MAT>::kSlots, XS = EPipe<MAT>::kX;
+    constexpr int NT = 32 * kBlockY, NV = EPipe<S>::kSlots, XS = EPipe<S>::kX, SB = EPipe<S>::SB;
+    constexpr int NS = EPipe<S>::kStages;
     constexpr int VB = W * int(sizeof(S));                 // bytes of one field vector
+    static_assert(VB <= SB && 2 * W <= SB, "a field vector and the row ids fill at most one slot");
+    static_assert(!PIPE || MAT, "the staged E sweep takes the row-indexed material");
     constexpr int NB = sizeof(S) < 4 ? 4 : int(sizeof(S));  // x-neighbour copy (>= 4 bytes)
     constexpr int NE = NB / int(sizeof(S));                 // elements in it; the neighbour is the last
     const int tid = threadIdx.y * 32 + threadIdx.x;
+    char* const pipe = reinterpret_cast<char*>(pipe_smem);
+    auto slot = [&](int stg, int q) { return pipe + ((size_t(stg) * NV + q) * NT + tid) * SB; };
     auto issue = [&](int kk, int stg) {
         const size_t cc = size_t(kk) * a.plane + row;
-        uint4* b = pipe_smem + size_t(stg) * NV * NT + tid;
-        cp_async<VB, false>(b + 0 * NT, a.Ex + cc);
-        cp_async<VB, false>(b + 1 * NT, a.Ey + cc);
-        cp_async<VB, false>(b + 2 * NT, a.Ez + cc);
-        cp_async<VB>(b + 3 * NT, a.Hx + cc);
-        cp_async<VB>(b + 4 * NT, a.Hy + cc);
-        cp_async<VB>(b + 5 * NT, a.Hz + cc);
-        cp_async<VB>(b + 6 * NT, a.Hz + cc - a.NxP);
-        cp_async<VB>(b + 7 * NT, a.Hx + cc - a.NxP);
-        if constexpr (MAT) {
-            cp_async<2 * W>(b + 8 * NT, a.bidx + cc);
-        } else {
-            cp_async<W * int(sizeof(T)), false>(b + 8 * NT, a.bEx + cc);
-            cp_async<W * int(sizeof(T)), false>(b + 9 * NT, a.bEy + cc);
-            cp_async<W * int(sizeof(T)), false>(b + 10 * NT, a.bEz + cc);
-        }
+        cp_async<VB, false>(slot(stg, 0), a.Ex + cc);
+        cp_async<VB, false>(slot(stg, 1), a.Ey + cc);
+        cp_async<VB, false>(slot(stg, 2), a.Ez + cc);
+        cp_async<VB>(slot(stg, 3), a.Hx + cc);
+        cp_async<VB>(slot(stg, 4), a.Hy + cc);
+        cp_async<VB>(slot(stg, 5), a.Hz + cc);
+        cp_async<VB>(slot(stg, 6), a.Hz + cc - a.NxP);
+        cp_async<VB>(slot(stg, 7), a.Hx + cc - a.NxP);
+        cp_async<2 * W>(slot(stg, 8), a.bidx + cc);
         if (pload && i0 > 0) {
-            cp_async<NB>(b + XS * NT, a.Hz + cc - NE);
-            cp_async<NB>(reinterpret_cast<char*>(b + XS * NT) + 8, a.Hy + cc - NE);
+            cp_async<NB>(slot(stg, XS), a.Hz + cc - NE);
+            cp_async<NB>(slot(stg, XS) + SB / 2, a.Hy + cc - NE);
         }
     };
     if constexpr (PIPE) {
-        if (act) issue(kb, 0);
-        cp_async_commit();
+        // planes kb .. kb + NS - 2 in flight before the loop
+#pragma unroll
+        for (int q = 0; q < NS - 1; ++q) {
+            if (act && kb + q < ke) issue(kb + q, q);
+            cp_async_commit();
+        }
     }
 
     for (int k = kb; k < ke; ++k) {
@@ -806,35 +852,31 @@ __device__ __forceinline__ void e_column(const StepArgs<S, T>& a, const SweepGeo
         T ex[W], ey[W], ez[W], bx[W], by[W], bz[W], hx[W], hy[W], hz[W], hzj[W], hxj[W];
         T hze = T(0), hye = T(0);
         if (PIPE && act) {
-            // the next plane into the other stage (its contents were used last iteration),
-            // then wait for this plane's copies
-            if (k + 1 < ke) issue(k + 1, (k + 1 - kb) & 1);
+            // plane k + NS - 1 into the stage read last iteration (its contents are used), then
+            // wait for this plane's copies
+            if (k + NS - 1 < ke) issue(k + NS - 1, (k + NS - 1 - kb) & (NS - 1));
             cp_async_commit();
-            cp_async_wait<1>();
-            const uint4* b = pipe_smem + size_t((k - kb) & 1) * NV * NT + tid;
-            Fld<S, T>::ld(reinterpret_cast<const S*>(b + 0 * NT), ex);
-            Fld<S, T>::ld(reinterpret_cast<const S*>(b + 1 * NT), ey);
-            Fld<S, T>::ld(reinterpret_cast<const S*>(b + 2 * NT), ez);
-            Fld<S, T>::ld(reinterpret_cast<const S*>(b + 3 * NT), hx);
-            Fld<S, T>::ld(reinterpret_cast<const S*>(b + 4 * NT), hy);
-            Fld<S, T>::ld(reinterpret_cast<const S*>(b + 5 * NT), hz);
-            Fld<S, T>::ld(reinterpret_cast<const S*>(b + 6 * NT), hzj);
-            Fld<S, T>::ld(reinterpret_cast<const S*>(b + 7 * NT), hxj);
+            cp_async_wait<NS - 1>();
+            const int stg = (k - kb) & (NS - 1);
+            Fld<S, T>::ld(reinterpret_cast<const S*>(slot(stg, 0)), ex);
+            Fld<S, T>::ld(reinterpret_cast<const S*>(slot(stg, 1)), ey);
+            Fld<S, T>::ld(reinterpret_cast<const S*>(slot(stg, 2)), ez);
+            Fld<S, T>::ld(reinterpret_cast<const S*>(slot(stg, 3)), hx);
+            Fld<S, T>::ld(reinterpret_cast<const S*>(slot(stg, 4)), hy);
+            Fld<S, T>::ld(reinterpret_cast<const S*>(slot(stg, 5)), hz);
+            Fld<S, T>::ld(reinterpret_cast<const S*>(slot(stg, 6)), hzj);
+            Fld<S, T>::ld(reinterpret_cast<const S*>(slot(stg, 7)), hxj);
             if constexpr (MAT) {
                 RowIds<W> idk;
-                const unsigned* w = reinterpret_cast<const unsigned*>(b + 8 * NT);
+                const unsigned* w = reinterpret_cast<const unsigned*>(slot(stg, 8));
 #pragma unroll
                 for (int q = 0; q < W / 2; ++q) idk.w[q] = w[q];
                 load_bE<MAT>(a, c, idk, bx, by, bz);
-            } else {
-                Vec<T>::ld(reinterpret_cast<const T*>(b + 8 * NT), bx);
-                Vec<T>::ld(reinterpret_cast<const T*>(b + 9 * NT), by);
-                Vec<T>::ld(reinterpret_cast<const T*>(b + 10 * NT), bz);
             }
             if (pload && i0 > 0) {
-                const S* xs = reinterpret_cast<const S*>(b + XS * NT);
-                hze = T(to_c(xs[NE - 1]));
-                hye = T(to_c(reinterpret_cast<const S*>(reinterpret_cast<const char*>(xs) + 8)[NE - 1]));
+                const char* xs = slot(stg, XS);
+                hze = T(to_c(reinterpret_cast<const S*>(xs)[NE - 1]));
+                hye = T(to_c(reinterpret_cast<const S*>(xs + SB / 2)[NE - 1]));
             }
         } else if (act) {
             Fld<S, T>::ld(a.Ex + c, ex);
@@ -891,39 +933,39 @@ __device__ __forceinline__ void e_column(const StepArgs<S, T>& a, const SweepGeo
             if (i < 1 || i >= a.NxT) continue;  // x = 0 plane and padding never updated
             const T hzx = (e > 0) ? hz[e - 1] : hzp;
             const T hyx = (e > 0) ? hy[e - 1] : hyp;
-            T dHz_dy = (hz[e] - hzj[e]) * idy;
-            T dHy_dz = (hy[e] - hym[e]) * idz;
-            T dHx_dz = (hx[e] - hxm[e]) * idz;
-            T dHz_dx = (hz[e] - hzx) * idx[e];
-            T dHy_dx = (hy[e] - hyx) * idx[e];
-            T dHx_dy = (hx[e] - hxj[e]) * idy;
+            T dHz_dy = dq(hz[e], hzj[e], idy);
+            T dHy_dz = dq(hy[e], hym[e], idz);
+            T dHx_dz = dq(hx[e], hxm[e], idz);
+            T dHz_dx = dq(hz[e], hzx, idx[e]);
+            T dHy_dx = dq(hy[e], hyx, idx[e]);
+            T dHx_dy = dq(hx[e], hxj[e], idy);
             if (ypml) {
-                pxy[e] = yb * pxy[e] + yc * dHz_dy; dHz_dy = psi_eff<S, T>(dHz_dy, yik, pxy[e], a.psc);
-                pzy[e] = yb * pzy[e] + yc * dHx_dy; dHx_dy = psi_eff<S, T>(dHx_dy, yik, pzy[e], a.psc);
+                pxy[e] = psi_rec(yb, pxy[e], yc, dHz_dy); dHz_dy = psi_eff<S, T>(dHz_dy, yik, pxy[e], a.psc);
+                pzy[e] = psi_rec(yb, pzy[e], yc, dHx_dy); dHx_dy = psi_eff<S, T>(dHx_dy, yik, pzy[e], a.psc);
             }
             if (zpml) {
-                pxz[e] = zb * pxz[e] + zc * dHy_dz; dHy_dz = psi_eff<S, T>(dHy_dz, zik, pxz[e], a.psc);
-                pyz[e] = zb * pyz[e] + zc * dHx_dz; dHx_dz = psi_eff<S, T>(dHx_dz, zik, pyz[e], a.psc);
+                pxz[e] = psi_rec(zb, pxz[e], zc, dHy_dz); dHy_dz = psi_eff<S, T>(dHy_dz, zik, pxz[e], a.psc);
+                pyz[e] = psi_rec(zb, pyz[e], zc, dHx_dz); dHx_dz = psi_eff<S, T>(dHx_dz, zik, pyz[e], a.psc);
             }
             if (xpml && in_pml(i, a.NxT, np)) {
                 const T b = __ldg(a.pbE[0] + i), cc = __ldg(a.pcE[0] + i), ik = __ldg(a.ik[0] + i);
-                x3[e] = b * x3[e] + cc * dHz_dx;
+                x3[e] = psi_rec(b, x3[e], cc, dHz_dx);
                 dHz_dx = psi_eff<S, T>(dHz_dx, ik, x3[e], a.psc);
-                x4[e] = b * x4[e] + cc * dHy_dx;
+                x4[e] = psi_rec(b, x4[e], cc, dHy_dx);
                 dHy_dx = psi_eff<S, T>(dHy_dx, ik, x4[e], a.psc);
             }
             T Jx = 0, Jy = 0, Jz = 0;
             for (int s = 0; s < src.n; ++s) {
                 if (src.si[s] == i && src.sj[s] == j && src.sk[s] == k) {
                     const T v = T(src.J[s]);
-                    if (src.sc[s] == 0) Jx += v;
-                    else if (src.sc[s] == 1) Jy += v;
-                    else Jz += v;
+                    if (src.sc[s] == 0) Jx = add_rn(Jx, v);
+                    else if (src.sc[s] == 1) Jy = add_rn(Jy, v);
+                    else Jz = add_rn(Jz, v);
                 }
             }
             if constexpr (SH) sheet_J(src, i, j, k, Jx, Jy, Jz);
-            ex[e] = ex[e] + bx[e] * ((dHz_dy - dHy_dz) - Jx);
-            ey[e] = ey[e] + by[e] * ((dHx_dz - dHz_dx) - Jy);
+            ex[e] = fma_rn(bx[e], sub_rn(sub_rn(dHz_dy, dHy_dz), Jx), ex[e]);
+            ey[e] = fma_rn(by[e], sub_rn(sub_rn(dHx_dz, dHz_dx), Jy), ey[e]);
             // Two-level gain: polarization with E^n, E update with -dP/dt, populations with E^{n+1}.
             int r = -1;
             size_t gidx = 0;
@@ -936,30 +978,31 @@ __device__ __forceinline__ void e_column(const StepArgs<S, T>& a, const SweepGeo
                 const T ez_old = ez[e];
                 const T P = Pcur[gidx], Pp = Pold[gidx];
                 T Nu = a.Nu[gidx], Ng = a.Ng[gidx];
-                const T ng_frac = (Ng - Nu) * g.inv_N0;
-                const T Pn = g.kapaN0 * (ng_frac * ez_old) + g.pa2 * P + g.pa3 * Pp;
-                const T dP = (Pn - P) * g.inv_dt;
-                ez[e] = ez[e] + bz[e] * (((dHy_dx - dHx_dy) - Jz) - dP * g.dp_scale);
-                const T e_avg = T(0.5) * (ez[e] + ez_old);
-                const T stim = e_avg * (Pn - P) * g.inv_dt * g.inv_hbar_omega;
-                T dNu = -g.inv_tau * Nu + stim;
-                T dNg = g.inv_tau * Nu - stim;
-                if (g.pump != T(0)) { dNu += g.pump * Ng; dNg -= g.pump * Ng; }
-                Nu = Nu + g.dt * dNu;
-                Ng = Ng + g.dt * dNg;
+                const T ng_frac = mul_rn(sub_rn(Ng, Nu), g.inv_N0);
+                const T Pn = fma_rn(g.pa3, Pp, fma_rn(g.pa2, P, mul_rn(g.kapaN0, mul_rn(ng_frac, ez_old))));
+                const T dPn = sub_rn(Pn, P);
+                const T dP = mul_rn(dPn, g.inv_dt);
+                ez[e] = fma_rn(bz[e], sub_rn(sub_rn(sub_rn(dHy_dx, dHx_dy), Jz), mul_rn(dP, g.dp_scale)), ez[e]);
+                const T e_avg = mul_rn(T(0.5), add_rn(ez[e], ez_old));
+                const T stim = mul_rn(mul_rn(mul_rn(e_avg, dPn), g.inv_dt), g.inv_hbar_omega);
+                T dNu = fma_rn(-g.inv_tau, Nu, stim);
+                T dNg = fma_rn(g.inv_tau, Nu, -stim);
+                if (g.pump != T(0)) { dNu = fma_rn(g.pump, Ng, dNu); dNg = fma_rn(-g.pump, Ng, dNg); }
+                Nu = fma_rn(g.dt, dNu, Nu);
+                Ng = fma_rn(g.dt, dNg, Ng);
                 Nu = fmax(T(0), Nu);
                 Ng = fmax(T(0), Ng);
                 if (g.clamp) {
-                    const T tot = Nu + Ng;
-                    if (tot > T(1e-30)) { const T sc = g.N0 / tot; Nu *= sc; Ng *= sc; }
+                    const T tot = add_rn(Nu, Ng);
+                    if (tot > T(1e-30)) { const T sc = div_rn(g.N0, tot); Nu = mul_rn(Nu, sc); Ng = mul_rn(Ng, sc); }
                     Nu = fmin(Nu, g.N0);
-                    Ng = g.N0 - Nu;
+                    Ng = sub_rn(g.N0, Nu);
                 }
                 Pold[gidx] = Pn;
                 a.Nu[gidx] = Nu;
                 a.Ng[gidx] = Ng;
             } else {
-                ez[e] = ez[e] + bz[e] * ((dHy_dx - dHx_dy) - Jz);
+                ez[e] = fma_rn(bz[e], sub_rn(sub_rn(dHy_dx, dHx_dy), Jz), ez[e]);
             }
         }
         if (act) {
@@ -1000,7 +1043,7 @@ __device__ __forceinline__ void update_E_block(const StepArgs<S, T>& a, const in
     }
 }
 
-// PIPE: interior columns stage their planes in shared memory (EPipe<MAT>::bytes() dynamic).
+// PIPE: interior columns stage their planes in shared memory (EPipe<S>::bytes() dynamic).
 template <typename S, typename T, bool SH = false, bool MAT = false, bool PIPE = false>
 __global__ void __launch_bounds__(32 * kBlockY, 2)
 k_update_E(const StepArgs<S, T> a, const int kchunk, const ESrc src, const SweepGeom g) {
@@ -1015,13 +1058,17 @@ k_update_E(const StepArgs<S, T> a, const int kchunk, const ESrc src, const Sweep
 // E(k) reads H(k), H(k-1) (done: E(s) waits for H(s) and H(s-1)).  E(s) runs about one slab
 // after H(s), while the E and H planes it reads are still in L2, so a cell costs DRAM bytes
 // for E, H and bE once each instead of E and H twice.  Blocks wait only on work handed out
-// before theirs (already running), so the waits always end; each is bounded by 2 s all the
-// same, after which the block flags the status word and leaves.
+// before theirs (already running), so the waits always end; each is bounded all the same
+// (wait_ns of %globaltimer, 2 s by default), after which the block flags the status word and
+// leaves.  An E tile also waits while the hold word (the counter after the per-slab counts)
+// is nonzero; the host clears it before every launch, and sets it only to make the waits
+// run out on purpose (the bounded-wait test).
 struct SlabPlan {
     int P;          // planes per slab
     int nslab;
     int gxH, nH;    // H tiles per slab: gxH columns x (nH / gxH) row groups
     int gxE, nE;
+    unsigned long long wait_ns;  // bound on one dependency wait
 };
 
 __device__ __forceinline__ unsigned ld_acquire(const unsigned* p) {
@@ -1030,14 +1077,16 @@ __device__ __forceinline__ unsigned ld_acquire(const unsigned* p) {
     return v;
 }
 
+// One resident block per SM: the H and E block code together need more than 128 registers.
 template <typename S, typename T, bool SH = false, bool MAT = false>
-__global__ void __launch_bounds__(32 * kBlockY, 2)
+__global__ void __launch_bounds__(32 * kBlockY, 1)
 k_step_slabs(const StepArgs<S, T> a, const ESrc src, const SweepGeom g, const SlabPlan p, unsigned* ctr,
              unsigned* status_w) {
     __shared__ int item_s;
     const int tid = threadIdx.y * 32 + threadIdx.x;
     const long long total = (long long)p.nslab * (p.nH + p.nE);
     unsigned* const hdone = ctr + 1;
+    const unsigned* const hold = ctr + 1 + p.nslab;
     for (;;) {
         if (tid == 0) item_s = int(atomicAdd(ctr, 1u));
         __syncthreads();
@@ -1063,8 +1112,9 @@ k_step_slabs(const StepArgs<S, T> a, const ESrc src, const SweepGeom g, const Sl
             bool ok = true;
             if (tid == 0) {
                 const unsigned long long t0 = global_ns();
-                while (ld_acquire(hdone + slab) < unsigned(p.nH) || (slab > 0 && ld_acquire(hdone + slab - 1) < unsigned(p.nH))) {
-                    if (global_ns() - t0 > kWaitNs) { ok = false; break; }
+                while (ld_acquire(hdone + slab) < unsigned(p.nH) ||
+                       (slab > 0 && ld_acquire(hdone + slab - 1) < unsigned(p.nH)) || ld_acquire(hold) != 0u) {
+                    if (global_ns() - t0 > p.wait_ns) { ok = false; break; }
                 }
             }
             if (!__syncthreads_and(ok)) {

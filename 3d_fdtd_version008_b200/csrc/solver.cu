@@ -11,10 +11,7 @@
 #include "host/outputs.hpp"
 #include "host/waveform.hpp"
 #include "kernels.cuh"
-#include "fused.cuh"
 
-#include <cuda.h>
-#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -70,18 +67,6 @@ __global__ void k_index_from_idx3(const uint16_t* __restrict__ src, uint16_t* __
     for (int r = threadIdx.y; r < 32; r += blockDim.y) {
         const int k = k0 + r, i = i0 + threadIdx.x;
         if (i < NxT && k < NzT) dst[(size_t(k) * NyT + j) * NxP + i] = tile[threadIdx.x][r];
-    }
-}
-
-// Full bE arrays from the index and the table (for the fused path, which streams them by TMA).
-template <typename T>
-__global__ void k_expand_material(const uint16_t* __restrict__ idx, const T* __restrict__ tab, size_t n, T* bx, T* by,
-                                  T* bz) {
-    for (size_t q = blockIdx.x * size_t(blockDim.x) + threadIdx.x; q < n; q += size_t(gridDim.x) * blockDim.x) {
-        const size_t r = 4 * size_t(idx[q]);
-        bx[q] = tab[r];
-        by[q] = tab[r + 1];
-        bz[q] = tab[r + 2];
     }
 }
 
@@ -228,8 +213,8 @@ __device__ void probe_dft_thread(const StepArgs<S, T>& a, const ProbeDev* __rest
         double s, c;
         sincospi(2.0 * freqs[m] * t, &s, &c);
         double* acc = dft + 2 * (size_t(p) * nf + m);
-        acc[0] += v * c * dt;
-        acc[1] -= v * s * dt;
+        acc[0] = __dadd_rn(acc[0], __dmul_rn(__dmul_rn(v, c), dt));
+        acc[1] = __dsub_rn(acc[1], __dmul_rn(__dmul_rn(v, s), dt));
     }
 }
 
@@ -507,7 +492,11 @@ __device__ __forceinline__ const StepArgs<S, float>& bargs(int r) {
 }
 
 // The blocks of the solves stored as S.  PIPE: interior columns stage their planes in shared
-// memory (HPipe::bytes() / EPipe<MAT>::bytes() dynamic), as in the single-solve sweeps.
+// memory (HPipe<S>::bytes() / EPipe<S>::bytes() dynamic, the same for every storage type), as in
+// the single-solve sweeps.
+static_assert(HPipe<float>::bytes() == HPipe<__half>::bytes() && HPipe<float>::bytes() == HPipe<__nv_bfloat16>::bytes() &&
+                  EPipe<float>::bytes() == EPipe<__half>::bytes() && EPipe<float>::bytes() == EPipe<__nv_bfloat16>::bytes(),
+              "the packed sweeps launch every storage form with one shared-memory size");
 template <typename S, bool PIPE>
 __global__ void __launch_bounds__(32 * kBlockY, 2) k_update_H_multi(const int4* __restrict__ tab) {
     const int4 e = tab[blockIdx.x];
@@ -669,9 +658,10 @@ public:
     void set_timing(int mode) override;
     void set_path(int path) override {
         if (path < 0 || path > 2)
-            throw Failure(FDTD_ERR_INVALID, "kernel path must be 0 (fused), 1 (two sweeps) or 2 (slab-ordered step)");
-        if (path == 0 && !std::is_same_v<S, T>) throw Failure(FDTD_ERR_UNSUPPORTED, "the fused path needs FP32 or FP64 storage");
-        if (path == 0 && pec_) throw Failure(FDTD_ERR_UNSUPPORTED, "the fused path needs a CPML boundary");
+            throw Failure(FDTD_ERR_INVALID, "kernel path must be 1 (two sweeps) or 2 (slab-ordered step)");
+        if (path == 0)
+            throw Failure(FDTD_ERR_UNSUPPORTED,
+                          "kernel path 0 (one fused H+E launch per step) is not built: it measured slower than the two sweeps");
         if (steps != 0) throw Failure(FDTD_ERR_INVALID, "the kernel path can only change before the first step");
         path_ = path;
     }
@@ -726,6 +716,7 @@ private:
     // path 2: k_step_slabs (persistent, slab-ordered H + E in one launch)
     SlabPlan plan_{};
     unsigned* d_ctr_ = nullptr;
+    bool slab_hold_ = false;  // FDTD_B200_SLAB_HOLD: E tiles wait on a hold word that nothing clears
     dim3 gridS_;
     void setup_slabs();
     dim3 gridH_, gridE_;
@@ -811,32 +802,21 @@ private:
     bool pipe_ = false, hpipe_ = false;
     using EKernel = void (*)(const StepArgs<S, T>, const int, const ESrc, const SweepGeom);
     EKernel e_kernel(bool sheets) const {
+        // the staged form exists for the indexed material only (pipe_ implies a_.bidx)
         static constexpr EKernel k[8] = {
-            k_update_E<S, T, false, false, false>, k_update_E<S, T, false, false, true>,
+            k_update_E<S, T, false, false, false>, k_update_E<S, T, false, false, false>,
             k_update_E<S, T, false, true, false>,  k_update_E<S, T, false, true, true>,
-            k_update_E<S, T, true, false, false>,  k_update_E<S, T, true, false, true>,
+            k_update_E<S, T, true, false, false>,  k_update_E<S, T, true, false, false>,
             k_update_E<S, T, true, true, false>,   k_update_E<S, T, true, true, true>};
         return k[4 * int(sheets) + 2 * int(a_.bidx != nullptr) + int(pipe_)];
     }
     // event timing: ev_[0..3] bracket H, E and the auxiliary kernels of one step
-    // kernel path 0: k_step_fused (fields and psi_H double-buffered, cur_ = buffer holding
-    // the latest state); path 1 (default, measured faster on B200): k_update_H +
-    // k_update_E in place on buffer 0.
-    int path_ = 1, cur_ = 0;
-    S* fld_[2][6] = {};
-    S* psiH_[2][6] = {};
-    FusedMaps maps_[2];
-    int kchunkF_ = 1;
-    dim3 gridF_;
-    size_t smemF_ = 0;
-    int threadsF_ = 0, shapeF_ = 0;
-    void (*launchF_)(dim3, int, size_t, cudaStream_t, const FusedMaps&, const FusedArgs<T>&, int, const ESrc&) = nullptr;
-    bool fused_ready_ = false;
+    // kernel path 1 (default): k_update_H + k_update_E in place; path 2: k_step_slabs.
+    int path_ = 1;
+    S* fld_[6] = {};
+    S* psiH_[6] = {};
     size_t psi_sz_[6] = {};
-    void ensure_fused();
-    void point_args_at(int buf);
-    void build_fused();
-    template <typename Shape> void setup_fused();
+    void point_args_at();
     int timing_ = FDTD_TIMING_OFF;
     cudaEvent_t ev_[4] = {nullptr, nullptr, nullptr, nullptr};
     fdtd_timing_v1 tm_{};
@@ -898,9 +878,8 @@ Solver<S, T>::Solver(const fdtd_setup_v1& s, int dev, const ShardSpec* shard) {
     a.kH1 = std::min(shard_.own1, shard_.NzG - 1 - shard_.kz0);
     a.kE0 = std::max(shard_.own0, 1 - shard_.kz0);
     a.kE1 = shard_.own1;
-    // buffer 1 (fields and psi_H) exists only for the fused path, made at its first step
-    for (int c = 0; c < 6; ++c) fld_[0][c] = alloc<S>(nflat_);
-    point_args_at(0);
+    for (int c = 0; c < 6; ++c) fld_[c] = alloc<S>(nflat_);
+    point_args_at();
 
     // bH must be uniform and aE = aH = 1 (sigma = 0, mu_r = 1).
     double bH = s.bH_uniform;
@@ -985,10 +964,10 @@ Solver<S, T>::Solver(const fdtd_setup_v1& s, int dev, const ShardSpec* shard) {
     if (const char* e = std::getenv("FDTD_B200_H_PIPE")) hpipe_ = std::string(e) != "0";
     if (const char* e = std::getenv("FDTD_B200_E_PIPE")) pipe_ = a.bidx != nullptr && std::string(e) != "0";
     if (hpipe_)
-        ck(cudaFuncSetAttribute(k_update_H<S, T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(HPipe::bytes())),
+        ck(cudaFuncSetAttribute(k_update_H<S, T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(HPipe<S>::bytes())),
            "cudaFuncSetAttribute");
     if (pipe_) {
-        const int smem = int(a.bidx ? EPipe<true>::bytes() : EPipe<false>::bytes());
+        const int smem = int(EPipe<S>::bytes());
         for (bool sh : {false, true})
             ck(cudaFuncSetAttribute(e_kernel(sh), cudaFuncAttributeMaxDynamicSharedMemorySize, smem),
                "cudaFuncSetAttribute");
@@ -1033,9 +1012,9 @@ Solver<S, T>::Solver(const fdtd_setup_v1& s, int dev, const ShardSpec* shard) {
         const size_t sz[6] = {ys, zs, zs, xs, xs, ys};
         for (int q = 0; q < 6; ++q) {
             psi_sz_[q] = sz[q];
-            psiH_[0][q] = alloc<S>(sz[q]);
+            psiH_[q] = alloc<S>(sz[q]);
             a.psiE[q] = alloc<S>(sz[q]);
-            a.psiH[q] = psiH_[0][q];
+            a.psiH[q] = psiH_[q];
         }
     }
 
@@ -1197,7 +1176,13 @@ void Solver<S, T>::setup_slabs() {
     plan_.gxE = int(gridE_.x);
     plan_.nE = int(gridE_.x * gridE_.y);
     if ((long long)plan_.nslab * (plan_.nH + plan_.nE) > 0x7fffffffLL) throw Failure(FDTD_ERR_INVALID, "grid too large for the slab-ordered step");
-    d_ctr_ = alloc<unsigned>(size_t(plan_.nslab) + 1);
+    // Bound on one dependency wait of an E tile: FDTD_B200_WAIT_NS nanoseconds (at least 1000),
+    // else 2 s.  FDTD_B200_SLAB_HOLD=1 leaves the hold word set, so that every E tile's wait
+    // runs out and the step ends with FDTD_ERR_TIMEOUT (how the bounded wait is tested).
+    plan_.wait_ns = kWaitNs;
+    if (const char* e = std::getenv("FDTD_B200_WAIT_NS")) plan_.wait_ns = std::max(1000ull, std::strtoull(e, nullptr, 10));
+    if (const char* e = std::getenv("FDTD_B200_SLAB_HOLD")) slab_hold_ = std::string(e) == "1";
+    d_ctr_ = alloc<unsigned>(size_t(plan_.nslab) + 2);
     int sms = 148, per = 0;
     ck(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device), "cudaDeviceGetAttribute");
     const auto slabs_fn = sheets_.empty() ? (a_.bidx ? k_step_slabs<S, T, false, true> : k_step_slabs<S, T, false, false>)
@@ -1209,104 +1194,9 @@ void Solver<S, T>::setup_slabs() {
 }
 
 template <typename S, typename T>
-void Solver<S, T>::point_args_at(int buf) {
-    a_.Ex = fld_[buf][0]; a_.Ey = fld_[buf][1]; a_.Ez = fld_[buf][2];
-    a_.Hx = fld_[buf][3]; a_.Hy = fld_[buf][4]; a_.Hz = fld_[buf][5];
-}
-
-PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
-    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
-    if (!fn) {
-        void* p = nullptr;
-        cudaDriverEntryPointQueryResult q{};
-        ck(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q), "cudaGetDriverEntryPoint");
-        if (q != cudaDriverEntryPointSuccess || !p) throw Failure(FDTD_ERR_CUDA, "cuTensorMapEncodeTiled unavailable");
-        fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
-    }
-    return fn;
-}
-
-// Tensor maps over the padded device layout (x fastest): E/H boxes of the fused tile plus
-// its halo, bE boxes of the tile.  Base addresses come from cudaMalloc (256-byte aligned);
-// row and plane strides are multiples of 128 bytes.
-// First step of the fused path: the second field / psi_H buffer starts as a copy of the
-// first, then the tensor maps over both are encoded.
-template <typename S, typename T>
-void Solver<S, T>::ensure_fused() {
-    if (fused_ready_) return;
-    if (a_.bidx && !a_.bEx) {  // the fused path streams the three arrays
-        T* be[3];
-        for (int c = 0; c < 3; ++c) be[c] = alloc<T>(nflat_, false);
-        k_expand_material<T><<<148 * 8, 256, 0, st_>>>(a_.bidx, a_.btab, nflat_, be[0], be[1], be[2]);
-        ++launches;
-        ck(cudaGetLastError(), "k_expand_material");
-        a_.bEx = be[0]; a_.bEy = be[1]; a_.bEz = be[2];
-    }
-    for (int c = 0; c < 6; ++c) {
-        fld_[1][c] = alloc<S>(nflat_, false);
-        ck(cudaMemcpyAsync(fld_[1][c], fld_[0][c], nflat_ * sizeof(S), cudaMemcpyDeviceToDevice, st_), "field copy");
-    }
-    for (int q = 0; q < 6; ++q) {
-        if (!psiH_[0][q]) continue;
-        psiH_[1][q] = alloc<S>(psi_sz_[q], false);
-        ck(cudaMemcpyAsync(psiH_[1][q], psiH_[0][q], psi_sz_[q] * sizeof(S), cudaMemcpyDeviceToDevice, st_), "psi copy");
-    }
-    build_fused();
-    fused_ready_ = true;
-}
-
-template <typename S, typename T>
-void Solver<S, T>::build_fused() {
-    const char* env = std::getenv("FDTD_B200_FUSED_SHAPE");
-    shapeF_ = env ? std::atoi(env) : 0;
-    if (shapeF_ == 1) setup_fused<typename ShapeSet<T>::S1>();
-    else if (shapeF_ == 2) setup_fused<typename ShapeSet<T>::S2>();
-    else { shapeF_ = 0; setup_fused<typename ShapeSet<T>::S0>(); }
-}
-
-template <typename S, typename T>
-template <typename Shape>
-void Solver<S, T>::setup_fused() {
-    using SM = FusedSmem<T, Shape>;
-    auto enc = tensor_map_encoder();
-    auto make = [&](const T* base, int bx, int by) {
-        CUtensorMap m;
-        cuuint64_t dims[3] = {cuuint64_t(NxP_), cuuint64_t(NyT_), cuuint64_t(NzT_)};
-        cuuint64_t strides[2] = {cuuint64_t(NxP_) * sizeof(T), cuuint64_t(plane_) * sizeof(T)};
-        cuuint32_t box[3] = {cuuint32_t(bx), cuuint32_t(by), 1u};
-        cuuint32_t es[3] = {1u, 1u, 1u};
-        CUresult r = enc(&m, sizeof(T) == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3,
-                         const_cast<T*>(base), dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
-                         CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
-                         CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-        if (r != CUDA_SUCCESS) throw Failure(FDTD_ERR_CUDA, "cuTensorMapEncodeTiled failed (" + std::to_string(int(r)) + ")");
-        return m;
-    };
-    const T* bE[3] = {a_.bEx, a_.bEy, a_.bEz};
-    for (int b = 0; b < 2; ++b) {
-        for (int c = 0; c < 3; ++c) {
-            maps_[b].E[c] = make(fld_[b][c], SM::PX, SM::PY);
-            maps_[b].H[c] = make(fld_[b][3 + c], SM::PX, SM::PY);
-            maps_[b].B[c] = make(bE[c], SM::TX, SM::TY);
-        }
-    }
-    smemF_ = sizeof(SM);
-    threadsF_ = Shape::THREADS;
-    launchF_ = &launch_fused<T, Shape>;
-    ck(cudaFuncSetAttribute(k_step_fused<T, Shape>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smemF_)),
-       "cudaFuncSetAttribute");
-    int per_sm = 1, sms = 148;
-    ck(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_step_fused<T, Shape>, threadsF_, smemF_),
-       "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
-    ck(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device), "cudaDeviceGetAttribute");
-    if (per_sm < 1) throw Failure(FDTD_ERR_CUDA, "fused step kernel does not fit on an SM");
-    const int gx = (NxT_ + SM::TX - 1) / SM::TX, gy = (NyT_ + SM::TY - 1) / SM::TY;
-    // z-chunks: about 8 waves of resident blocks, chunks of at least 32 planes
-    const int resident = sms * per_sm;
-    const int want = std::max(1, (resident * 8 + gx * gy - 1) / (gx * gy));
-    const int zc = std::max(1, std::min(want, NzT_ / 32));
-    kchunkF_ = (NzT_ + zc - 1) / zc;
-    gridF_ = dim3(gx, gy, (NzT_ + kchunkF_ - 1) / kchunkF_);
+void Solver<S, T>::point_args_at() {
+    a_.Ex = fld_[0]; a_.Ey = fld_[1]; a_.Ez = fld_[2];
+    a_.Hx = fld_[3]; a_.Hy = fld_[4]; a_.Hz = fld_[5];
 }
 
 template <typename S, typename T>
@@ -1466,19 +1356,14 @@ void Solver<S, T>::from_device(const D* src, double* h, double scale) {
 template <typename S, typename T>
 void Solver<S, T>::set_field(int comp, const double* h) {
     if (comp < 0 || comp > 5) throw Failure(FDTD_ERR_INVALID, "component must be 0..5");
-    // Both buffers of the fused path: cells the reference never updates must hold the same
-    // value in each.
-    to_device(h, fld_[cur_][comp], 1.0 / (comp < 3 ? sE_ : sH_));
-    if (fused_ready_)
-        ck(cudaMemcpyAsync(fld_[1 - cur_][comp], fld_[cur_][comp], nflat_ * sizeof(S), cudaMemcpyDeviceToDevice, st_),
-           "field copy");
+    to_device(h, fld_[comp], 1.0 / (comp < 3 ? sE_ : sH_));
     ck(cudaStreamSynchronize(st_), "set_field");
 }
 
 template <typename S, typename T>
 void Solver<S, T>::get_field(int comp, double* h) {
     if (comp < 0 || comp > 5) throw Failure(FDTD_ERR_INVALID, "component must be 0..5");
-    from_device(fld_[cur_][comp], h, comp < 3 ? sE_ : sH_);
+    from_device(fld_[comp], h, comp < 3 ? sE_ : sH_);
 }
 
 template <typename S, typename T>
@@ -1534,9 +1419,6 @@ void Solver<S, T>::ensure_series(uint64_t samples) {
 template <typename S, typename T>
 void Solver<S, T>::run(uint64_t n) {
     ck(cudaSetDevice(device), "cudaSetDevice");
-    if constexpr (std::is_same_v<S, T>) {
-        if (path_ == 0) ensure_fused();
-    }
     if (path_ == 2 && !d_ctr_) setup_slabs();
     const uint64_t n0 = steps;
     const uint64_t last = n0 + n;  // exclusive
@@ -1550,26 +1432,10 @@ void Solver<S, T>::run(uint64_t n) {
     for (uint64_t s = n0; s < last; ++s) {
         src_step(src, s);
         if (per_kernel) ck(cudaEventRecord(ev_[0], st_), "cudaEventRecord");
-        bool fused_step = false;
-        if constexpr (std::is_same_v<S, T>) fused_step = path_ == 0;
-        if (fused_step) {
-            if constexpr (std::is_same_v<S, T>) {
-            FusedArgs<T> fa;
-            fa.a = a_;
-            for (int q = 0; q < 6; ++q) {
-                fa.psiHs[q] = psiH_[cur_][q];
-                fa.psiHd[q] = psiH_[1 - cur_][q];
-            }
-            for (int c = 0; c < 3; ++c) { fa.dE[c] = fld_[1 - cur_][c]; fa.dH[c] = fld_[1 - cur_][3 + c]; }
-            fa.status_w = d_status_;
-            if (per_kernel) ck(cudaEventRecord(ev_[1], st_), "cudaEventRecord");
-            launchF_(gridF_, threadsF_, smemF_, st_, maps_[cur_], fa, kchunkF_, src);
-            cur_ = 1 - cur_;
-            point_args_at(cur_);
-            launches += 1;
-            }
-        } else if (path_ == 2) {
-            ck(cudaMemsetAsync(d_ctr_, 0, (size_t(plan_.nslab) + 1) * sizeof(unsigned), st_), "cudaMemsetAsync");
+        if (path_ == 2) {
+            ck(cudaMemsetAsync(d_ctr_, 0, (size_t(plan_.nslab) + 2) * sizeof(unsigned), st_), "cudaMemsetAsync");
+            if (slab_hold_)
+                ck(cudaMemsetAsync(d_ctr_ + plan_.nslab + 1, 0xff, sizeof(unsigned), st_), "cudaMemsetAsync");
             if (per_kernel) ck(cudaEventRecord(ev_[0], st_), "cudaEventRecord");
             const auto slabs = src.ns ? (a_.bidx ? k_step_slabs<S, T, true, true> : k_step_slabs<S, T, true, false>)
                                       : (a_.bidx ? k_step_slabs<S, T, false, true> : k_step_slabs<S, T, false, false>);
@@ -1577,10 +1443,10 @@ void Solver<S, T>::run(uint64_t n) {
             if (per_kernel) ck(cudaEventRecord(ev_[1], st_), "cudaEventRecord");
             launches += 1;
         } else {
-            if (hpipe_) k_update_H<S, T, true><<<gridH_, blk, HPipe::bytes(), st_>>>(a_, kchunkH_, geom_, src.step);
+            if (hpipe_) k_update_H<S, T, true><<<gridH_, blk, HPipe<S>::bytes(), st_>>>(a_, kchunkH_, geom_, src.step);
             else k_update_H<S, T><<<gridH_, blk, 0, st_>>>(a_, kchunkH_, geom_, src.step);
             if (per_kernel) ck(cudaEventRecord(ev_[1], st_), "cudaEventRecord");
-            const size_t smem = pipe_ ? (a_.bidx ? EPipe<true>::bytes() : EPipe<false>::bytes()) : 0;
+            const size_t smem = pipe_ ? EPipe<S>::bytes() : 0;
             e_kernel(src.ns != 0)<<<gridE_, blk, smem, st_>>>(a_, kchunkE_, src, geom_);
             launches += 2;
         }
@@ -1630,7 +1496,7 @@ void Solver<S, T>::run(uint64_t n) {
         tm_.steps += n;
     }
     if (status & kStatusTimeout)
-        throw Failure(FDTD_ERR_TIMEOUT, "a bounded device wait expired (TMA copy did not arrive); state is invalid");
+        throw Failure(FDTD_ERR_TIMEOUT, "a bounded device wait expired; the state is invalid and the handle stays stopped");
     if (status) {
         MonitorState ms{};
         ck(cudaMemcpy(&ms, d_ms_, sizeof(ms), cudaMemcpyDeviceToHost), "monitor state");
@@ -1647,7 +1513,7 @@ void Solver<S, T>::run(uint64_t n) {
 template <typename S, typename T>
 void Solver<S, T>::phase_H(uint64_t s) {
     const dim3 blk(32, kBlockY);
-    if (hpipe_) k_update_H<S, T, true><<<gridH_, blk, HPipe::bytes(), st_>>>(a_, kchunkH_, geom_, unsigned(s));
+    if (hpipe_) k_update_H<S, T, true><<<gridH_, blk, HPipe<S>::bytes(), st_>>>(a_, kchunkH_, geom_, unsigned(s));
     else k_update_H<S, T><<<gridH_, blk, 0, st_>>>(a_, kchunkH_, geom_, unsigned(s));
     ++launches;
 }
@@ -1658,7 +1524,7 @@ template <typename S, typename T>
 void Solver<S, T>::phase_E(uint64_t s, ESrc& src, bool monitor) {
     const dim3 blk(32, kBlockY);
     src_step(src, s);
-    const size_t smem = pipe_ ? (a_.bidx ? EPipe<true>::bytes() : EPipe<false>::bytes()) : 0;
+    const size_t smem = pipe_ ? EPipe<S>::bytes() : 0;
     e_kernel(src.ns != 0)<<<gridE_, blk, smem, st_>>>(a_, kchunkE_, src, geom_);
     ++launches;
     if (nprobes_) {
@@ -1997,11 +1863,11 @@ public:
             if (const char* e = std::getenv("FDTD_B200_BATCH_KCHUNK")) kchunk_ = std::max(0, std::atoi(e));
             for (int st = 0; st < 3; ++st) {
                 ck(cudaFuncSetAttribute(hkernel(st, true), cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        int(HPipe::bytes())),
+                                        int(HPipe<float>::bytes())),
                    "cudaFuncSetAttribute");
                 for (int sh = 0; sh < 2; ++sh)
                     ck(cudaFuncSetAttribute(ekernel(4 * st + 2 * sh + 1, true), cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                            int(EPipe<true>::bytes())),
+                                            int(EPipe<float>::bytes())),
                        "cudaFuncSetAttribute");
             }
         } catch (...) {
@@ -2260,12 +2126,12 @@ private:
         const dim3 blk(32, kBlockY);
         for (int q = 0; q < 3; ++q)
             if (nHk_[q + 1] > nHk_[q])
-                hkernel(q, hpipe_)<<<unsigned(nHk_[q + 1] - nHk_[q]), blk, hpipe_ ? HPipe::bytes() : 0, st_>>>(
+                hkernel(q, hpipe_)<<<unsigned(nHk_[q + 1] - nHk_[q]), blk, hpipe_ ? HPipe<float>::bytes() : 0, st_>>>(
                     d_tab_ + nHk_[q]);
         for (int q = 0; q < kEKinds; ++q)
             if (nEk_[q + 1] > nEk_[q]) {
                 const bool pipe = epipe_ && (q & 1);
-                ekernel(q, pipe)<<<unsigned(nEk_[q + 1] - nEk_[q]), blk, pipe ? EPipe<true>::bytes() : 0, st_>>>(
+                ekernel(q, pipe)<<<unsigned(nEk_[q + 1] - nEk_[q]), blk, pipe ? EPipe<float>::bytes() : 0, st_>>>(
                     d_tab_ + nH_ + nEk_[q]);
             }
         k_probe_multi<<<n, 128, 0, st_>>>();

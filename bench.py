@@ -546,6 +546,219 @@ def precision_study(args):
                       "config_file": cfg, "steps": n, "results": res}))
 
 
+PREC = {"fp32": PKG.PREC_FP32, "fp64": PKG.PREC_FP64, "fp16": PKG.PREC_FP16, "bf16": PKG.PREC_BF16}
+WORD = {"fp32": 4, "fp64": 8, "fp16": 2, "bf16": 2}
+DTYPE = {"fp32": "f32", "fp64": "f64", "fp16": "f32 (fp16 storage)", "bf16": "f32 (bf16 storage)"}
+
+
+def workload_config(setup, cfg: str, desc: str) -> dict:
+    """The workload, identical in both arms' lines (the reference arm runs the same grid)."""
+    return {"workload": desc, "config_file": cfg, "grid": list(setup.shape),
+            "total_cells": int(setup.shape[0] * setup.shape[1] * setup.shape[2])}
+
+
+def cpu_model() -> str:
+    try:
+        for ln in open("/proc/cpuinfo"):
+            if ln.startswith("model name"):
+                return ln.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def host_mem_gb() -> float:
+    try:
+        for ln in open("/proc/meminfo"):
+            if ln.startswith("MemAvailable"):
+                return int(ln.split()[1]) / 1e6
+    except OSError:
+        pass
+    return 0.0
+
+
+def reference_arm(args, cfg: str, sample_cfg: str, desc: str, K: int, W: int) -> dict:
+    """--impl reference: the reference's own time loop (src/3D_FDTD_version008.cpp:269-328,
+    compiled from its headers with its CMake flags, OpenMP on every host core) on the same
+    workload grid as the GPU arm, W untimed then K timed steps; one bench step = one time step
+    of the reference (the metric is per cell-update).  It needs the reference's ~41 full-grid
+    FP64 arrays in host memory; with less memory than that it times the bounded sample grid
+    and says so."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle
+    setup = PKG.Setup.from_file(PKG.config_path(cfg), mesh_only=True)
+    cells = setup.shape[0] * setup.shape[1] * setup.shape[2]
+    need_gb = 41 * 8 * cells / 1e9 * 1.1
+    cores = os.cpu_count() or 1
+    use = cfg if host_mem_gb() >= need_gb else sample_cfg
+    path = PKG.config_path(use)
+    t0 = time.time()
+    if oracle.REF_HARNESS_NATIVE.exists():
+        exe = oracle.REF_HARNESS_NATIVE
+        r = oracle.run_harness(path, W + K, "--no-fields", "--warmup", str(W), native=True,
+                               env={"OMP_NUM_THREADS": str(cores)})
+        shape = [r["meta"][k] for k in ("NxT", "NyT", "NzT")]
+        loop_s = float(r["meta"]["loop_seconds"])
+        kind = "reference"
+        what = f"{exe.relative_to(ROOT)} (the reference headers compiled with -O3 -march=x86-64-v3 -fopenmp)"
+    else:
+        s = PKG.Setup.from_file(path)
+        o = oracle.OracleSolve(s, 0)
+        o.run(W, threads=cores)
+        t1 = time.time()
+        o.run(K, threads=cores)
+        loop_s = time.time() - t1
+        shape = list(s.shape)
+        kind = "port"
+        what = "oracle/lib/libfdtd_oracle.so (C restatement of the reference loop, OpenMP)"
+    total = time.time() - t0
+    ncell = shape[0] * shape[1] * shape[2]
+    value = ncell * K / loop_s / 1e6
+    sample = (f"{use}: {shape[0]}x{shape[1]}x{shape[2]} total cells, {W} untimed + {K} timed steps of the reference "
+              f"loop (J clear, source, polarization, H, CPML-H, E with gain, CPML-E, probe, populations), {what}, "
+              f"{cores} threads on {cpu_model()}; loop {loop_s:.2f} s, process {total:.1f} s with set-up")
+    same = use == cfg
+    cfgd = workload_config(setup, cfg, desc) if same else dict(workload_config(setup, cfg, desc),
+                                                                 sample_grid=shape, sample_config=use)
+    return {"metric": "Mcell-updates/s", "value": round(value, 3), "unit": "Mcell-updates/s", "n_gpus": args.gpus,
+            "steps": K, "warmup": W, "ms_per_step": round(loop_s * 1e3 / K, 3), "higher_is_better": True,
+            "impl": "reference", "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": cfgd,
+            "detail": {"fdtd_steps_per_step": 1, "parallelism": f"OpenMP, {cores} host threads",
+                       "cpu_model": cpu_model(), "host_mem_available_gb": round(host_mem_gb(), 1),
+                       "same_grid_as_gpu_arm": same},
+            "cpu_baseline": {"value": round(value, 3), "unit": "Mcell-updates/s", "cores": cores, "kind": kind,
+                             "sample": sample},
+            "e2e": {"value": round(value, 3), "unit": "Mcell-updates/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+
+
+def e2e_run(setup, sample_cfg: str, prec: int, local: int, K: int, S: int, dist, world: int) -> dict:
+    """The metric through the public C ABI from host buffers: fdtd_create from the host setup
+    (H2D of the material row index and 1-D profiles, layout transpose on the device), K runs of
+    S steps each followed by a D2H read of that run's probe samples, a D2H read of the final Ez
+    field, fdtd_destroy -- all inside the timed region (wall clock, synchronised)."""
+    import numpy as np
+    cells = setup.shape[0] * setup.shape[1] * setup.shape[2]
+    coef_word = 8 if prec == PKG.PREC_FP64 else 4
+    warm = PKG.Solver(PKG.Setup.from_file(PKG.config_path(sample_cfg)), device=local, precision=prec)
+    warm.run(S)
+    warm.probe_series()
+    warm.field("Ez")
+    warm.close()
+    del warm
+    # bytes fdtd_create copies host -> device: the material (the setup's row index, 2 bytes per
+    # cell, and its row table -- or bE as three FP64 idx3 arrays), 1-D spacing / CPML arrays,
+    # gain box (counted before the timed region)
+    nrows = int(setup.view.n_bE_rows)
+    h2d = (2 * cells + 24 * nrows if nrows else 3 * cells * 8) + sum(8 * n for n in setup.shape) * 16
+    if setup.view.n_tls_regions:
+        m = setup.array("tls_region_map").reshape(setup.shape) >= 0
+        box = int(np.prod([np.ptp(np.nonzero(m.any(axis=tuple(x for x in range(3) if x != ax)))[0]) + 1
+                           for ax in range(3)]))
+        h2d += box * (2 * coef_word + 1)
+        del m
+    barrier(dist)
+    t0 = time.perf_counter()
+    s2 = PKG.Solver(setup, device=local, precision=prec)
+    d2h = 0
+    for _ in range(K):
+        s2.run(S)
+        series = s2.probe_series()
+        d2h += series[-S:].nbytes
+    ez = s2.field("Ez")
+    d2h += ez.nbytes
+    s2.close()
+    t_e2e = reduce_max(dist, time.perf_counter() - t0)
+    return {"value": round(cells * K * S * world / t_e2e / 1e6, 3), "unit": "Mcell-updates/s",
+            "h2d_bytes_per_step": int(h2d / K), "d2h_bytes_per_step": int(d2h / K), "seconds": round(t_e2e, 4)}
+
+
+def device_run(setup, form: str, shards: int, W: int, K: int, S: int, local: int, dist) -> dict:
+    """W untimed and K timed runs of S steps, inputs resident; device time from CUDA events on
+    the library's stream(s), max over ranks; the solve is returned open."""
+    sol = PKG.Solver(setup, device=local, precision=PREC[form], shards=shards)
+    for _ in range(W):
+        sol.run(S)
+    sol.synchronize()
+    sol.set_timing(PKG.TIMING_RUN)
+    barrier(dist)
+    clocks = ClockSampler(local)
+    clocks.start()
+    t_wall = time.perf_counter()
+    launches_a = sol.kernel_launches
+    for _ in range(K):
+        sol.run(S)
+    sol.synchronize()
+    t_wall = time.perf_counter() - t_wall
+    launches = sol.kernel_launches - launches_a
+    clk = clocks.stop()
+    barrier(dist)
+    dev_ms = sol.timing()["run_ms"]
+    return {"solve": sol, "dev_ms_max": reduce_max(dist, dev_ms), "wall_ms": t_wall * 1e3, "launches": launches,
+            "clocks": clk}
+
+
+def accuracy(sols: dict, ref) -> dict:
+    """Storage forms against the FP64 solve of the same run: relative L2 of the stacked E and
+    H components, of the probe series and of the DFT.  Each FP64 component is read once."""
+    import numpy as np
+    num = {f: {"E": 0.0, "H": 0.0} for f in sols}
+    den = {"E": 0.0, "H": 0.0}
+    for c in ("Ex", "Ey", "Ez", "Hx", "Hy", "Hz"):
+        b = ref.field(c)
+        den[c[0]] += float(np.dot(b.ravel(), b.ravel()))
+        for f, sol in sols.items():
+            d = sol.field(c)
+            np.subtract(d, b, out=d)
+            num[f][c[0]] += float(np.dot(d.ravel(), d.ravel()))
+            del d
+        del b
+    pr, dr = ref.probe_series(), ref.dft(0)
+
+    def rel(x, y):
+        return float(np.linalg.norm(np.ravel(x - y)) / np.linalg.norm(np.ravel(y)))
+    out = {}
+    for f, sol in sols.items():
+        ps, ds = sol.probe_series(), sol.dft(0)
+        out[f] = {"E_field_rel_l2": float((num[f]["E"] / den["E"]) ** 0.5),
+                  "H_field_rel_l2": float((num[f]["H"] / den["H"]) ** 0.5),
+                  "probe_rel_l2": rel(ps, pr), "dft_rel_l2": rel(ds, dr),
+                  "dft_peak_same_bin": bool(np.argmax(np.abs(ds)) == np.argmax(np.abs(dr)))}
+    return out
+
+
+def kernel_roofline(setup, form: str, S: int, K: int, local: int) -> dict:
+    """Per-kernel CUDA events (one synchronisation per step) on a whole solve of the workload:
+    the E sweep's algorithmic bytes per launch over its average launch time, against the
+    measured copy bandwidth of this pool's B200s."""
+    word = WORD[form]
+    coef_word = 8 if form == "fp64" else 4
+    sol = PKG.Solver(setup, device=local, precision=PREC[form])
+    alg = algorithmic_bytes(setup, word, coef_word, 2 if sol.material_rows else 0)
+    sol.run(S)
+    sol.set_timing(PKG.TIMING_KERNELS)
+    for _ in range(min(K, 5)):
+        sol.run(S)
+    tm = sol.timing()
+    sol.close()
+    e_ms = tm["e_ms"] / tm["steps"]
+    h_ms = tm["h_ms"] / tm["steps"]
+    peak, peak_src = peaks()
+    achieved = alg["e_bytes"] / (e_ms * 1e-3) / 1e9
+    traffic = None
+    prof = ROOT / "profiles" / f"k_update_E_b512_{form}_traffic.json"
+    if prof.exists():
+        traffic = json.loads(prof.read_text()).get("dram_bytes_per_launch")
+    return {"roofline": {"bound": "hbm", "kernel": "k_update_E", "achieved": round(achieved, 1), "peak": peak,
+                         "unit": "GB/s", "frac": round(achieved / peak, 4), "peak_source": peak_src,
+                         "traffic": traffic, "algorithmic_bytes_per_launch": alg["e_bytes"],
+                         "avg_launch_ms": round(e_ms, 5), "h_sweep_avg_launch_ms": round(h_ms, 5),
+                         "h_sweep_achieved": round(alg["h_bytes"] / (h_ms * 1e-3) / 1e9, 1)},
+            "hbm_gbs_step": round(alg["step_bytes"] / ((e_ms + h_ms) * 1e-3) / 1e9, 1),
+            "per_cell": round(alg["per_cell"], 2)}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -554,8 +767,12 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--workload", default="b512", choices=sorted(WORKLOADS))
     ap.add_argument("--fdtd-steps", type=int, default=10, help="time steps per bench step")
-    ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64", "fp16", "bf16"],
-                    help="field storage; fp16/bf16 store E, H, psi in 16 bits and compute in FP32")
+    ap.add_argument("--precision", default="fp64", choices=["fp32", "fp64", "fp16", "bf16"],
+                    help="the headline's storage: fp64 (the reference's arithmetic), fp32, or fp16/bf16 (E, H, "
+                         "psi stored in 16 bits, FP32 arithmetic)")
+    ap.add_argument("--forms", default="fp64,fp32,bf16,fp16",
+                    help="storage forms measured beside the headline, each with its roofline and its accuracy "
+                         "against the FP64 solve (the FP64 solve is needed for the accuracy blocks)")
     ap.add_argument("--serving", action="store_true",
                     help="serving form: a stream of small solves through the packed engine (own JSON line)")
     ap.add_argument("--serving-jobs", type=int, default=48)
@@ -608,162 +825,88 @@ def main():
     if args.impl == "reference":
         if rank != 0:
             return
-        value, info = cpu_reference(sample_cfg, K, W, S)
-        line = {"metric": "Mcell-updates/s", "value": round(value, 3), "unit": "Mcell-updates/s", "n_gpus": args.gpus,
-                "steps": K, "warmup": W, "higher_is_better": True, "impl": "reference", "scaling": "weak",
-                "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-                "config": {"workload": desc + " -- bounded CPU sample", "sample_config": sample_cfg,
-                           "fdtd_steps_per_step": S},
-                "cpu_baseline": info,
-                "e2e": {"value": round(value, 3), "unit": "Mcell-updates/s", "h2d_bytes_per_step": 0,
-                        "d2h_bytes_per_step": 0}}
-        print(json.dumps(line))
+        print(json.dumps(reference_arm(args, cfg, sample_cfg, desc, K, W)))
         return
 
-    prec = {"fp32": PKG.PREC_FP32, "fp64": PKG.PREC_FP64, "fp16": PKG.PREC_FP16, "bf16": PKG.PREC_BF16}[args.precision]
-    word = {"fp32": 4, "fp64": 8, "fp16": 2, "bf16": 2}[args.precision]
-    coef_word = 8 if prec == PKG.PREC_FP64 else 4
     setup = PKG.Setup.from_file(PKG.config_path(cfg))
     cells = setup.shape[0] * setup.shape[1] * setup.shape[2]
+    head = args.precision
+    forms = [head] + [f for f in args.forms.split(",") if f and f != head]
+
     # ---------------------------------------------------------------- e2e through the C ABI
     # Measured first, as a user's first solve in a process: after a warm-up solve of the same
     # physics on the small sample grid (CUDA context, kernel modules), before the device-
-    # resident runs, whose retired solves would leave the memory pool in their own pieces
-    # (measured: 0.58 s after a whole solve, 0.87-1.10 s after the 4-shard solve).
-    e2e = None
-    if not args.no_e2e:
-        import numpy as np
-        warm = PKG.Solver(PKG.Setup.from_file(PKG.config_path(sample_cfg)), device=local, precision=prec)
-        warm.run(S)
-        warm.probe_series()
-        warm.field("Ez")
-        warm.close()
-        del warm
-        # bytes fdtd_create copies host -> device: the material (the setup's row index, 2 bytes
-        # per cell, and its row table -- or bE as three FP64 idx3 arrays), 1-D spacing / CPML
-        # arrays, gain box (counted before the timed region)
-        nrows = int(setup.view.n_bE_rows)
-        h2d = (2 * cells + 24 * nrows if nrows else 3 * cells * 8) + sum(8 * n for n in setup.shape) * 16
-        if setup.view.n_tls_regions:
-            m = setup.array("tls_region_map").reshape(setup.shape) >= 0
-            box = int(np.prod([np.ptp(np.nonzero(m.any(axis=tuple(x for x in range(3) if x != ax)))[0]) + 1
-                               for ax in range(3)]))
-            h2d += box * (2 * coef_word + 1)
-            del m
-        barrier(dist)
-        t0 = time.perf_counter()
-        # the whole solve: creating four shards (four slices of the setup, four sets of buffers)
-        # costs more than their overlap saves over 200 steps (measured 1.7 s against 0.8 s)
-        s2 = PKG.Solver(setup, device=local, precision=prec)
-        d2h = 0
-        for _ in range(K):
-            s2.run(S)
-            series = s2.probe_series()
-            d2h += series[-S:].nbytes
-        ez = s2.field("Ez")
-        d2h += ez.nbytes
-        s2.close()
-        t_e2e = time.perf_counter() - t0
-        t_e2e = reduce_max(dist, t_e2e)
-        e2e = {"value": round(cells * K * S * world / t_e2e / 1e6, 3), "unit": "Mcell-updates/s",
-               "h2d_bytes_per_step": int(h2d / K), "d2h_bytes_per_step": int(d2h / K),
-               "seconds": round(t_e2e, 4)}
-        del ez, series, np
+    # resident runs, whose retired solves would leave the memory pool in their own pieces.
+    e2e = None if args.no_e2e else e2e_run(setup, sample_cfg, PREC[head], local, K, S, dist, world)
 
-    # ---------------------------------------------------------------- device-resident value
-    sol = PKG.Solver(setup, device=local, precision=prec, shards=args.shards)
-    whole = PKG.Solver(setup, device=local, precision=prec) if args.shards > 1 else sol
-    alg = algorithmic_bytes(setup, word, coef_word, 2 if whole.material_rows else 0)
-    if whole is not sol:
-        whole.close()
-    for _ in range(W):
-        sol.run(S)
-    sol.synchronize()
-    sol.set_timing(PKG.TIMING_RUN)  # one event pair per run() call on the library's stream
-    barrier(dist)
-    clocks = ClockSampler(local)
-    clocks.start()
-    t_wall = time.perf_counter()
-    launches_a = sol.kernel_launches
-    for _ in range(K):
-        sol.run(S)
-    sol.synchronize()
-    t_wall = time.perf_counter() - t_wall
-    launches_b = sol.kernel_launches
-    clk = clocks.stop()
-    barrier(dist)
-    dev_ms = sol.timing()["run_ms"]
-    dev_ms_max = reduce_max(dist, dev_ms)
-    # roofline pass: per-kernel events (one sync per step), a few bench steps after the timed
-    # region; a sharded run takes them from the whole solve (its kernels run per shard, overlapped)
-    if args.shards > 1:
-        sol.close()
-        sol = PKG.Solver(setup, device=local, precision=prec)
-        sol.run(S)
-    sol.set_timing(PKG.TIMING_KERNELS)
-    for _ in range(min(K, 5)):
-        sol.run(S)
-    tm = sol.timing()
-    steps_total = K * S
-    value = replica_value(cells, steps_total, world, dev_ms_max)
-    peak, peak_src = peaks()
-    path = int(os.environ.get("FDTD_B200_KERNEL_PATH", "1"))
-    fused = path in (0, 2)  # one launch per step carries the whole step's bytes
-    e_avg_ms = tm["e_ms"] / tm["steps"]
-    h_avg_ms = tm["h_ms"] / tm["steps"]
-    achieved_step = alg["step_bytes"] / ((e_avg_ms + h_avg_ms) * 1e-3) / 1e9
-    if fused:  # one launch per step: the dominant kernel carries the whole step's bytes
-        kern, kern_bytes, kern_ms = ("k_step_fused" if path == 0 else "k_step_slabs"), alg["step_bytes"], e_avg_ms + h_avg_ms
-    else:
-        kern, kern_bytes, kern_ms = "k_update_E", alg["e_bytes"], e_avg_ms
-    achieved_e = kern_bytes / (kern_ms * 1e-3) / 1e9
-    traffic = None
-    prof = ROOT / "profiles" / f"{kern}_{args.workload}_{args.precision}_traffic.json"
-    if prof.exists():
-        traffic = json.loads(prof.read_text()).get("dram_bytes_per_launch")
-    sol.close()
-    del sol
+    # ---------------------------------------------------------------- device-resident values
+    # Every storage form steps the same workload from the same state for W + K runs of S
+    # steps; the FP64 solve stays open as the accuracy reference of the others.
+    runs = {}
+    for f in forms:
+        runs[f] = device_run(setup, f, args.shards, W, K, S, local, dist)
+    ref_sol = runs["fp64"]["solve"] if "fp64" in runs else None
+    acc = {}
+    if ref_sol is not None:
+        acc = accuracy({f: runs[f]["solve"] for f in forms if f != "fp64"}, ref_sol)
+    for f in forms:
+        runs[f]["solve"].close()
+        runs[f]["solve"] = None
+    roof = {f: kernel_roofline(setup, f, S, K, local) for f in forms}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         _, cpu = cpu_reference(sample_cfg, 3, 3, 10 if args.workload == "b512" else S)
-
     if rank != 0:
+        if dist is not None:
+            dist.destroy_process_group()
         return
+
+    def block(f):
+        r = runs[f]
+        b = {"value": round(replica_value(cells, K * S, world, r["dev_ms_max"]), 3), "unit": "Mcell-updates/s",
+             "ms_per_step": round(r["dev_ms_max"] / K, 4), "dtype": DTYPE[f], "roofline": roof[f]["roofline"],
+             "hbm_gbs_step": roof[f]["hbm_gbs_step"], "algorithmic_bytes_per_cell_step": roof[f]["per_cell"]}
+        if f in acc:
+            b["accuracy_vs_fp64"] = acc[f]
+        return b
+
+    h = runs[head]
     line = {
         "metric": "Mcell-updates/s",
-        "value": round(value, 3),
+        "value": round(replica_value(cells, K * S, world, h["dev_ms_max"]), 3),
         "unit": "Mcell-updates/s",
         "n_gpus": world,
         "steps": K,
         "warmup": W,
-        "ms_per_step": round(dev_ms_max / K, 4),
+        "ms_per_step": round(h["dev_ms_max"] / K, 4),
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
-        "dtype": {"fp32": "f32", "fp64": "f64", "fp16": "f32 (fp16 storage)", "bf16": "f32 (bf16 storage)"}[args.precision],
+        "dtype": DTYPE[head],
         "data": "synthetic",
-        "config": {"workload": desc, "config_file": cfg, "total_cells": cells, "grid": list(setup.shape),
-                   "fdtd_steps_per_step": S,
-                   "parallelism": ("replicas" if world > 1 else "single GPU")
-                   + (f", {args.shards} z-shards overlapped on the GPU" if args.shards > 1 else ""),
-                   "roofline_timing": "whole (unsharded) solve, per-kernel events" if args.shards > 1 else "per-kernel events",
-                   "kernel_path": {0: "fused H+E (TMA)", 1: "separate H and E sweeps",
-                                   2: "slab-ordered H+E step (one launch, L2-resident slabs)"}[path],
-                   "fused_shape": os.environ.get("FDTD_B200_FUSED_SHAPE", "0"),
-                   "l2": "state (~%.1f GB) larger than L2, no flush" % (alg["cells"] * word * 9 / 1e9),
-                   "hbm_gbs_step": round(achieved_step, 1),
-                   "algorithmic_bytes_per_cell_step": round(alg["per_cell"], 2),
-                   "wall_ms_per_step": round(t_wall * 1e3 / K, 4)},
-        "roofline": {"bound": "hbm", "kernel": kern, "achieved": round(achieved_e, 1), "peak": peak,
-                     "unit": "GB/s", "frac": round(achieved_e / peak, 4), "peak_source": peak_src,
-                     "traffic": traffic, "algorithmic_bytes_per_launch": kern_bytes,
-                     "avg_launch_ms": round(kern_ms, 5)},
+        "config": workload_config(setup, cfg, desc),
+        "detail": {"fdtd_steps_per_step": S,
+                   "parallelism": ("replicas, one per GPU" if world > 1 else "single GPU")
+                   + (f", {args.shards} z-shards of the solve overlapped on the GPU" if args.shards > 1 else ""),
+                   "roofline_timing": "whole (unsharded) solve, per-kernel CUDA events on the library's stream",
+                   "kernel_path": "separate H and E sweeps",
+                   "l2": "state (%.1f GB of fields) larger than L2 (126 MB), no flush" % (cells * WORD[head] * 6 / 1e9),
+                   "wall_ms_per_step": round(h["wall_ms"] / K, 4),
+                   "accuracy_note": "each form against the FP64 solve after the same W + K runs of S steps "
+                                    "from the same initial state: relative L2 of the stacked E and H components, "
+                                    "of the probe series and of the 21-frequency DFT"},
+        "roofline": roof[head]["roofline"],
         "e2e": e2e,
         "cpu_baseline": cpu,
-        "gpu_launches": int(launches_b - launches_a),
-        "clocks": clk,
+        "gpu_launches": int(h["launches"]),
+        "clocks": h["clocks"],
     }
+    line["detail"]["hbm_gbs_step"] = roof[head]["hbm_gbs_step"]
+    line["detail"]["algorithmic_bytes_per_cell_step"] = roof[head]["per_cell"]
+    for f in forms:
+        if f != head:
+            line[f] = block(f)
     print(json.dumps(line))
     if dist is not None:
         dist.destroy_process_group()

@@ -270,9 +270,11 @@ int fdtd_material_rows(const fdtd_handle *h, uint64_t *rows);
 /* Select FDTD_TIMING_OFF / _RUN / _KERNELS; any call resets the totals. */
 int fdtd_set_timing(fdtd_handle *h, int mode);
 int fdtd_get_timing(fdtd_handle *h, fdtd_timing_v1 *out);
-/* Kernel path, before the first step only: 0 = one fused H+E launch per step with
- * TMA-staged planes, 1 = separate H and E sweeps (default), 2 = one persistent launch that
- * runs the H and E sweeps slab by slab in dependency order.  Results agree to rounding. */
+/* Kernel path, before the first step only: 1 = separate H and E sweeps (default), 2 = one
+ * persistent launch that runs the H and E sweeps slab by slab in dependency order (its
+ * device waits are bounded; an expired wait makes fdtd_run return FDTD_ERR_TIMEOUT).  Both
+ * paths give bit-identical results.  0 (one fused H+E launch per step) is reserved and
+ * refused with FDTD_ERR_UNSUPPORTED. */
 int fdtd_set_kernel_path(fdtd_handle *h, int path);
 /* Streams the reference's detector files of the parsed setup `s` -- the one whose view
  * created h -- while the handle steps (FieldMovie2D and PointFieldDetector,

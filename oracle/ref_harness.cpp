@@ -130,17 +130,18 @@ bool read_f64(const std::string& path, std::vector<double>& v) {
 
 int main(int argc, char** argv) {
     if (argc < 3) {
-        std::fprintf(stderr, "usage: %s PARAMS OUTDIR [--steps N] [--mesh-only] [--dump-materials] [--init DIR] [--no-fields] [--detectors]\n", argv[0]);
+        std::fprintf(stderr, "usage: %s PARAMS OUTDIR [--steps N] [--warmup W] [--mesh-only] [--dump-materials] [--init DIR] [--no-fields] [--detectors]\n", argv[0]);
         return 2;
     }
     const std::string params_path = fs::absolute(argv[1]).string();
     const std::string outdir = fs::absolute(argv[2]).string();
-    long long steps_override = -1;
+    long long steps_override = -1, warmup = 0;
     bool mesh_only = false, dump_materials = false, dump_fields = true, with_detectors = false;
     std::string init_dir;
     for (int a = 3; a < argc; ++a) {
         std::string s = argv[a];
         if (s == "--steps" && a + 1 < argc) steps_override = std::atoll(argv[++a]);
+        else if (s == "--warmup" && a + 1 < argc) warmup = std::max(0LL, std::atoll(argv[++a]));
         else if (s == "--mesh-only") mesh_only = true;
         else if (s == "--dump-materials") dump_materials = true;
         else if (s == "--no-fields") dump_fields = false;
@@ -524,8 +525,14 @@ int main(int argc, char** argv) {
     // ---- time loop (src/3D_FDTD_version008.cpp:269-328, serial path) ----
     const size_t nsteps = steps_override >= 0 ? size_t(steps_override) : P.nSteps;
     std::vector<double> probe_series;
+    // the first `warmup` steps run untimed; loop_seconds covers the remaining steps, and
+    // step_seconds lists each timed step
+    const size_t warm = std::min<size_t>(size_t(warmup), nsteps);
+    std::vector<double> step_s;
     auto t_begin = std::chrono::steady_clock::now();
+    auto t_step = t_begin;
     for (size_t n = 0; n < nsteps; ++n) {
+        if (n == warm) t_begin = t_step = std::chrono::steady_clock::now();
         std::fill(Jx.begin(), Jx.end(), 0.0);
         std::fill(Jy.begin(), Jy.end(), 0.0);
         std::fill(Jz.begin(), Jz.end(), 0.0);
@@ -565,14 +572,22 @@ int main(int argc, char** argv) {
         if (pop_detector) pop_detector->record(n, tls_state);
         if (pol_diagnostics) pol_diagnostics->record(n, tls_state, Ez, ctx.grid_spacing);
         if (tls_global_history) tls_global_history->record(n, tls_state);
+        if (n >= warm) {
+            const auto now = std::chrono::steady_clock::now();
+            step_s.push_back(std::chrono::duration<double>(now - t_step).count());
+            t_step = now;
+        }
     }
+    if (warm == nsteps) t_begin = std::chrono::steady_clock::now();
     if (pop_detector) pop_detector->finalize(tls_state);
     if (tls_global_history) tls_global_history->finalize();
     auto t_end = std::chrono::steady_clock::now();
     for (auto& det : dets) det->finalize();
     const double loop_s = std::chrono::duration<double>(t_end - t_begin).count();
-    meta << "  \"steps\": " << nsteps << ", \"loop_seconds\": " << loop_s << ", \"threads\": "
-         << omp_get_max_threads() << ",\n";
+    meta << "  \"steps\": " << nsteps << ", \"warmup_steps\": " << warm << ", \"loop_seconds\": " << loop_s
+         << ", \"threads\": " << omp_get_max_threads() << ", \"step_seconds\": [";
+    for (size_t q = 0; q < step_s.size(); ++q) meta << (q ? ", " : "") << step_s[q];
+    meta << "],\n";
 
     // Diagnostics at the final state (src/stability_monitor.hpp:155-178,
     // src/two_level_system.hpp:344-418).

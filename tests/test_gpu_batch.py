@@ -64,17 +64,58 @@ def test_batch_result_is_the_same_alone_and_in_the_mix(pkg):
 
 
 def test_batch_matches_single_solves(pkg):
-    """Against fdtd_create + fdtd_run: the packed kernels are a separate compilation of the
-    same block code, so the two agree to FP32 rounding (measured: 5e-5 on the probe series
-    after 150 steps, 4e-7 on the DFT), not bit for bit."""
+    """Against fdtd_create + fdtd_run, bit for bit: the packed kernels run the same block code
+    with explicitly rounded arithmetic (every product, difference and fused multiply-add is an
+    intrinsic, so no instantiation contracts differently), the same probe/DFT code, and the
+    monitor's max |E| does not depend on the reduction order.  The monitor's FP64 integrals
+    are sums in a different block order: 1e-12 relative."""
     setups = [(_setup(pkg, src, ov), n) for src, ov, n in CASES]
     got = _batch_results(pkg, setups)
     for (s, n), (series, dft, diag) in zip(setups, got):
         ref = _single(pkg, s, n)
-        assert np.linalg.norm(series - ref[0]) <= 2e-4 * np.linalg.norm(ref[0])
-        assert np.abs(dft - ref[1]).max() <= 1e-5 * np.abs(ref[1]).max()
-        assert abs(diag["max_E"] - ref[2]["max_E"]) <= 2e-4 * ref[2]["max_E"]
+        assert np.array_equal(series, ref[0]) and np.array_equal(dft, ref[1])
+        assert diag["max_E"] == ref[2]["max_E"]
+        for k in ("integrated_Nu", "integrated_Ng", "polarization_energy"):
+            assert abs(diag[k] - ref[2][k]) <= 1e-12 * abs(ref[2][k]), k
         assert diag["step"] == ref[2]["step"] and diag["steps_done"] == n
+
+
+@pytest.mark.parametrize("case", ["step_g0_sphere", "step_g2_planewave"])
+def test_batch_matches_reference_golden(pkg, case):
+    """Packed FP32 solves against the reference's own FP64 probe series (golden state of the
+    dielectric-sphere and plane-wave cases, src/3D_FDTD_version008.cpp:269-328 replayed by the
+    reference harness): within the single-solve FP32 bar, 1e-5 relative."""
+    from conftest import golden
+    g = golden(case)
+    s = pkg.Setup.from_file(GOLDEN / "cases" / (case + ".params"))
+    steps = g["meta"]["steps"]
+    (series, dft, diag), = _batch_results(pkg, [(s, steps)])
+    assert _rel(series, g["probe_series"].reshape(series.shape)) <= 1e-5
+    assert diag["stable"] == 1
+
+
+def test_batch_c0_matches_oracle(pkg, oracle):
+    """A packed FP32 solve of the 80^3 sphere config against the oracle (the C restatement of
+    the reference loop, FP64): probe series and DFT within 1e-5 relative."""
+    s = _setup(pkg, "c0_dipole_sphere.params", {})
+    ref = oracle.OracleSolve(s, 0).run(300)
+    (series, dft, _), = _batch_results(pkg, [(s, 300)])
+    assert _rel(series, ref.reshape(series.shape)) <= 1e-5
+    assert _rel(dft, oracle.dft(ref[:, 0], s.dt, s.array("dft_freqs"))) <= 1e-5
+
+
+def test_batch_gain_matches_oracle_at_fp32_storage_floor(pkg, oracle):
+    """A packed FP32 solve with gain (pump 1e11, zero initial field) against the FP64 oracle.
+    Here FP32 storage itself cannot reach 1e-5: the oracle's FP32 twin (the same formulas with
+    FP32 storage) is 3.4e-5 from FP64 on the probe series.  The packed solve must be within
+    1.5x of that floor (and below 5e-5), the DFT within 1e-5."""
+    s = _setup(pkg, GOLDEN / "cases" / "step_g1_gain.params", {"PUMP_RATE": "1e11"})
+    ref = oracle.OracleSolve(s, 0).run(120)
+    twin = oracle.OracleSolve(s, 1).run(120)
+    floor = _rel(twin, ref)
+    (series, dft, _), = _batch_results(pkg, [(s, 120)])
+    err = _rel(series, ref.reshape(series.shape))
+    assert err <= min(5e-5, 1.5 * floor), (err, floor)
 
 
 def test_batch_admits_by_memory_budget(pkg):
@@ -87,7 +128,7 @@ def test_batch_admits_by_memory_budget(pkg):
     assert [b.state(t)[0] for t in tickets] == [pkg.JOB_RESIDENT, pkg.JOB_QUEUED, pkg.JOB_QUEUED]
     _drain(pkg, b, tickets)
     first = b.probe_series(tickets[0])
-    assert np.linalg.norm(first - single[0]) <= 2e-4 * np.linalg.norm(single[0])
+    assert np.array_equal(first, single[0])
     for t in tickets[1:]:
         assert np.array_equal(b.probe_series(t), first)
     with pytest.raises(pkg.FdtdError) as e:
@@ -106,7 +147,7 @@ def test_batch_unstable_job_fails_alone(pkg):
     st, done = b.state(tb)
     assert st == pkg.JOB_FAILED and done == 101  # 11th threshold warning at monitor step 100
     assert b.state(tg)[0] == pkg.JOB_DONE
-    assert np.linalg.norm(b.probe_series(tg) - ref[0]) <= 2e-4 * np.linalg.norm(ref[0])
+    assert np.array_equal(b.probe_series(tg), ref[0])
     b.close()
 
 
@@ -183,7 +224,7 @@ def test_batch_mixed_storage_alone_and_in_the_mix(pkg, shape, monkeypatch):
 
 
 def _rel(a, b):
-    return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+    return float(np.linalg.norm(np.ravel(a) - np.ravel(b)) / np.linalg.norm(np.ravel(b)))
 
 
 # The bars of test_16bit_storage_spectrum (the single-solve 16-bit forms against FP64):
@@ -203,16 +244,16 @@ def test_batch_16bit_spectrum_against_fp64(pkg, precision, cfg, tol):
     assert _rel(d16, d64) <= tol
 
 
-def test_batch_bf16_matches_single_bf16_solve(pkg):
-    """Against fdtd_create + fdtd_run of the same BF16 solve (both with the staged sweeps; the
-    packed kernels are a separate compilation of the same block code): equal to BF16 rounding."""
+@pytest.mark.parametrize("precision", [3, 2])
+def test_batch_16bit_matches_single_16bit_solve(pkg, precision):
+    """Against fdtd_create + fdtd_run of the same BF16 / FP16 solve: the same explicitly rounded
+    block code, so the probe series, DFT and max |E| are bit-identical."""
     s = _setup(pkg, "c1_gain_slab.params", {"PUMP_RATE": "1e9"})
-    sol = pkg.Solver(s, precision=3, kernel_path=1)
+    sol = pkg.Solver(s, precision=precision, kernel_path=1)
     sol.run(300)
     ref = (sol.probe_series(), sol.dft(0), sol.diagnostics())
     sol.close()
-    (series, dft, diag), = _batch_views(pkg, [(s, _with_precision(s, 3), 300)])
-    assert _rel(series, ref[0]) <= 2e-2
-    assert np.abs(dft - ref[1]).max() <= 2e-2 * np.abs(ref[1]).max()
-    assert abs(diag["max_E"] - ref[2]["max_E"]) <= 2e-2 * ref[2]["max_E"]
+    (series, dft, diag), = _batch_views(pkg, [(s, _with_precision(s, precision), 300)])
+    assert np.array_equal(series, ref[0]) and np.array_equal(dft, ref[1])
+    assert diag["max_E"] == ref[2]["max_E"]
     assert diag["steps_done"] == 300
