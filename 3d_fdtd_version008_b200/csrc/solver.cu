@@ -28,6 +28,7 @@
 #include <numbers>
 #include <stdexcept>
 #include <string>
+#include <thread>
 #include <vector>
 
 namespace fdtdk {
@@ -1870,12 +1871,16 @@ public:
                                             int(EPipe<float>::bytes())),
                        "cudaFuncSetAttribute");
             }
+            worker_ = std::thread([this] { prepare_loop(); });
         } catch (...) {
             release_all();
             throw;
         }
     }
-    ~Batch() { release_all(); }
+    ~Batch() {
+        stop_worker();
+        release_all();
+    }
 
     uint64_t submit(const fdtd_setup_v1& s, uint64_t nsteps) {
         int storage = 0;
@@ -1891,42 +1896,59 @@ public:
         j.storage = storage;
         j.bytes = footprint(s);
         if (j.bytes > budget_) throw Failure(FDTD_ERR_OOM, "job footprint exceeds the batch memory budget");
+        std::lock_guard<std::mutex> l(mu_);
         const uint64_t t = next_++;
         jobs_.emplace(t, std::move(j));
         queue_.push_back(t);
+        cv_work_.notify_one();
         return t;
     }
 
-    // Admits what fits, then advances the resident solves by up to max_steps steps each,
-    // retiring solves as they reach their target.
+    // Splices in the solves the admission worker has made ready, then advances the resident
+    // solves by up to max_steps steps each, retiring solves as they reach their target and
+    // splicing in newly ready ones at every check.  With nothing resident it first waits for
+    // the worker to prepare every job that can be admitted (or returns when there is none).
     void run(uint64_t max_steps) {
         ck(cudaSetDevice(device_), "cudaSetDevice");
-        admit();
+        splice(true);
         for (uint64_t t = 0; t < max_steps && !res_.empty(); ++t) {
             step();
             bool finished = false;
             for (uint64_t r : res_) finished |= jobs_.at(r).steps() >= jobs_.at(r).target;
             if (finished || ++since_check_ >= kCheckEvery) {
                 check_and_retire();
-                admit();
+                splice(res_.empty());
             }
         }
         ck(cudaStreamSynchronize(st_), "batch run");
     }
 
-    Job& job(uint64_t t) {
-        auto it = jobs_.find(t);
-        if (it == jobs_.end()) throw Failure(FDTD_ERR_INVALID, "unknown ticket");
-        return it->second;
+    // A finished job's record (DONE or FAILED); the caller reads it without the worker
+    // touching it again.
+    Job& finished_job(uint64_t t) {
+        std::lock_guard<std::mutex> l(mu_);
+        Job& j = job_locked(t);
+        if (j.state != DONE && j.state != FAILED) throw Failure(FDTD_ERR_INVALID, "job has not finished");
+        return j;
+    }
+    // API state and steps done of any job.
+    void state_of(uint64_t t, int* state, uint64_t* steps_done) {
+        std::lock_guard<std::mutex> l(mu_);
+        Job& j = job_locked(t);
+        *state = j.state;
+        if (steps_done) *steps_done = j.state == RESIDENT ? j.steps() : j.state == QUEUED ? 0 : j.diag.steps_done;
     }
     void release(uint64_t t) {
-        Job& j = job(t);
+        std::lock_guard<std::mutex> l(mu_);
+        Job& j = job_locked(t);
         if (j.state != DONE && j.state != FAILED) throw Failure(FDTD_ERR_INVALID, "job has not finished");
         jobs_.erase(t);
     }
     uint32_t resident() const { return uint32_t(res_.size()); }
-    uint32_t queued() const { return uint32_t(queue_.size()); }
-    uint64_t used() const { return used_; }
+    uint32_t queued() const {
+        std::lock_guard<std::mutex> l(mu_);
+        return uint32_t(queue_.size() + preparing_ + ready_.size());
+    }
 
 private:
     static constexpr int kRing = 64;        // pinned per-step records in flight
@@ -1971,6 +1993,19 @@ private:
             throw Failure(FDTD_ERR_INVALID, "device " + std::to_string(dev) + " already has a packed engine in this process");
         owned.push_back(dev);
     }
+    Job& job_locked(uint64_t t) {
+        auto it = jobs_.find(t);
+        if (it == jobs_.end()) throw Failure(FDTD_ERR_INVALID, "unknown ticket");
+        return it->second;
+    }
+    void stop_worker() {
+        {
+            std::lock_guard<std::mutex> l(mu_);
+            stop_ = true;
+        }
+        cv_work_.notify_all();
+        if (worker_.joinable()) worker_.join();
+    }
     void release_all() {
         cudaSetDevice(device_);
         if (st_) cudaStreamSynchronize(st_);
@@ -1997,13 +2032,29 @@ private:
         return b + (64ull << 10) + 3ull * (s.NxT + NyT + NzT) * 8 * 8;
     }
 
-    void admit() {
-        bool changed = false;
-        while (!queue_.empty() && res_.size() < size_t(kMaxBatch)) {
+    // Admission worker: takes queued jobs first come, first served while their footprint fits
+    // the budget (counting resident, ready and in-preparation solves) and fewer than kMaxBatch
+    // are resident or on the way, and builds each one's Solver -- device allocation, set-up
+    // uploads, its probe series buffer -- on the solve's own stream, while the stepping thread
+    // keeps launching packed steps.  Ready solves wait in ready_ until the stepping thread
+    // splices them in (splice), so admission never stalls the packed step.
+    void prepare_loop() {
+        std::unique_lock<std::mutex> l(mu_);
+        for (;;) {
+            cv_work_.wait(l, [&] {
+                if (stop_) return true;
+                if (queue_.empty()) return false;
+                const Job& j = jobs_.at(queue_.front());
+                return used_ + j.bytes <= budget_ && nres_ + preparing_ + ready_.size() < size_t(kMaxBatch);
+            });
+            if (stop_) return;
             const uint64_t t = queue_.front();
-            Job& j = jobs_.at(t);
-            if (used_ + j.bytes > budget_) break;  // first come, first served
             queue_.pop_front();
+            Job& j = jobs_.at(t);
+            used_ += j.bytes;
+            ++preparing_;
+            l.unlock();
+            std::string err;
             try {
                 if (j.storage == 0) j.f32 = std::make_unique<Solver<float, float>>(*j.setup, device_);
                 else if (j.storage == 1) j.f16 = std::make_unique<Solver<__half, float>>(*j.setup, device_);
@@ -2012,17 +2063,42 @@ private:
                     v.ensure_series((j.target + v.save_every_ - 1) / v.save_every_);
                     ck(cudaStreamSynchronize(v.st_), "admit");
                 });
-                j.state = RESIDENT;
-                used_ += j.bytes;
-                res_.push_back(t);
-                changed = true;
             } catch (const std::exception& e) {
+                err = e.what();
                 j.drop();
-                j.state = FAILED;
-                j.err = e.what();
             }
+            l.lock();
+            --preparing_;
+            if (err.empty()) {
+                ready_.push_back(t);
+            } else {
+                j.state = FAILED;
+                j.err = err;
+                used_ -= j.bytes;
+            }
+            cv_ready_.notify_all();
         }
-        if (changed) rebuild();
+    }
+
+    // Moves the ready solves into the resident set (admission order) and rebuilds the packed
+    // tables.  wait (nothing resident, so the GPU is idle): first wait until the worker has
+    // prepared every job that can be admitted now, so a batch starts with all that fit.
+    void splice(bool wait) {
+        std::vector<uint64_t> add;
+        {
+            std::unique_lock<std::mutex> l(mu_);
+            auto admissible = [&] {
+                return !queue_.empty() && used_ + jobs_.at(queue_.front()).bytes <= budget_ &&
+                       nres_ + preparing_ + ready_.size() < size_t(kMaxBatch);
+            };
+            if (wait) cv_ready_.wait(l, [&] { return stop_ || (preparing_ == 0 && !admissible()); });
+            add.swap(ready_);
+            for (uint64_t t : add) jobs_.at(t).state = RESIDENT;
+            nres_ = res_.size() + add.size();
+        }
+        if (add.empty()) return;
+        res_.insert(res_.end(), add.begin(), add.end());
+        rebuild();
     }
 
     // Per-solve constants and the packed block tables.
@@ -2177,21 +2253,36 @@ private:
                 if (v.nprobes_ && v.nf_)
                     ck(cudaMemcpy(j.dft.data(), v.d_dft_, j.dft.size() * sizeof(double), cudaMemcpyDeviceToHost), "dft");
                 v.diagnostics(&j.diag);
-                j.state = status ? FAILED : DONE;
             });
             if (stay) { keep.push_back(t); continue; }
             j.drop();
+            std::lock_guard<std::mutex> l(mu_);
+            j.state = h_status_[r] ? FAILED : DONE;
             j.setup = nullptr;
             used_ -= j.bytes;
         }
         const bool changed = keep.size() != res_.size();
         res_.swap(keep);
+        {
+            std::lock_guard<std::mutex> l(mu_);
+            nres_ = res_.size();
+        }
+        cv_work_.notify_one();  // retired footprint and slots free up
         if (changed) rebuild();
     }
 
     int device_;
-    uint64_t budget_, used_ = 0, next_ = 1;
+    uint64_t budget_, used_ = 0, next_ = 1;  // used_: resident, ready and in-preparation footprints
     cudaStream_t st_ = nullptr;
+    // mu_ guards jobs_' structure, queue_, ready_, preparing_, nres_, used_ and the job states;
+    // a job's Solver belongs to the worker while it is being prepared and to the stepping
+    // thread from the splice on.
+    mutable std::mutex mu_;
+    std::condition_variable cv_work_, cv_ready_;
+    std::thread worker_;
+    bool stop_ = false;
+    size_t preparing_ = 0, nres_ = 0;
+    std::vector<uint64_t> ready_;
     std::map<uint64_t, Job> jobs_;
     std::deque<uint64_t> queue_;
     std::vector<uint64_t> res_;  // resident tickets in slot order
@@ -2842,18 +2933,13 @@ int fdtd_batch_run(fdtd_batch* b, uint64_t max_steps, uint32_t* n_resident, uint
 
 int fdtd_batch_job_state(fdtd_batch* b, uint64_t ticket, int* state, uint64_t* steps_done) {
     if (!b || !state) return FDTD_ERR_INVALID;
-    return bguard(b, [&] {
-        Batch::Job& j = b->b->job(ticket);
-        *state = j.state;
-        if (steps_done) *steps_done = j.live() ? j.steps() : j.diag.steps_done;
-    });
+    return bguard(b, [&] { b->b->state_of(ticket, state, steps_done); });
 }
 
 int fdtd_batch_probe_series(fdtd_batch* b, uint64_t ticket, double* out, uint64_t max_samples, uint64_t* n_samples) {
     if (!b || !n_samples) return FDTD_ERR_INVALID;
     return bguard(b, [&] {
-        Batch::Job& j = b->b->job(ticket);
-        if (j.state != Batch::DONE && j.state != Batch::FAILED) throw Failure(FDTD_ERR_INVALID, "job has not finished");
+        Batch::Job& j = b->b->finished_job(ticket);
         const uint64_t n = std::min<uint64_t>(max_samples, j.samples);
         if (out && n) std::memcpy(out, j.series.data(), n * j.nprobes * sizeof(double));
         *n_samples = j.samples;
@@ -2863,8 +2949,7 @@ int fdtd_batch_probe_series(fdtd_batch* b, uint64_t ticket, double* out, uint64_
 int fdtd_batch_dft(fdtd_batch* b, uint64_t ticket, uint32_t probe, double* re, double* im) {
     if (!b || !re || !im) return FDTD_ERR_INVALID;
     return bguard(b, [&] {
-        Batch::Job& j = b->b->job(ticket);
-        if (j.state != Batch::DONE && j.state != Batch::FAILED) throw Failure(FDTD_ERR_INVALID, "job has not finished");
+        Batch::Job& j = b->b->finished_job(ticket);
         if (probe >= j.nprobes) throw Failure(FDTD_ERR_INVALID, "probe index out of range");
         for (uint32_t m = 0; m < j.nf; ++m) {
             re[m] = j.dft[2 * (size_t(probe) * j.nf + m)];
@@ -2876,8 +2961,7 @@ int fdtd_batch_dft(fdtd_batch* b, uint64_t ticket, uint32_t probe, double* re, d
 int fdtd_batch_diagnostics(fdtd_batch* b, uint64_t ticket, fdtd_diagnostics_v1* out) {
     if (!b || !out) return FDTD_ERR_INVALID;
     return bguard(b, [&] {
-        Batch::Job& j = b->b->job(ticket);
-        if (j.state != Batch::DONE && j.state != Batch::FAILED) throw Failure(FDTD_ERR_INVALID, "job has not finished");
+        Batch::Job& j = b->b->finished_job(ticket);
         *out = j.diag;
     });
 }

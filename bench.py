@@ -237,19 +237,24 @@ def serving_job_text(core: tuple, steps_hint: int) -> str:
 
 
 def serving_bench(args):
-    """A stream of independent gain-slab solves (core edges log-uniform in 32..96 cells, aspect
-    1..2, steps uniform in 200..1000; FP32).  Throughput: all jobs queued at once, served by
-    the packed engine and one at a time by fdtd_create/fdtd_run.  Latency: the same jobs
-    arriving as a Poisson stream at 80 % of the packed engine's measured throughput; the
-    one-at-a-time server's latencies are its FIFO queue over its own measured service times."""
+    """The serving configuration's stream, bounded to --serving-jobs solves: gain-slab
+    microcavities with core edges log-uniform in 32..192 cells (aspect 1..2), steps uniform in
+    2000..20000, 8-cell CPML, FP32, admitted by footprint under a 150 GB budget (seed 3).
+    Throughput: all jobs queued at once, served by the packed engine, and one at a time by
+    fdtd_create/fdtd_run.  Latency: the same jobs arriving as a Poisson stream at 80 % of the
+    packed engine's measured throughput (the admission thread prepares arrivals while the
+    resident solves step); the one-at-a-time server's latencies are its FIFO queue over its own
+    measured service times."""
     import numpy as np
     rng = np.random.default_rng(3)
+    lo, hi = args.serving_edges
+    s_lo, s_hi = args.serving_steps
     jobs = []
     for _ in range(args.serving_jobs):
-        edge = float(np.exp(rng.uniform(np.log(32), np.log(96))))
+        edge = float(np.exp(rng.uniform(np.log(lo), np.log(hi))))
         asp = rng.uniform(1.0, 2.0, size=2)
         core = (int(edge), int(max(16, edge / asp[0])), int(max(16, edge / asp[1])))
-        steps = int(rng.integers(200, 1001))
+        steps = int(rng.integers(s_lo, s_hi + 1))
         jobs.append((core, steps))
     setups = [PKG.Setup.from_text(serving_job_text(c, n)) for c, n in jobs]
     cells = [s.shape[0] * s.shape[1] * s.shape[2] for s in setups]
@@ -318,8 +323,9 @@ def serving_bench(args):
         "metric": "solves/s (packed multi-solve engine)", "value": round(len(jobs) / packed_s, 3), "unit": "solves/s",
         "n_gpus": 1, "steps": len(jobs), "warmup": 0, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": "serving: stream of gain-slab microcavities, core edge 32-96 cells (aspect 1-2), "
-                               "200-1000 steps, 8-cell CPML, FP32", "jobs": len(jobs),
+        "config": {"workload": f"serving: stream of gain-slab microcavities, core edge {lo}-{hi} cells log-uniform "
+                               f"(aspect 1-2), {s_lo}-{s_hi} steps, 8-cell CPML, FP32, Poisson arrivals at 80 % load",
+                   "jobs": len(jobs), "jobs_note": "the first jobs of the seed-3 stream (the full stream is 4000)",
                    "cell_updates": int(work), "budget_GB": 150},
         "packed": {"seconds": round(packed_s, 3), "Mcell_updates_per_s": round(work / packed_s / 1e6, 1),
                    "p50_ms": pct(lat_packed, 50), "p95_ms": pct(lat_packed, 95), "p99_ms": pct(lat_packed, 99)},
@@ -331,23 +337,33 @@ def serving_bench(args):
     print(json.dumps(line))
 
 
+def c4_setups(pumps, steps: int):
+    """The sweep's cavities (configs/c4_cavity.params: the C1 recipe on the auto mesher's graded
+    mesh, 96 x 96 x 65 total cells), one per pump rate."""
+    text = PKG.config_path("c4_cavity.params").read_text().replace("N_STEPS = 20000", f"N_STEPS = {int(steps)}")
+    return [PKG.Setup.from_text(text.replace("PUMP_RATE = 1e9", f"PUMP_RATE = {float(p)!r}")) for p in pumps]
+
+
 def sweep_bench(args):
-    """The batched gain-laser sweep: 256 slab microcavities of 96 x 96 x 64 cells (80 x 80 x 48
-    core at 20 nm, 8-cell CPML, gain layer), pump W_p log-uniform in 1e7..1e11 1/s (seed 4),
-    BF16 field storage with FP32 arithmetic, FP32 populations, FP64 DFT, through the packed
-    engine; --sweep-steps steps each instead of 200000 (the rate is per step).  The same jobs
-    in FP32 storage are timed beside them.  Two figures per storage form: the whole sweep
-    (all jobs queued at once, admission included) and the packed step of 64 resident
-    cavities alone."""
+    """The batched gain-laser sweep: 256 slab microcavities on the auto mesher's graded mesh
+    (96 x 96 x 65 total cells, configs/c4_cavity.params), pump W_p log-uniform in 1e7..1e11
+    1/s (seed 4), BF16 field storage with FP32 arithmetic, FP32 populations, FP64 DFT, through
+    the packed engine, --sweep-steps steps each (200000 for the full sweep).  The same jobs in
+    FP32 storage are timed beside them unless --sweep-forms says otherwise.  Two figures per
+    storage form: the whole sweep (all jobs queued at once, admission included) and the packed
+    step of 64 resident cavities alone; the BF16 sweep also reports each cavity's end state
+    (population inversion, growth of the probe signal) against its pump."""
     import numpy as np
     rng = np.random.default_rng(4)
     pumps = np.exp(rng.uniform(np.log(1e7), np.log(1e11), size=args.sweep_jobs))
     n = args.sweep_steps
-    base = serving_job_text((80, 80, 48), n)
-    setups = [PKG.Setup.from_text(base.replace("PUMP_RATE = 1e9", f"PUMP_RATE = {float(p)!r}")) for p in pumps]
+    setups = c4_setups(pumps, n)
     cells = setups[0].shape[0] * setups[0].shape[1] * setups[0].shape[2]
     out = {}
-    for name, prec in (("bf16", PKG.PREC_BF16), ("fp32", PKG.PREC_FP32)):
+    ends = []
+    forms = [(f, {"bf16": PKG.PREC_BF16, "fp32": PKG.PREC_FP32, "fp16": PKG.PREC_FP16}[f])
+             for f in args.sweep_forms.split(",")]
+    for name, prec in forms:
         views = []
         for s in setups:
             v = PKG.SetupV1.from_buffer_copy(s.view)
@@ -371,6 +387,7 @@ def sweep_bench(args):
         t0 = time.perf_counter()
         ts = [b.submit(s, n, view=v) for s, v in zip(setups, views)]
         pending, failed = set(ts), 0
+        end = {}
         while pending:
             b.run(64)
             for t in list(pending):
@@ -378,10 +395,27 @@ def sweep_bench(args):
                 if st >= PKG.JOB_DONE:
                     failed += st == PKG.JOB_FAILED
                     b.dft(t)
+                    if name == forms[0][0]:
+                        d = b.diagnostics(t)
+                        ser = b.probe_series(t)[:, 0]
+                        end[t] = (d, ser)
                     b.release(t)
                     pending.discard(t)
         wall = time.perf_counter() - t0
         b.close()
+        if name == forms[0][0]:
+            dt = setups[0].view.dt
+            for q, t in enumerate(ts):
+                d, ser = end[t]
+                nu, ng = d["integrated_Nu"], d["integrated_Ng"]
+                # growth of the probe signal over the last half of the run (RMS of the two
+                # quarters), in 1/ps: > 0 would mean net gain
+                m = len(ser) // 4
+                r1 = float(np.sqrt(np.mean(ser[-2 * m:-m] ** 2))) if m else 0.0
+                r2 = float(np.sqrt(np.mean(ser[-m:] ** 2))) if m else 0.0
+                g = float(np.log(r2 / r1) / (m * dt) * 1e-12) if r1 > 0 and r2 > 0 else None
+                ends.append({"pump_per_s": float(pumps[q]), "inversion": round((nu - ng) / (nu + ng), 6),
+                             "late_growth_per_ps": round(g, 5) if g is not None else None})
         out[name] = {"sweep_seconds": round(wall, 3),
                      "sweep_Gcell_updates_per_s": round(len(setups) * cells * n / wall / 1e9, 2),
                      "packed_step_ms_64_cavities": round(step_s * 1e3, 4),
@@ -389,15 +423,32 @@ def sweep_bench(args):
                      "failed_jobs": int(failed),
                      "projected_hours_200000_steps": round(len(setups) / 64 * 200000 * step_s / 3600, 3)}
     line = {
-        "metric": "Gcell-updates/s (batched BF16 sweep, packed engine)", "value": out["bf16"]["sweep_Gcell_updates_per_s"],
+        "metric": "Gcell-updates/s (batched BF16 sweep, packed engine)", "value": out[forms[0][0]]["sweep_Gcell_updates_per_s"],
         "unit": "Gcell-updates/s", "n_gpus": 1, "steps": n, "warmup": 1, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "bf16 storage, f32 arithmetic", "data": "synthetic",
-        "config": {"workload": f"sweep: {len(setups)} gain-slab microcavities of 96x96x64 cells, pump log-uniform "
-                               "1e7-1e11 1/s, BF16 fields / FP32 populations / FP64 DFT", "jobs": len(setups),
+        "config": {"workload": f"sweep: {len(setups)} gain-slab microcavities on the auto mesher's graded mesh "
+                               f"({'x'.join(map(str, setups[0].shape))} cells, configs/c4_cavity.params), pump "
+                               "log-uniform 1e7-1e11 1/s, BF16 fields / FP32 populations / FP64 DFT", "jobs": len(setups),
                    "cells_per_job": cells, "steps_per_job": n, "budget_GB": 150},
-        "bf16": out["bf16"], "fp32": out["fp32"],
+        "cavity_end_state": ends,
+        "lasing": lasing_summary(ends),
     }
+    line.update(out)
     print(json.dumps(line))
+
+
+def lasing_summary(ends):
+    """Lasing threshold from the cavities' end states: the smallest pump whose cavity reached
+    population inversion (Nu > Ng) and whose probe signal grew over the last half of the run;
+    None when no cavity did, with the largest inversion reached."""
+    lasing = [e for e in ends if e["inversion"] > 0 and (e["late_growth_per_ps"] or -1) > 0]
+    top = max(ends, key=lambda e: e["inversion"]) if ends else None
+    return {"threshold_pump_per_s": min(e["pump_per_s"] for e in lasing) if lasing else None,
+            "max_inversion": top["inversion"] if top else None,
+            "pump_at_max_inversion": top["pump_per_s"] if top else None,
+            "note": "inversion = (int Nu - int Ng) / (int Nu + int Ng) over the gain layer at the end; it starts at -1 "
+                    "(all in the ground state) and the pump W_p raises it by about 2 W_p t, so a window of t = "
+                    "steps x dt bounds how far any cavity can get"}
 
 
 def ringdown(series, dt, t_from):
@@ -443,8 +494,7 @@ def sweep_check(args):
     pumps = np.exp(rng.uniform(np.log(1e7), np.log(1e11), size=256))
     idx = list(range(0, 256, 32))
     n = args.check_steps
-    base = serving_job_text((80, 80, 48), n)
-    setups = [PKG.Setup.from_text(base.replace("PUMP_RATE = 1e9", f"PUMP_RATE = {float(pumps[q])!r}")) for q in idx]
+    setups = c4_setups([pumps[q] for q in idx], n)
     dt = setups[0].view.dt
     t_from = 4000 * dt  # after the source pulse (t0 + 3 tau = 64 fs)
     t0 = time.perf_counter()
@@ -494,7 +544,8 @@ def sweep_check(args):
         "metric": "sweep fidelity: packed 16-bit storage vs FP64 on 8 cavities (max Q rel. error)", "unit": "rel. error",
         "value": forms[args.check_forms.split(",")[0]]["max_Q_rel_err"], "n_gpus": 1, "steps": n, "warmup": 0,
         "higher_is_better": False, "vs_baseline": None, "dtype": "storage forms vs f64", "data": "synthetic",
-        "config": {"workload": "8 of the sweep's 256 gain-slab microcavities of 96x96x64 cells (indices 0, 32, ..., 224)",
+        "config": {"workload": "8 of the sweep's 256 gain-slab microcavities on the graded mesh, "
+                               f"{'x'.join(map(str, setups[0].shape))} cells (indices 0, 32, ..., 224)",
                    "steps_per_job": n, "window_from_step": 4000, "pumps_per_s": [float(pumps[q]) for q in idx]},
         "fp64": {"peak_THz": [round(r[0] / 1e12, 4) for r in ref_rd], "growth_per_ps": [round(r[1] * 1e-12, 4) for r in ref_rd],
                  "Q": [round(r[2], 1) if r[2] else None for r in ref_rd],
@@ -776,10 +827,13 @@ def main():
     ap.add_argument("--serving", action="store_true",
                     help="serving form: a stream of small solves through the packed engine (own JSON line)")
     ap.add_argument("--serving-jobs", type=int, default=48)
+    ap.add_argument("--serving-edges", type=int, nargs=2, default=[32, 192], help="core edge range (cells)")
+    ap.add_argument("--serving-steps", type=int, nargs=2, default=[2000, 20000], help="step count range")
     ap.add_argument("--sweep", action="store_true",
                     help="the batched BF16 gain-laser sweep through the packed engine (own JSON line)")
     ap.add_argument("--sweep-jobs", type=int, default=256)
     ap.add_argument("--sweep-steps", type=int, default=1000, help="steps per cavity (the full sweep is 200000)")
+    ap.add_argument("--sweep-forms", default="bf16,fp32", help="storage forms of the sweep; the first reports end states")
     ap.add_argument("--sweep-probe-steps", type=int, default=200)
     ap.add_argument("--sweep-check", action="store_true",
                     help="the sweep's BF16 cavities against FP64 on 8 of them: peak, ring-down, Q (own JSON line)")

@@ -312,16 +312,22 @@ void fdtd_destroy(fdtd_handle *h);
 /* ------------------------------------------------------------ packed multi-solve engine */
 /* The serving form of the stepper: a queue of FP32, FP16 and BF16 solves (mixed freely; FP64
  * and PEC solves are refused with FDTD_ERR_UNSUPPORTED) on one GPU.  fdtd_batch_submit
- * queues a solve (the setup view and the arrays it points to must stay valid until the job
- * has finished); fdtd_batch_run admits queued jobs in order while their device footprint
- * fits budget_bytes and fewer than 64 are resident, then advances every resident solve by
- * up to max_steps steps, each step of all of them issued as one packed H and one packed E
- * launch per storage form present (E: per kind of solve) and one probe launch (plus one
- * monitor pair on monitor steps), and retires
- * solves that reach their step count or that the stability monitor stops.  The per-cell
- * arithmetic is fdtd_run's, so a job's probe series, DFT and diagnostics are the same as
- * from fdtd_create + fdtd_run on the same setup.  No counterpart in the reference (it runs
- * one solve per process); it replaces running the reference once per design point.
+ * queues a solve and returns at once (the setup view and the arrays it points to must stay
+ * valid until the job has finished).  An admission thread inside the batch takes queued jobs
+ * in order while their device footprint fits budget_bytes and fewer than 64 are resident or
+ * being prepared, and builds each one's device state (allocation, set-up uploads) on the
+ * job's own stream while the resident solves keep stepping.  fdtd_batch_run splices the
+ * prepared jobs in, then advances every resident solve by up to max_steps steps, each step
+ * of all of them issued as one packed H and one packed E launch per storage form present
+ * (E: per kind of solve) and one probe launch (plus one monitor pair on monitor steps); every
+ * 16 steps, and whenever a solve reaches its step count, it retires finished solves (and any
+ * the stability monitor stopped) and splices in newly prepared ones.  With nothing resident it
+ * first waits until every job that can be admitted is prepared, so a batch starts with all
+ * that fit.  n_queued counts jobs queued or being prepared.  The
+ * per-cell arithmetic is fdtd_run's, with every rounding explicit, so a job's probe series,
+ * DFT and max |E| are bit-identical to fdtd_create + fdtd_run on the same setup, alone or in
+ * any mix.  No counterpart in the reference (it runs one solve per process); it replaces
+ * running the reference once per design point.
  * A batch is driven from one host thread.  One batch per device at a time in a process (its
  * per-solve records live in the device's constant memory): fdtd_batch_create on a device
  * that has one returns FDTD_ERR_INVALID. */

@@ -257,3 +257,45 @@ def test_batch_16bit_matches_single_16bit_solve(pkg, precision):
     assert np.array_equal(series, ref[0]) and np.array_equal(dft, ref[1])
     assert diag["max_E"] == ref[2]["max_E"]
     assert diag["steps_done"] == 300
+
+
+def test_batch_job_submitted_while_others_step_is_bit_identical(pkg):
+    """Continuous batching: jobs submitted while others are resident and stepping are prepared
+    by the admission thread (device state built on their own streams) and spliced into the
+    packed step; each result is bit-identical to the same job run alone."""
+    first = [(_setup(pkg, src, ov), n) for src, ov, n in CASES[:2]]
+    late = [(_setup(pkg, src, ov), n) for src, ov, n in CASES[2:]]
+    b = pkg.Batch(budget_bytes=8 << 30)
+    t_first = [b.submit(s, n) for s, n in first]
+    b.run(24)
+    states = [b.state(t) for t in t_first]
+    assert all(st == pkg.JOB_RESIDENT and 0 < done < n for (st, done), (_, n) in zip(states, first))
+    t_late = [b.submit(s, n) for s, n in late]  # the first jobs are mid-run
+    _drain(pkg, b, t_first + t_late)
+    got = {}
+    for t, (s, n) in zip(t_first + t_late, first + late):
+        st, done = b.state(t)
+        assert st == pkg.JOB_DONE and done == n
+        got[t] = (b.probe_series(t), b.dft(t), b.diagnostics(t))
+        b.release(t)
+    b.close()
+    for t, sn in zip(t_first + t_late, first + late):
+        (series, dft, diag), = _batch_results(pkg, [sn])
+        assert np.array_equal(got[t][0], series) and np.array_equal(got[t][1], dft)
+        assert got[t][2]["max_E"] == diag["max_E"]
+
+
+def test_batch_run_waits_for_the_prepared_jobs(pkg):
+    """With nothing resident, fdtd_batch_run waits for the admission thread to prepare what can
+    be admitted instead of returning without stepping; n_queued counts jobs queued or in
+    preparation."""
+    s = _setup(pkg, "c0_dipole_sphere.params", {})
+    b = pkg.Batch(budget_bytes=8 << 30)
+    t = b.submit(s, 40)
+    r, q = b.run(8)
+    assert r == 1 and q == 0
+    st, done = b.state(t)
+    assert st == pkg.JOB_RESIDENT and done == 8
+    _drain(pkg, b, [t])
+    assert b.state(t) == (pkg.JOB_DONE, 40)
+    b.close()
