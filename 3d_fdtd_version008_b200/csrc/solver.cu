@@ -493,11 +493,7 @@ __device__ __forceinline__ const StepArgs<S, float>& bargs(int r) {
 }
 
 // The blocks of the solves stored as S.  PIPE: interior columns stage their planes in shared
-// memory (HPipe<S>::bytes() / EPipe<S>::bytes() dynamic, the same for every storage type), as in
-// the single-solve sweeps.
-static_assert(HPipe<float>::bytes() == HPipe<__half>::bytes() && HPipe<float>::bytes() == HPipe<__nv_bfloat16>::bytes() &&
-                  EPipe<float>::bytes() == EPipe<__half>::bytes() && EPipe<float>::bytes() == EPipe<__nv_bfloat16>::bytes(),
-              "the packed sweeps launch every storage form with one shared-memory size");
+// memory (HPipe<S>::bytes() / EPipe<S>::bytes() dynamic), as in the single-solve sweeps.
 template <typename S, bool PIPE>
 __global__ void __launch_bounds__(32 * kBlockY, 2) k_update_H_multi(const int4* __restrict__ tab) {
     const int4 e = tab[blockIdx.x];
@@ -1159,6 +1155,7 @@ Solver<S, T>::Solver(const fdtd_setup_v1& s, int dev, const ShardSpec* shard) {
     };
     kchunkH_ = chunk(NyT_ - 1, NzT_ - 1);
     kchunkE_ = chunk(NyT_, NzT_);
+    if (const char* e = std::getenv("FDTD_B200_KCHUNK")) kchunkH_ = kchunkE_ = std::max(1, std::atoi(e));
     if (gyE > 65535) throw Failure(FDTD_ERR_INVALID, "grid too large for the sweep launch shape (NyT)");
     gridH_ = dim3(gx, gyE, std::max(1, (a.kH1 + kchunkH_ - 1) / kchunkH_));
     gridE_ = dim3(gx, gyE, std::max(1, (a.kE1 + kchunkE_ - 1) / kchunkE_));
@@ -1863,12 +1860,11 @@ public:
             if (const char* e = std::getenv("FDTD_B200_BATCH_E_PIPE")) epipe_ = std::string(e) != "0";
             if (const char* e = std::getenv("FDTD_B200_BATCH_KCHUNK")) kchunk_ = std::max(0, std::atoi(e));
             for (int st = 0; st < 3; ++st) {
-                ck(cudaFuncSetAttribute(hkernel(st, true), cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        int(HPipe<float>::bytes())),
+                ck(cudaFuncSetAttribute(hkernel(st, true), cudaFuncAttributeMaxDynamicSharedMemorySize, int(hsmem(st))),
                    "cudaFuncSetAttribute");
                 for (int sh = 0; sh < 2; ++sh)
                     ck(cudaFuncSetAttribute(ekernel(4 * st + 2 * sh + 1, true), cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                            int(EPipe<float>::bytes())),
+                                            int(esmem(st))),
                        "cudaFuncSetAttribute");
             }
             worker_ = std::thread([this] { prepare_loop(); });
@@ -1962,6 +1958,9 @@ private:
                                    k_update_H_multi<__nv_bfloat16, false>, k_update_H_multi<__nv_bfloat16, true>};
         return k[2 * storage + int(pipe)];
     }
+    // dynamic shared memory of the staged sweeps of storage form st (0 FP32, 1 FP16, 2 BF16)
+    static size_t hsmem(int st) { return st == 0 ? HPipe<float>::bytes() : st == 1 ? HPipe<__half>::bytes() : HPipe<__nv_bfloat16>::bytes(); }
+    static size_t esmem(int st) { return st == 0 ? EPipe<float>::bytes() : st == 1 ? EPipe<__half>::bytes() : EPipe<__nv_bfloat16>::bytes(); }
     // kind = 4 storage + 2 SH + MAT; the staged form exists for the indexed material only
     static K ekernel(int kind, bool pipe) {
         static constexpr K k[kEKinds] = {
@@ -2202,12 +2201,12 @@ private:
         const dim3 blk(32, kBlockY);
         for (int q = 0; q < 3; ++q)
             if (nHk_[q + 1] > nHk_[q])
-                hkernel(q, hpipe_)<<<unsigned(nHk_[q + 1] - nHk_[q]), blk, hpipe_ ? HPipe<float>::bytes() : 0, st_>>>(
+                hkernel(q, hpipe_)<<<unsigned(nHk_[q + 1] - nHk_[q]), blk, hpipe_ ? hsmem(q) : 0, st_>>>(
                     d_tab_ + nHk_[q]);
         for (int q = 0; q < kEKinds; ++q)
             if (nEk_[q + 1] > nEk_[q]) {
                 const bool pipe = epipe_ && (q & 1);
-                ekernel(q, pipe)<<<unsigned(nEk_[q + 1] - nEk_[q]), blk, pipe ? EPipe<float>::bytes() : 0, st_>>>(
+                ekernel(q, pipe)<<<unsigned(nEk_[q + 1] - nEk_[q]), blk, pipe ? esmem(q / 4) : 0, st_>>>(
                     d_tab_ + nH_ + nEk_[q]);
             }
         k_probe_multi<<<n, 128, 0, st_>>>();

@@ -725,10 +725,11 @@ def e2e_run(setup, sample_cfg: str, prec: int, local: int, K: int, S: int, dist,
             "h2d_bytes_per_step": int(h2d / K), "d2h_bytes_per_step": int(d2h / K), "seconds": round(t_e2e, 4)}
 
 
-def device_run(setup, form: str, shards: int, W: int, K: int, S: int, local: int, dist) -> dict:
+def device_run(setup, form: str, shards: int, W: int, K: int, S: int, local: int, dist, devices=None) -> dict:
     """W untimed and K timed runs of S steps, inputs resident; device time from CUDA events on
-    the library's stream(s), max over ranks; the solve is returned open."""
-    sol = PKG.Solver(setup, device=local, precision=PREC[form], shards=shards)
+    the library's stream(s), max over ranks; the solve is returned open.  devices: the shards'
+    GPUs (one solve split over several GPUs), else all shards on `local`."""
+    sol = PKG.Solver(setup, device=local, precision=PREC[form], shards=shards, devices=devices)
     for _ in range(W):
         sol.run(S)
     sol.synchronize()
@@ -847,6 +848,9 @@ def main():
     # 4 z-shards on one GPU is the fastest schedule measured for the 536^3 workload (FP32
     # 65.8 -> 72.7, BF16 84.0 -> 100.5 Gcell-updates/s; 2 and 8 shards in between): the shards'
     # sweeps run on their own streams and fill each other's tails.  Results are identical.
+    ap.add_argument("--shard-gpus", action="store_true",
+                    help="with --gpus N > 1: one solve split along z over the N GPUs of this node, driven by one "
+                         "process (strong scaling; rank 0 only under torchrun), instead of N replicas")
     ap.add_argument("--shards", type=int, default=4,
                     help="z shards of the solve on this GPU (fdtd_create_sharded; their sweeps overlap)")
     args = ap.parse_args()
@@ -882,6 +886,12 @@ def main():
         print(json.dumps(reference_arm(args, cfg, sample_cfg, desc, K, W)))
         return
 
+    if args.shard_gpus and args.gpus > 1:
+        # one process drives the sharded solve on all N GPUs; under torchrun the other ranks
+        # have nothing to run
+        if rank != 0:
+            return
+        world, dist = 1, None
     setup = PKG.Setup.from_file(PKG.config_path(cfg))
     cells = setup.shape[0] * setup.shape[1] * setup.shape[2]
     head = args.precision
@@ -897,8 +907,12 @@ def main():
     # Every storage form steps the same workload from the same state for W + K runs of S
     # steps; the FP64 solve stays open as the accuracy reference of the others.
     runs = {}
+    shard_devs = list(range(args.gpus)) if args.shard_gpus and args.gpus > 1 else None
     for f in forms:
-        runs[f] = device_run(setup, f, args.shards, W, K, S, local, dist)
+        if shard_devs:
+            runs[f] = device_run(setup, f, len(shard_devs), W, K, S, 0, None, devices=shard_devs)
+        else:
+            runs[f] = device_run(setup, f, args.shards, W, K, S, local, dist)
     ref_sol = runs["fp64"]["solve"] if "fp64" in runs else None
     acc = {}
     if ref_sol is not None:
@@ -930,19 +944,20 @@ def main():
         "metric": "Mcell-updates/s",
         "value": round(replica_value(cells, K * S, world, h["dev_ms_max"]), 3),
         "unit": "Mcell-updates/s",
-        "n_gpus": world,
+        "n_gpus": args.gpus if shard_devs else world,
         "steps": K,
         "warmup": W,
         "ms_per_step": round(h["dev_ms_max"] / K, 4),
         "higher_is_better": True,
-        "scaling": "weak",
+        "scaling": "strong" if shard_devs else "weak",
         "vs_baseline": None,
         "dtype": DTYPE[head],
         "data": "synthetic",
         "config": workload_config(setup, cfg, desc),
         "detail": {"fdtd_steps_per_step": S,
-                   "parallelism": ("replicas, one per GPU" if world > 1 else "single GPU")
-                   + (f", {args.shards} z-shards of the solve overlapped on the GPU" if args.shards > 1 else ""),
+                   "parallelism": (f"1 solve sharded along z over {args.gpus} GPUs (peer halo copies)" if shard_devs else
+                                   ("replicas, one per GPU" if world > 1 else "single GPU")
+                                   + (f", {args.shards} z-shards of the solve overlapped on the GPU" if args.shards > 1 else "")),
                    "roofline_timing": "whole (unsharded) solve, per-kernel CUDA events on the library's stream",
                    "kernel_path": "separate H and E sweeps",
                    "l2": "state (%.1f GB of fields) larger than L2 (126 MB), no flush" % (cells * WORD[head] * 6 / 1e9),

@@ -531,3 +531,105 @@ def test_bounded_device_wait_expires_with_timeout_status(pkg, monkeypatch):
     sol.run(g["meta"]["steps"])
     assert field_rel_l2(fields(sol), ref_fields(g, sol.shape), "E") <= 1e-5
     sol.close()
+
+
+def _lockstep(pkg, s, precisions, marks, init=None):
+    """Solves of one setup in several storage forms, stepped together; at each step count of
+    `marks` yields (step, {precision: (fields, probe series, DFT)})."""
+    sols = {p: pkg.Solver(s, precision=p) for p in precisions}
+    if init:
+        for sol in sols.values():
+            for c, v in init.items():
+                sol.set_field(c, v.reshape(sol.shape))
+    done = 0
+    try:
+        for m in marks:
+            for sol in sols.values():
+                sol.run(m - done)
+            done = m
+            yield m, {p: (fields(sol), sol.probe_series(), sol.dft(0)) for p, sol in sols.items()}
+    finally:
+        for sol in sols.values():
+            sol.close()
+
+
+# The timed workload's physics on its profiling-size grid (280^3: 256^3 core, 12-cell CPML, slab
+# with a pumped gain layer).  FP32 against the FP64 mode, measured on a B200: 1000 steps 7.0e-6 /
+# 3.4e-6 / 4.4e-6 / 3.9e-6 (E, H, probe, DFT); 2000 steps 1.2e-4 / 7.8e-5 / 3.0e-5 / 3.2e-5, when
+# the pulse has left the grid and the rounding residual of its peak dominates the small field.
+def test_timed_workload_fp32_against_fp64_2000_steps(pkg):
+    s = pkg.Setup.from_file(pkg.config_path("b256_gain_slab.params"))
+    for m, r in _lockstep(pkg, s, (1, 0), (1000, 2000)):
+        (f64, p64, d64), (f32, p32, d32) = r[1], r[0]
+        eE, eH, ep, ed = field_rel_l2(f32, f64, "E"), field_rel_l2(f32, f64, "H"), rel(p32, p64), rel(d32, d64)
+        if m == 1000:
+            assert max(eE, eH, ep, ed) <= 1e-5, (m, eE, eH, ep, ed)
+        else:
+            assert eE <= 3e-4 and eH <= 2e-4 and ep <= 1e-4 and ed <= 1e-4, (m, eE, eH, ep, ed)
+        assert np.argmax(np.abs(d32)) == np.argmax(np.abs(d64))
+
+
+@pytest.mark.xfail(strict=True, reason="FP32 storage floor: after 2000 steps the decayed field is small against the "
+                                       "rounding of its peak (C0 E 3.6e-4, timed workload E 1.2e-4 against FP64); the "
+                                       "oracle's FP32 twin shows the same, so the north star's 1e-5 field bar holds "
+                                       "only while the pulse is in the grid")
+@pytest.mark.parametrize("cfg", ["c0_dipole_sphere.params", "b256_gain_slab.params"])
+def test_fp32_fields_within_1e5_after_2000_steps(pkg, cfg):
+    s = pkg.Setup.from_file(pkg.config_path(cfg))
+    for _, r in _lockstep(pkg, s, (1, 0), (2000,)):
+        assert field_rel_l2(r[0][0], r[1][0], "E") <= 1e-5 and field_rel_l2(r[0][0], r[1][0], "H") <= 1e-5
+
+
+def test_c1_gain_slab_2000_steps_vs_oracle(pkg, oracle):
+    """Config C1 (graded mesh, pumped gain layer, seeded field noise) for 2000 steps against the
+    oracle: FP64 within 1e-12 on fields, polarization and populations; FP32 within 2e-5 on the
+    fields (measured 9e-6 against the FP64 mode) and 1e-5 on the probe series and DFT."""
+    import os
+    s = pkg.Setup.from_file(pkg.config_path("c1_gain_slab.params"), overrides={"PUMP_RATE": "1e9"})
+    rng = np.random.default_rng(1)
+    o = oracle.OracleSolve(s, 0)
+    init = {c: rng.normal(0.0, 1e-6, o.E[0].size) for c in ("Ex", "Ey", "Ez")}
+    for c, v in init.items():
+        o.E["xyz".index(c[1])][:] = v
+    steps = 2000
+    p_ref = o.run(steps, threads=os.cpu_count() or 1)
+    ref = {c: o.field(c) for c in FIELDS}
+    gain = s.array("tls_region_map").reshape(s.shape) >= 0
+    d_ref = oracle.dft(p_ref[:, 0], s.dt, s.array("dft_freqs"))
+    for m, r in _lockstep(pkg, s, (1, 0), (steps,), init=init):
+        (f64, p64, d64), (f32, p32, d32) = r[1], r[0]
+        assert field_rel_l2(f64, ref, "E") <= 1e-12 and field_rel_l2(f64, ref, "H") <= 1e-12
+        assert rel(p64, p_ref.reshape(p64.shape)) <= 1e-12 and rel(d64, d_ref) <= 1e-12
+        assert field_rel_l2(f32, ref, "E") <= 2e-5 and field_rel_l2(f32, ref, "H") <= 2e-5
+        assert rel(p32, p_ref.reshape(p32.shape)) <= 1e-5 and rel(d32, d_ref) <= 1e-5
+    sol = pkg.Solver(s, precision=1)
+    for c, v in init.items():
+        sol.set_field(c, v.reshape(sol.shape))
+    sol.run(steps)
+    assert rel(sol.tls_state("Pz")[gain], o.Pz.reshape(s.shape)[gain]) <= 1e-12
+    assert rel(sol.tls_state("Nu")[gain], o.Nu.reshape(s.shape)[gain]) <= 1e-12
+    assert rel(sol.tls_state("Ng")[gain], o.Ng.reshape(s.shape)[gain]) <= 1e-12
+    sol.close()
+
+
+# 16-bit storage against the FP64 mode while the pulse is in the grid (C0, 600 steps; measured on a
+# B200: FP16 E 1.7e-3, H 2.1e-2, probe 1.3e-2, DFT 2.4e-3; BF16 E 1.2e-2, H 0.16, probe 2.3e-2, DFT
+# 4.1e-3).  The north star's 1e-3 field bar is not met by either form (next test).
+@pytest.mark.parametrize("precision,bars", [(2, (4e-3, 5e-2, 3e-2, 6e-3)), (3, (3e-2, 0.35, 5e-2, 1e-2))])
+def test_16bit_fields_against_fp64_in_the_active_window(pkg, precision, bars):
+    s = pkg.Setup.from_file(pkg.config_path("c0_dipole_sphere.params"))
+    for _, r in _lockstep(pkg, s, (1, precision), (600,)):
+        (f64, p64, d64), (f16, p16, d16) = r[1], r[precision]
+        got = (field_rel_l2(f16, f64, "E"), field_rel_l2(f16, f64, "H"), rel(p16, p64), rel(d16, d64))
+        assert all(g <= b for g, b in zip(got, bars)), got
+        assert np.argmax(np.abs(d16)) == np.argmax(np.abs(d64))
+
+
+@pytest.mark.xfail(strict=True, reason="16-bit storage rounds every stored E and H value to 11 (FP16) or 8 (BF16) "
+                                       "significant bits: the field L2 against FP64 is 2e-3 to 0.2 even in the active "
+                                       "window, above the north star's 1e-3")
+@pytest.mark.parametrize("precision", [2, 3])
+def test_16bit_fields_within_1e3_in_the_active_window(pkg, precision):
+    s = pkg.Setup.from_file(pkg.config_path("c0_dipole_sphere.params"))
+    for _, r in _lockstep(pkg, s, (1, precision), (600,)):
+        assert field_rel_l2(r[precision][0], r[1][0], "E") <= 1e-3 and field_rel_l2(r[precision][0], r[1][0], "H") <= 1e-3
