@@ -73,11 +73,15 @@ __global__ void k_index_from_idx3(const uint16_t* __restrict__ src, uint16_t* __
 
 // PECBoundary::apply_after_E (src/boundary.hpp:55-74): Ex = Ey = Ez = 0 on the six outer
 // faces, after the E update.  One thread per face cell, the z faces first, then y, then x,
-// so that consecutive threads write consecutive i where the layout allows.
+// so that consecutive threads write consecutive i where the layout allows.  The x and y faces
+// are zeroed on the planes [k0, k1) this grid owns; the z faces are the local planes zlo and
+// zhi, -1 where the face belongs to another shard (a whole solve: k0 = 0, k1 = NzT, zlo = 0,
+// zhi = NzT - 1).
 template <typename D>
-__global__ void k_pec_faces(D* __restrict__ Ex, D* __restrict__ Ey, D* __restrict__ Ez, int NxT, int NyT, int NzT,
-                            int NxP) {
-    const long long nz = (long long)NxT * NyT, ny = (long long)NxT * NzT, nx = (long long)NyT * NzT;
+__global__ void k_pec_faces(D* __restrict__ Ex, D* __restrict__ Ey, D* __restrict__ Ez, int NxT, int NyT, int NxP,
+                            int k0, int k1, int zlo, int zhi) {
+    const int nzp = k1 - k0;
+    const long long nz = (long long)NxT * NyT, ny = (long long)NxT * nzp, nx = (long long)NyT * nzp;
     const long long total = 2 * (nx + ny + nz);
     for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
          t += (long long)gridDim.x * blockDim.x) {
@@ -86,16 +90,17 @@ __global__ void k_pec_faces(D* __restrict__ Ex, D* __restrict__ Ey, D* __restric
         if (u < 2 * nz) {
             const int side = int(u / nz);
             u -= side * nz;
-            i = int(u % NxT); j = int(u / NxT); k = side ? NzT - 1 : 0;
+            i = int(u % NxT); j = int(u / NxT); k = side ? zhi : zlo;
+            if (k < 0) continue;
         } else if ((u -= 2 * nz) < 2 * ny) {
             const int side = int(u / ny);
             u -= side * ny;
-            i = int(u % NxT); k = int(u / NxT); j = side ? NyT - 1 : 0;
+            i = int(u % NxT); k = k0 + int(u / NxT); j = side ? NyT - 1 : 0;
         } else {
             u -= 2 * ny;
             const int side = int(u / nx);
             u -= side * nx;
-            j = int(u % NyT); k = int(u / NyT); i = side ? NxT - 1 : 0;
+            j = int(u % NyT); k = k0 + int(u / NyT); i = side ? NxT - 1 : 0;
         }
         const size_t q = (size_t(k) * NyT + j) * NxP + i;
         Ex[q] = from_d<D>(0.0);
@@ -814,6 +819,7 @@ private:
     S* psiH_[6] = {};
     size_t psi_sz_[6] = {};
     void point_args_at();
+    void pec_faces();  // PECBoundary after the E sweep: the faces of the planes this grid owns
     int timing_ = FDTD_TIMING_OFF;
     cudaEvent_t ev_[4] = {nullptr, nullptr, nullptr, nullptr};
     fdtd_timing_v1 tm_{};
@@ -953,10 +959,10 @@ Solver<S, T>::Solver(const fdtd_setup_v1& s, int dev, const ShardSpec* shard) {
         a.bEx = be[0]; a.bEy = be[1]; a.bEz = be[2];
     }
     // Where the staging pays (536^3 slab case, one B200): the E sweep with the row-indexed
-    // material in FP32 (-2 %) and 16-bit storage (-10 %); the H sweep with 16-bit storage only
-    // (-8 %; FP32 and FP64 +4 %).  With the three bE arrays the E staging takes 96 KB of shared
+    // material in FP32 (-2 %), FP64 (-3 %) and 16-bit storage (-10 %); the H sweep with 16-bit
+    // storage only (-8 %; FP32 and FP64 +4 %).  With the three bE arrays the E staging takes 96 KB of shared
     // memory per block, leaves L1 too small for the neighbour rows, and is 15 % slower.
-    pipe_ = a.bidx != nullptr && sizeof(S) <= 4;
+    pipe_ = a.bidx != nullptr;
     hpipe_ = sizeof(S) == 2;
     if (const char* e = std::getenv("FDTD_B200_H_PIPE")) hpipe_ = std::string(e) != "0";
     if (const char* e = std::getenv("FDTD_B200_E_PIPE")) pipe_ = a.bidx != nullptr && std::string(e) != "0";
@@ -1146,11 +1152,16 @@ Solver<S, T>::Solver(const fdtd_setup_v1& s, int dev, const ShardSpec* shard) {
     g.er = g.ne ? (32 * kBlockY) / g.ne : 1;
     const int gx = g.gxi + (g.ne ? 1 : 0);
     const int gyE = std::max((NyT_ + kBlockY - 1) / kBlockY, g.ne ? (NyT_ + g.er - 1) / g.er : 0);
-    // launch shapes: z-chunks so that the grid holds several waves of blocks
+    // launch shapes: z-chunks of at most 16 planes, and enough of them that the grid holds
+    // several waves of blocks.  Measured on the 536^3 CPML + gain workload (one B200): chunks
+    // of 67 -> 34 -> 16 planes take the E sweep from 1.258 to 1.159 to 1.107 ms (FP32) and from
+    // 1.006 to 0.900 to 0.868 ms (BF16), the H sweep from 1.025 to 0.972 ms (FP32); 12 and 8
+    // planes are no faster.  Short chunks balance the blocks' work (a chunk of an edge column
+    // or a CPML row runs longer than an interior one) and shorten the last wave.
     auto chunk = [&](int rows, int planes) {
         const int bxy = std::max(1, gx * ((rows + kBlockY - 1) / kBlockY));
         const int want = std::max(1, (148 * 16 + bxy - 1) / bxy);
-        const int zc = std::max(1, std::min(want, std::max(1, planes / 8)));
+        const int zc = std::max({1, std::min(want, std::max(1, planes / 8)), (planes + 15) / 16});
         return std::max(1, (planes + zc - 1) / zc);
     };
     kchunkH_ = chunk(NyT_ - 1, NzT_ - 1);
@@ -1189,6 +1200,17 @@ void Solver<S, T>::setup_slabs() {
        "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
     if (per < 1) throw Failure(FDTD_ERR_CUDA, "slab-ordered step kernel does not fit on an SM");
     gridS_ = dim3(unsigned(sms * per));
+}
+
+template <typename S, typename T>
+void Solver<S, T>::pec_faces() {
+    const int k0 = shard_.own0, k1 = shard_.own1;
+    const int zlo = shard_.kz0 + k0 == 0 ? k0 : -1;                 // global plane 0 is ours
+    const int zhi = shard_.kz0 + k1 == shard_.NzG ? k1 - 1 : -1;    // global plane NzG - 1 is ours
+    const long long faces = 2ll * ((long long)NxT_ * NyT_ + (long long)NxT_ * (k1 - k0) + (long long)NyT_ * (k1 - k0));
+    const unsigned nb = unsigned(std::min<long long>((faces + 255) / 256, 148 * 8));
+    k_pec_faces<S><<<nb, 256, 0, st_>>>(a_.Ex, a_.Ey, a_.Ez, NxT_, NyT_, NxP_, k0, k1, zlo, zhi);
+    ++launches;
 }
 
 template <typename S, typename T>
@@ -1448,12 +1470,7 @@ void Solver<S, T>::run(uint64_t n) {
             e_kernel(src.ns != 0)<<<gridE_, blk, smem, st_>>>(a_, kchunkE_, src, geom_);
             launches += 2;
         }
-        if (pec_) {
-            const long long faces = 2ll * ((long long)NxT_ * NyT_ + (long long)NxT_ * NzT_ + (long long)NyT_ * NzT_);
-            const unsigned nb = unsigned(std::min<long long>((faces + 255) / 256, 148 * 8));
-            k_pec_faces<S><<<nb, 256, 0, st_>>>(a_.Ex, a_.Ey, a_.Ez, NxT_, NyT_, NzT_, NxP_);
-            ++launches;
-        }
+        if (pec_) pec_faces();
         if (per_kernel) ck(cudaEventRecord(ev_[2], st_), "cudaEventRecord");
         if (nprobes_) {
             const long long sample = (s % save_every_ == 0) ? (long long)(s / save_every_) : -1;
@@ -1525,6 +1542,7 @@ void Solver<S, T>::phase_E(uint64_t s, ESrc& src, bool monitor) {
     const size_t smem = pipe_ ? EPipe<S>::bytes() : 0;
     e_kernel(src.ns != 0)<<<gridE_, blk, smem, st_>>>(a_, kchunkE_, src, geom_);
     ++launches;
+    if (pec_) pec_faces();
     if (nprobes_) {
         const int pthreads = int(nprobes_ * std::max<uint32_t>(nf_, 1));
         const long long sample = (s % save_every_ == 0) ? (long long)(s / save_every_) : -1;
@@ -1856,6 +1874,10 @@ public:
             ck(cudaHostAlloc(reinterpret_cast<void**>(&h_status_), sizeof(unsigned) * kMaxBatch, cudaHostAllocDefault),
                "cudaHostAlloc");
             ck(cudaMalloc(&d_status_, sizeof(unsigned) * kMaxBatch), "cudaMalloc");
+            ck(cudaMalloc(&d_poll_, sizeof(unsigned) * kMaxBatch), "cudaMalloc");
+            ck(cudaHostAlloc(reinterpret_cast<void**>(&h_poll_), sizeof(unsigned) * kMaxBatch, cudaHostAllocDefault),
+               "cudaHostAlloc");
+            ck(cudaEventCreateWithFlags(&poll_ev_, cudaEventDisableTiming), "cudaEventCreate");
             if (const char* e = std::getenv("FDTD_B200_BATCH_H_PIPE")) hpipe_ = std::string(e) != "0";
             if (const char* e = std::getenv("FDTD_B200_BATCH_E_PIPE")) epipe_ = std::string(e) != "0";
             if (const char* e = std::getenv("FDTD_B200_BATCH_KCHUNK")) kchunk_ = std::max(0, std::atoi(e));
@@ -1911,9 +1933,12 @@ public:
             step();
             bool finished = false;
             for (uint64_t r : res_) finished |= jobs_.at(r).steps() >= jobs_.at(r).target;
-            if (finished || ++since_check_ >= kCheckEvery) {
+            if (finished) {
                 check_and_retire();
                 splice(res_.empty());
+            } else if (++since_check_ >= kCheckEvery) {
+                poll();
+                splice(false);
             }
         }
         ck(cudaStreamSynchronize(st_), "batch run");
@@ -2014,6 +2039,10 @@ private:
         if (d_status_) cudaFree(d_status_);
         if (h_status_) cudaFreeHost(h_status_);
         d_status_ = nullptr; h_status_ = nullptr;
+        if (d_poll_) cudaFree(d_poll_);
+        if (h_poll_) cudaFreeHost(h_poll_);
+        if (poll_ev_) cudaEventDestroy(poll_ev_);
+        d_poll_ = nullptr; h_poll_ = nullptr; poll_ev_ = nullptr;
         for (auto& e : ring_ev_) if (e) cudaEventDestroy(e);
         if (st_) cudaStreamDestroy(st_);
         d_tab_ = nullptr; ticks_ = nullptr; st_ = nullptr;
@@ -2218,8 +2247,37 @@ private:
     }
 
     // Reads every resident solve's status word; retires finished and failed solves.
+    // Periodic status check that does not drain the stream: the resident solves' status words
+    // are gathered and copied to the host behind the queued steps, and read at the next poll
+    // once that copy has landed.  A stopped solve (rare) is then retired by the synchronous
+    // check.  Finished solves are known on the host from their step counts.
+    void poll() {
+        since_check_ = 0;
+        if (poll_pending_) {
+            const cudaError_t q = cudaEventQuery(poll_ev_);
+            if (q == cudaErrorNotReady) return;  // still behind queued work: look next time
+            ck(q, "status poll");
+            poll_pending_ = false;
+            bool stopped = false;
+            for (int r = 0; r < poll_n_; ++r) stopped |= h_poll_[r] != 0;
+            if (stopped) {
+                check_and_retire();
+                return;
+            }
+        }
+        const int n = int(res_.size());
+        if (!n) return;
+        k_status_multi<<<1, kMaxBatch, 0, st_>>>(n, d_poll_);
+        ck(cudaGetLastError(), "k_status_multi");
+        ck(cudaMemcpyAsync(h_poll_, d_poll_, n * sizeof(unsigned), cudaMemcpyDeviceToHost, st_), "status poll");
+        ck(cudaEventRecord(poll_ev_, st_), "cudaEventRecord");
+        poll_pending_ = true;
+        poll_n_ = n;
+    }
+
     void check_and_retire() {
         since_check_ = 0;
+        poll_pending_ = false;  // the synchronous check below sees every status
         const int n = int(res_.size());
         if (n) {
             k_status_multi<<<1, kMaxBatch, 0, st_>>>(n, d_status_);
@@ -2294,6 +2352,11 @@ private:
     uint64_t ring_ = 0;
     int since_check_ = 0;
     unsigned* d_status_ = nullptr;  // gathered status words
+    unsigned* d_poll_ = nullptr;    // the same, for the non-blocking poll
+    unsigned* h_poll_ = nullptr;
+    cudaEvent_t poll_ev_ = nullptr;
+    bool poll_pending_ = false;
+    int poll_n_ = 0;
     unsigned* h_status_ = nullptr;
     // Launch shape: staged H / E sweeps and planes per z-chunk (0: each solve's own).  Measured
     // on 64 resident gain cavities of 96x96x64 (one B200): 16 planes and both staged sweeps
@@ -2312,7 +2375,7 @@ private:
 // global z offset for the z CPML and the global plane ranges they update, so a sharded solve
 // computes the same values, cell for cell, as the whole solve.  The stability monitor reduces
 // each shard's owned planes and is evaluated once, on shard 0, which then hands its status
-// word to the others.  Kernel path 1 only, CPML only, no detector files.
+// word to the others.  Kernel path 1 only, CPML or PEC boundary, no detector files.
 template <typename S, typename T>
 class Sharded final : public SolverBase {
 public:
@@ -2396,7 +2459,6 @@ template <typename S, typename T>
 Sharded<S, T>::Sharded(const fdtd_setup_v1& s, int n, const int* devices) {
     NxT_ = s.NxT; NyT_ = s.NyT; NzT_ = s.NzT;
     if (n < 2) throw Failure(FDTD_ERR_INVALID, "a sharded solve needs at least 2 shards");
-    if (s.pec_boundary) throw Failure(FDTD_ERR_UNSUPPORTED, "a sharded solve needs a CPML boundary");
     for (int c = 0; c < 3; ++c)
         if (s.aE[c] || s.aH[c] || s.bH[c])
             throw Failure(FDTD_ERR_UNSUPPORTED, "a sharded solve takes uniform aE/aH/bH (passed as NULL)");

@@ -194,7 +194,9 @@ def cpu_reference(sample_cfg: str, steps: int, warmup: int, fdtd_steps: int):
         shape = [r["meta"][k] for k in ("NxT", "NyT", "NzT")]
         loop_s = float(r["meta"]["loop_seconds"])
         cells = shape[0] * shape[1] * shape[2]
-        kind, exe = "reference", "oracle/_ref/ref_harness_native (reference headers, -O3 -march=x86-64-v3 -fopenmp)"
+        exe_p = oracle.native_harness()
+        march = "x86-64-v4" if exe_p == oracle.REF_HARNESS_NATIVE_V4 else "x86-64-v3"
+        kind, exe = "reference", f"{exe_p.relative_to(ROOT)} (reference headers, -O3 -march={march} -fopenmp)"
     else:
         s = PKG.Setup.from_file(path)
         o = oracle.OracleSolve(s, 0)
@@ -645,13 +647,14 @@ def reference_arm(args, cfg: str, sample_cfg: str, desc: str, K: int, W: int) ->
     path = PKG.config_path(use)
     t0 = time.time()
     if oracle.REF_HARNESS_NATIVE.exists():
-        exe = oracle.REF_HARNESS_NATIVE
+        exe = oracle.native_harness()
         r = oracle.run_harness(path, W + K, "--no-fields", "--warmup", str(W), native=True,
                                env={"OMP_NUM_THREADS": str(cores)})
         shape = [r["meta"][k] for k in ("NxT", "NyT", "NzT")]
         loop_s = float(r["meta"]["loop_seconds"])
         kind = "reference"
-        what = f"{exe.relative_to(ROOT)} (the reference headers compiled with -O3 -march=x86-64-v3 -fopenmp)"
+        march = "x86-64-v4" if exe == oracle.REF_HARNESS_NATIVE_V4 else "x86-64-v3"
+        what = f"{exe.relative_to(ROOT)} (the reference headers compiled with -O3 -march={march} -fopenmp)"
     else:
         s = PKG.Setup.from_file(path)
         o = oracle.OracleSolve(s, 0)

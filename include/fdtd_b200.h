@@ -299,8 +299,9 @@ int fdtd_close_outputs(fdtd_handle *h);
  * each stepped by the same kernels with its global z offset; neighbouring shards exchange one
  * plane of E and one of H per step by device-to-device (peer) copies, and the stability
  * monitor is evaluated once for the whole solve.  The handle answers the same calls as a
- * whole solve (fields, gain state, probes, DFT, diagnostics) with identical values; kernel
- * path 1 only, CPML only, no detector files, timing off.  No counterpart in the reference's
+ * whole solve (fields, gain state, probes, DFT, diagnostics) with identical values; CPML or
+ * PEC boundary (each shard zeroes the PEC faces of the planes it owns); kernel path 1 only,
+ * whole-run timing only, no detector files.  No counterpart in the reference's
  * time loop; its slab-parallel variant (src/parallel_domain.hpp) splits one process's loop. */
 int fdtd_create_sharded(const fdtd_setup_v1 *setup, int nshards, const int *devices, fdtd_handle **out);
 /* Block until all device work of the handle is complete. */

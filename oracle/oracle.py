@@ -26,6 +26,24 @@ ORACLE_DIR = pathlib.Path(__file__).resolve().parent
 ORACLE_LIB = ORACLE_DIR / "lib" / "libfdtd_oracle.so"
 REF_HARNESS = ORACLE_DIR / "_ref" / "ref_harness"
 REF_HARNESS_NATIVE = ORACLE_DIR / "_ref" / "ref_harness_native"
+REF_HARNESS_NATIVE_V4 = ORACLE_DIR / "_ref" / "ref_harness_native_v4"
+
+
+def host_has_avx512() -> bool:
+    """True when this host's CPU runs x86-64-v4 code (AVX-512 F, BW, CD, DQ, VL)."""
+    try:
+        flags = next(ln for ln in open("/proc/cpuinfo") if ln.startswith("flags")).split()
+    except (OSError, StopIteration):
+        return False
+    return all(f in flags for f in ("avx512f", "avx512bw", "avx512cd", "avx512dq", "avx512vl"))
+
+
+def native_harness() -> pathlib.Path:
+    """The timed build of the reference harness for this host: x86-64-v4 where the CPU has
+    AVX-512, else x86-64-v3."""
+    if REF_HARNESS_NATIVE_V4.exists() and host_has_avx512():
+        return REF_HARNESS_NATIVE_V4
+    return REF_HARNESS_NATIVE
 # Where the reference's headers lie (only in the build container; the GPU hosts use the
 # prebuilt harness): FDTD_REFERENCE_SRC, else the checkout's default location.
 REF_SRC = pathlib.Path(os.environ.get("FDTD_REFERENCE_SRC", "/root/reference/3D_FDTD_version008/src"))
@@ -206,7 +224,7 @@ def run_harness(params_path, steps: int, *flags: str, native: bool = False, init
     and, under "frames", every file of its frames/ directory (relative path -> bytes).
     Without outdir it runs in a scratch directory under oracle/_ref/runs that is removed
     afterwards."""
-    exe = REF_HARNESS_NATIVE if native else REF_HARNESS
+    exe = native_harness() if native else REF_HARNESS
     if not exe.exists():
         raise FileNotFoundError(f"{exe} is missing: build it with make -C oracle ref")
     scratch = outdir is None

@@ -39,7 +39,8 @@ def run(pkg, s, precision, shards, steps):
 
 
 @pytest.mark.parametrize("case,shards", [("step_g1_gain", 2), ("step_g1_gain", 3), ("step_g2_planewave", 2),
-                                         ("step_g2_planewave", 4), ("c0_dipole_sphere.params", 3)])
+                                         ("step_g2_planewave", 4), ("c0_dipole_sphere.params", 3), ("step_g3_pec", 2),
+                                         ("step_g3_pec", 3)])
 @pytest.mark.parametrize("precision", [1, 0, 3])
 def test_sharded_matches_whole_solve(pkg, case, shards, precision):
     s = setup_for(pkg, case)
@@ -60,11 +61,25 @@ def test_sharded_matches_whole_solve(pkg, case, shards, precision):
     assert abs(dw["conservation_err"] - ds["conservation_err"]) <= 1e-12
 
 
+@pytest.mark.parametrize("precision,tol", [(1, 1e-12), (0, 1e-5)])
+def test_sharded_pec_matches_reference(pkg, precision, tol):
+    """PECBoundary split over 3 shards (each zeroes the faces of the planes it owns; the z faces
+    belong to the end shards) against the reference's own golden state."""
+    from conftest import field_rel_l2, golden
+    g = golden("step_g3_pec")
+    s = pkg.Setup.from_file(GOLDEN / "cases" / "step_g3_pec.params")
+    sol = pkg.Solver(s, precision=precision, shards=3)
+    sol.run(g["meta"]["steps"])
+    mine = {c: sol.field(c) for c in FIELDS}
+    ref = {c: g[c].reshape(sol.shape) for c in FIELDS}
+    assert field_rel_l2(mine, ref, "E") <= tol and field_rel_l2(mine, ref, "H") <= tol
+    for c in ("Ex", "Ey", "Ez"):
+        f = mine[c]
+        assert not (f[0].any() or f[-1].any() or f[:, 0].any() or f[:, -1].any() or f[:, :, 0].any() or f[:, :, -1].any())
+    sol.close()
+
+
 def test_sharded_refusals(pkg):
-    pec = pkg.Setup.from_file(GOLDEN / "cases" / "step_g3_pec.params")
-    with pytest.raises(pkg.FdtdError) as e:
-        pkg.Solver(pec, shards=2)
-    assert e.value.code == 7
     s = setup_for(pkg, "step_g1_gain")
     sol = pkg.Solver(s, shards=2)
     with pytest.raises(pkg.FdtdError):
