@@ -2230,7 +2230,7 @@ private:
         const dim3 blk(32, kBlockY);
         for (int q = 0; q < 3; ++q)
             if (nHk_[q + 1] > nHk_[q])
-                hkernel(q, hpipe_)<<<unsigned(nHk_[q + 1] - nHk_[q]), blk, hpipe_ ? hsmem(q) : 0, st_>>>(
+                hkernel(q, hpipe_ && q != 0)<<<unsigned(nHk_[q + 1] - nHk_[q]), blk, hpipe_ && q != 0 ? hsmem(q) : 0, st_>>>(
                     d_tab_ + nHk_[q]);
         for (int q = 0; q < kEKinds; ++q)
             if (nEk_[q + 1] > nEk_[q]) {
@@ -2358,12 +2358,15 @@ private:
     bool poll_pending_ = false;
     int poll_n_ = 0;
     unsigned* h_status_ = nullptr;
-    // Launch shape: staged H / E sweeps and planes per z-chunk (0: each solve's own).  Measured
-    // on 64 resident gain cavities of 96x96x64 (one B200): 16 planes and both staged sweeps
-    // take the packed step from 1.19 to 1.12 ms (BF16) and 1.15 to 1.09 ms (FP32); 32 and 64
-    // planes are slower than 16.  FDTD_B200_BATCH_KCHUNK / _H_PIPE / _E_PIPE override them.
+    // Launch shape: staged sweeps (the E sweep for every storage form, the H sweep for 16-bit
+    // storage, as for a single solve: staging the FP32 H sweep costs 4 %) and each solve's own
+    // z-chunks (at most 16 planes, shorter on small grids so that a lone solve still fills the
+    // GPU; 16-plane chunks for every solve had measured 1.19 -> 1.12 ms per packed step of 64
+    // BF16 cavities of 96x96x64 against each solve's chunks of the time, which were up to 64
+    // planes).  FDTD_B200_BATCH_KCHUNK (planes, 0 = each solve's own) / _H_PIPE / _E_PIPE
+    // override them.
     bool hpipe_ = true, epipe_ = true;
-    int kchunk_ = 16;
+    int kchunk_ = 0;
 };
 
 // ==================================================================== sharded solve

@@ -204,12 +204,12 @@ MIXED = [  # (setup source, overrides, steps, precision): all three storage form
 ]
 
 
-@pytest.mark.parametrize("shape", [{}, {"FDTD_B200_BATCH_KCHUNK": "0", "FDTD_B200_BATCH_H_PIPE": "0",
+@pytest.mark.parametrize("shape", [{}, {"FDTD_B200_BATCH_KCHUNK": "16", "FDTD_B200_BATCH_H_PIPE": "0",
                                       "FDTD_B200_BATCH_E_PIPE": "0"}])
 def test_batch_mixed_storage_alone_and_in_the_mix(pkg, shape, monkeypatch):
     """FP32, FP16 and BF16 solves resident together: each storage form's blocks run in their
     own launch, and each job's results are bit-identical alone and in the mix (default launch
-    shape: 16-plane z-chunks and staged sweeps; and each solve's own chunks, direct loads)."""
+    shape: each solve's own z-chunks and staged sweeps; and 16-plane chunks, direct loads)."""
     for k, v in shape.items():
         monkeypatch.setenv(k, v)
     jobs = []
