@@ -48,3 +48,20 @@ def test_raw_rms_fit_would_be_fooled_by_a_static_residual():
     g_raw = np.polyfit(tw, np.log(rms), 1)[0]
     _, g_est, _ = bench.ringdown(x, DT, 4000 * DT)
     assert abs(g_est - g) <= 0.02 * abs(g) and abs(g_raw - g) > 0.2 * abs(g)
+
+
+def test_ringdown_ignores_a_noise_floor_and_lines_outside_the_band():
+    """A low-Q ring-down (Q 46, as on the graded-mesh cavities) that decays into a white noise
+    floor, with a strong rounding-noise line at 3000 THz: the peak comes from the source band
+    and the rate from the part of the window above the floor."""
+    dt = 2.19e-17
+    n = 20000
+    t = np.arange(n) * dt
+    f, g = 194.7e12, -13.4e12
+    rng = np.random.default_rng(7)
+    x = np.exp(g * t) * np.sin(2 * np.pi * f * t) + 3e-4 * rng.standard_normal(n)
+    x += 2e-3 * np.sin(2 * np.pi * 3000e12 * t)
+    f_est, g_est, q_est = bench.ringdown(x, dt, 4000 * dt)
+    assert abs(f_est - f) <= 2e-3 * f
+    assert abs(g_est - g) <= 0.05 * abs(g)
+    assert q_est == pytest.approx(np.pi * f / -g, rel=0.05)
