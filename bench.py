@@ -2,18 +2,21 @@
 
 Workload (default): the 512^3 single solve with CPML and gain -- 512^3 core cells at
 20 nm + 12-cell CPML (536^3 = 154 M total cells), an n = 3.4 slab with a two-level gain
-layer, dipole source, Ez probe with a 21-frequency DFT, FP32 storage
+layer, dipole source, Ez probe with a 21-frequency DFT
 (3d_fdtd_version008_b200/configs/b512_gain_slab.params).
 
 A bench "step" is one fdtd_run() call that advances the solve by S = --fdtd-steps time
-steps (default 10).  `value` = total cell-updates / device time of K bench steps, in
-Mcell-updates/s, measured with CUDA events on the library's stream (the library records
-them; fdtd_get_timing) bracketed by barriers and synchronisation, max over ranks.  The
-field state (~7 GB) is far larger than L2 (126 MB), so no L2 flush is needed.
+steps (default 10).  The headline is the FP64 mode, the reference's own arithmetic: `value` =
+total cell-updates / device time of K bench steps, in Mcell-updates/s, measured with CUDA
+events on the library's stream(s) bracketed by barriers and synchronisation, max over ranks.
+FP32, BF16 and FP16 storage are measured in the same run (--forms) as blocks of the line, each
+with its roofline (per-kernel events of a whole solve) and its accuracy against the FP64 solve
+after the same W + K runs from the same state.  The field state (3.7-7.4 GB) is far larger
+than L2 (126 MB), so no L2 flush is needed.
 
 Multi-GPU (--gpus N under torchrun): replicas -- every rank runs an independent solve of
-the same workload (the reference has no distributed path; a single solve does not shard
-here), value = all ranks' cell-updates / max over ranks of the device time.
+the same workload, value = all ranks' cell-updates / max over ranks of the device time.  With
+--shard-gpus one process splits one solve along z over the N GPUs instead (strong scaling).
 
 e2e: the same metric through the public C ABI from host buffers: fdtd_create from the host
 setup (H2D of the material index and 1-D profiles, layout transpose on the device), K runs of
@@ -21,10 +24,12 @@ S steps each followed by a D2H read of that run's probe samples, a D2H read of t
 field, fdtd_destroy -- all inside the timed region (wall clock, synchronised).  It is taken
 first in the process, after a warm-up solve of the sample grid (CUDA context, kernel modules).
 
---impl reference: times the reference's own CPU loop (oracle/_ref/ref_harness_native, the
-reference headers compiled with its CMake flags and OpenMP on all host cores) on the bounded
-CPU sample of the workload (216^3 total cells, same per-cell physics); falls back to the
-oracle's C restatement when the reference binary is absent.
+--impl reference: times the reference's own CPU loop (the reference headers compiled with its
+CMake flags, OpenMP on all host cores) on the same 536^3 grid, W untimed and K timed steps;
+it falls back to the bounded 216^3 sample when the host lacks the memory for the reference's
+full-grid arrays, and to the oracle's C restatement when the reference binary is absent.
+
+--serving, --sweep, --sweep-check and --precision-study print lines of their own.
 """
 from __future__ import annotations
 
@@ -285,14 +290,23 @@ def serving_bench(args):
     t0 = time.perf_counter()
     tickets = [b.submit(s, n) for s, (_, n) in zip(setups, jobs)]
     pending = set(tickets)
+    occ = []  # (seconds since start, resident jobs) after every run call
     while pending:
-        b.run(32)
+        r, _ = b.run(32)
+        occ.append((time.perf_counter() - t0, r))
         for t in list(pending):
             if b.state(t)[0] >= PKG.JOB_DONE:
                 b.probe_series(t)
                 b.release(t)
                 pending.discard(t)
     packed_s = time.perf_counter() - t0
+    # time spent with r resident jobs, in bands
+    bands = {"1": 0.0, "2-4": 0.0, "5-16": 0.0, "17-64": 0.0}
+    prev = 0.0
+    for ts, r in occ:
+        key = "1" if r <= 1 else "2-4" if r <= 4 else "5-16" if r <= 16 else "17-64"
+        bands[key] += ts - prev
+        prev = ts
     # Poisson arrivals at 80 % of the packed throughput
     rate = 0.8 * len(jobs) / packed_s
     arrivals = np.cumsum(rng.exponential(1.0 / rate, size=len(jobs)))
@@ -334,6 +348,7 @@ def serving_bench(args):
         "one_at_a_time": {"seconds": round(plain_s, 3), "Mcell_updates_per_s": round(work / plain_s / 1e6, 1),
                           "p50_ms": pct(lat_plain, 50), "p95_ms": pct(lat_plain, 95), "p99_ms": pct(lat_plain, 99)},
         "throughput_ratio": round(plain_s / packed_s, 2),
+        "packed_seconds_by_resident_jobs": {k: round(v, 3) for k, v in bands.items()},
         "arrival_rate_per_s": round(rate, 2),
     }
     print(json.dumps(line))
@@ -617,6 +632,16 @@ WORD = {"fp32": 4, "fp64": 8, "fp16": 2, "bf16": 2}
 DTYPE = {"fp32": "f32", "fp64": "f64", "fp16": "f32 (fp16 storage)", "bf16": "f32 (bf16 storage)"}
 
 
+def shards_for(args, form: str) -> int:
+    """z shards of the solve on the GPU for a storage form: --shards, else the fastest measured
+    on the 536^3 workload (one B200, 20 x 10 steps): FP64 steps fastest whole (37.0 against 36.7
+    with 2 shards and 36.5 with 4); FP32, BF16 and FP16 with 4 shards (72.6 / 101.8 / 104.6
+    against 72.2 / 97.5 / 100.8 whole), whose sweeps' tails overlap on their streams."""
+    if args.shards:
+        return args.shards
+    return 1 if form == "fp64" else 4
+
+
 def workload_config(setup, cfg: str, desc: str) -> dict:
     """The workload, identical in both arms' lines (the reference arm runs the same grid)."""
     return {"workload": desc, "config_file": cfg, "grid": list(setup.shape),
@@ -861,13 +886,12 @@ def main():
     ap.add_argument("--study-steps", type=int, default=5000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
-    # 4 z-shards on one GPU is the fastest schedule measured for the 536^3 workload (FP32
-    # 65.8 -> 72.7, BF16 84.0 -> 100.5 Gcell-updates/s; 2 and 8 shards in between): the shards'
-    # sweeps run on their own streams and fill each other's tails.  Results are identical.
+    # z shards of the solve on one GPU (0: the fastest per storage form, shards_for); results are
+    # identical whatever the count.
     ap.add_argument("--shard-gpus", action="store_true",
                     help="with --gpus N > 1: one solve split along z over the N GPUs of this node, driven by one "
                          "process (strong scaling; rank 0 only under torchrun), instead of N replicas")
-    ap.add_argument("--shards", type=int, default=4,
+    ap.add_argument("--shards", type=int, default=0,
                     help="z shards of the solve on this GPU (fdtd_create_sharded; their sweeps overlap)")
     args = ap.parse_args()
     if args.warmup < 3:
@@ -928,7 +952,7 @@ def main():
         if shard_devs:
             runs[f] = device_run(setup, f, len(shard_devs), W, K, S, 0, None, devices=shard_devs)
         else:
-            runs[f] = device_run(setup, f, args.shards, W, K, S, local, dist)
+            runs[f] = device_run(setup, f, shards_for(args, f), W, K, S, local, dist)
     ref_sol = runs["fp64"]["solve"] if "fp64" in runs else None
     acc = {}
     if ref_sol is not None:
@@ -973,7 +997,8 @@ def main():
         "detail": {"fdtd_steps_per_step": S,
                    "parallelism": (f"1 solve sharded along z over {args.gpus} GPUs (peer halo copies)" if shard_devs else
                                    ("replicas, one per GPU" if world > 1 else "single GPU")
-                                   + (f", {args.shards} z-shards of the solve overlapped on the GPU" if args.shards > 1 else "")),
+                                   + (f", {shards_for(args, head)} z-shards of the solve overlapped on the GPU"
+                                      if shards_for(args, head) > 1 else "")),
                    "roofline_timing": "whole (unsharded) solve, per-kernel CUDA events on the library's stream",
                    "kernel_path": "separate H and E sweeps",
                    "l2": "state (%.1f GB of fields) larger than L2 (126 MB), no flush" % (cells * WORD[head] * 6 / 1e9),

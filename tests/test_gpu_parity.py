@@ -571,7 +571,7 @@ def test_timed_workload_fp32_against_fp64_2000_steps(pkg):
 
 @pytest.mark.xfail(strict=True, reason="FP32 storage floor: after 2000 steps the decayed field is small against the "
                                        "rounding of its peak (C0 E 3.6e-4, timed workload E 1.2e-4 against FP64); the "
-                                       "oracle's FP32 twin shows the same, so the north star's 1e-5 field bar holds "
+                                       "oracle's FP32 twin shows the same, so the FP32 parity bar of 1e-5 field L2 holds "
                                        "only while the pulse is in the grid")
 @pytest.mark.parametrize("cfg", ["c0_dipole_sphere.params", "b256_gain_slab.params"])
 def test_fp32_fields_within_1e5_after_2000_steps(pkg, cfg):
@@ -614,7 +614,7 @@ def test_c1_gain_slab_2000_steps_vs_oracle(pkg, oracle):
 
 # 16-bit storage against the FP64 mode while the pulse is in the grid (C0, 600 steps; measured on a
 # B200: FP16 E 1.7e-3, H 2.1e-2, probe 1.3e-2, DFT 2.4e-3; BF16 E 1.2e-2, H 0.16, probe 2.3e-2, DFT
-# 4.1e-3).  The north star's 1e-3 field bar is not met by either form (next test).
+# 4.1e-3).  The 1e-3 field bar set for 16-bit storage is met by neither form (next test).
 @pytest.mark.parametrize("precision,bars", [(2, (4e-3, 5e-2, 3e-2, 6e-3)), (3, (3e-2, 0.35, 5e-2, 1e-2))])
 def test_16bit_fields_against_fp64_in_the_active_window(pkg, precision, bars):
     s = pkg.Setup.from_file(pkg.config_path("c0_dipole_sphere.params"))
@@ -627,7 +627,7 @@ def test_16bit_fields_against_fp64_in_the_active_window(pkg, precision, bars):
 
 @pytest.mark.xfail(strict=True, reason="16-bit storage rounds every stored E and H value to 11 (FP16) or 8 (BF16) "
                                        "significant bits: the field L2 against FP64 is 2e-3 to 0.2 even in the active "
-                                       "window, above the north star's 1e-3")
+                                       "window, above the 1e-3 bar set for 16-bit storage")
 @pytest.mark.parametrize("precision", [2, 3])
 def test_16bit_fields_within_1e3_in_the_active_window(pkg, precision):
     s = pkg.Setup.from_file(pkg.config_path("c0_dipole_sphere.params"))
