@@ -1885,6 +1885,7 @@ public:
             if (const char* e = std::getenv("FDTD_B200_BATCH_H_PIPE")) hpipe_ = std::string(e) != "0";
             if (const char* e = std::getenv("FDTD_B200_BATCH_E_PIPE")) epipe_ = std::string(e) != "0";
             if (const char* e = std::getenv("FDTD_B200_BATCH_KCHUNK")) kchunk_ = std::max(0, std::atoi(e));
+            if (const char* e = std::getenv("FDTD_B200_BATCH_SOLO")) solo_ = std::string(e) != "0";
             for (int st = 0; st < 3; ++st) {
                 ck(cudaFuncSetAttribute(hkernel(st, true), cudaFuncAttributeMaxDynamicSharedMemorySize, int(hsmem(st))),
                    "cudaFuncSetAttribute");
@@ -1933,8 +1934,36 @@ public:
     void run(uint64_t max_steps) {
         ck(cudaSetDevice(device_), "cudaSetDevice");
         splice(true);
-        for (uint64_t t = 0; t < max_steps && !res_.empty(); ++t) {
+        for (uint64_t t = 0; t < max_steps && !res_.empty();) {
+            if (res_.size() == 1 && solo_) {
+                // One resident solve (the tail of a stream, or a lone request): step it with the
+                // single-solve launches (launch parameters instead of per-block argument records,
+                // no packed bookkeeping; measured 13-15 % faster per step than packed alone).  The
+                // block code and its explicit rounding are the same, so are the bits.  In chunks,
+                // so that arrivals are spliced in and the packed step resumes.
+                Job& j = jobs_.at(res_[0]);
+                const uint64_t n = std::min<uint64_t>({j.target - j.steps(), max_steps - t, uint64_t(kSoloChunk)});
+                ck(cudaStreamSynchronize(st_), "batch solo");  // its packed steps are done
+                bool stopped = false;
+                with(j, [&](auto& v) {
+                    try {
+                        v.run(n);
+                    } catch (const Failure& f) {
+                        if (f.code != FDTD_ERR_UNSTABLE) throw;
+                        stopped = true;  // the monitor stopped it: retired as failed below
+                    }
+                });
+                t += n;
+                if (stopped || j.steps() >= j.target) {
+                    check_and_retire();
+                    splice(res_.empty());
+                } else {
+                    splice(false);
+                }
+                continue;
+            }
             step();
+            ++t;
             bool finished = false;
             for (uint64_t r : res_) finished |= jobs_.at(r).steps() >= jobs_.at(r).target;
             if (finished) {
@@ -1978,6 +2007,7 @@ public:
 private:
     static constexpr int kRing = 64;        // pinned per-step records in flight
     static constexpr int kCheckEvery = 16;  // steps between status checks
+    static constexpr int kSoloChunk = 64;   // steps per single-solve run of a lone resident solve
     // E kernel kinds: storage (3) x plane-wave sheets x indexed material
     static constexpr int kEKinds = 12;
     using K = void (*)(const int4*);
@@ -2371,6 +2401,8 @@ private:
     // override them.
     bool hpipe_ = true, epipe_ = true;
     int kchunk_ = 0;
+    // A lone resident solve steps with the single-solve launches (FDTD_B200_BATCH_SOLO=0: packed).
+    bool solo_ = true;
 };
 
 // ==================================================================== sharded solve

@@ -299,3 +299,23 @@ def test_batch_run_waits_for_the_prepared_jobs(pkg):
     _drain(pkg, b, [t])
     assert b.state(t) == (pkg.JOB_DONE, 40)
     b.close()
+
+
+def test_batch_lone_job_steps_the_same_solo_or_packed(pkg, monkeypatch):
+    """A lone resident job is stepped with the single-solve launches (the tail of a stream);
+    with FDTD_B200_BATCH_SOLO=0 it stays in the packed kernels: the same bits either way, and a
+    job that the monitor stops fails at the same step."""
+    good = _setup(pkg, "c0_dipole_sphere.params", {})
+    bad = _setup(pkg, GOLDEN / "cases" / "step_g0_sphere.params", {"STABILITY_MAX_E": "1e-30"})
+    out = []
+    for mode in ("1", "0"):
+        monkeypatch.setenv("FDTD_B200_BATCH_SOLO", mode)
+        (series, dft, diag), = _batch_results(pkg, [(good, 250)])
+        b = pkg.Batch(budget_bytes=8 << 30)
+        tb = b.submit(bad, 400)
+        _drain(pkg, b, [tb])
+        out.append((series, dft, diag["max_E"], b.state(tb)))
+        b.close()
+    assert np.array_equal(out[0][0], out[1][0]) and np.array_equal(out[0][1], out[1][1])
+    assert out[0][2] == out[1][2]
+    assert out[0][3] == out[1][3] == (pkg.JOB_FAILED, 101)
