@@ -527,16 +527,31 @@ __device__ __forceinline__ void e_plain(const StepArgs<S, T>& a, const size_t c,
 // ---------------------------------------------------------------------------------
 // Launch geometry of the sweeps.  The x range of a row is split into the interior
 // [xi0, xi1) -- W-aligned vectors with no x-slab cell -- covered by gxi block columns of
-// 32-vector warp segments, and the edge vectors outside it (nl on the left, ne in total),
+// `lanes`-vector row segments, and the edge vectors outside it (nl on the left, ne in total),
 // which one extra block column packs er rows at a time, one thread per edge vector.
 // Interior warps therefore never diverge on the x slab, and edge threads all take the
-// general path together.
+// general path together.  An interior warp holds 32 / lanes adjacent rows of one block
+// column (lanes = 32, 16 or 8), so that a narrow interior does not leave most lanes idle:
+// a 100-vector interior fills 100 of 128 lanes in 32-lane rows, 100 of 104 in 8-lane rows.
 struct SweepGeom {
     int xi0, xi1;  // interior x range (cells)
     int gxi;       // interior block columns
     int nl, ne;    // edge vectors per row: on the left, in total
     int er;        // rows per edge block
+    int lanes;     // lanes per interior row segment (32, 16 or 8)
 };
+
+// Row and first vector of an interior thread: warp w of block row `by` holds rows
+// (by * kBlockY + w) * R .. + R - 1 (R = 32 / lanes), segment `lane / lanes` of the warp one row.
+struct InteriorLane {
+    int j;   // row (may lie outside the grid: the caller masks it)
+    int li;  // lane within the row segment
+};
+__device__ __forceinline__ InteriorLane interior_lane(const SweepGeom& g, const int by, const int lane) {
+    const int R = 32 / g.lanes;
+    const int seg = lane / g.lanes;
+    return {(by * kBlockY + int(threadIdx.y)) * R + seg, lane - seg * g.lanes};
+}
 
 // One thread's column of W-cell vectors (i0.., j, kb..ke-1), marching in +z.
 // Every load of an iteration (the vectors, the x-neighbour at the warp or interior edge,
@@ -551,9 +566,10 @@ struct HPipe : PipeShape<S> {
     static constexpr size_t bytes() { return size_t(PipeShape<S>::kStages) * kSlots * (32 * kBlockY) * PipeShape<S>::SB; }
 };
 
+// li: the thread's lane within its row segment of g.lanes lanes (interior columns).
 template <typename S, typename T, bool EDGE, bool PIPE = false>
 __device__ __forceinline__ void h_column(const StepArgs<S, T>& a, const SweepGeom& g, const int j, const int i0,
-                                         const bool act, const int kb, const int ke, const int lane,
+                                         const bool act, const int kb, const int ke, const int li,
                                          const unsigned step) {
     constexpr int W = Vec<T>::W;
     const int np = a.np, np2 = 2 * np;
@@ -569,9 +585,9 @@ __device__ __forceinline__ void h_column(const StepArgs<S, T>& a, const SweepGeo
     if (ypml) { yb = __ldg(a.pbH[1] + j); yc = __ldg(a.pcH[1] + j); yik = __ldg(a.ik[1] + j); }
     const bool xpml = EDGE && act && (i0 < np || i0 + W > a.NxT - np);
     const bool plain_row = act && !ypml && !xpml && i0 + W <= a.NxT - 1;
-    // Ey, Ez at i0+W come from memory at the warp edge, at the end of the interior (the
-    // next lane then holds no interior vector) and for every edge column
-    const bool nload = EDGE || lane == 31 || i0 + W >= g.xi1;
+    // Ey, Ez at i0+W come from memory at the end of the row segment, at the end of the
+    // interior (the next lane then holds no interior vector) and for every edge column
+    const bool nload = EDGE || li == g.lanes - 1 || i0 + W >= g.xi1;
 
     const size_t row = size_t(j) * a.NxP + i0;
     T ex0[W], ey0[W];
@@ -674,8 +690,8 @@ __device__ __forceinline__ void h_column(const StepArgs<S, T>& a, const SweepGeo
         // x-neighbour at i0+W: the next lane's first cell, or the loaded one
         T eyn = eye, ezn = eze;
         if (!EDGE) {
-            const T sy = __shfl_down_sync(kFull, ey0[0], 1);
-            const T sz = __shfl_down_sync(kFull, ez[0], 1);
+            const T sy = __shfl_down_sync(kFull, ey0[0], 1, g.lanes);
+            const T sz = __shfl_down_sync(kFull, ez[0], 1, g.lanes);
             if (!nload) { eyn = sy; ezn = sz; }
         }
         if (plain_row && !zpml) {
@@ -739,10 +755,15 @@ __device__ __forceinline__ void update_H_block(const StepArgs<S, T>& a, const in
     const int ke = min(bz * kchunk + kchunk, a.kH1);
     if (kb >= ke) return;
     if (bx < g.gxi) {
-        const int j = by * kBlockY + threadIdx.y;
-        if (j >= a.NyT - 1) return;  // whole warp: a warp is one row
-        const int i0 = g.xi0 + (bx * 32 + lane) * W;
-        h_column<S, T, false, PIPE>(a, g, j, i0, i0 < g.xi1, kb, ke, lane, step);
+        // H is updated for rows j < NyT - 1.  A warp with no such row leaves as a whole; in a
+        // warp that has one, a row beyond it stays in the loop (the shuffles need every lane)
+        // as inactive lanes on a valid row index, which load and store nothing.
+        const InteriorLane il = interior_lane(g, by, lane);
+        const int jlast = a.NyT - 2;
+        if ((by * kBlockY + int(threadIdx.y)) * (32 / g.lanes) > jlast) return;
+        const bool row_ok = il.j <= jlast;
+        const int i0 = g.xi0 + (bx * g.lanes + il.li) * W;
+        h_column<S, T, false, PIPE>(a, g, row_ok ? il.j : jlast, i0, row_ok && i0 < g.xi1, kb, ke, il.li, step);
     } else {
         const int t = threadIdx.y * 32 + lane;
         const int rr = t / g.ne, v = t - rr * g.ne;
@@ -750,7 +771,7 @@ __device__ __forceinline__ void update_H_block(const StepArgs<S, T>& a, const in
         if (rr >= g.er || j >= a.NyT - 1) return;
         const int i0 = v < g.nl ? v * W : g.xi1 + (v - g.nl) * W;
         if (i0 >= a.NxT) return;
-        h_column<S, T, true>(a, g, j, i0, true, kb, ke, lane, step);
+        h_column<S, T, true>(a, g, j, i0, true, kb, ke, 0, step);
     }
 }
 
@@ -766,9 +787,10 @@ k_update_H(const StepArgs<S, T> a, const int kchunk, const SweepGeom g, const un
 // CG: H is read through L2 only -- the slab-ordered step (k_step_slabs) reads H that other
 // SMs wrote in the same launch, which a stale L1 line could hide.  SH: the step has
 // plane-wave sheets (a separate instantiation keeps the sheet tests out of the common case).
+// li: the thread's lane within its row segment of g.lanes lanes (interior columns).
 template <typename S, typename T, bool EDGE, bool CG = false, bool SH = false, bool MAT = false, bool PIPE = false>
 __device__ __forceinline__ void e_column(const StepArgs<S, T>& a, const SweepGeom& g, const ESrc& src, const int j,
-                                         const int i0, const bool act, const int kb, const int ke, const int lane) {
+                                         const int i0, const bool act, const int kb, const int ke, const int li) {
     auto ldH = [](const S* p, T (&v)[Vec<T>::W]) {
         if constexpr (CG) Fld<S, T>::ldcg(p, v);
         else Fld<S, T>::ldg(p, v);
@@ -789,11 +811,12 @@ __device__ __forceinline__ void e_column(const StepArgs<S, T>& a, const SweepGeo
     T yb = 1, yc = 0, yik = 1;
     if (ypml) { yb = __ldg(a.pbE[1] + j); yc = __ldg(a.pcE[1] + j); yik = __ldg(a.ik[1] + j); }
     const bool xpml = EDGE && act && (i0 < np || i0 + W > a.NxT - np);
-    const bool grow = a.gain && j >= a.gj0 && j < a.gj0 + a.gY && i0 + W > a.gi0 && i0 < a.gi0 + a.gX;
+    // (the gain state is written outside the act-guarded stores: inactive lanes never enter it)
+    const bool grow = act && a.gain && j >= a.gj0 && j < a.gj0 + a.gY && i0 + W > a.gi0 && i0 < a.gi0 + a.gX;
     const bool plain_row = act && !ypml && !xpml && i0 >= 1 && i0 + W <= a.NxT;
-    // Hz, Hy at i0-1 come from memory at the warp edge (lane 0, which also holds the first
-    // interior vector) and for every edge column
-    const bool pload = EDGE || lane == 0;
+    // Hz, Hy at i0-1 come from memory at the start of the row segment (whose lane also holds
+    // the first interior vector) and for every edge column
+    const bool pload = EDGE || li == 0;
     T* const Pcur = src.parity ? a.P1 : a.P0;
     T* const Pold = src.parity ? a.P0 : a.P1;  // holds P^{n-1}, receives P^{n+1}
 
@@ -916,8 +939,8 @@ __device__ __forceinline__ void e_column(const StepArgs<S, T>& a, const SweepGeo
         // x-neighbour at i0-1: the previous lane's last cell, or the loaded one
         T hzp = hze, hyp = hye;
         if (!EDGE) {
-            const T sz = __shfl_up_sync(kFull, hz[W - 1], 1);
-            const T sy = __shfl_up_sync(kFull, hy[W - 1], 1);
+            const T sz = __shfl_up_sync(kFull, hz[W - 1], 1, g.lanes);
+            const T sy = __shfl_up_sync(kFull, hy[W - 1], 1, g.lanes);
             if (!pload) { hzp = sz; hyp = sy; }
         }
         const bool gplane = grow && k >= a.gk0 && k < a.gk0 + a.gZ;
@@ -1028,10 +1051,15 @@ __device__ __forceinline__ void update_E_block(const StepArgs<S, T>& a, const in
     const int ke = min(bz * kchunk + kchunk, a.kE1);
     if (kb >= ke) return;
     if (bx < g.gxi) {
-        const int j = by * kBlockY + threadIdx.y;
-        if (j < 1 || j >= a.NyT) return;  // E is updated for j >= 1 only; whole warp
-        const int i0 = g.xi0 + (bx * 32 + lane) * W;
-        e_column<S, T, false, CG, SH, MAT, PIPE>(a, g, src, j, i0, i0 < g.xi1, kb, ke, lane);
+        // E is updated for rows 1 <= j < NyT.  A warp with no such row leaves as a whole; in a
+        // warp that has one, the other rows stay in the loop as inactive lanes on row 1.
+        const InteriorLane il = interior_lane(g, by, lane);
+        const int R = 32 / g.lanes;
+        const int w0 = (by * kBlockY + int(threadIdx.y)) * R;
+        if (w0 + R - 1 < 1 || w0 >= a.NyT) return;
+        const bool row_ok = il.j >= 1 && il.j < a.NyT;
+        const int i0 = g.xi0 + (bx * g.lanes + il.li) * W;
+        e_column<S, T, false, CG, SH, MAT, PIPE>(a, g, src, row_ok ? il.j : 1, i0, row_ok && i0 < g.xi1, kb, ke, il.li);
     } else {
         const int t = threadIdx.y * 32 + lane;
         const int rr = t / g.ne, v = t - rr * g.ne;
@@ -1039,7 +1067,7 @@ __device__ __forceinline__ void update_E_block(const StepArgs<S, T>& a, const in
         if (rr >= g.er || j < 1 || j >= a.NyT) return;
         const int i0 = v < g.nl ? v * W : g.xi1 + (v - g.nl) * W;
         if (i0 >= a.NxT) return;
-        e_column<S, T, true, CG, SH, MAT>(a, g, src, j, i0, true, kb, ke, lane);
+        e_column<S, T, true, CG, SH, MAT>(a, g, src, j, i0, true, kb, ke, 0);
     }
 }
 

@@ -448,6 +448,7 @@ constexpr int kMonBlocks = 64;  // monitor blocks per solve
 struct BatchSolve {
     SweepGeom g;
     int kchunkH, kchunkE;
+    int storage;    // 0 FP32, 1 FP16, 2 BF16 (fills the gap before the pointers)
     const ProbeDev* probes;
     int nprobes, nf;
     const double* freqs;
@@ -459,8 +460,6 @@ struct BatchSolve {
     unsigned long long nflat;
     double dt;
     double sE, sH;  // stored fields are E / sE and H / sH (1 for FP32)
-    int storage;    // 0 FP32, 1 FP16, 2 BF16
-    int pad;
 };
 
 struct BatchTick {
@@ -1149,13 +1148,32 @@ Solver<S, T>::Solver(const fdtd_setup_v1& s, int dev, const ShardSpec* shard) {
     SweepGeom& g = geom_;
     g.xi0 = int(round_up(size_t(np_), size_t(W)));
     g.xi1 = std::max(g.xi0, ((NxT_ - np_) / W) * W);
-    g.gxi = (g.xi1 - g.xi0 + 32 * W - 1) / (32 * W);
+    // Interior row segments of 32, 16 or 8 lanes.  A narrow interior (at most two 32-lane
+    // segments) takes the width that leaves the fewest lanes idle in the last block column,
+    // ties to the wider segment (its warps load one x-neighbour per plane, not one per row);
+    // a wide one keeps 32-lane rows.  Measured on one B200, FP32 sweeps: a 156-cell-wide
+    // cavity (35 interior vectors) runs at 23.1 Gcell/s on 32-lane rows, 25.7 on 8-lane rows;
+    // the 536^3 grid (130 vectors, 81 % of 32-lane rows busy) at 74.2 on 32-lane rows, 71.6 on
+    // 16 and 68.9 on 8 -- with enough blocks to keep HBM busy the extra row ends cost more than
+    // the idle lanes.  FDTD_B200_LANES=32|16|8 sets the width (results do not depend on it).
+    const int nvec = (g.xi1 - g.xi0) / W;
+    g.lanes = 32;
+    if (nvec <= 64)
+        for (int L : {16, 8})
+            if ((nvec + L - 1) / L * L < (nvec + g.lanes - 1) / g.lanes * g.lanes) g.lanes = L;
+    if (const char* e = std::getenv("FDTD_B200_LANES")) {
+        const int L = std::atoi(e);
+        if (L != 32 && L != 16 && L != 8) throw Failure(FDTD_ERR_INVALID, "FDTD_B200_LANES must be 32, 16 or 8");
+        g.lanes = L;
+    }
+    const int rows_blk = kBlockY * (32 / g.lanes);  // rows of an interior block
+    g.gxi = (nvec + g.lanes - 1) / g.lanes;
     g.nl = g.xi0 / W;
     g.ne = g.nl + std::max(0, (NxT_ - g.xi1 + W - 1) / W);
     if (g.ne > 32 * kBlockY) throw Failure(FDTD_ERR_UNSUPPORTED, "CPML too thick for the sweep launch shape");
     g.er = g.ne ? (32 * kBlockY) / g.ne : 1;
     const int gx = g.gxi + (g.ne ? 1 : 0);
-    const int gyE = std::max((NyT_ + kBlockY - 1) / kBlockY, g.ne ? (NyT_ + g.er - 1) / g.er : 0);
+    const int gyE = std::max((NyT_ + rows_blk - 1) / rows_blk, g.ne ? (NyT_ + g.er - 1) / g.er : 0);
     // launch shapes: z-chunks of at most 16 planes, and enough of them that the grid holds
     // several waves of blocks.  Measured on the 536^3 CPML + gain workload (one B200): chunks
     // of 67 -> 34 -> 16 planes take the E sweep from 1.258 to 1.159 to 1.107 ms (FP32) and from
@@ -1163,7 +1181,7 @@ Solver<S, T>::Solver(const fdtd_setup_v1& s, int dev, const ShardSpec* shard) {
     // planes are no faster.  Short chunks balance the blocks' work (a chunk of an edge column
     // or a CPML row runs longer than an interior one) and shorten the last wave.
     auto chunk = [&](int rows, int planes) {
-        const int bxy = std::max(1, gx * ((rows + kBlockY - 1) / kBlockY));
+        const int bxy = std::max(1, gx * ((rows + rows_blk - 1) / rows_blk));
         const int want = std::max(1, (148 * 16 + bxy - 1) / bxy);
         const int zc = std::max({1, std::min(want, std::max(1, planes / 8)), (planes + 15) / 16});
         return std::max(1, (planes + zc - 1) / zc);
@@ -2196,7 +2214,6 @@ private:
                 b.sE = v.sE_;
                 b.sH = v.sH_;
                 b.storage = j.storage;
-                b.pad = 0;
                 ekind[r] = 4 * j.storage + 2 * int(!v.sheets_.empty()) + int(v.a_.bidx != nullptr);
             });
         }

@@ -223,6 +223,23 @@ def test_batch_mixed_storage_alone_and_in_the_mix(pkg, shape, monkeypatch):
         assert mixed[k][2]["max_E"] == diag["max_E"] and diag["nan_flags"] == 0
 
 
+def test_batch_lane_widths_give_identical_bits(pkg, monkeypatch):
+    """The packed sweeps run each solve's blocks with its own interior row width: the mix with
+    every solve on 32-lane rows and with the width each solve picks (8 or 16 lanes for these
+    narrow interiors) gives the same bits."""
+    jobs = []
+    for src, ov, n, prec in MIXED:
+        s = _setup(pkg, src, ov)
+        jobs.append((s, _with_precision(s, prec), n))
+    monkeypatch.setenv("FDTD_B200_LANES", "32")
+    wide = _batch_views(pkg, jobs)
+    monkeypatch.delenv("FDTD_B200_LANES")
+    auto = _batch_views(pkg, jobs)
+    for k in range(len(jobs)):
+        assert np.array_equal(wide[k][0], auto[k][0]) and np.array_equal(wide[k][1], auto[k][1]), k
+        assert wide[k][2]["max_E"] == auto[k][2]["max_E"], k
+
+
 def _rel(a, b):
     return float(np.linalg.norm(np.ravel(a) - np.ravel(b)) / np.linalg.norm(np.ravel(b)))
 

@@ -464,6 +464,40 @@ def test_staged_sweeps_match_direct_loads(pkg, precision, case, monkeypatch):
         assert np.array_equal(out[0][c], out[1][c]), c
 
 
+@pytest.mark.parametrize("precision,path", [(1, 1), (0, 1), (2, 1), (3, 1), (1, 2), (0, 2)])
+@pytest.mark.parametrize("case", ["step_g2_planewave", "step_g1_gain", "step_g3_pec", "c0_dipole_sphere"])
+def test_interior_lane_widths_give_identical_bits(pkg, precision, path, case, monkeypatch):
+    """Interior warps of 32-lane rows, two 16-lane rows or four 8-lane rows (FDTD_B200_LANES):
+    the same cells get the same explicitly rounded update, x-neighbours come from the shuffle
+    inside a row segment or from memory at its ends, rows past the grid edge ride along as
+    inactive lanes -- bit-identical fields.  The small cases have 2-3 interior vectors per row and
+    odd row counts (rows of a warp beyond the grid); c0 has 16 or 32 per row."""
+    src = GOLDEN / "cases" / (case + ".params") if case.startswith("step") else pkg.config_path(case + ".params")
+    s = pkg.Setup.from_file(src)
+    steps = 60 if case.startswith("step") else 150
+    out = []
+    for lanes in ("32", "16", "8"):
+        monkeypatch.setenv("FDTD_B200_LANES", lanes)
+        sol = pkg.Solver(s, precision=precision, kernel_path=path)
+        rng = np.random.default_rng(11)
+        for c in ("Ex", "Ey", "Ez"):
+            sol.set_field(c, rng.normal(0, 1e-3, sol.shape))
+        sol.run(steps)
+        out.append((fields(sol), sol.probe_series()))
+        sol.close()
+    for k in (1, 2):
+        for c in FIELDS:
+            assert np.array_equal(out[k][0][c], out[0][0][c]), (k, c)
+        assert np.array_equal(out[k][1], out[0][1]), k
+
+
+def test_lane_width_setting_is_checked(pkg, monkeypatch):
+    monkeypatch.setenv("FDTD_B200_LANES", "12")
+    s = pkg.Setup.from_file(GOLDEN / "cases" / "step_g3_pec.params")
+    with pytest.raises(pkg.FdtdError):
+        pkg.Solver(s, precision=0)
+
+
 def _bf16_run(pkg, s, rounding, steps, path=1):
     v = pkg.SetupV1.from_buffer_copy(s.view)
     v.rounding = rounding
