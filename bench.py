@@ -1005,7 +1005,15 @@ def main():
                    "wall_ms_per_step": round(h["wall_ms"] / K, 4),
                    "accuracy_note": "each form against the FP64 solve after the same W + K runs of S steps "
                                     "from the same initial state: relative L2 of the stacked E and H components, "
-                                    "of the probe series and of the 21-frequency DFT"},
+                                    "of the probe series and of the 21-frequency DFT",
+                   "accuracy_steps": (W + K) * S,
+                   "accuracy_window": "the default 230 steps lie in the rise of the dipole's pulse: the FP64 "
+                                      "Ez at the probe (50 cells from the source) stays below 2.0e-6 V/m, under "
+                                      "FP16's smallest subnormal at the automatic field scale (sE = 64, the "
+                                      "source cell's peak stored near 4096: 2^-24 sE = 3.8e-6 V/m), so the FP16 "
+                                      "probe and DFT read 0 (error 1.0); BF16 has FP32's range.  The 16-bit "
+                                      "forms over a whole pulse: the precision study (--precision-study) and "
+                                      "the sweep check (--sweep-check)"},
         "roofline": roof[head]["roofline"],
         "e2e": e2e,
         "cpu_baseline": cpu,

@@ -320,7 +320,9 @@ void fdtd_destroy(fdtd_handle *h);
  * job's own stream while the resident solves keep stepping.  fdtd_batch_run splices the
  * prepared jobs in, then advances every resident solve by up to max_steps steps, each step
  * of all of them issued as one packed H and one packed E launch per storage form present
- * (E: per kind of solve) and one probe launch (plus one monitor pair on monitor steps); every
+ * (E: per kind of solve) and one probe launch (plus one monitor pair on monitor steps); a
+ * lone resident solve is stepped with fdtd_run's own launches instead, 64 steps at a time
+ * (environment FDTD_B200_BATCH_SOLO=0 keeps it packed); every
  * 16 steps, and whenever a solve reaches its step count, it retires finished solves (and any
  * the stability monitor stopped) and splices in newly prepared ones.  With nothing resident it
  * first waits until every job that can be admitted is prepared, so a batch starts with all
