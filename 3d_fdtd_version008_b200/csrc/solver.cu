@@ -645,7 +645,10 @@ class Solver final : public SolverBase {
     friend class Sharded<S, T>;
 
 public:
-    explicit Solver(const fdtd_setup_v1& s, int dev, const ShardSpec* shard = nullptr);
+    // Device memory comes from the device's stream-ordered pool (pooled_, the default), or from
+    // cudaMalloc / cudaFree when the environment sets FDTD_B200_ALLOC=malloc for a solve that is
+    // not a packed-engine job (pooled = true: its retirement must not stall the resident solves).
+    explicit Solver(const fdtd_setup_v1& s, int dev, const ShardSpec* shard = nullptr, bool pooled = false);
     ~Solver() override;
     void run(uint64_t n) override;
     void set_field(int comp, const double* h) override;
@@ -671,8 +674,7 @@ public:
 private:
     template <typename U> U* alloc(size_t n, bool zero = true) {
         void* p = nullptr;
-        // stream-ordered: freeing a retired solve does not stall the device for the others
-        ck(cudaMallocAsync(&p, std::max<size_t>(n, 1) * sizeof(U), st_), "cudaMallocAsync");
+        dev_alloc(&p, std::max<size_t>(n, 1) * sizeof(U));
         ptrs_.push_back(p);
         dev_bytes += std::max<size_t>(n, 1) * sizeof(U);
         if (zero) ck(cudaMemsetAsync(p, 0, std::max<size_t>(n, 1) * sizeof(U), st_), "cudaMemsetAsync");
@@ -682,6 +684,20 @@ private:
         U* d = alloc<U>(v.size(), false);
         ck(cudaMemcpyAsync(d, v.data(), v.size() * sizeof(U), cudaMemcpyHostToDevice, st_), "cudaMemcpyAsync");
         return d;
+    }
+    // A solve's own arrays.  The stream-ordered pool (kept memory, see keep_pool_memory) makes
+    // retiring a packed job free for the resident ones and a repeated solve cheap to create and
+    // destroy.  Measured on one B200: growing the pool by 9 GB costs 53 ms against 5 ms for
+    // cudaMalloc, but create + destroy of a small solve cost 1-2 ms through the pool against
+    // 7-8 ms through cudaMalloc, and the FP64 sweeps ran 0.7 % slower on cudaMalloc'd fields.
+    bool pooled_ = true;
+    void dev_alloc(void** p, size_t bytes) {
+        if (pooled_) ck(cudaMallocAsync(p, bytes, st_), "cudaMallocAsync");
+        else ck(cudaMalloc(p, bytes), "cudaMalloc");
+    }
+    void dev_free(void* p) {
+        if (pooled_) cudaFreeAsync(p, st_);
+        else cudaFree(p);
     }
     double* staging();
     void attach_outputs(const fdtd::SimSetup& setup, const std::string& root) override;
@@ -693,12 +709,9 @@ private:
     void phase_E(uint64_t s, ESrc& src, bool monitor);
     void write_population_frame();
     void close_outputs() override;
-    // Host <-> device copies of FP64 arrays through two pinned chunks: the host-side copy of
-    // one chunk (OpenMP) overlaps the DMA of the other.
+    // Host <-> device copies of FP64 arrays through the device's two pinned chunks
+    // (pinned_chunks): the host-side copy of one chunk (OpenMP) overlaps the DMA of the other.
     static constexpr size_t kPinBytes = size_t(32) << 20;
-    void* pin_[2] = {nullptr, nullptr};
-    cudaEvent_t pin_ev_[2] = {nullptr, nullptr};
-    void ensure_pinned();
     void h2d(const double* h, double* d, size_t n);
     void d2h(const double* d, double* h, size_t n);
     void upload_gain_box(const double* idx3, const std::vector<int8_t>& reg, T* dst);
@@ -841,10 +854,12 @@ void keep_pool_memory(int dev) {
 }
 
 template <typename S, typename T>
-Solver<S, T>::Solver(const fdtd_setup_v1& s, int dev, const ShardSpec* shard) {
+Solver<S, T>::Solver(const fdtd_setup_v1& s, int dev, const ShardSpec* shard, bool pooled) {
     device = dev;
+    pooled_ = true;
+    if (const char* e = std::getenv("FDTD_B200_ALLOC")) pooled_ = pooled || std::string(e) != "malloc";
     ck(cudaSetDevice(dev), "cudaSetDevice");
-    keep_pool_memory(dev);
+    if (pooled_) keep_pool_memory(dev);
     ck(cudaStreamCreateWithFlags(&st_, cudaStreamNonBlocking), "cudaStreamCreate");
     constexpr int W = Vec<T>::W;
     NxT_ = int(s.NxT); NyT_ = int(s.NyT); NzT_ = int(s.NzT);
@@ -1270,31 +1285,46 @@ Solver<S, T>::~Solver() {
     for (int q = 0; q < kTlsSlots; ++q)
         if (trec_ev_[q]) cudaEventDestroy(trec_ev_[q]);
     for (auto& e : ev_) if (e) cudaEventDestroy(e);
-    for (void* p : ptrs_) cudaFreeAsync(p, st_);
-    if (d_stage_) cudaFreeAsync(d_stage_, st_);
-    for (int b = 0; b < 2; ++b) {
-        if (pin_[b]) cudaFreeHost(pin_[b]);
-        if (pin_ev_[b]) cudaEventDestroy(pin_ev_[b]);
-    }
+    for (void* p : ptrs_) dev_free(p);
+    if (d_stage_) dev_free(d_stage_);
+    if (d_series_) dev_free(d_series_);
     if (st_) cudaStreamDestroy(st_);
 }
 
 template <typename S, typename T>
 double* Solver<S, T>::staging() {
     if (!d_stage_) {
-        ck(cudaMallocAsync(reinterpret_cast<void**>(&d_stage_), size_t(NxT_) * NyT_ * NzT_ * sizeof(double), st_),
-           "cudaMallocAsync staging");
+        dev_alloc(reinterpret_cast<void**>(&d_stage_), size_t(NxT_) * NyT_ * NzT_ * sizeof(double));
         dev_bytes += size_t(NxT_) * NyT_ * NzT_ * sizeof(double);
     }
     return d_stage_;
 }
 
-template <typename S, typename T>
-void Solver<S, T>::ensure_pinned() {
-    for (int b = 0; b < 2; ++b) {
-        if (!pin_[b]) ck(cudaHostAlloc(&pin_[b], kPinBytes, cudaHostAllocDefault), "cudaHostAlloc");
-        if (!pin_ev_[b]) ck(cudaEventCreateWithFlags(&pin_ev_[b], cudaEventDisableTiming), "cudaEventCreate");
+// Two pinned staging chunks per device, shared by every solve of the process: made at the
+// first large copy on the device and kept for the life of the process, so that creating and
+// destroying a solve neither pins nor unpins host memory.  A copy holds them (mu) throughout.
+struct PinnedChunks {
+    std::mutex mu;
+    void* buf[2] = {nullptr, nullptr};
+    cudaEvent_t ev[2] = {nullptr, nullptr};
+};
+
+PinnedChunks& pinned_chunks(int dev, size_t bytes) {
+    static std::mutex m;
+    static std::map<int, PinnedChunks*> all;  // never freed: released with the process
+    PinnedChunks* p;
+    {
+        std::lock_guard<std::mutex> l(m);
+        PinnedChunks*& q = all[dev];
+        if (!q) q = new PinnedChunks;
+        p = q;
     }
+    std::lock_guard<std::mutex> l(p->mu);
+    for (int b = 0; b < 2; ++b) {
+        if (!p->buf[b]) ck(cudaHostAlloc(&p->buf[b], bytes, cudaHostAllocDefault), "cudaHostAlloc");
+        if (!p->ev[b]) ck(cudaEventCreateWithFlags(&p->ev[b], cudaEventDisableTiming), "cudaEventCreate");
+    }
+    return *p;
 }
 
 // memcpy split over the host threads (the pageable side of a chunk copy)
@@ -1315,16 +1345,18 @@ void Solver<S, T>::h2d(const double* h, double* d, size_t n) {
         ck(cudaStreamSynchronize(st_), "H2D");
         return;
     }
-    ensure_pinned();
+    PinnedChunks& pc = pinned_chunks(device, kPinBytes);
+    std::lock_guard<std::mutex> l(pc.mu);
     const size_t chunk = kPinBytes / sizeof(double);
     for (size_t off = 0, it = 0; off < n; off += chunk, ++it) {
         const int b = int(it & 1);
         const size_t m = std::min(chunk, n - off);
-        ck(cudaEventSynchronize(pin_ev_[b]), "pinned buffer");  // its previous DMA is done
-        par_copy(pin_[b], h + off, m * sizeof(double));
-        ck(cudaMemcpyAsync(d + off, pin_[b], m * sizeof(double), cudaMemcpyHostToDevice, st_), "H2D");
-        ck(cudaEventRecord(pin_ev_[b], st_), "cudaEventRecord");
+        ck(cudaEventSynchronize(pc.ev[b]), "pinned buffer");  // its previous DMA is done
+        par_copy(pc.buf[b], h + off, m * sizeof(double));
+        ck(cudaMemcpyAsync(d + off, pc.buf[b], m * sizeof(double), cudaMemcpyHostToDevice, st_), "H2D");
+        ck(cudaEventRecord(pc.ev[b], st_), "cudaEventRecord");
     }
+    ck(cudaStreamSynchronize(st_), "H2D");  // the chunks are free for the next copy
 }
 
 template <typename S, typename T>
@@ -1334,20 +1366,21 @@ void Solver<S, T>::d2h(const double* d, double* h, size_t n) {
         ck(cudaStreamSynchronize(st_), "D2H");
         return;
     }
-    ensure_pinned();
+    PinnedChunks& pc = pinned_chunks(device, kPinBytes);
+    std::lock_guard<std::mutex> l(pc.mu);
     const size_t chunk = kPinBytes / sizeof(double);
     const size_t nch = (n + chunk - 1) / chunk;
     auto issue = [&](size_t it) {
         const size_t off = it * chunk, m = std::min(chunk, n - off);
-        ck(cudaMemcpyAsync(pin_[it & 1], d + off, m * sizeof(double), cudaMemcpyDeviceToHost, st_), "D2H");
-        ck(cudaEventRecord(pin_ev_[it & 1], st_), "cudaEventRecord");
+        ck(cudaMemcpyAsync(pc.buf[it & 1], d + off, m * sizeof(double), cudaMemcpyDeviceToHost, st_), "D2H");
+        ck(cudaEventRecord(pc.ev[it & 1], st_), "cudaEventRecord");
     };
     if (nch) issue(0);
     for (size_t it = 0; it < nch; ++it) {
         if (it + 1 < nch) issue(it + 1);  // the other buffer was drained in the previous iteration
         const size_t off = it * chunk, m = std::min(chunk, n - off);
-        ck(cudaEventSynchronize(pin_ev_[it & 1]), "D2H chunk");
-        par_copy(h + off, pin_[it & 1], m * sizeof(double));
+        ck(cudaEventSynchronize(pc.ev[it & 1]), "D2H chunk");
+        par_copy(h + off, pc.buf[it & 1], m * sizeof(double));
     }
 }
 
@@ -1446,11 +1479,11 @@ void Solver<S, T>::ensure_series(uint64_t samples) {
     if (nprobes_ == 0 || samples <= series_cap_) return;
     uint64_t cap = std::max<uint64_t>(samples, series_cap_ * 2);
     double* d = nullptr;
-    ck(cudaMalloc(&d, cap * nprobes_ * sizeof(double)), "cudaMalloc series");
+    dev_alloc(reinterpret_cast<void**>(&d), cap * nprobes_ * sizeof(double));
     if (d_series_) {
         ck(cudaMemcpyAsync(d, d_series_, series_count_ * nprobes_ * sizeof(double), cudaMemcpyDeviceToDevice, st_), "series copy");
         ck(cudaStreamSynchronize(st_), "series copy");
-        cudaFree(d_series_);
+        dev_free(d_series_);
         dev_bytes -= series_cap_ * nprobes_ * sizeof(double);
     }
     d_series_ = d;
@@ -2136,9 +2169,9 @@ private:
             l.unlock();
             std::string err;
             try {
-                if (j.storage == 0) j.f32 = std::make_unique<Solver<float, float>>(*j.setup, device_);
-                else if (j.storage == 1) j.f16 = std::make_unique<Solver<__half, float>>(*j.setup, device_);
-                else j.bf16 = std::make_unique<Solver<__nv_bfloat16, float>>(*j.setup, device_);
+                if (j.storage == 0) j.f32 = std::make_unique<Solver<float, float>>(*j.setup, device_, nullptr, true);
+                else if (j.storage == 1) j.f16 = std::make_unique<Solver<__half, float>>(*j.setup, device_, nullptr, true);
+                else j.bf16 = std::make_unique<Solver<__nv_bfloat16, float>>(*j.setup, device_, nullptr, true);
                 with(j, [&](auto& v) {
                     v.ensure_series((j.target + v.save_every_ - 1) / v.save_every_);
                     ck(cudaStreamSynchronize(v.st_), "admit");
@@ -2475,11 +2508,9 @@ public:
         t->steps = tsteps_;
         t->run_ms = run_ms_;
     }
-    void attach_outputs(const fdtd::SimSetup&, const std::string&) override {
-        throw Failure(FDTD_ERR_UNSUPPORTED, "detector files are written by a whole solve only");
-    }
-    void flush_outputs() override {}
-    void close_outputs() override {}
+    void attach_outputs(const fdtd::SimSetup& setup, const std::string& root) override;
+    void flush_outputs() override;
+    void close_outputs() override;
 
 private:
     // A shard's slice of the setup view: the arrays it needs, copied out of the whole view.
@@ -2509,6 +2540,40 @@ private:
     cudaEvent_t tev_[2] = {};
     double run_ms_ = 0;
     uint64_t tsteps_ = 0;
+
+    // Detector files (fdtd_attach_outputs): the whole solve's plan and one writer thread.  At a
+    // save step every shard captures, on its own stream, the part of each movie slice that lies
+    // in the planes it holds and its two-level sums; the writer joins the parts once every
+    // shard's copy has completed.  A ring slot is reused after the writer is done with it.
+    static constexpr int kOutSlots = 4, kTlsSlots = 16;
+    static constexpr size_t kNoPart = ~size_t(0);
+    struct OutPart {
+        std::vector<size_t> off;    // per movie: byte offset of this shard's part in a slot, or kNoPart
+        std::vector<int> index;     // per movie: the slice index in the shard's local grid
+        std::vector<long long> d2;  // per movie: the part's second dimension
+        size_t slot_bytes = 0;
+        char* d_slot[kOutSlots] = {};
+        char* h_slot[kOutSlots] = {};
+        cudaEvent_t ev[kOutSlots] = {};
+        TlsRecord* d_trec = nullptr;
+        TlsRecord* h_trec = nullptr;
+        cudaEvent_t trec_ev[kTlsSlots] = {};
+        long long mon_t = -1;  // the PolarizationDiagnostics cell in this shard's gain box, or -1
+    };
+    std::unique_ptr<fdtd::OutputWriter> writer_;
+    fdtd::OutputPlan oplan_;
+    std::string oroot_;
+    std::vector<OutPart> out_;
+    std::mutex oslot_mu_;
+    std::condition_variable oslot_cv_;
+    int oslot_busy_[kOutSlots] = {}, trec_busy_[kTlsSlots] = {};
+    uint64_t oframe_ = 0, tls_count_ = 0, ots_written_ = 0;
+    bool pop_first_done_ = false;
+    void capture_movies();
+    void capture_tls(uint64_t s);
+    void write_point_samples();
+    void write_population_frame();
+    void free_outputs();
 };
 
 template <typename S, typename T>
@@ -2671,6 +2736,14 @@ Sharded<S, T>::Sharded(const fdtd_setup_v1& s, int n, const int* devices) {
 template <typename S, typename T>
 Sharded<S, T>::~Sharded() {
     for (auto& p : part_) p->sync();
+    if (writer_) {
+        try {
+            writer_->drain();
+        } catch (const std::exception&) {
+        }
+        writer_.reset();
+    }
+    free_outputs();
     for (auto* evs : {&evE_, &evH_, &evCpE_, &evCpH_, &evMon_})
         for (cudaEvent_t e : *evs) if (e) cudaEventDestroy(e);
     for (cudaEvent_t e : tev_) if (e) cudaEventDestroy(e);
@@ -2744,6 +2817,10 @@ void Sharded<S, T>::run(uint64_t n) {
             part_[r]->phase_E(s, src[r], mon);
             ck(cudaEventRecord(evE_[r], part_[r]->st_), "cudaEventRecord");
         }
+        if (writer_ && s % part_[0]->save_every_ == 0) {  // each shard after its own E sweep
+            if (!oplan_.movies.empty()) capture_movies();
+            if (oplan_.tls) capture_tls(s);
+        }
         if (mon) {
             Solver<S, T>& p0 = *part_[0];
             ck(cudaSetDevice(p0.device), "cudaSetDevice");
@@ -2806,6 +2883,7 @@ void Sharded<S, T>::run(uint64_t n) {
         launches += p->launches;
     }
     steps = done;
+    if (writer_) write_point_samples();
     if (status) throw Failure(FDTD_ERR_UNSTABLE, "stability monitor stopped the solve at step " + std::to_string(done - 1));
 }
 
@@ -2864,6 +2942,319 @@ template <typename S, typename T>
 void Sharded<S, T>::dft(uint32_t p, double* re, double* im) {
     if (p >= probe_at_.size()) throw Failure(FDTD_ERR_INVALID, "no DFT for this probe");
     part_[probe_at_[p].first]->dft(uint32_t(probe_at_[p].second), re, im);
+}
+
+// ---- detector files of a sharded solve
+template <typename S, typename T>
+void Sharded<S, T>::attach_outputs(const fdtd::SimSetup& Sp, const std::string& root) {
+    if (writer_) throw Failure(FDTD_ERR_INVALID, "outputs are already attached");
+    if (steps != 0) throw Failure(FDTD_ERR_INVALID, "outputs can only be attached before the first step");
+    if (Sp.NxT != NxT_ || Sp.NyT != NyT_ || Sp.NzT != NzT_ || Sp.save_every != part_[0]->save_every_)
+        throw Failure(FDTD_ERR_INVALID, "the setup does not match the handle (grid or SAVE_EVERY)");
+    fdtd::OutputPlan plan;
+    try {
+        plan = fdtd::make_output_plan(Sp);
+    } catch (const std::exception& e) {
+        throw Failure(FDTD_ERR_INVALID, e.what());
+    }
+    size_t comps = 0;
+    for (const auto& p : plan.points) comps += p.components.size();
+    if (comps != probe_at_.size()) throw Failure(FDTD_ERR_INVALID, "the setup's point detectors do not match the handle's probes");
+    try {
+        fdtd::write_setup_outputs(Sp, plan, root);
+    } catch (const std::exception& e) {
+        throw Failure(FDTD_ERR_IO, e.what());
+    }
+    const size_t word = plan.float64 ? sizeof(double) : sizeof(float);
+    out_.assign(part_.size(), OutPart{});
+    try {
+        for (size_t r = 0; r < part_.size(); ++r) {
+            Solver<S, T>& p = *part_[r];
+            OutPart& o = out_[r];
+            const int nz = int(slice_[r]->v.NzT), lo = lo_[r];
+            for (const auto& m : plan.movies) {
+                // XY at plane k: the owner's local plane; XZ / YZ: the shard's whole local z
+                // extent, of which the writer keeps the owned planes
+                size_t bytes = 0;
+                int idx = int(m.index);
+                long long d2 = (long long)m.dim2;
+                if (m.plane == 0) {
+                    if (idx >= z0_[r] && idx < z1_[r]) {
+                        idx -= lo;
+                        bytes = m.dim1 * m.dim2 * word;
+                    }
+                } else {
+                    d2 = nz;
+                    bytes = m.dim1 * size_t(nz) * word;
+                }
+                o.off.push_back(bytes ? o.slot_bytes : kNoPart);
+                o.index.push_back(idx);
+                o.d2.push_back(d2);
+                o.slot_bytes += round_up(bytes, 256);
+            }
+            ck(cudaSetDevice(p.device), "cudaSetDevice");
+            if (o.slot_bytes)
+                for (int q = 0; q < kOutSlots; ++q) {
+                    ck(cudaMalloc(reinterpret_cast<void**>(&o.d_slot[q]), o.slot_bytes), "cudaMalloc");
+                    ck(cudaHostAlloc(reinterpret_cast<void**>(&o.h_slot[q]), o.slot_bytes, cudaHostAllocDefault), "cudaHostAlloc");
+                    ck(cudaEventCreateWithFlags(&o.ev[q], cudaEventDisableTiming), "cudaEventCreate");
+                }
+            if (plan.tls) {
+                ck(cudaMalloc(reinterpret_cast<void**>(&o.d_trec), kTlsSlots * sizeof(TlsRecord)), "cudaMalloc");
+                ck(cudaHostAlloc(reinterpret_cast<void**>(&o.h_trec), kTlsSlots * sizeof(TlsRecord), cudaHostAllocDefault),
+                   "cudaHostAlloc");
+                for (int q = 0; q < kTlsSlots; ++q)
+                    ck(cudaEventCreateWithFlags(&o.trec_ev[q], cudaEventDisableTiming), "cudaEventCreate");
+                const StepArgs<S, T>& a = p.a_;
+                const long long mk = (long long)plan.mon_k;
+                if (p.has_gain_ && plan.mon_valid && mk >= z0_[r] && mk < z1_[r]) {
+                    const long long i = (long long)plan.mon_i - a.gi0, j = (long long)plan.mon_j - a.gj0, k = mk - lo - a.gk0;
+                    if (i >= 0 && i < a.gX && j >= 0 && j < a.gY && k >= 0 && k < a.gZ) o.mon_t = (k * a.gY + j) * a.gX + i;
+                }
+            }
+        }
+    } catch (...) {
+        free_outputs();
+        throw;
+    }
+    oplan_ = std::move(plan);
+    oroot_ = root;
+    writer_ = std::make_unique<fdtd::OutputWriter>();
+}
+
+template <typename S, typename T>
+void Sharded<S, T>::free_outputs() {
+    for (size_t r = 0; r < out_.size(); ++r) {
+        OutPart& o = out_[r];
+        cudaSetDevice(part_[r]->device);
+        for (int q = 0; q < kOutSlots; ++q) {
+            if (o.d_slot[q]) cudaFree(o.d_slot[q]);
+            if (o.h_slot[q]) cudaFreeHost(o.h_slot[q]);
+            if (o.ev[q]) cudaEventDestroy(o.ev[q]);
+        }
+        if (o.d_trec) cudaFree(o.d_trec);
+        if (o.h_trec) cudaFreeHost(o.h_trec);
+        for (int q = 0; q < kTlsSlots; ++q)
+            if (o.trec_ev[q]) cudaEventDestroy(o.trec_ev[q]);
+    }
+    out_.clear();
+}
+
+template <typename S, typename T>
+void Sharded<S, T>::capture_movies() {
+    const int sl = int(oframe_ % kOutSlots);
+    const size_t nm = oplan_.movies.size();
+    {
+        std::unique_lock<std::mutex> l(oslot_mu_);
+        oslot_cv_.wait(l, [&] { return oslot_busy_[sl] == 0; });
+        oslot_busy_[sl] = int(nm);
+    }
+    const int f64 = oplan_.float64 ? 1 : 0;
+    const size_t word = f64 ? sizeof(double) : sizeof(float);
+    for (size_t r = 0; r < part_.size(); ++r) {
+        Solver<S, T>& p = *part_[r];
+        OutPart& o = out_[r];
+        if (!o.slot_bytes) continue;
+        ck(cudaSetDevice(p.device), "cudaSetDevice");
+        for (size_t m = 0; m < nm; ++m) {
+            if (o.off[m] == kNoPart) continue;
+            const fdtd::MoviePlan& v = oplan_.movies[m];
+            const long long count = (long long)v.dim1 * o.d2[m];
+            const unsigned nb = unsigned(std::min<long long>((count + 255) / 256, 148 * 4));
+            k_slice<S><<<nb, 256, 0, p.st_>>>(p.a_.Ex, p.a_.Ey, p.a_.Ez, p.a_.Hx, p.a_.Hy, p.a_.Hz, int(NyT_), p.NxP_,
+                                               v.plane, o.index[m], v.component, o.d2[m], count, p.sE_, p.sH_,
+                                               o.d_slot[sl] + o.off[m], f64);
+            ++p.launches;
+        }
+        ck(cudaMemcpyAsync(o.h_slot[sl], o.d_slot[sl], o.slot_bytes, cudaMemcpyDeviceToHost, p.st_), "movie part D2H");
+        ck(cudaEventRecord(o.ev[sl], p.st_), "cudaEventRecord");
+    }
+    for (size_t m = 0; m < nm; ++m) {
+        const fdtd::MoviePlan& v = oplan_.movies[m];
+        auto frame = std::make_shared<std::vector<char>>(v.dim1 * v.dim2 * word);
+        fdtd::OutputWriter::Job j;
+        // join the shards' parts once their copies are complete (on the writer thread)
+        j.wait = [this, sl, m, frame, word] {
+            const fdtd::MoviePlan& v = oplan_.movies[m];
+            for (size_t r = 0; r < part_.size(); ++r) {
+                const OutPart& o = out_[r];
+                if (o.off[m] == kNoPart) continue;
+                cudaSetDevice(part_[r]->device);
+                if (cudaEventSynchronize(o.ev[sl]) != cudaSuccess) throw std::runtime_error("movie frame copy failed");
+                const char* part = o.h_slot[sl] + o.off[m];
+                if (v.plane == 0) {
+                    std::memcpy(frame->data(), part, frame->size());
+                    continue;
+                }
+                const size_t nz = size_t(o.d2[m]), own = size_t(z1_[r] - z0_[r]), skip = size_t(z0_[r] - lo_[r]);
+                for (size_t a = 0; a < v.dim1; ++a)
+                    std::memcpy(frame->data() + (a * v.dim2 + size_t(z0_[r])) * word, part + (a * nz + skip) * word,
+                                own * word);
+            }
+        };
+        j.done = [this, sl, frame] {
+            {
+                std::lock_guard<std::mutex> l(oslot_mu_);
+                --oslot_busy_[sl];
+            }
+            oslot_cv_.notify_all();
+        };
+        j.path = fdtd::frame_path(oplan_, oroot_, m, oframe_);
+        j.data = frame->data();
+        j.bytes = frame->size();
+        writer_->submit(std::move(j));
+    }
+    ++oframe_;
+}
+
+template <typename S, typename T>
+void Sharded<S, T>::capture_tls(uint64_t s) {
+    if (!pop_first_done_) {
+        write_population_frame();
+        pop_first_done_ = true;
+    }
+    const int sl = int(tls_count_++ % kTlsSlots);
+    {
+        std::unique_lock<std::mutex> l(oslot_mu_);
+        oslot_cv_.wait(l, [&] { return trec_busy_[sl] == 0; });
+        trec_busy_[sl] = 3;
+    }
+    for (size_t r = 0; r < part_.size(); ++r) {
+        Solver<S, T>& p = *part_[r];
+        OutPart& o = out_[r];
+        ck(cudaSetDevice(p.device), "cudaSetDevice");
+        ck(cudaMemsetAsync(o.d_trec + sl, 0, sizeof(TlsRecord), p.st_), "cudaMemsetAsync");
+        if (p.has_gain_) {
+            const size_t ng = size_t(p.a_.gX) * p.a_.gY * p.a_.gZ;
+            const unsigned nb = unsigned(std::max<size_t>(1, std::min<size_t>((ng + 255) / 256, 148 * 4)));
+            k_tls_reduce<S, T><<<nb, 256, 0, p.st_>>>(p.a_, p.d_dx_, p.d_dy_, p.d_dz_, int((s + 1) & 1), p.sE_,
+                                                        o.d_trec + sl, o.mon_t);
+            ++p.launches;
+        }
+        ck(cudaMemcpyAsync(o.h_trec + sl, o.d_trec + sl, sizeof(TlsRecord), cudaMemcpyDeviceToHost, p.st_), "TLS record D2H");
+        ck(cudaEventRecord(o.trec_ev[sl], p.st_), "cudaEventRecord");
+    }
+    // the whole solve's record: the shards' sums added in shard order; Pz and dPz/dt from the
+    // shard that holds the cell (the others leave them 0)
+    auto sum = std::make_shared<TlsRecord>();
+    const double dt = part_[0]->dt_;
+    const std::string dir = fdtd::run_dir(oplan_, oroot_);
+    auto release = [this, sl] {
+        {
+            std::lock_guard<std::mutex> l(oslot_mu_);
+            --trec_busy_[sl];
+        }
+        oslot_cv_.notify_all();
+    };
+    fdtd::OutputWriter::Job a, b, c;
+    a.wait = [this, sl, sum] {
+        std::memset(sum.get(), 0, sizeof(TlsRecord));
+        for (size_t r = 0; r < part_.size(); ++r) {
+            cudaSetDevice(part_[r]->device);
+            if (cudaEventSynchronize(out_[r].trec_ev[sl]) != cudaSuccess) throw std::runtime_error("two-level record copy failed");
+            const TlsRecord& x = out_[r].h_trec[sl];
+            sum->acc.int_Nu += x.acc.int_Nu;
+            sum->acc.int_Ng += x.acc.int_Ng;
+            sum->acc.p_energy += x.acc.p_energy;
+            if (out_[r].mon_t >= 0) {
+                sum->P_center = x.P_center;
+                sum->dP_dt = x.dP_dt;
+            }
+        }
+    };
+    a.text = [sum, s, dt] { return fdtd::inversion_line(s, dt, sum->acc.int_Nu, sum->acc.int_Ng); };
+    a.path = dir + "/populations/inversion_time.csv";
+    b.text = [sum, s, dt] { return fdtd::polarization_line(s, dt, sum->P_center, sum->dP_dt, sum->acc.p_energy); };
+    b.path = dir + "/polarization/polarization_time.csv";
+    c.text = [sum, s, dt] { return fdtd::global_history_line(s, dt, sum->acc.int_Nu, sum->acc.int_Ng); };
+    c.path = dir + "/tls_global_history.csv";
+    for (fdtd::OutputWriter::Job* j : {&a, &b, &c}) {
+        j->append = true;
+        j->done = release;
+        writer_->submit(std::move(*j));
+    }
+}
+
+template <typename S, typename T>
+void Sharded<S, T>::write_population_frame() {
+    // PopulationTimeSeriesDetector::write_binary_frame: the full-grid Nu and Ng, FP64, idx3,
+    // gathered from the shards' owned planes
+    const size_t N = size_t(NxT_) * NyT_ * NzT_;
+    const std::string dir = fdtd::run_dir(oplan_, oroot_) + "/populations/";
+    for (int w : {int(FDTD_TLS_NU), int(FDTD_TLS_NG)}) {
+        auto buf = std::make_shared<std::vector<double>>(N);
+        get_tls(w, buf->data());
+        fdtd::OutputWriter::Job j;
+        j.path = dir + (w == FDTD_TLS_NU ? "populations_Nu.bin" : "populations_Ng.bin");
+        j.data = buf->data();
+        j.bytes = N * sizeof(double);
+        j.append = true;
+        j.done = [buf] {};
+        writer_->submit(std::move(j));
+    }
+}
+
+template <typename S, typename T>
+void Sharded<S, T>::write_point_samples() {
+    const size_t np = probe_at_.size();
+    if (oplan_.points.empty() || !np) return;
+    uint64_t count = 0;
+    probe_series(nullptr, 0, &count);
+    if (count <= ots_written_) return;
+    std::vector<double> v(size_t(count) * np);
+    probe_series(v.data(), count, nullptr);
+    const uint64_t n0 = ots_written_, n = count - ots_written_;
+    const std::string dir = fdtd::run_dir(oplan_, oroot_);
+    size_t col = 0;
+    for (const auto& p : oplan_.points) {
+        for (int c : p.components) {
+            auto buf = std::make_shared<std::vector<char>>();
+            if (oplan_.float64) {
+                buf->resize(n * sizeof(double));
+                for (uint64_t t = 0; t < n; ++t) std::memcpy(buf->data() + t * 8, &v[(n0 + t) * np + col], 8);
+            } else {
+                buf->resize(n * sizeof(float));
+                for (uint64_t t = 0; t < n; ++t) {
+                    const float f = float(v[(n0 + t) * np + col]);
+                    std::memcpy(buf->data() + t * 4, &f, 4);
+                }
+            }
+            fdtd::OutputWriter::Job j;
+            j.path = dir + "/" + p.name + "/" + fdtd::component_name(c) + "_ts.bin";
+            j.data = buf->data();
+            j.bytes = buf->size();
+            j.append = true;
+            j.done = [buf] {};
+            writer_->submit(std::move(j));
+            ++col;
+        }
+    }
+    ots_written_ = count;
+}
+
+template <typename S, typename T>
+void Sharded<S, T>::flush_outputs() {
+    if (!writer_) return;
+    try {
+        writer_->drain();
+    } catch (const std::exception& e) {
+        throw Failure(FDTD_ERR_IO, e.what());
+    }
+}
+
+template <typename S, typename T>
+void Sharded<S, T>::close_outputs() {
+    if (!writer_) return;
+    if (oplan_.tls) {  // PopulationTimeSeriesDetector::finalize: the last frame and the metadata
+        write_population_frame();
+        try {
+            fdtd::write_population_metadata(oplan_, oroot_);
+        } catch (const std::exception& e) {
+            throw Failure(FDTD_ERR_IO, e.what());
+        }
+    }
+    flush_outputs();
+    writer_.reset();
 }
 }  // namespace
 

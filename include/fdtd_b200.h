@@ -301,7 +301,9 @@ int fdtd_close_outputs(fdtd_handle *h);
  * monitor is evaluated once for the whole solve.  The handle answers the same calls as a
  * whole solve (fields, gain state, probes, DFT, diagnostics) with identical values; CPML or
  * PEC boundary (each shard zeroes the PEC faces of the planes it owns); kernel path 1 only,
- * whole-run timing only, no detector files.  No counterpart in the reference's
+ * whole-run timing only.  Detector files (fdtd_attach_outputs) are the whole solve's: each
+ * shard captures the part of every movie slice in the planes it owns and its two-level sums,
+ * and one writer thread joins them into the reference's files.  No counterpart in the reference's
  * time loop; its slab-parallel variant (src/parallel_domain.hpp) splits one process's loop. */
 int fdtd_create_sharded(const fdtd_setup_v1 *setup, int nshards, const int *devices, fdtd_handle **out);
 /* Block until all device work of the handle is complete. */

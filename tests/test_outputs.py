@@ -136,6 +136,44 @@ def test_streamed_outputs_match_reference(pkg, outdir, precision, tol):
     sol.close()
 
 
+def _run_files(pkg, s, outdir, precision, shards, sub):
+    sol = pkg.Solver(s, precision=precision, shards=shards)
+    d = pathlib.Path(outdir) / sub
+    sol.attach_outputs(d)
+    sol.run(17)
+    sol.run(13)
+    sol.close_outputs()
+    sol.close()
+    root = d / "frames"
+    return {str(f.relative_to(root)): f.read_bytes() for f in root.rglob("*") if f.is_file()}
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision,shards", [(1, 2), (1, 3), (0, 3)])
+def test_sharded_outputs_match_whole_solve(pkg, outdir, precision, shards):
+    """A solve split into z shards writes the whole solve's files: movie frames joined from the
+    shards' owned planes (XY slices from the shard that holds the plane, XZ / YZ slices from
+    every shard), point series from the shard that holds the probe, population frames gathered,
+    the two-level sums added over the shards.  The fields are bit-identical, so are the frames,
+    series and population frames; the CSV sums differ only by FP64 summation order."""
+    s = pkg.Setup.from_file(CASE)
+    whole = _run_files(pkg, s, outdir, precision, 1, "whole")
+    split = _run_files(pkg, s, outdir, precision, shards, "split")
+    assert set(split) == set(whole), sorted(set(split) ^ set(whole))
+    for k in sorted(whole):
+        if k.endswith(".csv"):
+            h1, a = csv_rows(split[k])
+            h2, b = csv_rows(whole[k])
+            assert h1 == h2 and a.shape == b.shape, k
+            scale = np.maximum(np.abs(b).max(axis=0), 1e-300)
+            assert np.all(np.abs(a - b) <= 1e-12 * scale), (k, np.abs(a - b).max(axis=0) / scale)
+        elif not k.endswith("mesh_info.json"):
+            assert split[k] == whole[k], k
+    # the reference's file set (the whole solve's files are checked against the reference's
+    # values in test_streamed_outputs_match_reference)
+    assert set(split) == set(ref_files())
+
+
 @pytest.mark.gpu
 def test_float32_outputs(pkg, outdir):
     s = pkg.Setup.from_text(CASE.read_text() + "\nWRITE_FLOAT64 = false\n")
