@@ -189,6 +189,34 @@ template <> __device__ __forceinline__ double from_d<double>(double v) { return 
 template <> __device__ __forceinline__ __half from_d<__half>(double v) { return __double2half(v); }
 template <> __device__ __forceinline__ __nv_bfloat16 from_d<__nv_bfloat16>(double v) { return __double2bfloat16(v); }
 
+// 16-bit storage, interior columns: a thread holds 8 cells of an array as one 16-byte word
+// (uint4) and updates them as two 4-cell halves; half h is cells 4h .. 4h+3, the word's
+// (x, y) or (z, w).
+template <typename S>
+__device__ __forceinline__ void unpack4(const uint2 u, float (&a)[4]) {
+    if constexpr (std::is_same_v<S, __half>) {
+        const float2 lo = __half22float2(*reinterpret_cast<const __half2*>(&u.x));
+        const float2 hi = __half22float2(*reinterpret_cast<const __half2*>(&u.y));
+        a[0] = lo.x; a[1] = lo.y; a[2] = hi.x; a[3] = hi.y;
+    } else {
+        const float2 lo = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&u.x));
+        const float2 hi = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&u.y));
+        a[0] = lo.x; a[1] = lo.y; a[2] = hi.x; a[3] = hi.y;
+    }
+}
+__device__ __forceinline__ uint2 half_of(const uint4& v, int h) { return h ? make_uint2(v.z, v.w) : make_uint2(v.x, v.y); }
+// cell 0 and cell 7 of a word, as FP32
+template <typename S>
+__device__ __forceinline__ float first_of(const uint4& v) {
+    const unsigned short b = (unsigned short)(v.x & 0xffffu);
+    return to_c(*reinterpret_cast<const S*>(&b));
+}
+template <typename S>
+__device__ __forceinline__ float last_of(const uint4& v) {
+    const unsigned short b = (unsigned short)(v.w >> 16);
+    return to_c(*reinterpret_cast<const S*>(&b));
+}
+
 // Explicitly rounded arithmetic of the update formulas.  Every product, difference and
 // fused multiply-add of an update goes through one of these, so the compiler can neither
 // contract nor reassociate them: every instantiation of one update (the single-solve sweeps,
@@ -405,25 +433,25 @@ template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
 
 // Shared-memory staging of the sweeps' interior columns.  A slot holds one field vector of
-// one thread (SB bytes: 16 for 32/64-bit storage, 8 for 16-bit), slots are slot-major so a
-// warp's slots are consecutive, and kStages planes of slots form a ring: the thread copies
-// plane k + kStages - 1 while it computes plane k.  16-bit storage fills half the bytes of a
-// 16-byte slot, so it runs four stages (three planes in flight) in the shared memory that
-// 32/64-bit storage spends on two.
-template <typename S>
+// one thread (SB bytes), slots are slot-major so a warp's slots are consecutive, and kStages
+// planes of slots form a ring: the thread copies plane k + kStages - 1 while it computes
+// plane k.  A 16-byte slot holds 4 FP32 or 2 FP64 cells, or the 8 cells of an H-sweep vector
+// of 16-bit storage; the E sweep's 4-cell 16-bit vectors fill 8-byte slots and run four stages
+// (three planes in flight) in the shared memory the others spend on two.
+template <int SB_, int STAGES>
 struct PipeShape {
-    static constexpr int SB = sizeof(S) == 2 ? 8 : 16;
-    static constexpr int kStages = sizeof(S) == 2 ? 4 : 2;
+    static constexpr int SB = SB_;
+    static constexpr int kStages = STAGES;
 };
 
 // E sweep slots: 0-2 E, 3-5 H, 6 Hz(j-1), 7 Hx(j-1), 8 the material row ids, last: Hz and
 // Hy at i0-1 for the warp's first lane (at byte 0 and SB/2 of the slot).  Staging is used with
 // the row-indexed material only.
 template <typename S>
-struct EPipe : PipeShape<S> {
+struct EPipe : PipeShape<sizeof(S) == 2 ? 8 : 16, sizeof(S) == 2 ? 4 : 2> {
     static constexpr int kSlots = 10;
     static constexpr int kX = kSlots - 1;
-    static constexpr size_t bytes() { return size_t(PipeShape<S>::kStages) * kSlots * (32 * kBlockY) * PipeShape<S>::SB; }
+    static constexpr size_t bytes() { return size_t(EPipe::kStages) * kSlots * (32 * kBlockY) * EPipe::SB; }
 };
 
 // True when a point source or (SH) a plane-wave sheet touches one of the W cells (i0.., j, k).
@@ -526,7 +554,8 @@ __device__ __forceinline__ void e_plain(const StepArgs<S, T>& a, const size_t c,
 
 // ---------------------------------------------------------------------------------
 // Launch geometry of the sweeps.  The x range of a row is split into the interior
-// [xi0, xi1) -- W-aligned vectors with no x-slab cell -- covered by gxi block columns of
+// [xi0, xi1) -- vectors with no x-slab cell, of W cells (8 for 16-bit storage, whose field
+// arrays are offset so that xi0 falls on a 16-byte boundary) -- covered by gxi block columns of
 // `lanes`-vector row segments, and the edge vectors outside it (nl on the left, ne in total),
 // which one extra block column packs er rows at a time, one thread per edge vector.
 // Interior warps therefore never diverge on the x slab, and edge threads all take the
@@ -540,6 +569,15 @@ struct SweepGeom {
     int er;        // rows per edge block
     int lanes;     // lanes per interior row segment (32, 16 or 8)
 };
+
+// Interior block columns of the E sweep: gxi, except for 16-bit storage, whose E sweep runs
+// 4-cell vectors over the interior that the H sweep covers with 8-cell ones (H measured 10-12 %
+// faster with 8-cell vectors, E 0-11 % slower, on the 536^3 workload).
+template <typename S>
+__host__ __device__ __forceinline__ int gxi_E(const SweepGeom& g) {
+    if constexpr (sizeof(S) == 2) return ((g.xi1 - g.xi0) / 4 + g.lanes - 1) / g.lanes;
+    else return g.gxi;
+}
 
 // Row and first vector of an interior thread: warp w of block row `by` holds rows
 // (by * kBlockY + w) * R .. + R - 1 (R = 32 / lanes), segment `lane / lanes` of the warp one row.
@@ -561,9 +599,9 @@ __device__ __forceinline__ InteriorLane interior_lane(const SweepGeom& g, const 
 // H sweep slots (as EPipe): 0-1 Ex, Ey at k+1, 2 Ez, 3 Ex(j+1), 4 Ez(j+1), 5-7 H, 8 Ey and Ez
 // at i0+W for the lanes that load it (at byte 0 and SB/2 of the slot).
 template <typename S>
-struct HPipe : PipeShape<S> {
+struct HPipe : PipeShape<16, 2> {
     static constexpr int kSlots = 9;
-    static constexpr size_t bytes() { return size_t(PipeShape<S>::kStages) * kSlots * (32 * kBlockY) * PipeShape<S>::SB; }
+    static constexpr size_t bytes() { return size_t(HPipe::kStages) * kSlots * (32 * kBlockY) * HPipe::SB; }
 };
 
 // li: the thread's lane within its row segment of g.lanes lanes (interior columns).
@@ -744,6 +782,181 @@ __device__ __forceinline__ void h_column(const StepArgs<S, T>& a, const SweepGeo
     }
 }
 
+// 16-bit storage, interior column: the thread's 8 cells (i0 .. i0+7, i0 16-byte aligned) of
+// every array come as one 16-byte word per plane (PIPE: one 16-byte cp.async each), and the
+// two 4-cell halves take h_column's update in the same order: the same bits.  Ey, Ez at
+// i0+8 come from the next lane's first cell or, at the end of the row segment or of the
+// interior, from memory.
+template <typename S, bool PIPE>
+__device__ __forceinline__ void h_column8(const StepArgs<S, float>& a, const SweepGeom& g, const int j, const int i0,
+                                          const bool act, const int kb, const int ke, const int li,
+                                          const unsigned step) {
+    using T = float;
+    constexpr int W = 4;
+    const int np = a.np, np2 = 2 * np;
+    const T nbH = -a.bH;
+
+    T idx[2][W];
+#pragma unroll
+    for (int h = 0; h < 2; ++h)
+#pragma unroll
+        for (int e = 0; e < W; ++e) idx[h][e] = act ? __ldg(a.idx + i0 + 4 * h + e) : T(0);
+    const T idy = __ldg(a.idy + j);
+    const bool ypml = in_pml(j, a.NyT, np);
+    const int jy = ypml ? slab_index(j, a.NyT, np) : 0;
+    T yb = 1, yc = 0, yik = 1;
+    if (ypml) { yb = __ldg(a.pbH[1] + j); yc = __ldg(a.pcH[1] + j); yik = __ldg(a.ik[1] + j); }
+    const bool nload = li == g.lanes - 1 || i0 + 8 >= g.xi1;
+    const bool xn = nload && i0 + 8 < a.NxT;
+
+    const size_t row = size_t(j) * a.NxP + i0;
+    auto ld16 = [](const S* p) { return __ldg(reinterpret_cast<const uint4*>(p)); };
+    uint4 ex0 = make_uint4(0, 0, 0, 0), ey0 = make_uint4(0, 0, 0, 0);
+    if (act) {
+        ex0 = ld16(a.Ex + size_t(kb) * a.plane + row);
+        ey0 = ld16(a.Ey + size_t(kb) * a.plane + row);
+    }
+
+    extern __shared__ uint4 pipe_smem[];
+    constexpr int NT = 32 * kBlockY, NV = HPipe<S>::kSlots, NS = HPipe<S>::kStages;
+    const int tid = threadIdx.y * 32 + threadIdx.x;
+    char* const pipe = reinterpret_cast<char*>(pipe_smem);
+    auto slot = [&](int stg, int q) { return pipe + ((size_t(stg) * NV + q) * NT + tid) * 16; };
+    auto issue = [&](int kk, int stg) {
+        const size_t cc = size_t(kk) * a.plane + row;
+        cp_async<16>(slot(stg, 0), a.Ex + cc + a.plane);
+        cp_async<16>(slot(stg, 1), a.Ey + cc + a.plane);
+        cp_async<16>(slot(stg, 2), a.Ez + cc);
+        cp_async<16>(slot(stg, 3), a.Ex + cc + a.NxP);
+        cp_async<16>(slot(stg, 4), a.Ez + cc + a.NxP);
+        cp_async<16, false>(slot(stg, 5), a.Hx + cc);
+        cp_async<16, false>(slot(stg, 6), a.Hy + cc);
+        cp_async<16, false>(slot(stg, 7), a.Hz + cc);
+        if (xn) {
+            cp_async<4>(slot(stg, 8), a.Ey + cc + 8);
+            cp_async<4>(slot(stg, 8) + 8, a.Ez + cc + 8);
+        }
+    };
+    if constexpr (PIPE) {
+#pragma unroll
+        for (int q = 0; q < NS - 1; ++q) {
+            if (act && kb + q < ke) issue(kb + q, q);
+            cp_async_commit();
+        }
+    }
+
+    for (int k = kb; k < ke; ++k) {
+        const size_t c = size_t(k) * a.plane + row;
+        uint4 ex1, ey1, ez, exj, ezj, hx, hy, hz;
+        T eye = T(0), eze = T(0);
+        if (PIPE && act) {
+            if (k + NS - 1 < ke) issue(k + NS - 1, (k + NS - 1 - kb) & (NS - 1));
+            cp_async_commit();
+            cp_async_wait<NS - 1>();
+            const int stg = (k - kb) & (NS - 1);
+            ex1 = *reinterpret_cast<const uint4*>(slot(stg, 0));
+            ey1 = *reinterpret_cast<const uint4*>(slot(stg, 1));
+            ez = *reinterpret_cast<const uint4*>(slot(stg, 2));
+            exj = *reinterpret_cast<const uint4*>(slot(stg, 3));
+            ezj = *reinterpret_cast<const uint4*>(slot(stg, 4));
+            hx = *reinterpret_cast<const uint4*>(slot(stg, 5));
+            hy = *reinterpret_cast<const uint4*>(slot(stg, 6));
+            hz = *reinterpret_cast<const uint4*>(slot(stg, 7));
+            if (xn) {
+                const char* xs = slot(stg, 8);
+                eye = T(to_c(reinterpret_cast<const S*>(xs)[0]));
+                eze = T(to_c(reinterpret_cast<const S*>(xs + 8)[0]));
+            }
+        } else if (act) {
+            ex1 = ld16(a.Ex + c + a.plane);
+            ey1 = ld16(a.Ey + c + a.plane);
+            ez = ld16(a.Ez + c);
+            exj = ld16(a.Ex + c + a.NxP);
+            ezj = ld16(a.Ez + c + a.NxP);
+            hx = *reinterpret_cast<const uint4*>(a.Hx + c);
+            hy = *reinterpret_cast<const uint4*>(a.Hy + c);
+            hz = *reinterpret_cast<const uint4*>(a.Hz + c);
+            if (xn) { eye = to_c(a.Ey[c + 8]); eze = to_c(a.Ez[c + 8]); }
+        } else {
+            ex1 = ey1 = ez = exj = ezj = hx = hy = hz = make_uint4(0, 0, 0, 0);
+        }
+        const T idz = __ldg(a.idz + k);
+        const bool zpml = in_pml(k + a.kz0, a.NzG, np);
+        T zb = 1, zc = 0, zik = 1;
+        if (zpml) { zb = __ldg(a.pbH[2] + k); zc = __ldg(a.pcH[2] + k); zik = __ldg(a.ik[2] + k); }
+        // Ey, Ez at i0+8: the next lane's first cell, or the loaded one
+        const T sy = __shfl_down_sync(kFull, first_of<S>(ey0), 1, g.lanes);
+        const T sz = __shfl_down_sync(kFull, first_of<S>(ez), 1, g.lanes);
+        const T eyn8 = nload ? eye : sy, ezn8 = nload ? eze : sz;
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int ih = i0 + 4 * h;
+            const size_t ch = c + 4 * h;
+            T vex0[W], vex1[W], vey0[W], vey1[W], vez[W], vexj[W], vezj[W], vhx[W], vhy[W], vhz[W];
+            unpack4<S>(half_of(ex0, h), vex0); unpack4<S>(half_of(ex1, h), vex1);
+            unpack4<S>(half_of(ey0, h), vey0); unpack4<S>(half_of(ey1, h), vey1);
+            unpack4<S>(half_of(ez, h), vez);
+            unpack4<S>(half_of(exj, h), vexj); unpack4<S>(half_of(ezj, h), vezj);
+            unpack4<S>(half_of(hx, h), vhx); unpack4<S>(half_of(hy, h), vhy); unpack4<S>(half_of(hz, h), vhz);
+            // x-neighbour of the half's last cell: the other half's first cell, or i0+8
+            T eyn = eyn8, ezn = ezn8;
+            if (h == 0) {
+                T t[W];
+                unpack4<S>(half_of(ey0, 1), t); eyn = t[0];
+                unpack4<S>(half_of(ez, 1), t); ezn = t[0];
+            }
+            const bool plain = act && !ypml && ih + W <= a.NxT - 1;
+            if (plain && !zpml) {
+                h_plain<S, T>(a, ch, vex0, vex1, vey0, vey1, vez, vexj, vezj, eyn, ezn, vhx, vhy, vhz, idx[h], idy, idz, step);
+                continue;
+            }
+            size_t zs = 0, ys = 0;
+            T pxy[W], pzy[W], pxz[W], pyz[W];  // psi Hx_y, Hz_y, Hx_z, Hy_z
+            if (zpml) {
+                zs = (size_t(slab_index(k + a.kz0, a.NzG, np)) * a.NyT + j) * a.NxP + ih;
+                if (act) { Fld<S, T>::ld(a.psiH[1] + zs, pxz); Fld<S, T>::ld(a.psiH[2] + zs, pyz); }
+            }
+            if (ypml) {
+                ys = (size_t(k) * np2 + jy) * a.NxP + ih;
+                if (act) { Fld<S, T>::ld(a.psiH[0] + ys, pxy); Fld<S, T>::ld(a.psiH[5] + ys, pzy); }
+            }
+#pragma unroll
+            for (int e = 0; e < W; ++e) {
+                const int i = ih + e;
+                if (i >= a.NxT - 1) continue;  // last x plane (and padding) never updated
+                const T eyx = (e < W - 1) ? vey0[e + 1] : eyn;
+                const T ezx = (e < W - 1) ? vez[e + 1] : ezn;
+                T dEz_dy = dq(vezj[e], vez[e], idy);
+                T dEy_dz = dq(vey1[e], vey0[e], idz);
+                T dEx_dz = dq(vex1[e], vex0[e], idz);
+                T dEz_dx = dq(ezx, vez[e], idx[h][e]);
+                T dEy_dx = dq(eyx, vey0[e], idx[h][e]);
+                T dEx_dy = dq(vexj[e], vex0[e], idy);
+                if (ypml) {
+                    pxy[e] = psi_rec(yb, pxy[e], yc, dEz_dy); dEz_dy = psi_eff<S, T>(dEz_dy, yik, pxy[e], a.psc);
+                    pzy[e] = psi_rec(yb, pzy[e], yc, dEx_dy); dEx_dy = psi_eff<S, T>(dEx_dy, yik, pzy[e], a.psc);
+                }
+                if (zpml) {
+                    pxz[e] = psi_rec(zb, pxz[e], zc, dEy_dz); dEy_dz = psi_eff<S, T>(dEy_dz, zik, pxz[e], a.psc);
+                    pyz[e] = psi_rec(zb, pyz[e], zc, dEx_dz); dEx_dz = psi_eff<S, T>(dEx_dz, zik, pyz[e], a.psc);
+                }
+                vhx[e] = fma_rn(nbH, sub_rn(dEz_dy, dEy_dz), vhx[e]);
+                vhy[e] = fma_rn(nbH, sub_rn(dEx_dz, dEz_dx), vhy[e]);
+                vhz[e] = fma_rn(nbH, sub_rn(dEy_dx, dEx_dy), vhz[e]);
+            }
+            if (act) {
+                st_field(a, a.Hx, ch, vhx, 3, step);
+                st_field(a, a.Hy, ch, vhy, 4, step);
+                st_field(a, a.Hz, ch, vhz, 5, step);
+                if (zpml) { Fld<S, T>::st(a.psiH[1] + zs, pxz); Fld<S, T>::st(a.psiH[2] + zs, pyz); }
+                if (ypml) { Fld<S, T>::st(a.psiH[0] + ys, pxy); Fld<S, T>::st(a.psiH[5] + ys, pzy); }
+            }
+        }
+        ex0 = ex1;
+        ey0 = ey1;
+    }
+}
+
 // One block of the H sweep: block (bx, by, bz) of the solve's launch grid.
 template <typename S, typename T, bool PIPE = false>
 __device__ __forceinline__ void update_H_block(const StepArgs<S, T>& a, const int kchunk, const SweepGeom& g,
@@ -762,8 +975,13 @@ __device__ __forceinline__ void update_H_block(const StepArgs<S, T>& a, const in
         const int jlast = a.NyT - 2;
         if ((by * kBlockY + int(threadIdx.y)) * (32 / g.lanes) > jlast) return;
         const bool row_ok = il.j <= jlast;
-        const int i0 = g.xi0 + (bx * g.lanes + il.li) * W;
-        h_column<S, T, false, PIPE>(a, g, row_ok ? il.j : jlast, i0, row_ok && i0 < g.xi1, kb, ke, il.li, step);
+        if constexpr (sizeof(S) == 2) {  // 8-cell interior vectors
+            const int i0 = g.xi0 + (bx * g.lanes + il.li) * 8;
+            h_column8<S, PIPE>(a, g, row_ok ? il.j : jlast, i0, row_ok && i0 < g.xi1, kb, ke, il.li, step);
+        } else {
+            const int i0 = g.xi0 + (bx * g.lanes + il.li) * W;
+            h_column<S, T, false, PIPE>(a, g, row_ok ? il.j : jlast, i0, row_ok && i0 < g.xi1, kb, ke, il.li, step);
+        }
     } else {
         const int t = threadIdx.y * 32 + lane;
         const int rr = t / g.ne, v = t - rr * g.ne;
@@ -1050,7 +1268,7 @@ __device__ __forceinline__ void update_E_block(const StepArgs<S, T>& a, const in
     const int kb = max(bz * kchunk, a.kE0);
     const int ke = min(bz * kchunk + kchunk, a.kE1);
     if (kb >= ke) return;
-    if (bx < g.gxi) {
+    if (bx < gxi_E<S>(g)) {
         // E is updated for rows 1 <= j < NyT.  A warp with no such row leaves as a whole; in a
         // warp that has one, the other rows stay in the loop as inactive lanes on row 1.
         const InteriorLane il = interior_lane(g, by, lane);

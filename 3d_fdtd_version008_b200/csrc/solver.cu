@@ -828,6 +828,7 @@ private:
     // kernel path 1 (default): k_update_H + k_update_E in place; path 2: k_step_slabs.
     int path_ = 1;
     S* fld_[6] = {};
+    int xoff_ = 0;  // the field arrays start xoff_ elements into their allocation
     S* psiH_[6] = {};
     size_t psi_sz_[6] = {};
     void point_args_at();
@@ -899,7 +900,12 @@ Solver<S, T>::Solver(const fdtd_setup_v1& s, int dev, const ShardSpec* shard, bo
     a.kH1 = std::min(shard_.own1, shard_.NzG - 1 - shard_.kz0);
     a.kE0 = std::max(shard_.own0, 1 - shard_.kz0);
     a.kE1 = shard_.own1;
-    for (int c = 0; c < 6; ++c) fld_[c] = alloc<S>(nflat_);
+    // 16-bit storage: the H sweep's 8-cell interior vectors start at xi0 = np rounded up to 4
+    // cells; the field arrays are offset by xoff_ elements so that xi0 (and every interior
+    // vector) falls on a 16-byte boundary.  Every kernel addresses them from the offset pointer.
+    xoff_ = 0;
+    if constexpr (sizeof(S) == 2) xoff_ = int((8 - round_up(size_t(np_), size_t(W)) % 8) % 8);
+    for (int c = 0; c < 6; ++c) fld_[c] = alloc<S>(nflat_ + 8) + xoff_;
     point_args_at();
 
     // bH must be uniform and aE = aH = 1 (sigma = 0, mu_r = 1).
@@ -1161,8 +1167,11 @@ Solver<S, T>::Solver(const fdtd_setup_v1& s, int dev, const ShardSpec* shard, bo
 
     // x split: W-aligned interior without x-slab cells, and the edge vectors around it
     SweepGeom& g = geom_;
+    // interior vectors of WI cells (16-bit storage: 8 in the H sweep, one 16-byte word per
+    // array; its E sweep covers the same interior with 4-cell vectors, gxi_E), edge vectors of W
+    constexpr int WI = sizeof(S) == 2 ? 8 : W;
     g.xi0 = int(round_up(size_t(np_), size_t(W)));
-    g.xi1 = std::max(g.xi0, ((NxT_ - np_) / W) * W);
+    g.xi1 = std::max(g.xi0, g.xi0 + (NxT_ - np_ - g.xi0) / WI * WI);
     // Interior row segments of 32, 16 or 8 lanes.  A narrow interior (at most two 32-lane
     // segments) takes the width that leaves the fewest lanes idle in the last block column,
     // ties to the wider segment (its warps load one x-neighbour per plane, not one per row);
@@ -1171,7 +1180,7 @@ Solver<S, T>::Solver(const fdtd_setup_v1& s, int dev, const ShardSpec* shard, bo
     // the 536^3 grid (130 vectors, 81 % of 32-lane rows busy) at 74.2 on 32-lane rows, 71.6 on
     // 16 and 68.9 on 8 -- with enough blocks to keep HBM busy the extra row ends cost more than
     // the idle lanes.  FDTD_B200_LANES=32|16|8 sets the width (results do not depend on it).
-    const int nvec = (g.xi1 - g.xi0) / W;
+    const int nvec = (g.xi1 - g.xi0) / WI;
     g.lanes = 32;
     if (nvec <= 64)
         for (int L : {16, 8})
@@ -1187,7 +1196,7 @@ Solver<S, T>::Solver(const fdtd_setup_v1& s, int dev, const ShardSpec* shard, bo
     g.ne = g.nl + std::max(0, (NxT_ - g.xi1 + W - 1) / W);
     if (g.ne > 32 * kBlockY) throw Failure(FDTD_ERR_UNSUPPORTED, "CPML too thick for the sweep launch shape");
     g.er = g.ne ? (32 * kBlockY) / g.ne : 1;
-    const int gx = g.gxi + (g.ne ? 1 : 0);
+    const int gxH = g.gxi + (g.ne ? 1 : 0), gxE = gxi_E<S>(g) + (g.ne ? 1 : 0);
     const int gyE = std::max((NyT_ + rows_blk - 1) / rows_blk, g.ne ? (NyT_ + g.er - 1) / g.er : 0);
     // launch shapes: z-chunks of at most 16 planes, and enough of them that the grid holds
     // several waves of blocks.  Measured on the 536^3 CPML + gain workload (one B200): chunks
@@ -1195,18 +1204,18 @@ Solver<S, T>::Solver(const fdtd_setup_v1& s, int dev, const ShardSpec* shard, bo
     // 1.006 to 0.900 to 0.868 ms (BF16), the H sweep from 1.025 to 0.972 ms (FP32); 12 and 8
     // planes are no faster.  Short chunks balance the blocks' work (a chunk of an edge column
     // or a CPML row runs longer than an interior one) and shorten the last wave.
-    auto chunk = [&](int rows, int planes) {
+    auto chunk = [&](int rows, int planes, int gx) {
         const int bxy = std::max(1, gx * ((rows + rows_blk - 1) / rows_blk));
         const int want = std::max(1, (148 * 16 + bxy - 1) / bxy);
         const int zc = std::max({1, std::min(want, std::max(1, planes / 8)), (planes + 15) / 16});
         return std::max(1, (planes + zc - 1) / zc);
     };
-    kchunkH_ = chunk(NyT_ - 1, NzT_ - 1);
-    kchunkE_ = chunk(NyT_, NzT_);
+    kchunkH_ = chunk(NyT_ - 1, NzT_ - 1, gxH);
+    kchunkE_ = chunk(NyT_, NzT_, gxE);
     if (const char* e = std::getenv("FDTD_B200_KCHUNK")) kchunkH_ = kchunkE_ = std::max(1, std::atoi(e));
     if (gyE > 65535) throw Failure(FDTD_ERR_INVALID, "grid too large for the sweep launch shape (NyT)");
-    gridH_ = dim3(gx, gyE, std::max(1, (a.kH1 + kchunkH_ - 1) / kchunkH_));
-    gridE_ = dim3(gx, gyE, std::max(1, (a.kE1 + kchunkE_ - 1) / kchunkE_));
+    gridH_ = dim3(gxH, gyE, std::max(1, (a.kH1 + kchunkH_ - 1) / kchunkH_));
+    gridE_ = dim3(gxE, gyE, std::max(1, (a.kE1 + kchunkE_ - 1) / kchunkE_));
     if (const char* p = std::getenv("FDTD_B200_KERNEL_PATH")) set_path(std::atoi(p));
     ck(cudaStreamSynchronize(st_), "setup upload");
 }
