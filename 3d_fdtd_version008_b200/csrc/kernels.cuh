@@ -296,14 +296,17 @@ struct StepArgs {
     int sr;                           // BF16 storage: E and H stores rounded stochastically
 };
 
-// W values of field array `arr` (Ex..Hz = 0..5) at local offset c.  With a.sr (BF16 storage)
-// they are rounded stochastically, keyed by (global cell, array, step), so a cell's rounding
-// is the same whatever the launch shape, sharding or packing; else rounded to nearest.
-template <typename S, typename T>
+// W values of field array `arr` (Ex..Hz = 0..5) at local offset c.  With stochastic rounding
+// (BF16 storage) they are rounded stochastically, keyed by (global cell, array, step), so a
+// cell's rounding is the same whatever the launch shape, sharding or packing; else rounded to
+// nearest.  SRM: 0 nearest, 1 stochastic (the single-solve sweeps, compiled per mode so that
+// the default kernel carries no stochastic-rounding code), 2 as a.sr says (the packed and
+// slab-ordered kernels, whose launches serve both).
+template <int SRM = 2, typename S, typename T>
 __device__ __forceinline__ void st_field(const StepArgs<S, T>& a, S* p, size_t c, const T (&v)[Vec<T>::W], unsigned arr,
                                          unsigned step) {
-    if constexpr (std::is_same_v<S, __nv_bfloat16>) {
-        if (a.sr) {
+    if constexpr (std::is_same_v<S, __nv_bfloat16> && SRM != 0) {
+        if (SRM == 1 || a.sr) {
             const unsigned cell = unsigned(c + size_t(a.kz0) * size_t(a.plane));
             const unsigned salt = mix32(step * 0x9e3779b9u + arr);
             unsigned short h[4];
@@ -494,7 +497,7 @@ __device__ __forceinline__ void sheet_J(const ESrc& src, int i, int j, int k, T&
 // updated.  Same operations in the same order as the general update with psi, J and dP/dt
 // absent; the general path carries per-cell tests that cost more issue slots than the
 // arithmetic itself, and about 85 % of the cells of a CPML-bounded grid are plain.
-template <typename S, typename T>
+template <typename S, typename T, int SRM = 2>
 __device__ __forceinline__ void h_plain(const StepArgs<S, T>& a, const size_t c, const T (&ex0)[Vec<T>::W],
                                         const T (&ex1)[Vec<T>::W], const T (&ey0)[Vec<T>::W],
                                         const T (&ey1)[Vec<T>::W], const T (&ez)[Vec<T>::W],
@@ -517,12 +520,12 @@ __device__ __forceinline__ void h_plain(const StepArgs<S, T>& a, const size_t c,
         hy[e] = fma_rn(nbH, sub_rn(dEx_dz, dEz_dx), hy[e]);
         hz[e] = fma_rn(nbH, sub_rn(dEy_dx, dEx_dy), hz[e]);
     }
-    st_field(a, a.Hx, c, hx, 3, step);
-    st_field(a, a.Hy, c, hy, 4, step);
-    st_field(a, a.Hz, c, hz, 5, step);
+    st_field<SRM>(a, a.Hx, c, hx, 3, step);
+    st_field<SRM>(a, a.Hy, c, hy, 4, step);
+    st_field<SRM>(a, a.Hz, c, hz, 5, step);
 }
 
-template <typename S, typename T>
+template <typename S, typename T, int SRM = 2>
 __device__ __forceinline__ void e_plain(const StepArgs<S, T>& a, const size_t c, T (&ex)[Vec<T>::W], T (&ey)[Vec<T>::W],
                                         T (&ez)[Vec<T>::W], const T (&bx)[Vec<T>::W], const T (&by)[Vec<T>::W],
                                         const T (&bz)[Vec<T>::W], const T (&hx)[Vec<T>::W],
@@ -547,9 +550,9 @@ __device__ __forceinline__ void e_plain(const StepArgs<S, T>& a, const size_t c,
         ey[e] = fma_rn(by[e], sub_rn(dHx_dz, dHz_dx), ey[e]);
         ez[e] = fma_rn(bz[e], sub_rn(dHy_dx, dHx_dy), ez[e]);
     }
-    st_field(a, a.Ex, c, ex, 0, step);
-    st_field(a, a.Ey, c, ey, 1, step);
-    st_field(a, a.Ez, c, ez, 2, step);
+    st_field<SRM>(a, a.Ex, c, ex, 0, step);
+    st_field<SRM>(a, a.Ey, c, ey, 1, step);
+    st_field<SRM>(a, a.Ez, c, ez, 2, step);
 }
 
 // ---------------------------------------------------------------------------------
@@ -605,7 +608,7 @@ struct HPipe : PipeShape<16, 2> {
 };
 
 // li: the thread's lane within its row segment of g.lanes lanes (interior columns).
-template <typename S, typename T, bool EDGE, bool PIPE = false>
+template <typename S, typename T, bool EDGE, bool PIPE = false, int SRM = 2>
 __device__ __forceinline__ void h_column(const StepArgs<S, T>& a, const SweepGeom& g, const int j, const int i0,
                                          const bool act, const int kb, const int ke, const int li,
                                          const unsigned step) {
@@ -733,7 +736,7 @@ __device__ __forceinline__ void h_column(const StepArgs<S, T>& a, const SweepGeo
             if (!nload) { eyn = sy; ezn = sz; }
         }
         if (plain_row && !zpml) {
-            h_plain<S, T>(a, c, ex0, ex1, ey0, ey1, ez, exj, ezj, eyn, ezn, hx, hy, hz, idx, idy, idz, step);
+            h_plain<S, T, SRM>(a, c, ex0, ex1, ey0, ey1, ez, exj, ezj, eyn, ezn, hx, hy, hz, idx, idy, idz, step);
 #pragma unroll
             for (int e = 0; e < W; ++e) { ex0[e] = ex1[e]; ey0[e] = ey1[e]; }
             continue;
@@ -770,9 +773,9 @@ __device__ __forceinline__ void h_column(const StepArgs<S, T>& a, const SweepGeo
             hz[e] = fma_rn(nbH, sub_rn(dEy_dx, dEx_dy), hz[e]);
         }
         if (act) {
-            st_field(a, a.Hx, c, hx, 3, step);
-            st_field(a, a.Hy, c, hy, 4, step);
-            st_field(a, a.Hz, c, hz, 5, step);
+            st_field<SRM>(a, a.Hx, c, hx, 3, step);
+            st_field<SRM>(a, a.Hy, c, hy, 4, step);
+            st_field<SRM>(a, a.Hz, c, hz, 5, step);
             if (zpml) { Fld<S, T>::st(a.psiH[1] + zs, pxz); Fld<S, T>::st(a.psiH[2] + zs, pyz); }
             if (ypml) { Fld<S, T>::st(a.psiH[0] + ys, pxy); Fld<S, T>::st(a.psiH[5] + ys, pzy); }
             if (xpml) xpsi_store<S, T>(a.psiH[3], a.psiH[4], a, k, j, i0, 0, a.NxT - 1, x3, x4);
@@ -787,7 +790,7 @@ __device__ __forceinline__ void h_column(const StepArgs<S, T>& a, const SweepGeo
 // two 4-cell halves take h_column's update in the same order: the same bits.  Ey, Ez at
 // i0+8 come from the next lane's first cell or, at the end of the row segment or of the
 // interior, from memory.
-template <typename S, bool PIPE>
+template <typename S, bool PIPE, int SRM = 2>
 __device__ __forceinline__ void h_column8(const StepArgs<S, float>& a, const SweepGeom& g, const int j, const int i0,
                                           const bool act, const int kb, const int ke, const int li,
                                           const unsigned step) {
@@ -907,7 +910,7 @@ __device__ __forceinline__ void h_column8(const StepArgs<S, float>& a, const Swe
             }
             const bool plain = act && !ypml && ih + W <= a.NxT - 1;
             if (plain && !zpml) {
-                h_plain<S, T>(a, ch, vex0, vex1, vey0, vey1, vez, vexj, vezj, eyn, ezn, vhx, vhy, vhz, idx[h], idy, idz, step);
+                h_plain<S, T, SRM>(a, ch, vex0, vex1, vey0, vey1, vez, vexj, vezj, eyn, ezn, vhx, vhy, vhz, idx[h], idy, idz, step);
                 continue;
             }
             size_t zs = 0, ys = 0;
@@ -945,9 +948,9 @@ __device__ __forceinline__ void h_column8(const StepArgs<S, float>& a, const Swe
                 vhz[e] = fma_rn(nbH, sub_rn(dEy_dx, dEx_dy), vhz[e]);
             }
             if (act) {
-                st_field(a, a.Hx, ch, vhx, 3, step);
-                st_field(a, a.Hy, ch, vhy, 4, step);
-                st_field(a, a.Hz, ch, vhz, 5, step);
+                st_field<SRM>(a, a.Hx, ch, vhx, 3, step);
+                st_field<SRM>(a, a.Hy, ch, vhy, 4, step);
+                st_field<SRM>(a, a.Hz, ch, vhz, 5, step);
                 if (zpml) { Fld<S, T>::st(a.psiH[1] + zs, pxz); Fld<S, T>::st(a.psiH[2] + zs, pyz); }
                 if (ypml) { Fld<S, T>::st(a.psiH[0] + ys, pxy); Fld<S, T>::st(a.psiH[5] + ys, pzy); }
             }
@@ -958,7 +961,7 @@ __device__ __forceinline__ void h_column8(const StepArgs<S, float>& a, const Swe
 }
 
 // One block of the H sweep: block (bx, by, bz) of the solve's launch grid.
-template <typename S, typename T, bool PIPE = false>
+template <typename S, typename T, bool PIPE = false, int SRM = 2>
 __device__ __forceinline__ void update_H_block(const StepArgs<S, T>& a, const int kchunk, const SweepGeom& g,
                                                const int bx, const int by, const int bz, const unsigned step) {
     constexpr int W = Vec<T>::W;
@@ -977,10 +980,10 @@ __device__ __forceinline__ void update_H_block(const StepArgs<S, T>& a, const in
         const bool row_ok = il.j <= jlast;
         if constexpr (sizeof(S) == 2) {  // 8-cell interior vectors
             const int i0 = g.xi0 + (bx * g.lanes + il.li) * 8;
-            h_column8<S, PIPE>(a, g, row_ok ? il.j : jlast, i0, row_ok && i0 < g.xi1, kb, ke, il.li, step);
+            h_column8<S, PIPE, SRM>(a, g, row_ok ? il.j : jlast, i0, row_ok && i0 < g.xi1, kb, ke, il.li, step);
         } else {
             const int i0 = g.xi0 + (bx * g.lanes + il.li) * W;
-            h_column<S, T, false, PIPE>(a, g, row_ok ? il.j : jlast, i0, row_ok && i0 < g.xi1, kb, ke, il.li, step);
+            h_column<S, T, false, PIPE, SRM>(a, g, row_ok ? il.j : jlast, i0, row_ok && i0 < g.xi1, kb, ke, il.li, step);
         }
     } else {
         const int t = threadIdx.y * 32 + lane;
@@ -989,16 +992,16 @@ __device__ __forceinline__ void update_H_block(const StepArgs<S, T>& a, const in
         if (rr >= g.er || j >= a.NyT - 1) return;
         const int i0 = v < g.nl ? v * W : g.xi1 + (v - g.nl) * W;
         if (i0 >= a.NxT) return;
-        h_column<S, T, true>(a, g, j, i0, true, kb, ke, 0, step);
+        h_column<S, T, true, false, SRM>(a, g, j, i0, true, kb, ke, 0, step);
     }
 }
 
 // Two resident blocks per SM (at most 128 registers; a third block would spill).
 // PIPE: interior columns stage their planes in shared memory (HPipe<S>::bytes() dynamic).
-template <typename S, typename T, bool PIPE = false>
+template <typename S, typename T, bool PIPE = false, int SRM = 2>
 __global__ void __launch_bounds__(32 * kBlockY, 2)
 k_update_H(const StepArgs<S, T> a, const int kchunk, const SweepGeom g, const unsigned step) {
-    update_H_block<S, T, PIPE>(a, kchunk, g, blockIdx.x, blockIdx.y, blockIdx.z, step);
+    update_H_block<S, T, PIPE, SRM>(a, kchunk, g, blockIdx.x, blockIdx.y, blockIdx.z, step);
 }
 
 // ---------------------------------------------------------------------------------
@@ -1006,7 +1009,8 @@ k_update_H(const StepArgs<S, T> a, const int kchunk, const SweepGeom g, const un
 // SMs wrote in the same launch, which a stale L1 line could hide.  SH: the step has
 // plane-wave sheets (a separate instantiation keeps the sheet tests out of the common case).
 // li: the thread's lane within its row segment of g.lanes lanes (interior columns).
-template <typename S, typename T, bool EDGE, bool CG = false, bool SH = false, bool MAT = false, bool PIPE = false>
+template <typename S, typename T, bool EDGE, bool CG = false, bool SH = false, bool MAT = false, bool PIPE = false,
+          int SRM = 2>
 __device__ __forceinline__ void e_column(const StepArgs<S, T>& a, const SweepGeom& g, const ESrc& src, const int j,
                                          const int i0, const bool act, const int kb, const int ke, const int li) {
     auto ldH = [](const S* p, T (&v)[Vec<T>::W]) {
@@ -1163,7 +1167,7 @@ __device__ __forceinline__ void e_column(const StepArgs<S, T>& a, const SweepGeo
         }
         const bool gplane = grow && k >= a.gk0 && k < a.gk0 + a.gZ;
         if (plain_row && !zpml && !gplane && !src_in_vector<SH>(src, i0, j, k, W)) {
-            e_plain<S, T>(a, c, ex, ey, ez, bx, by, bz, hx, hy, hz, hzj, hxj, hxm, hym, hzp, hyp, idx, idy, idz, src.step);
+            e_plain<S, T, SRM>(a, c, ex, ey, ez, bx, by, bz, hx, hy, hz, hzj, hxj, hxm, hym, hzp, hyp, idx, idy, idz, src.step);
 #pragma unroll
             for (int e = 0; e < W; ++e) { hxm[e] = hx[e]; hym[e] = hy[e]; }
             continue;
@@ -1247,9 +1251,9 @@ __device__ __forceinline__ void e_column(const StepArgs<S, T>& a, const SweepGeo
             }
         }
         if (act) {
-            st_field(a, a.Ex, c, ex, 0, src.step);
-            st_field(a, a.Ey, c, ey, 1, src.step);
-            st_field(a, a.Ez, c, ez, 2, src.step);
+            st_field<SRM>(a, a.Ex, c, ex, 0, src.step);
+            st_field<SRM>(a, a.Ey, c, ey, 1, src.step);
+            st_field<SRM>(a, a.Ez, c, ez, 2, src.step);
             if (zpml) { Fld<S, T>::st(a.psiE[1] + zs, pxz); Fld<S, T>::st(a.psiE[2] + zs, pyz); }
             if (ypml) { Fld<S, T>::st(a.psiE[0] + ys, pxy); Fld<S, T>::st(a.psiE[5] + ys, pzy); }
             if (xpml) xpsi_store<S, T>(a.psiE[3], a.psiE[4], a, k, j, i0, 1, a.NxT, x3, x4);
@@ -1259,7 +1263,7 @@ __device__ __forceinline__ void e_column(const StepArgs<S, T>& a, const SweepGeo
     }
 }
 
-template <typename S, typename T, bool CG = false, bool SH = false, bool MAT = false, bool PIPE = false>
+template <typename S, typename T, bool CG = false, bool SH = false, bool MAT = false, bool PIPE = false, int SRM = 2>
 __device__ __forceinline__ void update_E_block(const StepArgs<S, T>& a, const int kchunk, const ESrc& src,
                                                const SweepGeom& g, const int bx, const int by, const int bz) {
     constexpr int W = Vec<T>::W;
@@ -1277,7 +1281,7 @@ __device__ __forceinline__ void update_E_block(const StepArgs<S, T>& a, const in
         if (w0 + R - 1 < 1 || w0 >= a.NyT) return;
         const bool row_ok = il.j >= 1 && il.j < a.NyT;
         const int i0 = g.xi0 + (bx * g.lanes + il.li) * W;
-        e_column<S, T, false, CG, SH, MAT, PIPE>(a, g, src, row_ok ? il.j : 1, i0, row_ok && i0 < g.xi1, kb, ke, il.li);
+        e_column<S, T, false, CG, SH, MAT, PIPE, SRM>(a, g, src, row_ok ? il.j : 1, i0, row_ok && i0 < g.xi1, kb, ke, il.li);
     } else {
         const int t = threadIdx.y * 32 + lane;
         const int rr = t / g.ne, v = t - rr * g.ne;
@@ -1285,15 +1289,15 @@ __device__ __forceinline__ void update_E_block(const StepArgs<S, T>& a, const in
         if (rr >= g.er || j < 1 || j >= a.NyT) return;
         const int i0 = v < g.nl ? v * W : g.xi1 + (v - g.nl) * W;
         if (i0 >= a.NxT) return;
-        e_column<S, T, true, CG, SH, MAT>(a, g, src, j, i0, true, kb, ke, 0);
+        e_column<S, T, true, CG, SH, MAT, false, SRM>(a, g, src, j, i0, true, kb, ke, 0);
     }
 }
 
 // PIPE: interior columns stage their planes in shared memory (EPipe<S>::bytes() dynamic).
-template <typename S, typename T, bool SH = false, bool MAT = false, bool PIPE = false>
+template <typename S, typename T, bool SH = false, bool MAT = false, bool PIPE = false, int SRM = 2>
 __global__ void __launch_bounds__(32 * kBlockY, 2)
 k_update_E(const StepArgs<S, T> a, const int kchunk, const ESrc src, const SweepGeom g) {
-    update_E_block<S, T, false, SH, MAT, PIPE>(a, kchunk, src, g, blockIdx.x, blockIdx.y, blockIdx.z);
+    update_E_block<S, T, false, SH, MAT, PIPE, SRM>(a, kchunk, src, g, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 
 // ---------------------------------------------------------------------------------

@@ -814,15 +814,33 @@ private:
     // The sweeps' interior columns stage their planes in shared memory through cp.async
     // (FDTD_B200_E_PIPE / FDTD_B200_H_PIPE = 0 / 1 override the defaults set in the constructor).
     bool pipe_ = false, hpipe_ = false;
+    // BF16 stores with stochastic rounding: the sweeps are compiled per rounding mode (SRM 0 / 1),
+    // so that the common round-to-nearest kernel carries no stochastic-rounding code.
+    int srm_ = 0;
+    template <int SRM>
+    static void e_kernels(void (*(&k)[8])(const StepArgs<S, T>, const int, const ESrc, const SweepGeom)) {
+        // the staged form exists for the indexed material only (pipe_ implies a_.bidx)
+        k[0] = k_update_E<S, T, false, false, false, SRM>; k[1] = k_update_E<S, T, false, false, false, SRM>;
+        k[2] = k_update_E<S, T, false, true, false, SRM>;  k[3] = k_update_E<S, T, false, true, true, SRM>;
+        k[4] = k_update_E<S, T, true, false, false, SRM>;  k[5] = k_update_E<S, T, true, false, false, SRM>;
+        k[6] = k_update_E<S, T, true, true, false, SRM>;   k[7] = k_update_E<S, T, true, true, true, SRM>;
+    }
     using EKernel = void (*)(const StepArgs<S, T>, const int, const ESrc, const SweepGeom);
     EKernel e_kernel(bool sheets) const {
-        // the staged form exists for the indexed material only (pipe_ implies a_.bidx)
-        static constexpr EKernel k[8] = {
-            k_update_E<S, T, false, false, false>, k_update_E<S, T, false, false, false>,
-            k_update_E<S, T, false, true, false>,  k_update_E<S, T, false, true, true>,
-            k_update_E<S, T, true, false, false>,  k_update_E<S, T, true, false, false>,
-            k_update_E<S, T, true, true, false>,   k_update_E<S, T, true, true, true>};
+        EKernel k[8];
+        if constexpr (std::is_same_v<S, __nv_bfloat16>) {
+            if (srm_) e_kernels<1>(k);
+            else e_kernels<0>(k);
+        } else {
+            e_kernels<0>(k);
+        }
         return k[4 * int(sheets) + 2 * int(a_.bidx != nullptr) + int(pipe_)];
+    }
+    using HKernel = void (*)(const StepArgs<S, T>, const int, const SweepGeom, const unsigned);
+    HKernel h_kernel() const {
+        if constexpr (std::is_same_v<S, __nv_bfloat16>)
+            if (srm_) return hpipe_ ? k_update_H<S, T, true, 1> : k_update_H<S, T, false, 1>;
+        return hpipe_ ? k_update_H<S, T, true, 0> : k_update_H<S, T, false, 0>;
     }
     // event timing: ev_[0..3] bracket H, E and the auxiliary kernels of one step
     // kernel path 1 (default): k_update_H + k_update_E in place; path 2: k_step_slabs.
@@ -990,8 +1008,9 @@ Solver<S, T>::Solver(const fdtd_setup_v1& s, int dev, const ShardSpec* shard, bo
     hpipe_ = sizeof(S) == 2;
     if (const char* e = std::getenv("FDTD_B200_H_PIPE")) hpipe_ = std::string(e) != "0";
     if (const char* e = std::getenv("FDTD_B200_E_PIPE")) pipe_ = a.bidx != nullptr && std::string(e) != "0";
+    srm_ = std::is_same_v<S, __nv_bfloat16> && s.rounding == FDTD_ROUND_STOCHASTIC ? 1 : 0;
     if (hpipe_)
-        ck(cudaFuncSetAttribute(k_update_H<S, T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(HPipe<S>::bytes())),
+        ck(cudaFuncSetAttribute(h_kernel(), cudaFuncAttributeMaxDynamicSharedMemorySize, int(HPipe<S>::bytes())),
            "cudaFuncSetAttribute");
     if (pipe_) {
         const int smem = int(EPipe<S>::bytes());
@@ -1527,8 +1546,7 @@ void Solver<S, T>::run(uint64_t n) {
             if (per_kernel) ck(cudaEventRecord(ev_[1], st_), "cudaEventRecord");
             launches += 1;
         } else {
-            if (hpipe_) k_update_H<S, T, true><<<gridH_, blk, HPipe<S>::bytes(), st_>>>(a_, kchunkH_, geom_, src.step);
-            else k_update_H<S, T><<<gridH_, blk, 0, st_>>>(a_, kchunkH_, geom_, src.step);
+            h_kernel()<<<gridH_, blk, hpipe_ ? HPipe<S>::bytes() : 0, st_>>>(a_, kchunkH_, geom_, src.step);
             if (per_kernel) ck(cudaEventRecord(ev_[1], st_), "cudaEventRecord");
             const size_t smem = pipe_ ? EPipe<S>::bytes() : 0;
             e_kernel(src.ns != 0)<<<gridE_, blk, smem, st_>>>(a_, kchunkE_, src, geom_);
@@ -1592,8 +1610,7 @@ void Solver<S, T>::run(uint64_t n) {
 template <typename S, typename T>
 void Solver<S, T>::phase_H(uint64_t s) {
     const dim3 blk(32, kBlockY);
-    if (hpipe_) k_update_H<S, T, true><<<gridH_, blk, HPipe<S>::bytes(), st_>>>(a_, kchunkH_, geom_, unsigned(s));
-    else k_update_H<S, T><<<gridH_, blk, 0, st_>>>(a_, kchunkH_, geom_, unsigned(s));
+    h_kernel()<<<gridH_, blk, hpipe_ ? HPipe<S>::bytes() : 0, st_>>>(a_, kchunkH_, geom_, unsigned(s));
     ++launches;
 }
 
