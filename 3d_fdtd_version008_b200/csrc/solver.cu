@@ -28,6 +28,8 @@
 #include <numbers>
 #include <stdexcept>
 #include <string>
+#include <future>
+#include <optional>
 #include <thread>
 #include <vector>
 
@@ -872,6 +874,57 @@ void keep_pool_memory(int dev) {
     done.push_back(dev);
 }
 
+// The setup's full-grid checks that need no device: the material index's range and the gain
+// cells' bounding box and placement.  A solve runs them on a helper thread while it allocates
+// its device arrays (for a large first solve both take tens of milliseconds: growing the device
+// pool, scanning a 536^3 region map).
+struct GridScan {
+    bool bad_index = false;  // a bE_index entry >= n_bE_rows
+    int lo[3] = {0, 0, 0}, hi[3] = {-1, -1, -1};
+    long long out_of_range = 0, on_boundary = 0;
+};
+
+GridScan scan_grid(const fdtd_setup_v1& s, bool pec) {
+    GridScan g;
+    const int NxT = int(s.NxT), NyT = int(s.NyT), NzT = int(s.NzT);
+    const size_t N = size_t(NxT) * NyT * NzT;
+    if (s.bE_index && s.n_bE_rows > 0 && s.n_bE_rows <= 65535) {
+        const uint16_t* hidx = s.bE_index;
+        const uint32_t nr = s.n_bE_rows;
+        uint16_t bad = 0;
+#pragma omp parallel for reduction(| : bad) schedule(static)
+        for (long long q = 0; q < (long long)N; ++q) bad |= uint16_t(hidx[q] >= nr);
+        g.bad_index = bad != 0;
+    }
+    if (s.n_tls_regions > 0 && s.tls_region_map) {
+        int lo0 = NxT, lo1 = NyT, lo2 = NzT, hi0 = -1, hi1 = -1, hi2 = -1;
+        long long out_of_range = 0, on_boundary = 0;
+        const int nreg = int(s.n_tls_regions);
+#pragma omp parallel for reduction(min : lo0, lo1, lo2) reduction(max : hi0, hi1, hi2) \
+    reduction(+ : out_of_range, on_boundary) schedule(static)
+        for (int i = 0; i < NxT; ++i)
+            for (int j = 0; j < NyT; ++j)
+                for (int k = 0; k < NzT; ++k) {
+                    const int32_t r = s.tls_region_map[(size_t(i) * NyT + j) * NzT + k];
+                    if (r < 0) continue;
+                    out_of_range += r >= nreg;
+                    on_boundary += (i == 0 || j == 0 || k == 0) ||
+                                   (pec && (i == NxT - 1 || j == NyT - 1 || k == NzT - 1));
+                    lo0 = std::min(lo0, i); hi0 = std::max(hi0, i);
+                    lo1 = std::min(lo1, j); hi1 = std::max(hi1, j);
+                    lo2 = std::min(lo2, k); hi2 = std::max(hi2, k);
+                }
+        g.lo[0] = lo0; g.lo[1] = lo1; g.lo[2] = lo2;
+        g.hi[0] = hi0; g.hi[1] = hi1; g.hi[2] = hi2;
+        g.out_of_range = out_of_range;
+        g.on_boundary = on_boundary;
+    }
+    return g;
+}
+
+struct PinnedChunks;
+PinnedChunks& pinned_chunks(int dev, size_t bytes);
+
 template <typename S, typename T>
 Solver<S, T>::Solver(const fdtd_setup_v1& s, int dev, const ShardSpec* shard, bool pooled) {
     device = dev;
@@ -885,6 +938,15 @@ Solver<S, T>::Solver(const fdtd_setup_v1& s, int dev, const ShardSpec* shard, bo
     np_ = int(s.npml);
     pec_ = s.pec_boundary != 0;
     if (pec_ && np_ != 0) throw Failure(FDTD_ERR_INVALID, "a PEC boundary has no CPML layer: npml must be 0");
+    // (the task reads only the caller's view; an exception below waits for it in the future's
+    // destructor)
+    std::future<GridScan> scan_task = std::async(std::launch::async, scan_grid, std::cref(s), pec_);
+    std::optional<GridScan> scanned;
+    auto scan = [&]() -> const GridScan& {
+        if (!scanned) scanned = scan_task.get();
+        return *scanned;
+    };
+    pinned_chunks(dev, kPinBytes);  // the process's first solve makes the staging chunks
     NxP_ = int(round_up(size_t(NxT_), 128 / sizeof(S)));
     if constexpr (!std::is_same_v<S, T>) {
         // 16-bit storage: E' = E / sE, H' = H / sH with sH = sE / eta0 so that E' and H' have
@@ -957,11 +1019,7 @@ Solver<S, T>::Solver(const fdtd_setup_v1& s, int dev, const ShardSpec* shard, bo
         for (uint32_t r = 0; r < s.n_bE_rows; ++r)
             for (int c = 0; c < 3; ++c) rows[r][c] = s.bE_rows[3 * size_t(r) + c];
         hidx = s.bE_index;
-        const uint32_t nr = s.n_bE_rows;
-        uint16_t bad = 0;
-#pragma omp parallel for reduction(| : bad) schedule(static)
-        for (long long q = 0; q < (long long)N; ++q) bad |= uint16_t(hidx[q] >= nr);
-        if (bad) throw Failure(FDTD_ERR_INVALID, "bE_index holds a row number >= n_bE_rows");
+        if (scan().bad_index) throw Failure(FDTD_ERR_INVALID, "bE_index holds a row number >= n_bE_rows");
         have_index = true;
     } else if (want_index) {
         have_index = fdtd::distinct_rows(s.bE, N, rows, rid);
@@ -1071,28 +1129,13 @@ Solver<S, T>::Solver(const fdtd_setup_v1& s, int dev, const ShardSpec* shard, bo
     if (s.n_tls_regions > 0) {
         if (!s.tls_region_map || !s.tls_regions) throw Failure(FDTD_ERR_INVALID, "gain regions without region map");
         if (s.n_tls_regions > 127) throw Failure(FDTD_ERR_UNSUPPORTED, "more than 127 gain regions");
-        int lo0 = NxT_, lo1 = NyT_, lo2 = NzT_, hi0 = -1, hi1 = -1, hi2 = -1;
-        long long out_of_range = 0, on_boundary = 0;
-        const int nreg = int(s.n_tls_regions);
-#pragma omp parallel for reduction(min : lo0, lo1, lo2) reduction(max : hi0, hi1, hi2) \
-    reduction(+ : out_of_range, on_boundary) schedule(static)
-        for (int i = 0; i < NxT_; ++i)
-            for (int j = 0; j < NyT_; ++j)
-                for (int k = 0; k < NzT_; ++k) {
-                    const int32_t r = s.tls_region_map[(size_t(i) * NyT_ + j) * NzT_ + k];
-                    if (r < 0) continue;
-                    out_of_range += r >= nreg;
-                    on_boundary += (i == 0 || j == 0 || k == 0) ||
-                                   (pec_ && (i == NxT_ - 1 || j == NyT_ - 1 || k == NzT_ - 1));
-                    lo0 = std::min(lo0, i); hi0 = std::max(hi0, i);
-                    lo1 = std::min(lo1, j); hi1 = std::max(hi1, j);
-                    lo2 = std::min(lo2, k); hi2 = std::max(hi2, k);
-                }
-        if (out_of_range) throw Failure(FDTD_ERR_INVALID, "region map entry out of range");
-        if (on_boundary)
+        const GridScan& gs = scan();
+        if (gs.out_of_range) throw Failure(FDTD_ERR_INVALID, "region map entry out of range");
+        if (gs.on_boundary)
             throw Failure(FDTD_ERR_UNSUPPORTED, pec_ ? "gain cells on the outer faces of a PEC grid"
                                                      : "gain cells on the i=0/j=0/k=0 boundary planes");
-        const int lo[3] = {lo0, lo1, lo2}, hi[3] = {hi0, hi1, hi2};
+        const int* lo = gs.lo;
+        const int* hi = gs.hi;
         if (hi[0] >= 0) {
             has_gain_ = true;
             a.gain = 1;
