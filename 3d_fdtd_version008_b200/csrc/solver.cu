@@ -875,9 +875,9 @@ void keep_pool_memory(int dev) {
 }
 
 // The setup's full-grid checks that need no device: the material index's range and the gain
-// cells' bounding box and placement.  A solve runs them on a helper thread while it allocates
-// its device arrays (for a large first solve both take tens of milliseconds: growing the device
-// pool, scanning a 536^3 region map).
+// cells' bounding box and placement.  A large solve runs them on a helper thread while it
+// allocates its device arrays (for a 536^3 first solve both take tens of milliseconds: growing
+// the device pool, scanning the region map).
 struct GridScan {
     bool bad_index = false;  // a bE_index entry >= n_bE_rows
     int lo[3] = {0, 0, 0}, hi[3] = {-1, -1, -1};
@@ -938,9 +938,13 @@ Solver<S, T>::Solver(const fdtd_setup_v1& s, int dev, const ShardSpec* shard, bo
     np_ = int(s.npml);
     pec_ = s.pec_boundary != 0;
     if (pec_ && np_ != 0) throw Failure(FDTD_ERR_INVALID, "a PEC boundary has no CPML layer: npml must be 0");
-    // (the task reads only the caller's view; an exception below waits for it in the future's
-    // destructor)
-    std::future<GridScan> scan_task = std::async(std::launch::async, scan_grid, std::cref(s), pec_);
+    // A grid of 2^25 cells or more is scanned on a helper thread (the task reads only the
+    // caller's view; an exception below waits for it in the future's destructor); a smaller one
+    // in this thread when the result is first needed, where a thread and its OpenMP team would
+    // cost more than the scan.
+    const bool big = uint64_t(s.NxT) * s.NyT * s.NzT >= (uint64_t(1) << 25);
+    std::future<GridScan> scan_task =
+        std::async(big ? std::launch::async : std::launch::deferred, scan_grid, std::cref(s), pec_);
     std::optional<GridScan> scanned;
     auto scan = [&]() -> const GridScan& {
         if (!scanned) scanned = scan_task.get();
