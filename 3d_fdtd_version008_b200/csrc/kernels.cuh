@@ -2,11 +2,11 @@
 //
 // Device layout: every 3-D array is stored x-fastest, (k, j, i) -> (k*NyT + j)*NxP + i,
 // rows padded to NxP (a multiple of 128 bytes).  A thread owns W = 16/sizeof(T)
-// consecutive x cells (one 128-bit load per array), a warp owns one 32*W-cell row
-// segment, and each thread marches in +z through a chunk of planes carrying the
-// z-neighbour plane in registers (2.5D blocking).  x-neighbours come from the adjacent
-// lane by warp shuffle (one scalar load at the warp edge), y-neighbours from the
-// adjacent row through L1.
+// consecutive x cells (one 128-bit load per array; 16-bit storage: 4 cells, and 8 in the
+// H sweep's interior), a warp owns one row segment of 32, 16 or 8 vectors, and each
+// thread marches in +z through a chunk of planes carrying the z-neighbour plane in
+// registers (2.5D blocking).  x-neighbours come from the adjacent lane by warp shuffle
+// (one scalar load at the segment edge), y-neighbours from the adjacent row through L1.
 //
 // Physics per step n (reference order, src/3D_FDTD_version008.cpp:269-328):
 //   k_update_H : H -= bH * curl E with the CPML psi_H recursion fused in
