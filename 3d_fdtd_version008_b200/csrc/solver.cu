@@ -500,20 +500,20 @@ __device__ __forceinline__ const StepArgs<S, float>& bargs(int r) {
 
 // The blocks of the solves stored as S.  PIPE: interior columns stage their planes in shared
 // memory (HPipe<S>::bytes() / EPipe<S>::bytes() dynamic), as in the single-solve sweeps.
-template <typename S, bool PIPE>
+template <typename S, bool PIPE, int SRM>
 __global__ void __launch_bounds__(32 * kBlockY, 2) k_update_H_multi(const int4* __restrict__ tab) {
     const int4 e = tab[blockIdx.x];
-    update_H_block<S, float, PIPE>(bargs<S>(e.x), c_bsolve[e.x].kchunkH, c_bsolve[e.x].g, e.y, e.z, e.w,
+    update_H_block<S, float, PIPE, SRM>(bargs<S>(e.x), c_bsolve[e.x].kchunkH, c_bsolve[e.x].g, e.y, e.z, e.w,
                                    c_btick[e.x].src.step);
 }
 
 // SH / MAT: the blocks of solves with plane-wave sheets / an indexed material; the table lists
 // each (storage, SH, MAT) kind in a separate run, so a solve runs the same code whatever else
 // is resident.
-template <typename S, bool SH, bool MAT, bool PIPE>
+template <typename S, bool SH, bool MAT, bool PIPE, int SRM>
 __global__ void __launch_bounds__(32 * kBlockY, 2) k_update_E_multi(const int4* __restrict__ tab) {
     const int4 e = tab[blockIdx.x];
-    update_E_block<S, float, false, SH, MAT, PIPE>(bargs<S>(e.x), c_bsolve[e.x].kchunkE, c_btick[e.x].src,
+    update_E_block<S, float, false, SH, MAT, PIPE, SRM>(bargs<S>(e.x), c_bsolve[e.x].kchunkE, c_btick[e.x].src,
                                                    c_bsolve[e.x].g, e.y, e.z, e.w);
 }
 
@@ -2010,12 +2010,13 @@ public:
             if (const char* e = std::getenv("FDTD_B200_BATCH_E_PIPE")) epipe_ = std::string(e) != "0";
             if (const char* e = std::getenv("FDTD_B200_BATCH_KCHUNK")) kchunk_ = std::max(0, std::atoi(e));
             if (const char* e = std::getenv("FDTD_B200_BATCH_SOLO")) solo_ = std::string(e) != "0";
-            for (int st = 0; st < 3; ++st) {
-                ck(cudaFuncSetAttribute(hkernel(st, true), cudaFuncAttributeMaxDynamicSharedMemorySize, int(hsmem(st))),
+            for (int f = 0; f < kForms; ++f) {
+                ck(cudaFuncSetAttribute(hkernel(f, true), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        int(hsmem(storage_of(f)))),
                    "cudaFuncSetAttribute");
                 for (int sh = 0; sh < 2; ++sh)
-                    ck(cudaFuncSetAttribute(ekernel(4 * st + 2 * sh + 1, true), cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                            int(esmem(st))),
+                    ck(cudaFuncSetAttribute(ekernel(4 * f + 2 * sh + 1, true), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                            int(esmem(storage_of(f)))),
                        "cudaFuncSetAttribute");
             }
             worker_ = std::thread([this] { prepare_loop(); });
@@ -2132,31 +2133,40 @@ private:
     static constexpr int kRing = 64;        // pinned per-step records in flight
     static constexpr int kCheckEvery = 16;  // steps between status checks
     static constexpr int kSoloChunk = 64;   // steps per single-solve run of a lone resident solve
-    // E kernel kinds: storage (3) x plane-wave sheets x indexed material
-    static constexpr int kEKinds = 12;
+    // Sweep forms: 0 FP32, 1 FP16, 2 BF16 rounded to nearest, 3 BF16 rounded stochastically (the
+    // packed sweeps are compiled per rounding mode, as the single-solve ones).  E kernel kinds:
+    // form (4) x plane-wave sheets x indexed material.
+    static constexpr int kForms = 4;
+    static constexpr int kEKinds = 16;
+    static int storage_of(int form) { return form == 3 ? 2 : form; }
     using K = void (*)(const int4*);
-    static K hkernel(int storage, bool pipe) {
-        static constexpr K k[6] = {k_update_H_multi<float, false>,         k_update_H_multi<float, true>,
-                                   k_update_H_multi<__half, false>,        k_update_H_multi<__half, true>,
-                                   k_update_H_multi<__nv_bfloat16, false>, k_update_H_multi<__nv_bfloat16, true>};
-        return k[2 * storage + int(pipe)];
+    static K hkernel(int form, bool pipe) {
+        static constexpr K k[2 * kForms] = {
+            k_update_H_multi<float, false, 0>,         k_update_H_multi<float, true, 0>,
+            k_update_H_multi<__half, false, 0>,        k_update_H_multi<__half, true, 0>,
+            k_update_H_multi<__nv_bfloat16, false, 0>, k_update_H_multi<__nv_bfloat16, true, 0>,
+            k_update_H_multi<__nv_bfloat16, false, 1>, k_update_H_multi<__nv_bfloat16, true, 1>};
+        return k[2 * form + int(pipe)];
     }
     // dynamic shared memory of the staged sweeps of storage form st (0 FP32, 1 FP16, 2 BF16)
     static size_t hsmem(int st) { return st == 0 ? HPipe<float>::bytes() : st == 1 ? HPipe<__half>::bytes() : HPipe<__nv_bfloat16>::bytes(); }
     static size_t esmem(int st) { return st == 0 ? EPipe<float>::bytes() : st == 1 ? EPipe<__half>::bytes() : EPipe<__nv_bfloat16>::bytes(); }
-    // kind = 4 storage + 2 SH + MAT; the staged form exists for the indexed material only
+    // kind = 4 form + 2 SH + MAT; the staged form exists for the indexed material only
     static K ekernel(int kind, bool pipe) {
         static constexpr K k[kEKinds] = {
-            k_update_E_multi<float, false, false, false>,         k_update_E_multi<float, false, true, false>,
-            k_update_E_multi<float, true, false, false>,          k_update_E_multi<float, true, true, false>,
-            k_update_E_multi<__half, false, false, false>,        k_update_E_multi<__half, false, true, false>,
-            k_update_E_multi<__half, true, false, false>,         k_update_E_multi<__half, true, true, false>,
-            k_update_E_multi<__nv_bfloat16, false, false, false>, k_update_E_multi<__nv_bfloat16, false, true, false>,
-            k_update_E_multi<__nv_bfloat16, true, false, false>,  k_update_E_multi<__nv_bfloat16, true, true, false>};
+            k_update_E_multi<float, false, false, false, 0>,         k_update_E_multi<float, false, true, false, 0>,
+            k_update_E_multi<float, true, false, false, 0>,          k_update_E_multi<float, true, true, false, 0>,
+            k_update_E_multi<__half, false, false, false, 0>,        k_update_E_multi<__half, false, true, false, 0>,
+            k_update_E_multi<__half, true, false, false, 0>,         k_update_E_multi<__half, true, true, false, 0>,
+            k_update_E_multi<__nv_bfloat16, false, false, false, 0>, k_update_E_multi<__nv_bfloat16, false, true, false, 0>,
+            k_update_E_multi<__nv_bfloat16, true, false, false, 0>,  k_update_E_multi<__nv_bfloat16, true, true, false, 0>,
+            k_update_E_multi<__nv_bfloat16, false, false, false, 1>, k_update_E_multi<__nv_bfloat16, false, true, false, 1>,
+            k_update_E_multi<__nv_bfloat16, true, false, false, 1>,  k_update_E_multi<__nv_bfloat16, true, true, false, 1>};
         static constexpr K kp[kEKinds] = {
-            nullptr, k_update_E_multi<float, false, true, true>,         nullptr, k_update_E_multi<float, true, true, true>,
-            nullptr, k_update_E_multi<__half, false, true, true>,        nullptr, k_update_E_multi<__half, true, true, true>,
-            nullptr, k_update_E_multi<__nv_bfloat16, false, true, true>, nullptr, k_update_E_multi<__nv_bfloat16, true, true, true>};
+            nullptr, k_update_E_multi<float, false, true, true, 0>,         nullptr, k_update_E_multi<float, true, true, true, 0>,
+            nullptr, k_update_E_multi<__half, false, true, true, 0>,        nullptr, k_update_E_multi<__half, true, true, true, 0>,
+            nullptr, k_update_E_multi<__nv_bfloat16, false, true, true, 0>, nullptr, k_update_E_multi<__nv_bfloat16, true, true, true, 0>,
+            nullptr, k_update_E_multi<__nv_bfloat16, false, true, true, 1>, nullptr, k_update_E_multi<__nv_bfloat16, true, true, true, 1>};
         return pipe && kp[kind] ? kp[kind] : k[kind];
     }
 
@@ -2293,7 +2303,7 @@ private:
         std::vector<BatchArgs> args(n);
         std::vector<BatchSolve> bs(n);
         std::vector<int4> tab;
-        std::vector<int> ekind(n);
+        std::vector<int> ekind(n), form(n);
         for (int r = 0; r < n; ++r) {
             Job& j = jobs_.at(res_[r]);
             BatchSolve& b = bs[r];
@@ -2320,7 +2330,8 @@ private:
                 b.sE = v.sE_;
                 b.sH = v.sH_;
                 b.storage = j.storage;
-                ekind[r] = 4 * j.storage + 2 * int(!v.sheets_.empty()) + int(v.a_.bidx != nullptr);
+                form[r] = j.storage == 2 && v.a_.sr ? 3 : j.storage;
+                ekind[r] = 4 * form[r] + 2 * int(!v.sheets_.empty()) + int(v.a_.bidx != nullptr);
             });
         }
         // the solve's launch shape with z-chunks of kc planes over planes [0, k1)
@@ -2331,12 +2342,12 @@ private:
                     for (unsigned x = 0; x < g.x; ++x) tab.push_back(make_int4(r, int(x), int(y), int(z)));
         };
         nHk_[0] = 0;
-        for (int st = 0; st < 3; ++st) {  // H blocks by storage form, then E blocks by kind
+        for (int f = 0; f < kForms; ++f) {  // H blocks by sweep form, then E blocks by kind
             for (int r = 0; r < n; ++r) {
                 Job& j = jobs_.at(res_[r]);
-                if (j.storage == st) with(j, [&](auto& v) { add_blocks(r, zchunks(v.gridH_, v.a_.kH1, bs[r].kchunkH)); });
+                if (form[r] == f) with(j, [&](auto& v) { add_blocks(r, zchunks(v.gridH_, v.a_.kH1, bs[r].kchunkH)); });
             }
-            nHk_[st + 1] = tab.size();
+            nHk_[f + 1] = tab.size();
         }
         nH_ = tab.size();
         nEk_[0] = 0;
@@ -2385,14 +2396,16 @@ private:
         ck(cudaMemcpyToSymbolAsync(c_btick, tk, n * sizeof(BatchTick), 0, cudaMemcpyHostToDevice, st_), "step records");
         ck(cudaEventRecord(ring_ev_[slot], st_), "cudaEventRecord");
         const dim3 blk(32, kBlockY);
-        for (int q = 0; q < 3; ++q)
-            if (nHk_[q + 1] > nHk_[q])
-                hkernel(q, hpipe_ && q != 0)<<<unsigned(nHk_[q + 1] - nHk_[q]), blk, hpipe_ && q != 0 ? hsmem(q) : 0, st_>>>(
+        for (int q = 0; q < kForms; ++q)
+            if (nHk_[q + 1] > nHk_[q]) {
+                const bool pipe = hpipe_ && q != 0;
+                hkernel(q, pipe)<<<unsigned(nHk_[q + 1] - nHk_[q]), blk, pipe ? hsmem(storage_of(q)) : 0, st_>>>(
                     d_tab_ + nHk_[q]);
+            }
         for (int q = 0; q < kEKinds; ++q)
             if (nEk_[q + 1] > nEk_[q]) {
                 const bool pipe = epipe_ && (q & 1);
-                ekernel(q, pipe)<<<unsigned(nEk_[q + 1] - nEk_[q]), blk, pipe ? esmem(q / 4) : 0, st_>>>(
+                ekernel(q, pipe)<<<unsigned(nEk_[q + 1] - nEk_[q]), blk, pipe ? esmem(storage_of(q / 4)) : 0, st_>>>(
                     d_tab_ + nH_ + nEk_[q]);
             }
         k_probe_multi<<<n, 128, 0, st_>>>();
@@ -2502,7 +2515,7 @@ private:
     std::vector<uint64_t> res_;  // resident tickets in slot order
     int4* d_tab_ = nullptr;
     size_t tab_cap_ = 0, nH_ = 0;
-    size_t nHk_[4] = {};          // H blocks of storage form q are table entries [nHk_[q], nHk_[q + 1])
+    size_t nHk_[kForms + 1] = {};  // H blocks of sweep form q are table entries [nHk_[q], nHk_[q + 1])
     size_t nEk_[kEKinds + 1] = {};  // E blocks of kind q are entries [nEk_[q], nEk_[q + 1]) after the H ones
     BatchTick* ticks_ = nullptr;
     cudaEvent_t ring_ev_[kRing] = {};
