@@ -149,13 +149,14 @@ def _run_files(pkg, s, outdir, precision, shards, sub):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("precision,shards", [(1, 2), (1, 3), (0, 3)])
+@pytest.mark.parametrize("precision,shards", [(1, 2), (1, 3), (0, 3), (3, 3), (2, 2)])
 def test_sharded_outputs_match_whole_solve(pkg, outdir, precision, shards):
     """A solve split into z shards writes the whole solve's files: movie frames joined from the
     shards' owned planes (XY slices from the shard that holds the plane, XZ / YZ slices from
     every shard), point series from the shard that holds the probe, population frames gathered,
     the two-level sums added over the shards.  The fields are bit-identical, so are the frames,
-    series and population frames; the CSV sums differ only by FP64 summation order."""
+    series and population frames; the CSV sums differ only by FP64 summation order.  FP64, FP32,
+    BF16 and FP16 storage."""
     s = pkg.Setup.from_file(CASE)
     whole = _run_files(pkg, s, outdir, precision, 1, "whole")
     split = _run_files(pkg, s, outdir, precision, shards, "split")
