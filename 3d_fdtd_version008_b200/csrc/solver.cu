@@ -3284,35 +3284,51 @@ template <typename S, typename T>
 void Sharded<S, T>::write_point_samples() {
     const size_t np = probe_at_.size();
     if (oplan_.points.empty() || !np) return;
-    uint64_t count = 0;
-    probe_series(nullptr, 0, &count);
+    uint64_t count = 0;  // every shard samples the same steps
+    for (auto& p : part_)
+        if (p->nprobes_) count = std::max(count, p->series_count_);
     if (count <= ots_written_) return;
-    std::vector<double> v(size_t(count) * np);
-    probe_series(v.data(), count, nullptr);
     const uint64_t n0 = ots_written_, n = count - ots_written_;
+    // only the samples not yet written, from each shard that holds probes
+    std::vector<std::vector<double>> col(part_.size());
+    for (size_t r = 0; r < part_.size(); ++r) {
+        Solver<S, T>& p = *part_[r];
+        if (!p.nprobes_) continue;
+        col[r].resize(size_t(n) * p.nprobes_);
+        ck(cudaSetDevice(p.device), "cudaSetDevice");
+        ck(cudaMemcpy(col[r].data(), p.d_series_ + size_t(n0) * p.nprobes_, col[r].size() * sizeof(double),
+                      cudaMemcpyDeviceToHost),
+           "probe samples D2H");
+    }
     const std::string dir = fdtd::run_dir(oplan_, oroot_);
-    size_t col = 0;
-    for (const auto& p : oplan_.points) {
-        for (int c : p.components) {
+    size_t q = 0;  // global probe index, in the plan's order
+    for (const auto& pt : oplan_.points) {
+        for (int c : pt.components) {
+            const auto [r, lq] = probe_at_[q];
+            const uint32_t pn = part_[r]->nprobes_;
+            auto value = [&](uint64_t t) { return col[r][size_t(t) * pn + size_t(lq)]; };
             auto buf = std::make_shared<std::vector<char>>();
             if (oplan_.float64) {
                 buf->resize(n * sizeof(double));
-                for (uint64_t t = 0; t < n; ++t) std::memcpy(buf->data() + t * 8, &v[(n0 + t) * np + col], 8);
+                for (uint64_t t = 0; t < n; ++t) {
+                    const double d = value(t);
+                    std::memcpy(buf->data() + t * 8, &d, 8);
+                }
             } else {
                 buf->resize(n * sizeof(float));
                 for (uint64_t t = 0; t < n; ++t) {
-                    const float f = float(v[(n0 + t) * np + col]);
+                    const float f = float(value(t));
                     std::memcpy(buf->data() + t * 4, &f, 4);
                 }
             }
             fdtd::OutputWriter::Job j;
-            j.path = dir + "/" + p.name + "/" + fdtd::component_name(c) + "_ts.bin";
+            j.path = dir + "/" + pt.name + "/" + fdtd::component_name(c) + "_ts.bin";
             j.data = buf->data();
             j.bytes = buf->size();
             j.append = true;
             j.done = [buf] {};
             writer_->submit(std::move(j));
-            ++col;
+            ++q;
         }
     }
     ots_written_ = count;
